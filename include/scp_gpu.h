@@ -1,0 +1,143 @@
+/* scp_gpu.h -- C ABI of libscpgpu.so, the B200 (sm_100a) lattice time-stepper
+ * for the complex / gauged Cosserat Q-ball model of kardianos/scp sfa/sim.
+ *
+ * The reference keeps its GPU stepper as file-static host functions inside
+ * the driver translation unit (sfa/sim/scp_sim.cu).  This header replaces
+ * that set with an opaque-handle C ABI: plain pointers and sizes, no CUDA or
+ * C++ types, every call returns a status code and nothing calls exit().
+ *
+ *   reference (sfa/sim/scp_sim.cu)                 replaced by
+ *   gpu_alloc            :2659  cudaMalloc per array  scp_gpu_init
+ *   gpu_set_constants    :2915  __constant__ copies   scp_gpu_init
+ *   gpu_upload           :2768  H2D of all columns    scp_gpu_init
+ *   host init_gauss_project + first force :5151-5245  scp_gpu_init (on device)
+ *   gpu_verlet_step      :2971  9-12 launches/step    scp_gpu_step (1 launch/step)
+ *   run_gpu_diagnostics  :3764  atomics + D2H         scp_gpu_diag (deterministic)
+ *   snap_hook/downcast   :3607, :1734                 scp_gpu_snapshot
+ *   gpu_download         :2822                        scp_gpu_snapshot (dtype f64)
+ *   gpu_free             :2880                        scp_gpu_free
+ *
+ * Column order of host_cols[] is the SFA registration order of the reference
+ * snapshot writer (sfa/sim/scp_sim.c:2862-2897):
+ *    0- 2 phi_x..z   3- 5 theta_x..z   6- 8 phi_vx..vz   9-11 theta_vx..vz
+ *   12-14 phiim_*   15-17 thetaim_*   18-20 phiim_v*    21-23 thetaim_v*
+ *   24-26 th_x..z   27-29 E_x..z      (24-29 only when complex_gauge=1)
+ * Each column is N^3 values, site index (i*N + j)*N + k, k fastest.
+ *
+ * Threading: one handle is driven by one host thread at a time.  Every handle
+ * owns its own CUDA stream; distinct handles may run concurrently.
+ */
+#ifndef SCP_GPU_H
+#define SCP_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCP_GPU_ABI_VERSION 1
+#define SCP_GPU_MAX_COLS 30
+
+/* status codes */
+#define SCP_OK              0
+#define SCP_EINVAL         -1   /* bad parameter or handle */
+#define SCP_ENOMEM         -2   /* device allocation failed */
+#define SCP_ECUDA          -3   /* CUDA runtime error (see scp_gpu_last_cuda_error) */
+#define SCP_ENETCHARGE     -4   /* gauged + periodic seed is not net-neutral */
+#define SCP_EGAUSS         -5   /* Gauss projection CG did not converge */
+#define SCP_ENONFINITE     -6   /* a field went NaN/Inf (device flag) */
+#define SCP_EUNSUPPORTED   -7   /* configuration outside the implemented subset */
+#define SCP_ENODEV         -8   /* no usable CUDA device */
+#define SCP_EBUSY          -9   /* serving queue full / request slot unavailable */
+#define SCP_ETIMEOUT      -10   /* a bounded device wait gave up */
+
+/* precision modes */
+#define SCP_PREC_FP64   0   /* all state and arithmetic in FP64 */
+#define SCP_PREC_FP32C  1   /* FP32 state, compensated hi/lo positions, FP64 reductions */
+
+/* snapshot dtypes: the SFA dtype codes (sfa/format/sfa.h:86-90) */
+#define SCP_DTYPE_F16 0
+#define SCP_DTYPE_F32 1
+#define SCP_DTYPE_F64 2
+
+/* Physics / grid parameters: the subset of the reference Config that the
+ * complex (complex_phi=1) and gauged (complex_gauge=1) stepper reads
+ * (sfa/sim/scp_config.h:22-160).  Masses are passed squared, as the reference
+ * stores them after cfg_set (scp_config.h:222-223). */
+typedef struct {
+    int32_t N;                /* grid edge, >= 3 */
+    double  L;                /* half width; the caller passes dx = 2L/(N-1) */
+    double  dx, dt;           /* dt = dt_factor*dx (scp_sim.c:204-205) */
+    double  m2, mtheta2, eta, mu, kappa;
+    int32_t complex_gauge;    /* 1: compact U(1) links on every link */
+    double  g_gauge;          /* gauge coupling; must be > 0 when complex_gauge=1 */
+    int32_t bc_type;          /* 0 absorbing sphere, 2 periodic (1 unsupported) */
+    double  damp_width, damp_rate;
+    int32_t precision_mode;   /* SCP_PREC_FP64 or SCP_PREC_FP32C */
+    double  qdiag_radius, qdiag_probe1, qdiag_probe2;
+    int32_t gauss_project;    /* 1: one-time Gauss projection at init (reference default) */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t tile_variant;     /* 0: autotuned default; >0 selects a fixed tile shape */
+} scp_gpu_params;
+
+/* Diagnostic slots: the reference diag TSV columns after "t"
+ * (sfa/sim/scp_sim.c:2993-3003), same order and meaning. */
+enum {
+    SCP_DIAG_E_PHI_KIN = 0, SCP_DIAG_E_THETA_KIN, SCP_DIAG_E_GRAD, SCP_DIAG_E_MASS,
+    SCP_DIAG_E_POT, SCP_DIAG_E_TGRAD, SCP_DIAG_E_TMASS, SCP_DIAG_E_COUPLING,
+    SCP_DIAG_E_TOTAL, SCP_DIAG_PHI_MAX, SCP_DIAG_P_MAX, SCP_DIAG_P_INT, SCP_DIAG_THETA_RMS,
+    SCP_DIAG_Q_PHI, SCP_DIAG_Q_THETA, SCP_DIAG_Q_TOTAL, SCP_DIAG_S_MAX, SCP_DIAG_R_CORE,
+    SCP_DIAG_OMEGA_CORE, SCP_DIAG_Q_CORE, SCP_DIAG_THP1U, SCP_DIAG_THP1V, SCP_DIAG_THP2U,
+    SCP_DIAG_THP2V, SCP_DIAG_GAUSS_MAX, SCP_DIAG_GAUSS_L2, SCP_DIAG_E_EM, SCP_DIAG_Q_FLUX,
+    SCP_DIAG_Q_P0, SCP_DIAG_Q_P1, SCP_DIAG_Q_P2,
+    SCP_DIAG_CENTROID_X, SCP_DIAG_CENTROID_Y, SCP_DIAG_CENTROID_Z,
+    SCP_DIAG_NSLOTS = 40
+};
+typedef struct { double v[SCP_DIAG_NSLOTS]; } scp_gpu_diag_out;
+
+typedef struct {
+    int64_t steps_done;       /* leapfrog steps taken since init */
+    double  time;             /* steps_done * dt */
+    double  G_offset;         /* frozen Gauss offset measured after projection */
+    int32_t cg_iterations;    /* Gauss projection CG iterations */
+    int32_t precision_mode;
+    int64_t device_bytes;     /* device memory held by the handle */
+    double  state_bytes_per_site;   /* persistent bytes per site of the layout */
+    double  step_bytes_per_site;    /* algorithmic bytes moved per site-update */
+    int32_t tile_x, tile_y, seg_len; /* tile shape in use */
+} scp_gpu_info;
+
+typedef struct scp_gpu scp_gpu;
+
+/* Allocate device state, upload the host columns (24 complex or 30 gauged),
+ * and run the start-up sequence of the reference main (scp_sim.cu:5151-5245):
+ * net-charge check (gauged, periodic), Gauss projection, first force. */
+int  scp_gpu_init(const scp_gpu_params *p, const double *const *host_cols, scp_gpu **out);
+/* Same as scp_gpu_init, but the columns are device pointers (no H2D copy). */
+int  scp_gpu_init_device(const scp_gpu_params *p, const double *const *dev_cols, scp_gpu **out);
+/* Enqueue nsteps fused leapfrog steps on the handle's stream (asynchronous). */
+int  scp_gpu_step(scp_gpu *h, int nsteps);
+/* Wait for all work on the handle's stream; reports a pending NaN/Inf flag. */
+int  scp_gpu_sync(scp_gpu *h);
+/* FP64 reductions of the current state; synchronises.  Deterministic. */
+int  scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out);
+/* Copy the current state to host columns in dtype (SCP_DTYPE_*); the f32/f16
+ * casts are done on the device with the reference's conversion rules. */
+int  scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols);
+int  scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info);
+/* Time nsteps on the handle's stream with CUDA events recorded on that
+ * stream; *ms_out receives the device time of the whole batch. */
+int  scp_gpu_time_steps(scp_gpu *h, int nsteps, double *ms_out);
+/* The handle's cudaStream_t, as an opaque pointer. */
+void *scp_gpu_stream(scp_gpu *h);
+void scp_gpu_free(scp_gpu *h);
+const char *scp_gpu_errstr(int code);
+const char *scp_gpu_last_cuda_error(void);
+int  scp_gpu_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCP_GPU_H */

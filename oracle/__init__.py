@@ -1,0 +1,216 @@
+"""TEST INFRASTRUCTURE ONLY -- the parity checker.
+
+Two CPU implementations of the reference's complex / gauged stepper, used by
+tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline legs only:
+
+* ``Oracle``: ctypes face of liboracle.so, the C restatement in scp_oracle.c.
+* ``run_reference``: the reference binary itself (oracle/_ref/scp_sim, built
+  unmodified from kardianos/scp sfa/sim/scp_sim.c by oracle/Makefile), fed
+  through an SFA seed file and read back from its output frame and diag TSV.
+
+The product (scp_b200, libscpgpu.so) never imports this package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_BIN = os.path.join(HERE, "_ref", "scp_sim")
+SFA_TOOL = os.path.join(HERE, "_ref", "sfa_tool")
+NDIAG = 31
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [
+        ("N", ctypes.c_int), ("L", ctypes.c_double), ("dx", ctypes.c_double), ("dt", ctypes.c_double),
+        ("m2", ctypes.c_double), ("mtheta2", ctypes.c_double), ("eta", ctypes.c_double),
+        ("mu", ctypes.c_double), ("kappa", ctypes.c_double), ("gauge", ctypes.c_int),
+        ("g", ctypes.c_double), ("bc_type", ctypes.c_int), ("damp_width", ctypes.c_double),
+        ("damp_rate", ctypes.c_double), ("qdiag_radius", ctypes.c_double),
+        ("qdiag_probe1", ctypes.c_double), ("qdiag_probe2", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compile liboracle.so (and, with the reference tree present, _ref/)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    ref = os.environ.get("SCP_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "sfa", "sim")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.POINTER(OrcParams), ctypes.POINTER(vp), ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_int)]
+        L.orc_create.restype = vp
+        L.orc_free.argtypes = [vp]
+        L.orc_step.argtypes = [vp, ctypes.c_int]
+        L.orc_get.argtypes = [vp, ctypes.POINTER(vp)]
+        L.orc_diag.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.orc_g_offset.argtypes = [vp]
+        L.orc_g_offset.restype = ctypes.c_double
+        L.orc_cg_iterations.argtypes = [vp]
+        L.orc_accelerations.argtypes = [vp, ctypes.POINTER(vp)]
+        L.orc_gauge_xform_test.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        L.orc_gauge_xform_test.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _orc_params(p) -> OrcParams:
+    o = OrcParams()
+    o.N, o.L, o.dx, o.dt = p.N, p.L, p.dx, p.dt
+    o.m2, o.mtheta2, o.eta, o.mu, o.kappa = p.m2, p.mtheta2, p.eta, p.mu, p.kappa
+    o.gauge = 1 if p.gauged else 0
+    o.g = p.g_gauge
+    o.bc_type, o.damp_width, o.damp_rate = p.bc_type, p.damp_width, p.damp_rate
+    o.qdiag_radius, o.qdiag_probe1, o.qdiag_probe2 = p.qdiag_radius, p.qdiag_probe1, p.qdiag_probe2
+    return o
+
+
+class Oracle:
+    """C restatement of the reference stepper holding one state."""
+
+    def __init__(self, params, cols: Sequence[np.ndarray], project: bool = True):
+        self.params = params
+        self.ncols = params.ncols
+        src = [np.ascontiguousarray(c, dtype=np.float64).reshape(-1) for c in cols]
+        arr = (ctypes.c_void_p * self.ncols)(*[c.ctypes.data for c in src])
+        st = ctypes.c_int(0)
+        h = lib().orc_create(ctypes.byref(_orc_params(params)), arr, 1 if project else 0, ctypes.byref(st))
+        if not h:
+            raise RuntimeError(f"orc_create failed with status {st.value}")
+        self._h = ctypes.c_void_p(h)
+
+    def step(self, n: int) -> None:
+        lib().orc_step(self._h, int(n))
+
+    def cols(self) -> list[np.ndarray]:
+        n3 = self.params.N ** 3
+        out = [np.empty(n3) for _ in range(self.ncols)]
+        arr = (ctypes.c_void_p * self.ncols)(*[c.ctypes.data for c in out])
+        lib().orc_get(self._h, arr)
+        return out
+
+    def diag(self) -> np.ndarray:
+        buf = (ctypes.c_double * NDIAG)()
+        lib().orc_diag(self._h, buf)
+        return np.array(buf[:])
+
+    def accelerations(self) -> list[np.ndarray]:
+        n3 = self.params.N ** 3
+        out = [np.empty(n3) for _ in range(15)]
+        arr = (ctypes.c_void_p * 15)(*[c.ctypes.data for c in out])
+        lib().orc_accelerations(self._h, arr)
+        return out
+
+    @property
+    def g_offset(self) -> float:
+        return lib().orc_g_offset(self._h)
+
+    @property
+    def cg_iterations(self) -> int:
+        return lib().orc_cg_iterations(self._h)
+
+    def gauge_xform_test(self) -> tuple[float, np.ndarray]:
+        rel = (ctypes.c_double * 10)()
+        worst = lib().orc_gauge_xform_test(self._h, rel)
+        return worst, np.array(rel[:])
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().orc_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- reference binary
+
+def reference_available() -> bool:
+    return os.path.exists(REF_BIN) and os.path.exists(SFA_TOOL)
+
+
+def write_seed(path: str, params, cols: Sequence[np.ndarray]) -> None:
+    raw = path + ".raw"
+    np.concatenate([np.ascontiguousarray(c, dtype=np.float64).reshape(-1) for c in cols]).tofile(raw)
+    subprocess.run([SFA_TOOL, "write", path, str(params.N), repr(params.L), repr(params.dt),
+                    str(len(cols)), raw], check=True, capture_output=True)
+    os.remove(raw)
+
+
+def read_frame(path: str, frame: int, n3: int) -> tuple[list[str], list[np.ndarray]]:
+    raw = path + f".f{frame}.raw"
+    res = subprocess.run([SFA_TOOL, "read", path, str(frame), raw], check=True, capture_output=True, text=True)
+    names = [ln.split()[0] for ln in res.stdout.strip().splitlines()]
+    data = np.fromfile(raw)
+    os.remove(raw)
+    return names, [data[i * n3:(i + 1) * n3] for i in range(len(names))]
+
+
+def read_diag(path: str) -> tuple[list[str], np.ndarray]:
+    with open(path) as f:
+        header = f.readline().rstrip("\n").split("\t")
+        rows = [[float(x) for x in ln.split("\t")] for ln in f if ln.strip()]
+    return header, np.array(rows)
+
+
+def run_reference(params, cols: Sequence[np.ndarray], nsteps: int, diag_every: int | None = None,
+                  threads: int | None = None, workdir: str | None = None, extra_cfg: dict | None = None,
+                  read_final: bool = True) -> dict:
+    """Run the reference binary on the given initial columns for nsteps.
+
+    Returns {'cols': final columns (SFA order) or None, 'names', 'diag_header',
+    'diag' rows, 'wall_ms_per_step', 'stdout'}.
+    """
+    if not reference_available():
+        raise RuntimeError("reference binary not built (oracle/_ref)")
+    tmp = tempfile.mkdtemp(prefix="scpref_", dir=workdir)
+    seed = os.path.join(tmp, "seed.sfa")
+    write_seed(seed, params, cols)
+    T = nsteps * params.dt
+    de = diag_every if diag_every else nsteps
+    kv = dict(init="sfa", init_sfa=seed, init_frame=0, T=repr(T), precision="f64",
+              output=os.path.join(tmp, "out.sfa"), diag_file=os.path.join(tmp, "diag.tsv"),
+              snap_dt=repr(T if read_final else 1e9 * params.dt), diag_dt=repr(de * params.dt))
+    if extra_cfg:
+        kv.update(extra_cfg)
+    cfg = os.path.join(tmp, "run.cfg")
+    with open(cfg, "w") as f:
+        f.write(params.to_cfg(**kv))
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = str(threads or os.cpu_count() or 1)
+    res = subprocess.run([REF_BIN, cfg], capture_output=True, text=True, env=env, cwd=tmp)
+    if res.returncode != 0:
+        raise RuntimeError(f"reference run failed ({res.returncode}): {res.stderr[-2000:]}")
+    wall = None
+    for ln in res.stdout.splitlines():
+        if ln.startswith("Wall:") and "ms/step" in ln:
+            wall = float(ln.split()[-1].replace("ms/step", ""))
+    out = {"stdout": res.stdout, "wall_ms_per_step": wall, "dir": tmp}
+    hdr, rows = read_diag(os.path.join(tmp, "diag.tsv"))
+    out["diag_header"], out["diag"] = hdr, rows
+    if read_final:
+        names, fc = read_frame(os.path.join(tmp, "out.sfa"), -1, params.N ** 3)
+        out["names"], out["cols"] = names, fc
+    return out

@@ -1,0 +1,795 @@
+/* scp_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of the reference's complex (v66) and gauged (v69) lattice
+ * leapfrog stepper, kardianos/scp sfa/sim/scp_sim.c, single fabric, no Higgs,
+ * no second gauge, bc_type 0 (absorbing sphere) or 2 (periodic).  It is the
+ * checker for the CUDA library's parity tests and is never part of the
+ * product.  Parity of this restatement is pinned against the reference
+ * binary itself (oracle/_ref/scp_sim, built from the reference sources by
+ * oracle/Makefile) through the fixtures in tests/golden/.
+ *
+ * Each routine cites the reference function it restates; the arithmetic is
+ * written in the same operation order so that the restatement agrees with
+ * the reference to rounding (the reference is built with gcc's default FMA
+ * contraction, this file with -ffp-contract=off, so agreement is to a few
+ * ulps per step, not bitwise).
+ */
+#include "scp_oracle.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_PI 3.14159265358979323846
+
+/* field slots of the packed state: positions q[0..11] = u0..2 v0..2 tu0..2 tv0..2,
+ * velocities p[0..11] in the same order */
+enum { U0 = 0, V0 = 3, TU0 = 6, TV0 = 9 };
+
+struct orc_state {
+    orc_params P;
+    long N3;
+    double *q[12], *p[12], *a[12];   /* positions, velocities, accelerations */
+    double *th[3], *E[3], *K[3];     /* links, electric field, E-kick */
+    double *lc[3], *ls[3], *ps[3];   /* scratch: link cos/sin, plaquette sines */
+    double G_offset;
+    int cg_iters;
+    double *mem;
+};
+
+/* ---------------------------------------------------------------- helpers */
+
+typedef struct { long ip, im, jp, jm, kp, km; } nbr_t;
+
+static inline nbr_t nbrs(int N, long idx) {
+    const long NN = (long)N * N;
+    int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+    int ip = (i + 1) % N, im = (i - 1 + N) % N, jp = (j + 1) % N, jm = (j - 1 + N) % N;
+    int kp = (k + 1) % N, km = (k - 1 + N) % N;
+    nbr_t n;
+    n.ip = (long)ip * NN + (long)j * N + k;  n.im = (long)im * NN + (long)j * N + k;
+    n.jp = (long)i * NN + (long)jp * N + k;  n.jm = (long)i * NN + (long)jm * N + k;
+    n.kp = (long)i * NN + (long)j * N + kp;  n.km = (long)i * NN + (long)j * N + km;
+    return n;
+}
+
+/* curl component a of the 3-vector field F at a site
+ * (restates curl_component, scp_sim.c:409-415) */
+static inline double curl_a(double *const F[3], int a, const nbr_t *n, double idx1) {
+    if (a == 0) return (F[2][n->jp] - F[2][n->jm] - F[1][n->kp] + F[1][n->km]) * idx1;
+    if (a == 1) return (F[0][n->kp] - F[0][n->km] - F[2][n->ip] + F[2][n->im]) * idx1;
+    return (F[1][n->ip] - F[1][n->im] - F[0][n->jp] + F[0][n->jm]) * idx1;
+}
+
+static inline double wrap_angle(double v) {
+    return v - 2.0 * ORC_PI * rint(v / (2.0 * ORC_PI));
+}
+
+/* ---------------------------------------------------------------- forces */
+
+/* compute_forces_complex, scp_sim.c:931-994 */
+static void forces_complex(orc_state *s) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long N3 = s->N3;
+    const double idx2 = 1.0 / (P->dx * P->dx), idx1 = 1.0 / (2.0 * P->dx);
+    const double MU = P->mu, KAPPA = P->kappa, MASS2 = P->m2, MTHETA2 = P->mtheta2, ETA = P->eta;
+    double *const *q = s->q;
+    double *const *acc = s->a;
+    double *const U[3] = {q[0], q[1], q[2]}, *const Vv[3] = {q[3], q[4], q[5]};
+    double *const TU[3] = {q[6], q[7], q[8]}, *const TV[3] = {q[9], q[10], q[11]};
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        double u0 = U[0][idx], u1 = U[1][idx], u2 = U[2][idx];
+        double v0 = Vv[0][idx], v1 = Vv[1][idx], v2 = Vv[2][idx];
+        double s0 = u0 * u0 + v0 * v0, s1 = u1 * u1 + v1 * v1, s2 = u2 * u2 + v2 * v2;
+        double sp = s0 * s1 * s2;
+        double den = 1.0 + KAPPA * sp;
+        double Vp = 0.5 * MU / (den * den);
+        double rest[3] = {s1 * s2, s0 * s2, s0 * s1};
+        for (int a = 0; a < 3; a++) {
+            double x = U[a][idx];
+            double lap = (U[a][n.ip] + U[a][n.im] + U[a][n.jp] + U[a][n.jm] + U[a][n.kp] + U[a][n.km]
+                          - 6.0 * x) * idx2;
+            acc[U0 + a][idx] = lap - MASS2 * x - 2.0 * Vp * x * rest[a] + ETA * curl_a(TU, a, &n, idx1);
+            x = Vv[a][idx];
+            lap = (Vv[a][n.ip] + Vv[a][n.im] + Vv[a][n.jp] + Vv[a][n.jm] + Vv[a][n.kp] + Vv[a][n.km]
+                   - 6.0 * x) * idx2;
+            acc[V0 + a][idx] = lap - MASS2 * x - 2.0 * Vp * x * rest[a] + ETA * curl_a(TV, a, &n, idx1);
+            x = TU[a][idx];
+            lap = (TU[a][n.ip] + TU[a][n.im] + TU[a][n.jp] + TU[a][n.jm] + TU[a][n.kp] + TU[a][n.km]
+                   - 6.0 * x) * idx2;
+            acc[TU0 + a][idx] = lap - MTHETA2 * x + ETA * curl_a(U, a, &n, idx1);
+            x = TV[a][idx];
+            lap = (TV[a][n.ip] + TV[a][n.im] + TV[a][n.jp] + TV[a][n.jm] + TV[a][n.kp] + TV[a][n.km]
+                   - 6.0 * x) * idx2;
+            acc[TV0 + a][idx] = lap - MTHETA2 * x + ETA * curl_a(Vv, a, &n, idx1);
+        }
+    }
+}
+
+static void link_trig(orc_state *s) {
+    for (int d = 0; d < 3; d++) {
+        double *th = s->th[d], *c = s->lc[d], *sn = s->ls[d];
+#pragma omp parallel for schedule(static)
+        for (long idx = 0; idx < s->N3; idx++) { c[idx] = cos(th[idx]); sn[idx] = sin(th[idx]); }
+    }
+}
+
+/* plaquette angle in plane (a,b) at site idx with forward neighbours np[] */
+static inline double plaq_angle(double *const th[3], int a, int b, long idx, const long np[3]) {
+    return th[a][idx] + th[b][np[a]] - th[a][np[b]] - th[b][idx];
+}
+
+/* compute_forces_complex_gauge, scp_sim.c:1053-1263 (G2 = HIG = 0) */
+static void forces_gauge(orc_state *s) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long N3 = s->N3;
+    const double dx = P->dx, idx2 = 1.0 / (dx * dx), idx1 = 1.0 / (2.0 * dx), inva = 1.0 / dx;
+    const double MU = P->mu, KAPPA = P->kappa, MASS2 = P->m2, MTHETA2 = P->mtheta2, ETA = P->eta;
+    const double GG = P->g, STP = 1.0 / (GG * dx * dx * dx);
+    static const int pa[3] = {0, 1, 2}, pb[3] = {1, 2, 0};
+    static const int ci1[3] = {1, 2, 0}, ci2[3] = {2, 0, 1};
+
+    /* pass A: link cos/sin */
+    link_trig(s);
+    /* pass B: plaquette sines, planes (0,1) (1,2) (2,0) */
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        long np[3] = {n.ip, n.jp, n.kp};
+        for (int p = 0; p < 3; p++) s->ps[p][idx] = sin(plaq_angle(s->th, pa[p], pb[p], idx, np));
+    }
+    /* pass C: matter accelerations and E-kick */
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        long np[3] = {n.ip, n.jp, n.kp}, nm[3] = {n.im, n.jm, n.km};
+        double fu[6], fv[6];
+        for (int a = 0; a < 3; a++) {
+            fu[a] = s->q[U0 + a][idx];      fv[a] = s->q[V0 + a][idx];
+            fu[3 + a] = s->q[TU0 + a][idx]; fv[3 + a] = s->q[TV0 + a][idx];
+        }
+        double TRp[3][6], TIp[3][6], TRm[3][6], TIm[3][6], tup[3][3], tvp[3][3];
+        for (int d = 0; d < 3; d++) {
+            double cP = s->lc[d][idx], sP = s->ls[d][idx];
+            double cM = s->lc[d][nm[d]], sM = s->ls[d][nm[d]];
+            for (int a = 0; a < 3; a++) {
+                double upn = s->q[U0 + a][np[d]], vpn = s->q[V0 + a][np[d]];
+                double umn = s->q[U0 + a][nm[d]], vmn = s->q[V0 + a][nm[d]];
+                double tpn = s->q[TU0 + a][np[d]], wpn = s->q[TV0 + a][np[d]];
+                double tmn = s->q[TU0 + a][nm[d]], wmn = s->q[TV0 + a][nm[d]];
+                TRp[d][a] = cP * upn - sP * vpn;       TIp[d][a] = cP * vpn + sP * upn;
+                TRm[d][a] = cM * umn + sM * vmn;       TIm[d][a] = cM * vmn - sM * umn;
+                TRp[d][3 + a] = cP * tpn - sP * wpn;   TIp[d][3 + a] = cP * wpn + sP * tpn;
+                TRm[d][3 + a] = cM * tmn + sM * wmn;   TIm[d][3 + a] = cM * wmn - sM * tmn;
+                tup[d][a] = tpn; tvp[d][a] = wpn;
+            }
+        }
+        double s0 = fu[0] * fu[0] + fv[0] * fv[0];
+        double s1 = fu[1] * fu[1] + fv[1] * fv[1];
+        double s2 = fu[2] * fu[2] + fv[2] * fv[2];
+        double sp = s0 * s1 * s2;
+        double den = 1.0 + KAPPA * sp;
+        double Vp = 0.5 * MU / (den * den);
+        double rest[3] = {s1 * s2, s0 * s2, s0 * s1};
+        double DcU[3][6], DcV[3][6];
+        for (int d = 0; d < 3; d++)
+            for (int f = 0; f < 6; f++) {
+                DcU[d][f] = (TRp[d][f] - TRm[d][f]) * idx1;
+                DcV[d][f] = (TIp[d][f] - TIm[d][f]) * idx1;
+            }
+        for (int a = 0; a < 3; a++) {
+            int d1 = ci1[a], d2 = ci2[a];
+            double reDxT = DcU[d1][3 + d2] - DcU[d2][3 + d1];
+            double imDxT = DcV[d1][3 + d2] - DcV[d2][3 + d1];
+            double reDxP = DcU[d1][d2] - DcU[d2][d1];
+            double imDxP = DcV[d1][d2] - DcV[d2][d1];
+            double lapUP = (TRp[0][a] + TRm[0][a] + TRp[1][a] + TRm[1][a] + TRp[2][a] + TRm[2][a]
+                            - 6.0 * fu[a]) * idx2;
+            double lapVP = (TIp[0][a] + TIm[0][a] + TIp[1][a] + TIm[1][a] + TIp[2][a] + TIm[2][a]
+                            - 6.0 * fv[a]) * idx2;
+            double lapUT = (TRp[0][3 + a] + TRm[0][3 + a] + TRp[1][3 + a] + TRm[1][3 + a]
+                            + TRp[2][3 + a] + TRm[2][3 + a] - 6.0 * fu[3 + a]) * idx2;
+            double lapVT = (TIp[0][3 + a] + TIm[0][3 + a] + TIp[1][3 + a] + TIm[1][3 + a]
+                            + TIp[2][3 + a] + TIm[2][3 + a] - 6.0 * fv[3 + a]) * idx2;
+            s->a[U0 + a][idx] = lapUP - MASS2 * fu[a] - 2.0 * Vp * fu[a] * rest[a] + ETA * reDxT;
+            s->a[V0 + a][idx] = lapVP - MASS2 * fv[a] - 2.0 * Vp * fv[a] * rest[a] + ETA * imDxT;
+            s->a[TU0 + a][idx] = lapUT - MTHETA2 * fu[3 + a] + ETA * reDxP;
+            s->a[TV0 + a][idx] = lapVT - MTHETA2 * fv[3 + a] + ETA * imDxP;
+        }
+        double *const *ps = s->ps;
+        double st[3];
+        st[0] = (ps[0][idx] - ps[0][nm[1]]) - (ps[2][idx] - ps[2][nm[2]]);
+        st[1] = -(ps[0][idx] - ps[0][nm[0]]) + (ps[1][idx] - ps[1][nm[2]]);
+        st[2] = (ps[2][idx] - ps[2][nm[0]]) - (ps[1][idx] - ps[1][nm[1]]);
+        for (int d = 0; d < 3; d++) {
+            double cP = s->lc[d][idx], sP = s->ls[d][idx];
+            double Jg = 0.0;
+            for (int a = 0; a < 3; a++) {
+                Jg += fu[a] * TIp[d][a] - fv[a] * TRp[d][a];
+                Jg += fu[3 + a] * TIp[d][3 + a] - fv[3 + a] * TRp[d][3 + a];
+            }
+            int d1 = ci1[d], d2 = ci2[d];
+            double WpR1 = cP * fu[d2] + sP * fv[d2], WpI1 = cP * fv[d2] - sP * fu[d2];
+            double WpR2 = cP * fu[d1] + sP * fv[d1], WpI2 = cP * fv[d1] - sP * fu[d1];
+            double T12 = (fu[3 + d1] * TIp[d][d2] - fv[3 + d1] * TRp[d][d2])
+                       + (tup[d][d1] * WpI1 - tvp[d][d1] * WpR1);
+            double T21 = (fu[3 + d2] * TIp[d][d1] - fv[3 + d2] * TRp[d][d1])
+                       + (tup[d][d2] * WpI2 - tvp[d][d2] * WpR2);
+            double Jlat = inva * Jg - 0.5 * ETA * (T12 - T21);
+            s->K[d][idx] = STP * st[d] + GG * Jlat;
+        }
+    }
+}
+
+static void forces(orc_state *s) {
+    if (s->P.gauge) forces_gauge(s); else forces_complex(s);
+}
+
+/* ---------------------------------------------------------------- stepping */
+
+/* apply_damping, scp_sim.c:1440-1473 (complex + gauged members only) */
+static void damping(orc_state *s) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long NN = (long)N * N;
+    const double L = P->L, dx = P->dx, DW = P->damp_width, DR = P->damp_rate;
+    if (DW <= 0 || DR <= 0) return;
+    const double R_damp = L - DW;
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < s->N3; idx++) {
+        int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        double x = -L + i * dx, y = -L + j * dx, z = -L + k * dx;
+        double r = sqrt(x * x + y * y + z * z);
+        if (r > R_damp) {
+            double sc = (r - R_damp) / DW;
+            if (sc > 1) sc = 1;
+            double d = 1.0 - DR * sc * sc;
+            for (int f = 0; f < 12; f++) s->p[f][idx] *= d;
+            if (P->gauge) for (int c = 0; c < 3; c++) s->E[c][idx] *= d;
+        }
+    }
+}
+
+static void half_kick(orc_state *s, double hdt) {
+    for (int f = 0; f < 12; f++) {
+        double *v = s->p[f], *a = s->a[f];
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < s->N3; i++) v[i] += hdt * a[i];
+    }
+    if (s->P.gauge)
+        for (int c = 0; c < 3; c++) {
+            double *E = s->E[c], *K = s->K[c];
+#pragma omp parallel for schedule(static)
+            for (long i = 0; i < s->N3; i++) E[i] += hdt * K[i];
+        }
+}
+
+/* verlet_step, scp_sim.c:1583-1716: kick, drift (+ link drift and wrap),
+ * forces, kick, boundary */
+static void verlet(orc_state *s) {
+    const double dt = s->P.dt, hdt = 0.5 * dt;
+    half_kick(s, hdt);
+    for (int f = 0; f < 12; f++) {
+        double *x = s->q[f], *v = s->p[f];
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < s->N3; i++) x[i] += dt * v[i];
+    }
+    if (s->P.gauge) {
+        const double gad = -s->P.g * s->P.dx * dt;
+        for (int c = 0; c < 3; c++) {
+            double *th = s->th[c], *E = s->E[c];
+#pragma omp parallel for schedule(static)
+            for (long i = 0; i < s->N3; i++) th[i] = wrap_angle(th[i] + gad * E[i]);
+        }
+    }
+    forces(s);
+    half_kick(s, hdt);
+    if (s->P.bc_type == 0) damping(s);
+}
+
+void orc_step(orc_state *s, int nsteps) {
+    for (int n = 0; n < nsteps; n++) verlet(s);
+}
+
+/* ---------------------------------------------------------------- Gauss law */
+
+static inline double rho_at(const orc_state *s, long idx) {
+    double r = 0;
+    for (int a = 0; a < 3; a++)
+        r += s->q[U0 + a][idx] * s->p[V0 + a][idx] - s->q[V0 + a][idx] * s->p[U0 + a][idx]
+           + s->q[TU0 + a][idx] * s->p[TV0 + a][idx] - s->q[TV0 + a][idx] * s->p[TU0 + a][idx];
+    return r;
+}
+
+/* gauss_residual_at, scp_sim.c:2176-2181 */
+static inline double gauss_at(const orc_state *s, long idx, const nbr_t *n) {
+    double divE = (s->E[0][idx] - s->E[0][n->im] + s->E[1][idx] - s->E[1][n->jm]
+                   + s->E[2][idx] - s->E[2][n->km]) / s->P.dx;
+    return divE - s->P.g * rho_at(s, idx);
+}
+
+/* net_charge_check, scp_sim.c:2264-2279: 0 when neutral */
+static int net_charge_ok(const orc_state *s) {
+    const double dV = s->P.dx * s->P.dx * s->P.dx;
+    double qn = 0, qa = 0;
+#pragma omp parallel for reduction(+ : qn, qa) schedule(static)
+    for (long idx = 0; idx < s->N3; idx++) {
+        double r = rho_at(s, idx);
+        qn += r * dV;
+        qa += fabs(r) * dV;
+    }
+    return !(fabs(qn) > 1e-6 * fmax(qa, 1.0));
+}
+
+/* init_gauss_project, scp_sim.c:2284-2400: CG on -lap chi = G - mean(G),
+ * E += forward gradient of chi, freeze G_offset = mean(G) */
+static int gauss_project(orc_state *s) {
+    const int N = s->P.N;
+    const long N3 = s->N3;
+    const double dx = s->P.dx, idx2 = 1.0 / (dx * dx);
+    double *b = malloc(N3 * sizeof(double)), *xv = calloc(N3, sizeof(double));
+    double *r = malloc(N3 * sizeof(double)), *pp = malloc(N3 * sizeof(double));
+    double *Ap = malloc(N3 * sizeof(double));
+    if (!b || !xv || !r || !pp || !Ap) return -4;
+    double gsum = 0, gmax0 = 0;
+#pragma omp parallel for reduction(+ : gsum) schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        b[idx] = gauss_at(s, idx, &n);
+        gsum += b[idx];
+    }
+    double gbar = gsum / (double)N3;
+#pragma omp parallel for reduction(max : gmax0) schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        b[idx] -= gbar;
+        double d = fabs(b[idx]);
+        if (d > gmax0) gmax0 = d;
+    }
+    const double tol = 1e-13 * fmax(1.0, gmax0);
+    memcpy(r, b, N3 * sizeof(double));
+    memcpy(pp, b, N3 * sizeof(double));
+    double rz = 0;
+#pragma omp parallel for reduction(+ : rz) schedule(static)
+    for (long idx = 0; idx < N3; idx++) rz += r[idx] * r[idx];
+    int it = 0;
+    double rmax = gmax0;
+    while (rmax > tol && it < 20000) {
+        double pAp = 0;
+#pragma omp parallel for reduction(+ : pAp) schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            nbr_t n = nbrs(N, idx);
+            double lap = (pp[n.ip] + pp[n.im] + pp[n.jp] + pp[n.jm] + pp[n.kp] + pp[n.km] - 6.0 * pp[idx]) * idx2;
+            Ap[idx] = -lap;
+            pAp += pp[idx] * Ap[idx];
+        }
+        double alpha = rz / pAp, rz2 = 0, xsum = 0, rm = 0;
+#pragma omp parallel for reduction(+ : rz2, xsum) reduction(max : rm) schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            xv[idx] += alpha * pp[idx];
+            r[idx] -= alpha * Ap[idx];
+            rz2 += r[idx] * r[idx];
+            xsum += xv[idx];
+            double d = fabs(r[idx]);
+            if (d > rm) rm = d;
+        }
+        double xbar = xsum / (double)N3, beta = rz2 / rz;
+#pragma omp parallel for schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            xv[idx] -= xbar;
+            pp[idx] = r[idx] + beta * pp[idx];
+        }
+        rz = rz2;
+        rmax = rm;
+        it++;
+    }
+    int ok = !(rmax > tol);
+    if (ok) {
+#pragma omp parallel for schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            nbr_t n = nbrs(N, idx);
+            s->E[0][idx] += (xv[n.ip] - xv[idx]) / dx;
+            s->E[1][idx] += (xv[n.jp] - xv[idx]) / dx;
+            s->E[2][idx] += (xv[n.kp] - xv[idx]) / dx;
+        }
+        double osum = 0;
+#pragma omp parallel for reduction(+ : osum) schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            nbr_t n = nbrs(N, idx);
+            osum += gauss_at(s, idx, &n);
+        }
+        s->G_offset = osum / (double)N3;
+    }
+    s->cg_iters = it;
+    free(b); free(xv); free(r); free(pp); free(Ap);
+    return ok ? 0 : -3;
+}
+
+/* ---------------------------------------------------------------- diagnostics */
+
+/* compute_energy_complex (scp_sim.c:1823-1880) or compute_energy_complex_gauge
+ * (:1886-2036) into out[0..10]; theta_rms_complex/P_integrated_complex
+ * (:2041-2061) into out[11..12] */
+static void diag_energy(orc_state *s, double *out) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long N3 = s->N3;
+    const double dx = P->dx, dV = dx * dx * dx, idx1 = 1.0 / (2.0 * dx);
+    const double MU = P->mu, KAPPA = P->kappa, MASS2 = P->m2, MTHETA2 = P->mtheta2, ETA = P->eta;
+    const int G = P->gauge;
+    const double GG = P->g, BPRE = G ? 1.0 / (GG * GG * dx * dx * dx * dx) : 0.0;
+    static const int ci1[3] = {1, 2, 0}, ci2[3] = {2, 0, 1};
+    double *const U[3] = {s->q[0], s->q[1], s->q[2]}, *const Vv[3] = {s->q[3], s->q[4], s->q[5]};
+    double *const TU[3] = {s->q[6], s->q[7], s->q[8]}, *const TV[3] = {s->q[9], s->q[10], s->q[11]};
+    if (G) link_trig(s);
+    double epk = 0, etk = 0, eg = 0, em = 0, ep = 0, etg = 0, etm = 0, ec = 0, pm = 0, Pm = 0, eem = 0;
+#pragma omp parallel for reduction(+ : epk, etk, eg, em, ep, etg, etm, ec, eem) reduction(max : pm, Pm) schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        double s2[3];
+        if (!G) {
+            for (int a = 0; a < 3; a++) {
+                double u = U[a][idx], v = Vv[a][idx], tu = TU[a][idx], tv = TV[a][idx];
+                s2[a] = u * u + v * v;
+                epk += 0.5 * (s->p[U0 + a][idx] * s->p[U0 + a][idx] + s->p[V0 + a][idx] * s->p[V0 + a][idx]) * dV;
+                etk += 0.5 * (s->p[TU0 + a][idx] * s->p[TU0 + a][idx] + s->p[TV0 + a][idx] * s->p[TV0 + a][idx]) * dV;
+                double gx = (U[a][n.ip] - U[a][n.im]) * idx1, gy = (U[a][n.jp] - U[a][n.jm]) * idx1;
+                double gz = (U[a][n.kp] - U[a][n.km]) * idx1;
+                double hx = (Vv[a][n.ip] - Vv[a][n.im]) * idx1, hy = (Vv[a][n.jp] - Vv[a][n.jm]) * idx1;
+                double hz = (Vv[a][n.kp] - Vv[a][n.km]) * idx1;
+                eg += 0.5 * (gx * gx + gy * gy + gz * gz + hx * hx + hy * hy + hz * hz) * dV;
+                em += 0.5 * MASS2 * (u * u + v * v) * dV;
+                double tgx = (TU[a][n.ip] - TU[a][n.im]) * idx1, tgy = (TU[a][n.jp] - TU[a][n.jm]) * idx1;
+                double tgz = (TU[a][n.kp] - TU[a][n.km]) * idx1;
+                double thx = (TV[a][n.ip] - TV[a][n.im]) * idx1, thy = (TV[a][n.jp] - TV[a][n.jm]) * idx1;
+                double thz = (TV[a][n.kp] - TV[a][n.km]) * idx1;
+                etg += 0.5 * (tgx * tgx + tgy * tgy + tgz * tgz + thx * thx + thy * thy + thz * thz) * dV;
+                etm += 0.5 * MTHETA2 * (tu * tu + tv * tv) * dV;
+                double mod = sqrt(s2[a]);
+                if (mod > pm) pm = mod;
+                double ctu = curl_a(TU, a, &n, idx1), ctv = curl_a(TV, a, &n, idx1);
+                ec -= ETA * (u * ctu + v * ctv) * dV;
+            }
+        } else {
+            long np[3] = {n.ip, n.jp, n.kp}, nm[3] = {n.im, n.jm, n.km};
+            double fu[6], fv[6];
+            for (int a = 0; a < 3; a++) {
+                fu[a] = U[a][idx]; fv[a] = Vv[a][idx]; fu[3 + a] = TU[a][idx]; fv[3 + a] = TV[a][idx];
+            }
+            double DcU[3][6], DcV[3][6];
+            for (int d = 0; d < 3; d++) {
+                double cP = s->lc[d][idx], sP = s->ls[d][idx];
+                double cM = s->lc[d][nm[d]], sM = s->ls[d][nm[d]];
+                for (int a = 0; a < 3; a++) {
+                    double upn = U[a][np[d]], vpn = Vv[a][np[d]], umn = U[a][nm[d]], vmn = Vv[a][nm[d]];
+                    double tpn = TU[a][np[d]], wpn = TV[a][np[d]], tmn = TU[a][nm[d]], wmn = TV[a][nm[d]];
+                    DcU[d][a] = ((cP * upn - sP * vpn) - (cM * umn + sM * vmn)) * idx1;
+                    DcV[d][a] = ((cP * vpn + sP * upn) - (cM * vmn - sM * umn)) * idx1;
+                    DcU[d][3 + a] = ((cP * tpn - sP * wpn) - (cM * tmn + sM * wmn)) * idx1;
+                    DcV[d][3 + a] = ((cP * wpn + sP * tpn) - (cM * wmn - sM * tmn)) * idx1;
+                }
+            }
+            for (int a = 0; a < 3; a++) {
+                s2[a] = fu[a] * fu[a] + fv[a] * fv[a];
+                epk += 0.5 * (s->p[U0 + a][idx] * s->p[U0 + a][idx] + s->p[V0 + a][idx] * s->p[V0 + a][idx]) * dV;
+                etk += 0.5 * (s->p[TU0 + a][idx] * s->p[TU0 + a][idx] + s->p[TV0 + a][idx] * s->p[TV0 + a][idx]) * dV;
+                eg += 0.5 * (DcU[0][a] * DcU[0][a] + DcU[1][a] * DcU[1][a] + DcU[2][a] * DcU[2][a]
+                             + DcV[0][a] * DcV[0][a] + DcV[1][a] * DcV[1][a] + DcV[2][a] * DcV[2][a]) * dV;
+                em += 0.5 * MASS2 * s2[a] * dV;
+                etg += 0.5 * (DcU[0][3 + a] * DcU[0][3 + a] + DcU[1][3 + a] * DcU[1][3 + a]
+                              + DcU[2][3 + a] * DcU[2][3 + a] + DcV[0][3 + a] * DcV[0][3 + a]
+                              + DcV[1][3 + a] * DcV[1][3 + a] + DcV[2][3 + a] * DcV[2][3 + a]) * dV;
+                etm += 0.5 * MTHETA2 * (fu[3 + a] * fu[3 + a] + fv[3 + a] * fv[3 + a]) * dV;
+                double mod = sqrt(s2[a]);
+                if (mod > pm) pm = mod;
+                double reDxT = DcU[ci1[a]][3 + ci2[a]] - DcU[ci2[a]][3 + ci1[a]];
+                double imDxT = DcV[ci1[a]][3 + ci2[a]] - DcV[ci2[a]][3 + ci1[a]];
+                ec -= ETA * (fu[a] * reDxT + fv[a] * imDxT) * dV;
+            }
+            double ee = 0.5 * (s->E[0][idx] * s->E[0][idx] + s->E[1][idx] * s->E[1][idx]
+                               + s->E[2][idx] * s->E[2][idx]);
+            double bb = 0.0;
+            static const int pa[3] = {0, 1, 2}, pb[3] = {1, 2, 0};
+            for (int p = 0; p < 3; p++) bb += 1.0 - cos(plaq_angle(s->th, pa[p], pb[p], idx, np));
+            eem += (ee + BPRE * bb) * dV;
+        }
+        double sp = s2[0] * s2[1] * s2[2];
+        ep += (MU / 2.0) * sp / (1.0 + KAPPA * sp) * dV;
+        double Pmod = sqrt(sp);
+        if (Pmod > Pm) Pm = Pmod;
+    }
+    double trs = 0, pint = 0;
+#pragma omp parallel for reduction(+ : trs, pint) schedule(static)
+    for (long i = 0; i < N3; i++) {
+        for (int a = 0; a < 3; a++) trs += TU[a][i] * TU[a][i] + TV[a][i] * TV[a][i];
+        double a0 = U[0][i] * U[0][i] + Vv[0][i] * Vv[0][i];
+        double a1 = U[1][i] * U[1][i] + Vv[1][i] * Vv[1][i];
+        double a2 = U[2][i] * U[2][i] + Vv[2][i] * Vv[2][i];
+        pint += sqrt(a0 * a1 * a2) * dV;
+    }
+    out[0] = epk; out[1] = etk; out[2] = eg; out[3] = em; out[4] = ep;
+    out[5] = etg; out[6] = etm; out[7] = ec;
+    out[8] = epk + etk + eg + em + ep + etg + etm + ec + eem;
+    out[9] = pm; out[10] = Pm; out[11] = pint; out[12] = sqrt(trs / (6.0 * N3));
+}
+
+/* compute_charges, scp_sim.c:2074-2169, into out[13..23] and out[28..30] */
+static void diag_charges(orc_state *s, double *out) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long NN = (long)N * N, N3 = s->N3;
+    const double L = P->L, dx = P->dx, dV = dx * dx * dx, R2 = P->qdiag_radius * P->qdiag_radius;
+    double qp = 0, qt = 0, smax = 0, M0 = 0, cx = 0, cy = 0, cz = 0, qc = 0, qp0 = 0, qp1 = 0, qp2 = 0;
+#pragma omp parallel for reduction(+ : qp, qt, M0, cx, cy, cz, qc, qp0, qp1, qp2) reduction(max : smax) schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        double x = -L + i * dx, y = -L + j * dx, z = -L + k * dx;
+        double rho2 = 0, sp = 1.0, qpv = 0, qtv = 0;
+        for (int a = 0; a < 3; a++) {
+            double u = s->q[U0 + a][idx], v = s->q[V0 + a][idx];
+            double ud = s->p[U0 + a][idx], vd = s->p[V0 + a][idx];
+            double tu = s->q[TU0 + a][idx], tv = s->q[TV0 + a][idx];
+            double tud = s->p[TU0 + a][idx], tvd = s->p[TV0 + a][idx];
+            double qa = u * vd - v * ud;
+            qpv += qa;
+            if (a == 0) qp0 += qa; else if (a == 1) qp1 += qa; else qp2 += qa;
+            qtv += tu * tvd - tv * tud;
+            double s2a = u * u + v * v;
+            rho2 += s2a;
+            sp *= s2a;
+        }
+        qp += qpv; qt += qtv;
+        if (x * x + y * y + z * z <= R2) qc += qpv + qtv;
+        if (sp > smax) smax = sp;
+        M0 += rho2;
+        cx += x * rho2; cy += y * rho2; cz += z * rho2;
+    }
+    out[13] = qp * dV; out[14] = qt * dV; out[15] = qp * dV + qt * dV; out[16] = smax;
+    out[19] = qc * dV;
+    out[28] = qp0 * dV; out[29] = qp1 * dV; out[30] = qp2 * dV;
+    /* omega_core at the lowest-index voxel with s >= smax*(1-1e-12) */
+    long smax_idx = -1;
+    const double sthr = smax * (1.0 - 1e-12);
+    for (long idx = 0; idx < N3; idx++) {
+        double sp = 1.0;
+        for (int a = 0; a < 3; a++) {
+            double u = s->q[U0 + a][idx], v = s->q[V0 + a][idx];
+            sp *= u * u + v * v;
+        }
+        if (sp >= sthr) { smax_idx = idx; break; }
+    }
+    out[18] = 0.0;
+    if (smax_idx >= 0) {
+        double u0 = s->q[U0][smax_idx], v0 = s->q[V0][smax_idx];
+        double ud0 = s->p[U0][smax_idx], vd0 = s->p[V0][smax_idx];
+        double den = u0 * u0 + v0 * v0;
+        if (den >= 1e-20) out[18] = (u0 * vd0 - v0 * ud0) / den;
+    }
+    int jc = (int)lround(L / dx);
+    if (jc < 0) jc = 0; if (jc > N - 1) jc = N - 1;
+    int i1 = (int)lround((P->qdiag_probe1 + L) / dx);
+    if (i1 < 0) i1 = 0; if (i1 > N - 1) i1 = N - 1;
+    int i2 = (int)lround((P->qdiag_probe2 + L) / dx);
+    if (i2 < 0) i2 = 0; if (i2 > N - 1) i2 = N - 1;
+    long p1 = (long)i1 * NN + (long)jc * N + jc, p2 = (long)i2 * NN + (long)jc * N + jc;
+    out[20] = s->q[TU0 + 1][p1]; out[21] = s->q[TV0 + 1][p1];
+    out[22] = s->q[TU0 + 1][p2]; out[23] = s->q[TV0 + 1][p2];
+    M0 *= dV;
+    if (M0 < 1e-30) { out[17] = 0; return; }
+    cx = cx * dV / M0; cy = cy * dV / M0; cz = cz * dV / M0;
+    double rsum = 0;
+#pragma omp parallel for reduction(+ : rsum) schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        double x = -L + i * dx, y = -L + j * dx, z = -L + k * dx;
+        double rho2 = 0;
+        for (int a = 0; a < 3; a++) {
+            double u = s->q[U0 + a][idx], v = s->q[V0 + a][idx];
+            rho2 += u * u + v * v;
+        }
+        rsum += ((x - cx) * (x - cx) + (y - cy) * (y - cy) + (z - cz) * (z - cz)) * rho2;
+    }
+    out[17] = sqrt(rsum * dV / M0);
+}
+
+/* compute_gauss, scp_sim.c:2186-2243, into out[24..27] */
+static void diag_gauss(orc_state *s, double *out) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long NN = (long)N * N, N3 = s->N3;
+    const double L = P->L, dx = P->dx, dV = dx * dx * dx, GG = P->g, OFF = s->G_offset;
+    const double Rint = (P->bc_type == 0) ? (L - P->damp_width - dx) : 1e300, Rint2 = Rint * Rint;
+    const double Rcube = P->qdiag_radius;
+    static const int pa[3] = {0, 1, 2}, pb[3] = {1, 2, 0};
+    double gmax = 0, gl2 = 0, eem = 0, fsum = 0;
+    long nOmega = 0, nC = 0;
+#pragma omp parallel for reduction(+ : gl2, eem, fsum, nOmega, nC) reduction(max : gmax) schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        nbr_t n = nbrs(N, idx);
+        long np[3] = {n.ip, n.jp, n.kp};
+        double x = -L + i * dx, y = -L + j * dx, z = -L + k * dx;
+        double divE = (s->E[0][idx] - s->E[0][n.im] + s->E[1][idx] - s->E[1][n.jm]
+                       + s->E[2][idx] - s->E[2][n.km]) / dx;
+        double G = gauss_at(s, idx, &n);
+        if (x * x + y * y + z * z < Rint2) {
+            double d = fabs(G - OFF);
+            if (d > gmax) gmax = d;
+            gl2 += (G - OFF) * (G - OFF);
+            nOmega++;
+        }
+        double ee = 0.5 * (s->E[0][idx] * s->E[0][idx] + s->E[1][idx] * s->E[1][idx]
+                           + s->E[2][idx] * s->E[2][idx]);
+        if (GG != 0) {
+            double bb = 0;
+            for (int p = 0; p < 3; p++) bb += 1.0 - cos(plaq_angle(s->th, pa[p], pb[p], idx, np));
+            ee += bb / (GG * GG * dx * dx * dx * dx);
+        }
+        eem += ee * dV;
+        if (fabs(x) <= Rcube && fabs(y) <= Rcube && fabs(z) <= Rcube) { fsum += divE * dV; nC++; }
+    }
+    out[24] = gmax;
+    out[25] = (nOmega > 0) ? sqrt(gl2 / (double)nOmega) : 0.0;
+    out[26] = eem;
+    out[27] = (GG != 0) ? (fsum - OFF * (double)nC * dV) / GG : 0.0;
+}
+
+int orc_diag(orc_state *s, double *out) {
+    for (int i = 0; i < 31; i++) out[i] = 0.0;
+    diag_energy(s, out);
+    diag_charges(s, out);
+    if (s->P.gauge) diag_gauss(s, out);
+    return 31;
+}
+
+/* ---------------------------------------------------------------- lifecycle */
+
+orc_state *orc_create(const orc_params *p, const double *const *cols, int project, int *status) {
+    *status = 0;
+    if (!p || p->N < 3 || p->dx <= 0 || p->dt <= 0 || (p->gauge && p->g == 0.0)) { *status = -1; return NULL; }
+    orc_state *s = calloc(1, sizeof(orc_state));
+    if (!s) { *status = -4; return NULL; }
+    s->P = *p;
+    s->N3 = (long)p->N * p->N * p->N;
+    int nblk = 36 + (p->gauge ? 18 : 0);
+    s->mem = calloc((size_t)nblk * s->N3, sizeof(double));
+    if (!s->mem) { free(s); *status = -4; return NULL; }
+    double *m = s->mem;
+    for (int f = 0; f < 12; f++) { s->q[f] = m; m += s->N3; }
+    for (int f = 0; f < 12; f++) { s->p[f] = m; m += s->N3; }
+    for (int f = 0; f < 12; f++) { s->a[f] = m; m += s->N3; }
+    if (p->gauge)
+        for (int c = 0; c < 3; c++) {
+            s->th[c] = m; m += s->N3; s->E[c] = m; m += s->N3; s->K[c] = m; m += s->N3;
+            s->lc[c] = m; m += s->N3; s->ls[c] = m; m += s->N3; s->ps[c] = m; m += s->N3;
+        }
+    /* column order -> packed slots */
+    size_t bytes = s->N3 * sizeof(double);
+    for (int a = 0; a < 3; a++) {
+        memcpy(s->q[U0 + a], cols[0 + a], bytes);  memcpy(s->q[TU0 + a], cols[3 + a], bytes);
+        memcpy(s->p[U0 + a], cols[6 + a], bytes);  memcpy(s->p[TU0 + a], cols[9 + a], bytes);
+        memcpy(s->q[V0 + a], cols[12 + a], bytes); memcpy(s->q[TV0 + a], cols[15 + a], bytes);
+        memcpy(s->p[V0 + a], cols[18 + a], bytes); memcpy(s->p[TV0 + a], cols[21 + a], bytes);
+        if (p->gauge) { memcpy(s->th[a], cols[24 + a], bytes); memcpy(s->E[a], cols[27 + a], bytes); }
+    }
+    if (p->gauge) {
+        if (p->bc_type == 2 && !net_charge_ok(s)) { orc_free(s); *status = -2; return NULL; }
+        if (project) {
+            int rc = gauss_project(s);
+            if (rc) { orc_free(s); *status = rc; return NULL; }
+        }
+    }
+    forces(s);
+    return s;
+}
+
+void orc_free(orc_state *s) {
+    if (!s) return;
+    free(s->mem);
+    free(s);
+}
+
+void orc_get(const orc_state *s, double *const *cols) {
+    size_t bytes = s->N3 * sizeof(double);
+    for (int a = 0; a < 3; a++) {
+        memcpy(cols[0 + a], s->q[U0 + a], bytes);  memcpy(cols[3 + a], s->q[TU0 + a], bytes);
+        memcpy(cols[6 + a], s->p[U0 + a], bytes);  memcpy(cols[9 + a], s->p[TU0 + a], bytes);
+        memcpy(cols[12 + a], s->q[V0 + a], bytes); memcpy(cols[15 + a], s->q[TV0 + a], bytes);
+        memcpy(cols[18 + a], s->p[V0 + a], bytes); memcpy(cols[21 + a], s->p[TV0 + a], bytes);
+        if (s->P.gauge) { memcpy(cols[24 + a], s->th[a], bytes); memcpy(cols[27 + a], s->E[a], bytes); }
+    }
+}
+
+double orc_g_offset(const orc_state *s) { return s->G_offset; }
+int orc_cg_iterations(const orc_state *s) { return s->cg_iters; }
+
+void orc_accelerations(orc_state *s, double *const *acc) {
+    forces(s);
+    size_t bytes = s->N3 * sizeof(double);
+    for (int a = 0; a < 3; a++) {
+        memcpy(acc[0 + a], s->a[U0 + a], bytes);  memcpy(acc[3 + a], s->a[TU0 + a], bytes);
+        memcpy(acc[6 + a], s->a[V0 + a], bytes);  memcpy(acc[9 + a], s->a[TV0 + a], bytes);
+        if (s->P.gauge) memcpy(acc[12 + a], s->K[a], bytes);
+        else memset(acc[12 + a], 0, bytes);
+    }
+}
+
+/* do_test_gauge_xform, scp_sim.c:2461-2556 */
+double orc_gauge_xform_test(orc_state *s, double *rel_out10) {
+    if (!s->P.gauge) return -1.0;
+    const int N = s->P.N;
+    const long N3 = s->N3;
+    const double GG = s->P.g;
+    forces(s);
+    double *bf = malloc(10 * N3 * sizeof(double)), *alpha = malloc(N3 * sizeof(double));
+    if (!bf || !alpha) { free(bf); free(alpha); return -1.0; }
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        for (int a = 0; a < 3; a++) {
+            bf[a * N3 + idx] = s->a[U0 + a][idx] * s->a[U0 + a][idx] + s->a[V0 + a][idx] * s->a[V0 + a][idx];
+            bf[(3 + a) * N3 + idx] = s->a[TU0 + a][idx] * s->a[TU0 + a][idx]
+                                   + s->a[TV0 + a][idx] * s->a[TV0 + a][idx];
+            bf[(6 + a) * N3 + idx] = s->K[a][idx];
+        }
+        bf[9 * N3 + idx] = gauss_at(s, idx, &n);
+        uint64_t g = (uint64_t)idx * 6364136223846793005ULL + 1442695040888963407ULL;
+        g = g * 6364136223846793005ULL + 1442695040888963407ULL;
+        alpha[idx] = (((double)(g >> 11)) / 9007199254740992.0 - 0.5) * 20.0;
+    }
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        long np[3] = {n.ip, n.jp, n.kp};
+        double ca = cos(GG * alpha[idx]), sa = sin(GG * alpha[idx]);
+        for (int a = 0; a < 3; a++) {
+            double *pairs[4][2] = {{s->q[U0 + a], s->q[V0 + a]}, {s->p[U0 + a], s->p[V0 + a]},
+                                   {s->q[TU0 + a], s->q[TV0 + a]}, {s->p[TU0 + a], s->p[TV0 + a]}};
+            for (int w = 0; w < 4; w++) {
+                double u = pairs[w][0][idx], v = pairs[w][1][idx];
+                pairs[w][0][idx] = ca * u + sa * v;
+                pairs[w][1][idx] = ca * v - sa * u;
+            }
+        }
+        for (int d = 0; d < 3; d++) s->th[d][idx] = wrap_angle(s->th[d][idx] + GG * (alpha[np[d]] - alpha[idx]));
+    }
+    forces(s);
+    double worst = 0;
+    for (int qn = 0; qn < 10; qn++) {
+        double sc = 0, dm = 0;
+        for (long idx = 0; idx < N3; idx++) {
+            nbr_t n = nbrs(N, idx);
+            double after;
+            if (qn < 3) after = s->a[U0 + qn][idx] * s->a[U0 + qn][idx] + s->a[V0 + qn][idx] * s->a[V0 + qn][idx];
+            else if (qn < 6) after = s->a[TU0 + qn - 3][idx] * s->a[TU0 + qn - 3][idx]
+                                   + s->a[TV0 + qn - 3][idx] * s->a[TV0 + qn - 3][idx];
+            else if (qn < 9) after = s->K[qn - 6][idx];
+            else after = gauss_at(s, idx, &n);
+            double b0 = bf[qn * N3 + idx];
+            if (fabs(b0) > sc) sc = fabs(b0);
+            double d = fabs(after - b0);
+            if (d > dm) dm = d;
+        }
+        double rel = dm / fmax(sc, 1.0);
+        if (rel_out10) rel_out10[qn] = rel;
+        if (rel > worst) worst = rel;
+    }
+    free(bf);
+    free(alpha);
+    return worst;
+}
+
+int orc_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -1,0 +1,66 @@
+/* scp_oracle.h -- CPU restatement of the reference's complex / gauged lattice
+ * stepper (kardianos/scp sfa/sim/scp_sim.c), used ONLY as the checker of the
+ * parity tests, smoke() and the CPU-baseline leg of bench.py.  Nothing in the
+ * product links, loads or calls it.
+ *
+ * Column order of every state array passed in or out (the SFA snapshot
+ * registration order of sfa/sim/scp_sim.c:2862-2897):
+ *    0- 2 phi_{x,y,z}      (u_a = Re Phi_a)
+ *    3- 5 theta_{x,y,z}    (tu_a = Re Theta_a)
+ *    6- 8 phi_v{x,y,z}     (du_a/dt)
+ *    9-11 theta_v{x,y,z}   (dtu_a/dt)
+ *   12-14 phiim_{x,y,z}    (v_a = Im Phi_a)
+ *   15-17 thetaim_{x,y,z}  (tv_a = Im Theta_a)
+ *   18-20 phiim_v{x,y,z}
+ *   21-23 thetaim_v{x,y,z}
+ *   24-26 th_{x,y,z}       (link angles, gauged only)
+ *   27-29 E_{x,y,z}        (link electric field, gauged only)
+ *
+ * Diagnostic slots (orc_diag) follow the reference diag TSV column order
+ * (sfa/sim/scp_sim.c:2993-3003) without the leading time column; see
+ * SCP_DIAG_* in include/scp_gpu.h, which uses the same numbering.
+ */
+#ifndef SCP_ORACLE_H
+#define SCP_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int N;
+    double L, dx, dt;
+    double m2, mtheta2, eta, mu, kappa;
+    int gauge;          /* complex_gauge with g != 0 */
+    double g;           /* g_gauge */
+    int bc_type;        /* 0 absorbing sphere, 2 periodic */
+    double damp_width, damp_rate;
+    double qdiag_radius, qdiag_probe1, qdiag_probe2;
+} orc_params;
+
+typedef struct orc_state orc_state;
+
+/* Allocates the state, copies the 24/30 columns in, and (gauged) runs the
+ * net-charge check when bc_type==2 and the one-time Gauss projection, then the
+ * initial force evaluation -- the start-up sequence of scp_sim.c main
+ * (:2806-2836).  Returns NULL on failure; *status gets a negative code
+ * (-1 bad params, -2 net charge, -3 CG did not converge, -4 alloc). */
+orc_state *orc_create(const orc_params *p, const double *const *cols, int project, int *status);
+void orc_free(orc_state *s);
+void orc_step(orc_state *s, int nsteps);
+void orc_get(const orc_state *s, double *const *cols);
+/* 31 diagnostics in TSV order (see header comment); returns slot count */
+int orc_diag(orc_state *s, double *out);
+double orc_g_offset(const orc_state *s);
+int orc_cg_iterations(const orc_state *s);
+/* accelerations of the current positions: 24 arrays in column order
+ * 0-2 phi_acc, 3-5 theta_acc, 6-8 phiim_acc, 9-11 thetaim_acc, and E_acc 12-14 */
+void orc_accelerations(orc_state *s, double *const *acc);
+/* random lattice gauge transform KAT of scp_sim.c:2461-2556; returns the
+ * worst relative deviation over the 10 invariants (<=1e-12 passes) */
+double orc_gauge_xform_test(orc_state *s, double *rel_out10);
+int orc_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

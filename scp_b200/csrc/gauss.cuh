@@ -1,0 +1,179 @@
+// gauss.cuh -- start-up constraint handling of the gauged stepper, on device:
+// the net-charge check (net_charge_check, sfa/sim/scp_sim.c:2264-2279) and the
+// one-time Gauss projection (init_gauss_project, :2284-2400): conjugate
+// gradients on -lap(chi) = G - mean(G) with the periodic 7-point Laplacian,
+// chi kept zero-mean, then E_d += (chi(x+d) - chi(x))/dx and the frozen
+// offset G_offset = mean(G).  The reference runs this on the host even in its
+// CUDA build (scp_sim.cu:5151-5155); here every sweep is a kernel and all
+// dot products use the deterministic reductions of reduce.cuh.
+#pragma once
+#include "reduce.cuh"
+
+namespace scp {
+
+struct GaussArgs {
+    const double *X;   // positions (u v tu tv th), 15 arrays
+    double *S;         // momenta (du dv dtu dtv E), 15 arrays; E updated in place
+    int N;
+    long long N3;
+    double dx, g;
+};
+
+__device__ __forceinline__ double rho_site(const GaussArgs &a, long long idx) {
+    double r = 0.0;
+    for (int c = 0; c < 3; c++)
+        r += a.X[(FU + c) * a.N3 + idx] * a.S[(FV + c) * a.N3 + idx]
+           - a.X[(FV + c) * a.N3 + idx] * a.S[(FU + c) * a.N3 + idx]
+           + a.X[(FTU + c) * a.N3 + idx] * a.S[(FTV + c) * a.N3 + idx]
+           - a.X[(FTV + c) * a.N3 + idx] * a.S[(FTU + c) * a.N3 + idx];
+    return r;
+}
+
+__device__ __forceinline__ double gauss_site(const GaussArgs &a, long long idx) {
+    const int N = a.N;
+    const long long NN = (long long)N * N;
+    const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+    const double *E0 = a.S + (FTH + 0) * a.N3, *E1 = a.S + (FTH + 1) * a.N3, *E2 = a.S + (FTH + 2) * a.N3;
+    const long long im = (long long)wrapi(i - 1, N) * NN + (long long)j * N + k;
+    const long long jm = (long long)i * NN + (long long)wrapi(j - 1, N) * N + k;
+    const long long km = (long long)i * NN + (long long)j * N + wrapi(k - 1, N);
+    const double divE = (E0[idx] - E0[im] + E1[idx] - E1[jm] + E2[idx] - E2[km]) / a.dx;
+    return divE - a.g * rho_site(a, idx);
+}
+
+// sums of rho*dV and |rho|*dV
+__global__ void __launch_bounds__(kRedThreads) net_charge_kernel(GaussArgs a, double dV, double *part) {
+    __shared__ double scratch[2 * 32];
+    double S[2] = {0.0, 0.0}, M[1] = {0.0};
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.N3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const double r = rho_site(a, idx);
+        S[0] += r * dV;
+        S[1] += fabs(r) * dV;
+    }
+    block_fold<2, 0>(S, M, scratch, part);
+}
+
+// b = G(x); partial sum of b
+__global__ void __launch_bounds__(kRedThreads) gauss_rhs_kernel(GaussArgs a, double *b, double *part) {
+    __shared__ double scratch[32];
+    double S[1] = {0.0}, M[1] = {0.0};
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.N3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const double G = gauss_site(a, idx);
+        b[idx] = G;
+        S[0] += G;
+    }
+    block_fold<1, 0>(S, M, scratch, part);
+}
+
+// CG scalars kept on the device
+enum : int { CG_GBAR = 0, CG_GMAX0, CG_RZ, CG_PAP, CG_ALPHA, CG_BETA, CG_XBAR, CG_RMAX, CG_RZ2, CG_N };
+
+// b -= gbar; r = p = b; chi = 0; partial sum r^2, max |b|
+__global__ void __launch_bounds__(kRedThreads) cg_start_kernel(long long n3, double *b, double *r, double *p,
+                                                               double *x, const double *cg, double *part) {
+    __shared__ double scratch[2 * 32];
+    double S[1] = {0.0}, M[1] = {0.0};
+    const double gbar = cg[CG_GBAR];
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const double v = b[idx] - gbar;
+        b[idx] = v; r[idx] = v; p[idx] = v; x[idx] = 0.0;
+        M[0] = fmax(M[0], fabs(v));
+        S[0] += v * v;
+    }
+    block_fold<1, 1>(S, M, scratch, part);
+}
+
+// Ap = -lap(p); partial sum p.Ap
+__global__ void __launch_bounds__(kRedThreads) cg_apply_kernel(int N, long long n3, double idx2, const double *p,
+                                                               double *Ap, double *part) {
+    __shared__ double scratch[32];
+    double S[1] = {0.0}, M[1] = {0.0};
+    const long long NN = (long long)N * N;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        const double lap = (p[(long long)wrapi(i + 1, N) * NN + (long long)j * N + k]
+                            + p[(long long)wrapi(i - 1, N) * NN + (long long)j * N + k]
+                            + p[(long long)i * NN + (long long)wrapi(j + 1, N) * N + k]
+                            + p[(long long)i * NN + (long long)wrapi(j - 1, N) * N + k]
+                            + p[(long long)i * NN + (long long)j * N + wrapi(k + 1, N)]
+                            + p[(long long)i * NN + (long long)j * N + wrapi(k - 1, N)] - 6.0 * p[idx]) * idx2;
+        Ap[idx] = -lap;
+        S[0] += p[idx] * Ap[idx];
+    }
+    block_fold<1, 0>(S, M, scratch, part);
+}
+
+// x += alpha p; r -= alpha Ap; partial sums r.r, sum x, max |r|
+__global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long long n3, double *x, double *r, const double *p,
+                                                                const double *Ap, const double *cg, double *part) {
+    __shared__ double scratch[3 * 32];
+    double S[2] = {0.0, 0.0}, M[1] = {0.0};
+    const double alpha = cg[CG_ALPHA];
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const double xv = x[idx] + alpha * p[idx];
+        const double rv = r[idx] - alpha * Ap[idx];
+        x[idx] = xv; r[idx] = rv;
+        S[0] += rv * rv;
+        S[1] += xv;
+        M[0] = fmax(M[0], fabs(rv));
+    }
+    block_fold<2, 1>(S, M, scratch, part);
+}
+
+// x -= xbar; p = r + beta p
+__global__ void cg_dir_kernel(long long n3, double *x, const double *r, double *p, const double *cg) {
+    const double xbar = cg[CG_XBAR], beta = cg[CG_BETA];
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        x[idx] -= xbar;
+        p[idx] = r[idx] + beta * p[idx];
+    }
+}
+
+// single-thread scalar bookkeeping between CG sweeps
+__global__ void cg_scalar_kernel(int stage, double n3d, const double *fold, double *cg) {
+    if (threadIdx.x | blockIdx.x) return;
+    switch (stage) {
+        case 0: cg[CG_GBAR] = fold[0] / n3d; break;                          // gbar
+        case 1: cg[CG_RZ] = fold[0]; cg[CG_GMAX0] = fold[1]; cg[CG_RMAX] = fold[1]; break;
+        case 2: cg[CG_PAP] = fold[0]; cg[CG_ALPHA] = cg[CG_RZ] / fold[0]; break;
+        case 3:
+            cg[CG_RZ2] = fold[0];
+            cg[CG_XBAR] = fold[1] / n3d;
+            cg[CG_BETA] = fold[0] / cg[CG_RZ];
+            cg[CG_RZ] = fold[0];
+            cg[CG_RMAX] = fold[2];
+            break;
+    }
+}
+
+// E_d += (chi(x+d) - chi(x))/dx
+__global__ void gauss_correct_kernel(GaussArgs a, const double *chi) {
+    const int N = a.N;
+    const long long NN = (long long)N * N;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.N3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        const double c0 = chi[idx];
+        a.S[(FTH + 0) * a.N3 + idx] += (chi[(long long)wrapi(i + 1, N) * NN + (long long)j * N + k] - c0) / a.dx;
+        a.S[(FTH + 1) * a.N3 + idx] += (chi[(long long)i * NN + (long long)wrapi(j + 1, N) * N + k] - c0) / a.dx;
+        a.S[(FTH + 2) * a.N3 + idx] += (chi[(long long)i * NN + (long long)j * N + wrapi(k + 1, N)] - c0) / a.dx;
+    }
+}
+
+// partial sums of G (for G_offset)
+__global__ void __launch_bounds__(kRedThreads) gauss_sum_kernel(GaussArgs a, double *part) {
+    __shared__ double scratch[32];
+    double S[1] = {0.0}, M[1] = {0.0};
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.N3;
+         idx += (long long)gridDim.x * blockDim.x)
+        S[0] += gauss_site(a, idx);
+    block_fold<1, 0>(S, M, scratch, part);
+}
+
+}  // namespace scp

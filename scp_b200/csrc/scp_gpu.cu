@@ -1,0 +1,624 @@
+// scp_gpu.cu -- host side of the C ABI declared in include/scp_gpu.h.
+//
+// One handle = one simulation on one device with its own stream.  Device
+// state (FP64 mode), each buffer NF = 12 (complex) or 15 (gauged) arrays of
+// N^3 doubles, field-major, site index (i*N + j)*N + k:
+//   X[0], X[1]  positions u v tu tv [th], double-buffered (stencil input and
+//               output of the fused step)
+//   W           half-step momenta w = v + hdt*a [and E + hdt*K], in place
+//   S           synchronous momenta v [and E] of the last completed step
+// After a scp_gpu_step call, X[cur^1] and S hold the state at the current
+// time (what diagnostics and snapshots read) and X[cur], W the drifted
+// positions and half-kicked momenta the next launch starts from.
+#include "../../include/scp_gpu.h"
+#include "common.cuh"
+#include "diag.cuh"
+#include "fp32c.cuh"
+#include "gauss.cuh"
+#include "reduce.cuh"
+#include "snapshot.cuh"
+#include "step_f64.cuh"
+
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+
+using namespace scp;
+
+static thread_local char g_cuda_err[256] = "";
+
+#define CK(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            snprintf(g_cuda_err, sizeof g_cuda_err, "%s at %s:%d", cudaGetErrorString(e_), \
+                     __FILE__, __LINE__);                                              \
+            return e_ == cudaErrorMemoryAllocation ? SCP_ENOMEM : SCP_ECUDA;           \
+        }                                                                              \
+    } while (0)
+
+namespace {
+
+using StepFn = void (*)(StepIO64, StepConsts, TileGrid);
+
+struct TileShape { int tx, ty; };
+// tile_variant 1..: fixed shapes; 0 picks the default for the mode
+static const TileShape kShapes[] = {{32, 4}, {32, 4}, {32, 8}, {16, 8}, {64, 2}};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+template <int TX, int TY>
+StepFn pick_f64(bool g, bool f, bool s, bool d) {
+#define SCP_SEL(G, F, S, D) if (g == G && f == F && s == S && d == D) return step_f64_kernel<TX, TY, G, F, S, D>;
+    SCP_SEL(false, false, false, false) SCP_SEL(false, false, false, true)
+    SCP_SEL(false, false, true, false)  SCP_SEL(false, false, true, true)
+    SCP_SEL(false, true, false, false)  SCP_SEL(false, true, false, true)
+    SCP_SEL(false, true, true, false)   SCP_SEL(false, true, true, true)
+    SCP_SEL(true, false, false, false)  SCP_SEL(true, false, false, true)
+    SCP_SEL(true, false, true, false)   SCP_SEL(true, false, true, true)
+    SCP_SEL(true, true, false, false)   SCP_SEL(true, true, false, true)
+    SCP_SEL(true, true, true, false)    SCP_SEL(true, true, true, true)
+#undef SCP_SEL
+    return nullptr;
+}
+
+template <int TX, int TY>
+size_t smem_f64(bool g) {
+    return g ? F64Layout<TX, TY, true>::smem_bytes : F64Layout<TX, TY, false>::smem_bytes;
+}
+
+StepFn step_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
+    switch (shape) {
+        case 2: *smem = smem_f64<32, 8>(g); return pick_f64<32, 8>(g, f, s, d);
+        case 3: *smem = smem_f64<16, 8>(g); return pick_f64<16, 8>(g, f, s, d);
+        case 4: *smem = smem_f64<64, 2>(g); return pick_f64<64, 2>(g, f, s, d);
+        default: *smem = smem_f64<32, 4>(g); return pick_f64<32, 4>(g, f, s, d);
+    }
+}
+
+}  // namespace
+
+struct scp_gpu {
+    scp_gpu_params p;
+    StepConsts c;
+    int N;
+    long long N3;
+    int gauged, nf, prec;
+    int device;
+    cudaStream_t stream = nullptr;
+    // FP64 state
+    double *slab = nullptr;
+    double *X[2] = {nullptr, nullptr};
+    double *W = nullptr, *S = nullptr;
+    int cur = 0;
+    // FP32-compensated state
+    Fp32cState f32;
+    // scratch
+    double *part = nullptr, *fold = nullptr, *cg = nullptr, *point = nullptr;
+    int *flag = nullptr;
+    double *h_small = nullptr;   // pinned
+    void *stage = nullptr;       // snapshot down-conversion staging (N3 doubles)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // launch geometry
+    int shape;
+    TileGrid tg;
+    int grid;
+    int64_t steps = 0;
+    double G_offset = 0.0;
+    int cg_iters = 0;
+    int64_t dev_bytes = 0;
+};
+
+static int validate(const scp_gpu_params *p) {
+    if (!p) return SCP_EINVAL;
+    if (p->N < 4 || p->N > 2048) return SCP_EINVAL;
+    if (!(p->dx > 0) || !(p->dt > 0)) return SCP_EINVAL;
+    if (p->complex_gauge && !(p->g_gauge > 0)) return SCP_EINVAL;
+    if (p->bc_type != 0 && p->bc_type != 2) return SCP_EUNSUPPORTED;
+    if (p->precision_mode != SCP_PREC_FP64 && p->precision_mode != SCP_PREC_FP32C) return SCP_EINVAL;
+    if (p->tile_variant < 0 || p->tile_variant >= kNumShapes) return SCP_EINVAL;
+    return SCP_OK;
+}
+
+static void fill_consts(scp_gpu *h) {
+    const scp_gpu_params &p = h->p;
+    StepConsts &c = h->c;
+    c.N = p.N;
+    c.N3 = (long long)p.N * p.N * p.N;
+    c.idx2 = 1.0 / (p.dx * p.dx);
+    c.idx1 = 1.0 / (2.0 * p.dx);
+    c.inva = 1.0 / p.dx;
+    c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
+    c.dt = p.dt;
+    c.hdt = 0.5 * p.dt;
+    c.g = p.complex_gauge ? p.g_gauge : 0.0;
+    c.gad = -c.g * p.dx * p.dt;
+    c.stp = p.complex_gauge ? 1.0 / (p.g_gauge * p.dx * p.dx * p.dx) : 0.0;
+    c.L = p.L; c.dx = p.dx;
+    c.damp_width = p.damp_width;
+    c.damp_rate = p.damp_rate;
+}
+
+static bool damping_on(const scp_gpu *h) {
+    return h->p.bc_type == 0 && h->p.damp_width > 0 && h->p.damp_rate > 0;
+}
+
+// Choose the i-segment length that minimises (waves x planes per item),
+// planes per item counting the two halo planes a segment re-reads.
+static void plan_tiles(scp_gpu *h, int tx, int ty, int slots) {
+    const int N = h->N;
+    TileGrid tg;
+    tg.ntx = (N + tx - 1) / tx;
+    tg.nty = (N + ty - 1) / ty;
+    const int ntiles = tg.ntx * tg.nty;
+    double best = 1e300;
+    int best_seg = N;
+    const int cands[] = {4, 6, 8, 10, 12, 16, 20, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 1024, 2048};
+    for (int s : cands) {
+        if (s > N) break;
+        const long long items = (long long)ntiles * ((N + s - 1) / s);
+        const long long waves = (items + slots - 1) / slots;
+        const double cost = (double)waves * (s + 2);
+        if (cost < best - 1e-9 || (cost < best + 1e-9 && s > best_seg)) { best = cost; best_seg = s; }
+    }
+    {   // whole column as one segment
+        const long long waves = (ntiles + slots - 1) / slots;
+        const double cost = (double)waves * (N + 2);
+        if (cost < best - 1e-9) { best = cost; best_seg = N; }
+    }
+    tg.seg = best_seg;
+    tg.nseg = (N + best_seg - 1) / best_seg;
+    tg.nitems = ntiles * tg.nseg;
+    h->tg = tg;
+    h->grid = tg.nitems < slots ? tg.nitems : slots;
+}
+
+static int setup_launch(scp_gpu *h) {
+    int shape = h->p.tile_variant;
+    if (shape == 0) shape = h->gauged ? 1 : 1;
+    h->shape = shape;
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    const TileShape ts = kShapes[shape];
+    int slots = nsm;
+    if (h->prec == SCP_PREC_FP64) {
+        size_t smem = 0;
+        // raise the dynamic shared-memory cap of every variant of this shape
+        for (int v = 0; v < 16; v++) {
+            StepFn fn = step_fn(shape, h->gauged, v & 1, (v >> 1) & 1, (v >> 2) & 1, &smem);
+            if ((v >> 3) & 1) continue;
+            CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        }
+        StepFn fn = step_fn(shape, h->gauged, false, false, false, &smem);
+        int occ = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)fn, ts.tx * ts.ty, smem));
+        if (occ < 1) return SCP_EUNSUPPORTED;
+        slots = nsm * occ;
+    } else {
+        int occ = 0;
+        CK(fp32c_occupancy(h->gauged, ts.tx, ts.ty, &occ));
+        if (occ < 1) return SCP_EUNSUPPORTED;
+        slots = nsm * occ;
+    }
+    plan_tiles(h, ts.tx, ts.ty, slots);
+    return SCP_OK;
+}
+
+static int launch_f64(scp_gpu *h, bool first, bool sync) {
+    size_t smem = 0;
+    StepFn fn = step_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
+    const TileShape ts = kShapes[h->shape];
+    StepIO64 io;
+    io.xin = h->X[h->cur];
+    io.xout = h->X[h->cur ^ 1];
+    io.win = first ? h->S : h->W;
+    io.wout = h->W;
+    io.sout = h->S;
+    io.flag = h->flag;
+    fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+    CK(cudaGetLastError());
+    h->cur ^= 1;
+    return SCP_OK;
+}
+
+// ---------------------------------------------------------------- Gauss law
+
+static double fold_get(scp_gpu *h, int q) {   // after a synchronising copy
+    return h->h_small[q];
+}
+
+static int fold_to_host(scp_gpu *h, int nq) {
+    CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * nq, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SCP_OK;
+}
+
+static GaussArgs gauss_args(scp_gpu *h, const double *X, double *S) {
+    GaussArgs a;
+    a.X = X; a.S = S; a.N = h->N; a.N3 = h->N3; a.dx = h->p.dx; a.g = h->p.g_gauge;
+    return a;
+}
+
+// net_charge_check + init_gauss_project on the state in (X, S)
+static int gauss_startup(scp_gpu *h, const double *X, double *S) {
+    const long long n3 = h->N3;
+    const int nb = red_blocks(n3);
+    GaussArgs a = gauss_args(h, X, S);
+    const double dV = h->p.dx * h->p.dx * h->p.dx;
+    int rc;
+    if (h->p.bc_type == 2) {
+        net_charge_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, dV, h->part);
+        fold_partials_kernel<2, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+        CK(cudaGetLastError());
+        if ((rc = fold_to_host(h, 2))) return rc;
+        const double qn = fold_get(h, 0), qa = fold_get(h, 1);
+        if (fabs(qn) > 1e-6 * fmax(qa, 1.0)) return SCP_ENETCHARGE;
+    }
+    if (!h->p.gauss_project) return SCP_OK;
+    double *tmp = nullptr;
+    CK(cudaMallocAsync(&tmp, sizeof(double) * 5 * n3, h->stream));
+    double *b = tmp, *x = tmp + n3, *r = tmp + 2 * n3, *p = tmp + 3 * n3, *Ap = tmp + 4 * n3;
+    const double n3d = (double)n3, idx2 = 1.0 / (h->p.dx * h->p.dx);
+    gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, b, h->part);
+    fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(0, n3d, h->fold, h->cg);
+    cg_start_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, b, r, p, x, h->cg, h->part);
+    fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(1, n3d, h->fold, h->cg);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_small, h->cg, sizeof(double) * CG_N, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const double tol = 1e-13 * fmax(1.0, h->h_small[CG_GMAX0]);
+    double rmax = h->h_small[CG_RMAX];
+    int it = 0;
+    while (rmax > tol && it < 20000) {
+        cg_apply_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->N, n3, idx2, p, Ap, h->part);
+        fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+        cg_scalar_kernel<<<1, 1, 0, h->stream>>>(2, n3d, h->fold, h->cg);
+        cg_update_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, p, Ap, h->cg, h->part);
+        fold_partials_kernel<2, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+        cg_scalar_kernel<<<1, 1, 0, h->stream>>>(3, n3d, h->fold, h->cg);
+        cg_dir_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, p, h->cg);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h->h_small, h->cg + CG_RMAX, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        rmax = h->h_small[0];
+        it++;
+    }
+    h->cg_iters = it;
+    if (rmax > tol) {
+        cudaFreeAsync(tmp, h->stream);
+        return SCP_EGAUSS;
+    }
+    gauss_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, x);
+    gauss_sum_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, h->part);
+    fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    CK(cudaGetLastError());
+    CK(cudaFreeAsync(tmp, h->stream));
+    if ((rc = fold_to_host(h, 1))) return rc;
+    h->G_offset = fold_get(h, 0) / n3d;
+    return SCP_OK;
+}
+
+// ---------------------------------------------------------------- lifecycle
+
+static int alloc_common(scp_gpu *h) {
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&h->part, sizeof(double) * kRedMaxBlocks * 32));
+    CK(cudaMalloc(&h->fold, sizeof(double) * 64));
+    CK(cudaMalloc(&h->cg, sizeof(double) * 16));
+    CK(cudaMalloc(&h->point, sizeof(double) * 8));
+    CK(cudaMalloc(&h->flag, sizeof(int)));
+    CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    CK(cudaMallocHost(&h->h_small, sizeof(double) * 64));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    h->dev_bytes += sizeof(double) * (kRedMaxBlocks * 32 + 64 + 16 + 8);
+    return SCP_OK;
+}
+
+static int init_common(const scp_gpu_params *p, const double *const *cols, bool on_device, scp_gpu **out) {
+    if (!out) return SCP_EINVAL;
+    *out = nullptr;
+    int rc = validate(p);
+    if (rc) return rc;
+    if (!cols) return SCP_EINVAL;
+    const int ncols = p->complex_gauge ? 30 : 24;
+    for (int c = 0; c < ncols; c++)
+        if (!cols[c]) return SCP_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p->device || p->device < 0) return SCP_ENODEV;
+    CK(cudaSetDevice(p->device));
+    scp_gpu *h = new scp_gpu();
+    h->p = *p;
+    h->device = p->device;
+    h->N = p->N;
+    h->N3 = (long long)p->N * p->N * p->N;
+    h->gauged = p->complex_gauge ? 1 : 0;
+    h->nf = h->gauged ? 15 : 12;
+    h->prec = p->precision_mode;
+    fill_consts(h);
+    auto fail = [&](int code) { scp_gpu_free(h); return code; };
+    if ((rc = alloc_common(h))) return fail(rc);
+    const long long n3 = h->N3;
+    const size_t blk = sizeof(double) * (size_t)h->nf * n3;
+    // FP64 staging of the initial state: X[0] = x_0, S = v_0 (also the
+    // working layout of FP64 mode)
+    {
+        cudaError_t e = cudaMalloc(&h->slab, 4 * blk);
+        if (e != cudaSuccess) { cudaGetLastError(); return fail(SCP_ENOMEM); }
+        h->dev_bytes += 4 * blk;
+    }
+    h->X[0] = h->slab;
+    h->X[1] = h->slab + (size_t)h->nf * n3;
+    h->W = h->slab + 2 * (size_t)h->nf * n3;
+    h->S = h->slab + 3 * (size_t)h->nf * n3;
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int c = 0; c < ncols; c++) {
+        int field, mom;
+        sfa_col_source(c, &field, &mom);
+        double *dst = (mom ? h->S : h->X[0]) + (size_t)field * n3;
+        cudaError_t e = cudaMemcpyAsync(dst, cols[c], sizeof(double) * n3, kind, h->stream);
+        if (e != cudaSuccess) {
+            snprintf(g_cuda_err, sizeof g_cuda_err, "%s (column %d upload)", cudaGetErrorString(e), c);
+            return fail(SCP_ECUDA);
+        }
+    }
+    if (h->gauged && (rc = gauss_startup(h, h->X[0], h->S))) return fail(rc);
+    if ((rc = setup_launch(h))) return fail(rc);
+    CK(cudaMalloc(&h->stage, sizeof(double) * n3));
+    h->dev_bytes += sizeof(double) * n3;
+    h->cur = 0;
+    if (h->prec == SCP_PREC_FP64) {
+        if ((rc = launch_f64(h, true, false))) return fail(rc);
+    } else {
+        if ((rc = fp32c_init(&h->f32, h->c, h->gauged, h->X[0], h->S, kShapes[h->shape].tx, kShapes[h->shape].ty,
+                             h->tg, h->grid, damping_on(h), h->flag, h->stream))) {
+            snprintf(g_cuda_err, sizeof g_cuda_err, "%s", fp32c_last_error());
+            return fail(rc);
+        }
+        h->dev_bytes += h->f32.bytes;
+        // the FP64 slab only staged the start; keep X[0]/S as the FP64 view
+        // buffers that diagnostics expand into (the other two are released)
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    *out = h;
+    return SCP_OK;
+}
+
+extern "C" {
+
+int scp_gpu_init(const scp_gpu_params *p, const double *const *host_cols, scp_gpu **out) {
+    return init_common(p, host_cols, false, out);
+}
+
+int scp_gpu_init_device(const scp_gpu_params *p, const double *const *dev_cols, scp_gpu **out) {
+    return init_common(p, dev_cols, true, out);
+}
+
+int scp_gpu_step(scp_gpu *h, int nsteps) {
+    if (!h || nsteps < 0) return SCP_EINVAL;
+    if (nsteps == 0) return SCP_OK;
+    CK(cudaSetDevice(h->device));
+    int rc;
+    for (int n = 0; n < nsteps; n++) {
+        const bool last = (n == nsteps - 1);
+        if (h->prec == SCP_PREC_FP64) rc = launch_f64(h, false, last);
+        else rc = fp32c_step(&h->f32, last, h->stream);
+        if (rc) return rc;
+    }
+    h->steps += nsteps;
+    return SCP_OK;
+}
+
+int scp_gpu_sync(scp_gpu *h) {
+    if (!h) return SCP_EINVAL;
+    CK(cudaSetDevice(h->device));
+    CK(cudaMemcpyAsync(h->h_small, h->flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    int f = 0;
+    memcpy(&f, h->h_small, sizeof(int));
+    return f ? SCP_ENONFINITE : SCP_OK;
+}
+
+// FP64 view of the current state (FP32C expands into the staging slab first)
+static int current_view(scp_gpu *h, ViewF64 *v) {
+    v->N3 = h->N3;
+    if (h->prec == SCP_PREC_FP64) {
+        v->X = h->X[h->cur ^ 1];
+        v->S = h->S;
+        return SCP_OK;
+    }
+    int rc = fp32c_expand(&h->f32, h->X[0], h->S, h->stream);
+    if (rc) return rc;
+    v->X = h->X[0];
+    v->S = h->S;
+    return SCP_OK;
+}
+
+int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
+    if (!h || !out) return SCP_EINVAL;
+    CK(cudaSetDevice(h->device));
+    ViewF64 V;
+    int rc = current_view(h, &V);
+    if (rc) return rc;
+    const scp_gpu_params &p = h->p;
+    DiagConsts c;
+    c.N = h->N; c.N3 = h->N3; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx; c.idx1 = 1.0 / (2.0 * p.dx);
+    c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
+    c.gauged = h->gauged;
+    c.g = h->gauged ? p.g_gauge : 0.0;
+    c.bpre = h->gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
+    c.R2 = p.qdiag_radius * p.qdiag_radius;
+    c.Rcube = p.qdiag_radius;
+    const double Rint = (p.bc_type == 0) ? (p.L - p.damp_width - p.dx) : 1e300;
+    c.Rint2 = Rint * Rint;
+    c.G_offset = h->G_offset;
+    const int nb = red_blocks(h->N3);
+    diag_pass1_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->part);
+    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    diag_pass2_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->fold, h->part);
+    fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold + 40);
+    diag_point_kernel<ViewF64><<<1, 32, 0, h->stream>>>(V, c, h->fold + 40, p.qdiag_probe1, p.qdiag_probe2,
+                                                        h->point);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * 42, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_small + 48, h->point, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const double *f1 = h->h_small, *f2 = h->h_small + 40, *pt = h->h_small + 48;
+    const double dV = c.dV;
+    double *o = out->v;
+    for (int q = 0; q < SCP_DIAG_NSLOTS; q++) o[q] = 0.0;
+    o[SCP_DIAG_E_PHI_KIN] = f1[DS_EPK];
+    o[SCP_DIAG_E_THETA_KIN] = f1[DS_ETK];
+    o[SCP_DIAG_E_GRAD] = f1[DS_EG];
+    o[SCP_DIAG_E_MASS] = f1[DS_EM];
+    o[SCP_DIAG_E_POT] = f1[DS_EP];
+    o[SCP_DIAG_E_TGRAD] = f1[DS_ETG];
+    o[SCP_DIAG_E_TMASS] = f1[DS_ETM];
+    o[SCP_DIAG_E_COUPLING] = f1[DS_EC];
+    o[SCP_DIAG_E_TOTAL] = f1[DS_EPK] + f1[DS_ETK] + f1[DS_EG] + f1[DS_EM] + f1[DS_EP] + f1[DS_ETG] +
+                          f1[DS_ETM] + f1[DS_EC] + (h->gauged ? f1[DS_EEM] : 0.0);
+    o[SCP_DIAG_PHI_MAX] = f1[DS_NSUM + DM_PM];
+    o[SCP_DIAG_P_MAX] = f1[DS_NSUM + DM_PMAX];
+    o[SCP_DIAG_P_INT] = f1[DS_PINT];
+    o[SCP_DIAG_THETA_RMS] = sqrt(f1[DS_TRS] / (6.0 * (double)h->N3));
+    o[SCP_DIAG_Q_PHI] = f1[DS_QP] * dV;
+    o[SCP_DIAG_Q_THETA] = f1[DS_QT] * dV;
+    o[SCP_DIAG_Q_TOTAL] = f1[DS_QP] * dV + f1[DS_QT] * dV;
+    o[SCP_DIAG_S_MAX] = f1[DS_NSUM + DM_SMAX];
+    const double M0 = f1[DS_M0] * dV;
+    o[SCP_DIAG_R_CORE] = (M0 < 1e-30) ? 0.0 : sqrt(f2[0] * dV / M0);
+    o[SCP_DIAG_OMEGA_CORE] = pt[0];
+    o[SCP_DIAG_Q_CORE] = f1[DS_QC] * dV;
+    o[SCP_DIAG_THP1U] = pt[1]; o[SCP_DIAG_THP1V] = pt[2];
+    o[SCP_DIAG_THP2U] = pt[3]; o[SCP_DIAG_THP2V] = pt[4];
+    if (h->gauged) {
+        o[SCP_DIAG_GAUSS_MAX] = f1[DS_NSUM + DM_GMAX];
+        o[SCP_DIAG_GAUSS_L2] = f1[DS_NOM] > 0 ? sqrt(f1[DS_GL2] / f1[DS_NOM]) : 0.0;
+        o[SCP_DIAG_E_EM] = f1[DS_EEM];
+        o[SCP_DIAG_Q_FLUX] = (f1[DS_FSUM] - h->G_offset * f1[DS_NC] * dV) / p.g_gauge;
+    }
+    o[SCP_DIAG_Q_P0] = f1[DS_QP0] * dV;
+    o[SCP_DIAG_Q_P1] = f1[DS_QP1] * dV;
+    o[SCP_DIAG_Q_P2] = f1[DS_QP2] * dV;
+    if (!(M0 < 1e-30)) {
+        o[SCP_DIAG_CENTROID_X] = f1[DS_CX] * dV / M0;
+        o[SCP_DIAG_CENTROID_Y] = f1[DS_CY] * dV / M0;
+        o[SCP_DIAG_CENTROID_Z] = f1[DS_CZ] * dV / M0;
+    }
+    if (!isfinite(o[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
+    return SCP_OK;
+}
+
+int scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols) {
+    if (!h || !host_cols) return SCP_EINVAL;
+    if (dtype != SCP_DTYPE_F16 && dtype != SCP_DTYPE_F32 && dtype != SCP_DTYPE_F64) return SCP_EINVAL;
+    CK(cudaSetDevice(h->device));
+    ViewF64 V;
+    int rc = current_view(h, &V);
+    if (rc) return rc;
+    const int ncols = h->gauged ? 30 : 24;
+    const long long n3 = h->N3;
+    const int nb = red_blocks(n3);
+    for (int c = 0; c < ncols; c++) {
+        if (!host_cols[c]) return SCP_EINVAL;
+        int field, mom;
+        sfa_col_source(c, &field, &mom);
+        const double *src = (mom ? V.S : V.X) + (size_t)field * n3;
+        if (dtype == SCP_DTYPE_F64) {
+            CK(cudaMemcpyAsync(host_cols[c], src, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
+        } else if (dtype == SCP_DTYPE_F32) {
+            cast_f32_kernel<<<nb, kRedThreads, 0, h->stream>>>(src, (float *)h->stage, n3);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(host_cols[c], h->stage, sizeof(float) * n3, cudaMemcpyDeviceToHost, h->stream));
+        } else {
+            cast_f16_kernel<<<nb, kRedThreads, 0, h->stream>>>(src, (uint16_t *)h->stage, n3);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(host_cols[c], h->stage, sizeof(uint16_t) * n3, cudaMemcpyDeviceToHost, h->stream));
+        }
+        CK(cudaStreamSynchronize(h->stream));   // staging buffer reused per column
+    }
+    return SCP_OK;
+}
+
+int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
+    if (!h || !info) return SCP_EINVAL;
+    memset(info, 0, sizeof *info);
+    info->steps_done = h->steps;
+    info->time = (double)h->steps * h->p.dt;
+    info->G_offset = h->G_offset;
+    info->cg_iterations = h->cg_iters;
+    info->precision_mode = h->prec;
+    info->device_bytes = h->dev_bytes;
+    if (h->prec == SCP_PREC_FP64) {
+        info->state_bytes_per_site = 2.0 * 8.0 * h->nf;   // x + w words
+        info->step_bytes_per_site = 2.0 * info->state_bytes_per_site;
+    } else {
+        info->state_bytes_per_site = h->f32.state_bytes_per_site;
+        info->step_bytes_per_site = 2.0 * h->f32.state_bytes_per_site;
+    }
+    info->tile_x = kShapes[h->shape].tx;
+    info->tile_y = kShapes[h->shape].ty;
+    info->seg_len = h->tg.seg;
+    return SCP_OK;
+}
+
+int scp_gpu_time_steps(scp_gpu *h, int nsteps, double *ms_out) {
+    if (!h || !ms_out || nsteps < 1) return SCP_EINVAL;
+    CK(cudaSetDevice(h->device));
+    CK(cudaEventRecord(h->ev0, h->stream));
+    int rc = scp_gpu_step(h, nsteps);
+    if (rc) return rc;
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    *ms_out = ms;
+    return SCP_OK;
+}
+
+void *scp_gpu_stream(scp_gpu *h) { return h ? (void *)h->stream : nullptr; }
+
+void scp_gpu_free(scp_gpu *h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    fp32c_free(&h->f32);
+    cudaFree(h->slab);
+    cudaFree(h->part);
+    cudaFree(h->fold);
+    cudaFree(h->cg);
+    cudaFree(h->point);
+    cudaFree(h->flag);
+    cudaFree(h->stage);
+    if (h->h_small) cudaFreeHost(h->h_small);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+const char *scp_gpu_errstr(int code) {
+    switch (code) {
+        case SCP_OK: return "ok";
+        case SCP_EINVAL: return "invalid argument";
+        case SCP_ENOMEM: return "device out of memory";
+        case SCP_ECUDA: return "CUDA runtime error";
+        case SCP_ENETCHARGE: return "gauged periodic seed is not net-neutral (use +/- pairs or bc_type=0)";
+        case SCP_EGAUSS: return "Gauss projection did not converge";
+        case SCP_ENONFINITE: return "non-finite field value";
+        case SCP_EUNSUPPORTED: return "configuration not supported";
+        case SCP_ENODEV: return "no CUDA device";
+        case SCP_EBUSY: return "busy";
+        case SCP_ETIMEOUT: return "bounded wait expired";
+        default: return "unknown error";
+    }
+}
+
+const char *scp_gpu_last_cuda_error(void) { return g_cuda_err; }
+
+int scp_gpu_abi_version(void) { return SCP_GPU_ABI_VERSION; }
+
+}  // extern "C"

@@ -1,0 +1,162 @@
+"""Run parameters of the lattice stepper, mirroring the subset of the
+reference ``Config`` (sfa/sim/scp_config.h:22-215) that the complex
+(``complex_phi=1``) and gauged (``complex_gauge=1``) stepper reads.
+
+Keys and defaults follow the reference: masses are given as ``m``/``m_theta``
+and stored squared (scp_config.h:222-223), ``dx = 2L/(N-1)`` and
+``dt = dt_factor*dx`` (sfa/sim/scp_sim.c:204-205).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+
+PREC_FP64 = 0
+PREC_FP32C = 1
+
+
+class CParams(ctypes.Structure):
+    """ctypes mirror of ``scp_gpu_params`` (include/scp_gpu.h)."""
+
+    _fields_ = [
+        ("N", ctypes.c_int32),
+        ("L", ctypes.c_double),
+        ("dx", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("m2", ctypes.c_double),
+        ("mtheta2", ctypes.c_double),
+        ("eta", ctypes.c_double),
+        ("mu", ctypes.c_double),
+        ("kappa", ctypes.c_double),
+        ("complex_gauge", ctypes.c_int32),
+        ("g_gauge", ctypes.c_double),
+        ("bc_type", ctypes.c_int32),
+        ("damp_width", ctypes.c_double),
+        ("damp_rate", ctypes.c_double),
+        ("precision_mode", ctypes.c_int32),
+        ("qdiag_radius", ctypes.c_double),
+        ("qdiag_probe1", ctypes.c_double),
+        ("qdiag_probe2", ctypes.c_double),
+        ("gauss_project", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("tile_variant", ctypes.c_int32),
+    ]
+
+
+@dataclasses.dataclass
+class Params:
+    """Grid, physics and mode settings of one simulation.
+
+    Defaults are the reference defaults (scp_config.h:165-215) except the
+    grid, which defaults to the 64^3, dx=0.5, dt=0.1 periodic case.
+    """
+
+    N: int = 64
+    L: float = 15.75
+    dt_factor: float = 0.2
+    m: float = 1.5
+    m_theta: float = 0.0
+    eta: float = 0.5
+    mu: float = -41.345
+    kappa: float = 50.0
+    complex_gauge: int = 0
+    g_gauge: float = 0.05
+    bc_type: int = 2
+    damp_width: float = 3.0
+    damp_rate: float = 0.01
+    precision: int = PREC_FP64
+    qdiag_radius: float = 8.0
+    qdiag_probe1: float = 8.0
+    qdiag_probe2: float = 16.0
+    gauss_project: int = 1
+    device: int = 0
+    tile_variant: int = 0
+
+    @property
+    def dx(self) -> float:
+        return 2.0 * self.L / (self.N - 1)
+
+    @property
+    def dt(self) -> float:
+        return self.dt_factor * self.dx
+
+    @property
+    def m2(self) -> float:
+        return self.m * self.m
+
+    @property
+    def mtheta2(self) -> float:
+        return self.m_theta * self.m_theta
+
+    @property
+    def gauged(self) -> bool:
+        return bool(self.complex_gauge) and self.g_gauge != 0.0
+
+    @property
+    def ncols(self) -> int:
+        return 30 if self.complex_gauge else 24
+
+    def steps_for(self, T: float) -> int:
+        """Step count of a run of length T, as the reference rounds it."""
+        return int(math.floor(T / self.dt + 0.5))
+
+    def to_c(self) -> CParams:
+        c = CParams()
+        c.N = self.N
+        c.L = self.L
+        c.dx = self.dx
+        c.dt = self.dt
+        c.m2 = self.m2
+        c.mtheta2 = self.mtheta2
+        c.eta = self.eta
+        c.mu = self.mu
+        c.kappa = self.kappa
+        c.complex_gauge = 1 if self.complex_gauge else 0
+        c.g_gauge = self.g_gauge
+        c.bc_type = self.bc_type
+        c.damp_width = self.damp_width
+        c.damp_rate = self.damp_rate
+        c.precision_mode = self.precision
+        c.qdiag_radius = self.qdiag_radius
+        c.qdiag_probe1 = self.qdiag_probe1
+        c.qdiag_probe2 = self.qdiag_probe2
+        c.gauss_project = self.gauss_project
+        c.device = self.device
+        c.tile_variant = self.tile_variant
+        return c
+
+    def to_cfg(self, **extra) -> str:
+        """The same run as reference ``key = value`` config text."""
+        kv = {
+            "N": self.N, "L": repr(self.L), "dt_factor": repr(self.dt_factor),
+            "m": repr(self.m), "m_theta": repr(self.m_theta), "eta": repr(self.eta),
+            "mu": repr(self.mu), "kappa": repr(self.kappa), "complex_phi": 1,
+            "complex_gauge": int(self.complex_gauge), "g_gauge": repr(self.g_gauge),
+            "bc_type": self.bc_type, "damp_width": repr(self.damp_width),
+            "damp_rate": repr(self.damp_rate), "qdiag_radius": repr(self.qdiag_radius),
+            "qdiag_probe1": repr(self.qdiag_probe1), "qdiag_probe2": repr(self.qdiag_probe2),
+        }
+        kv.update(extra)
+        return "".join(f"{k} = {v}\n" for k, v in kv.items())
+
+
+# Column names of the SFA snapshot schema in registration order
+# (sfa/sim/scp_sim.c:2862-2897).
+COLUMN_NAMES = (
+    "phi_x", "phi_y", "phi_z", "theta_x", "theta_y", "theta_z",
+    "phi_vx", "phi_vy", "phi_vz", "theta_vx", "theta_vy", "theta_vz",
+    "phiim_x", "phiim_y", "phiim_z", "thetaim_x", "thetaim_y", "thetaim_z",
+    "phiim_vx", "phiim_vy", "phiim_vz", "thetaim_vx", "thetaim_vy", "thetaim_vz",
+    "th_x", "th_y", "th_z", "E_x", "E_y", "E_z",
+)
+
+# Diagnostic slot names: the reference diag TSV columns after "t"
+# (scp_sim.c:2993-3003), then centroid extras.
+DIAG_NAMES = (
+    "E_phi_kin", "E_theta_kin", "E_grad", "E_mass", "E_pot", "E_tgrad", "E_tmass",
+    "E_coupling", "E_total", "phi_max", "P_max", "P_int", "theta_rms",
+    "Q_phi", "Q_theta", "Q_total", "s_max", "r_core", "omega_core", "Q_core",
+    "thp1u", "thp1v", "thp2u", "thp2v", "gauss_max", "gauss_l2", "E_em", "Q_flux",
+    "Q_p0", "Q_p1", "Q_p2", "centroid_x", "centroid_y", "centroid_z",
+)
