@@ -1,0 +1,276 @@
+"""Benchmark of the B200 lattice stepper (see DESIGN.md for the accounting).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c1|c0|c2|c2f|c4f]
+
+One step = one leapfrog step over the whole grid of the workload.  The
+default workload is the gauged FP64 128^3 two-ball run (e = 0.1, dx = 0.5,
+dt = 0.1).  Under torchrun (N > 1) every rank runs an independent replica
+(the stepper does not shard); the reported value is the sum over ranks
+divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (seed workload, precision, description)
+    "c1": ("c1", 0, "gauged FP64 128^3, e=0.1, two balls omega=+-0.8 20 sites apart"),
+    "c0": ("c0", 0, "ungauged complex FP64 64^3, one ball omega=0.8"),
+    "c2": ("c2", 0, "gauged FP64 256^3 + N(0,0.01) thermal noise"),
+    "c2f": ("c2", 1, "gauged FP32-compensated 256^3 + N(0,0.01) thermal noise"),
+    "c4f": ("c4", 1, "gauged FP32-compensated 512^3, eight co-phase balls"),
+}
+METRIC = "site-updates/s"
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(workload: str):
+    """DRAM bytes per site-update of the step kernel from the committed ncu
+    summary (profiles/step_kernel_<workload>.md, line 'traffic_bytes_per_site: X')."""
+    p = os.path.join(ROOT, "profiles", f"step_kernel_{workload}.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_site:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+def cpu_baseline(params, cols, nsteps: int) -> dict:
+    import oracle
+    if not oracle.reference_available():
+        return {"value": None, "unit": METRIC, "cores": 0, "kind": "reference",
+                "sample": "reference binary not built"}
+    threads = os.cpu_count() or 1
+    r = oracle.run_reference(params, cols, nsteps, diag_every=nsteps, threads=threads, read_final=False)
+    ms = r["wall_ms_per_step"]
+    n3 = params.N ** 3
+    return {"value": n3 / (ms * 1e-3), "unit": METRIC, "cores": threads, "kind": "reference",
+            "sample": f"{nsteps} steps of the same workload, reference scp_sim (OpenMP, {threads} threads), "
+                      f"loop wall time {ms:.2f} ms/step"}
+
+
+def run_reference_arm(args, rank, world):
+    from scp_b200 import seeds
+    seed, prec, desc = WORKLOADS[args.workload]
+    params = seeds.params_for(seed)
+    cfg = {"workload": desc, "N": params.N, "steps_sample": args.warmup + args.steps,
+           "parallelism": "cpu-openmp"}
+    if rank != 0:
+        return None
+    st = seeds.make_state(seed, params)
+    cb = cpu_baseline(params, st.cols(), args.warmup + args.steps)
+    val = cb["value"]
+    line = {"metric": METRIC, "value": val, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": (params.N ** 3 / val * 1e3) if val else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": cfg, "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--n", type=int, default=0, help="override the grid edge (profiling a smaller case)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = env_rank()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = dist_mod
+
+    if args.impl == "reference":
+        line = run_reference_arm(args, rank, world)
+        if rank == 0 and line:
+            print(json.dumps(line))
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    from scp_b200 import seeds
+    from scp_b200.api import Simulation
+    seed, prec, desc = WORKLOADS[args.workload]
+    over = dict(N=args.n, L=(args.n - 1) / 4.0) if args.n else {}
+    params = seeds.params_for(seed, precision=prec, device=local, **over)
+    st = seeds.make_state(seed, params)
+    cols = st.cols()
+    n3 = params.N ** 3
+
+    def barrier():
+        if dist:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    sim = Simulation(params, cols)
+    sim.step(args.warmup)
+    sim.sync()
+    barrier()
+    clk = Clocks(local)
+    clk.start()
+    ms = sim.time_steps(args.steps)
+    sim.sync()
+    clocks = clk.stop()
+    barrier()
+    info = sim.info()
+    ms_max = ms
+    if dist:
+        import torch
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = n3 * args.steps * world / (ms_max * 1e-3)
+    bytes_site = info.step_bytes_per_site
+    achieved = bytes_site * n3 / (ms / args.steps * 1e-3) / 1e9
+    peaks = measured_peaks()
+    sim.close()
+
+    e2e = None
+    if not args.no_e2e:
+        # end to end through the C ABI: host columns in (H2D inside init),
+        # Gauss projection and first force, K steps with diagnostics every
+        # 10 steps (D2H), final FP64 snapshot back to host
+        barrier()
+        nd = 0
+        t0 = time.perf_counter()
+        sim2 = Simulation(params, cols)
+        done = 0
+        while done < args.steps:
+            k = min(10, args.steps - done)
+            sim2.step(k)
+            done += k
+            sim2.diag_vector()
+            nd += 1
+        snap = sim2.snapshot()
+        t1 = time.perf_counter()
+        sim2.close()
+        wall = t1 - t0
+        if dist:
+            import torch
+            t = torch.tensor([wall], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wall = float(t.item())
+        h2d = sum(c.nbytes for c in cols)
+        d2h = sum(c.nbytes for c in snap) + nd * 8 * 53
+        e2e = {"value": n3 * args.steps * world / wall, "unit": METRIC,
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "wall_s": wall, "includes": "init upload, Gauss projection, steps, diag every 10 steps, "
+                                           "final f64 snapshot"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if prec == 0 else "f32c",
+        "data": "synthetic",
+        "config": {"workload": desc, "N": params.N, "precision": "fp64" if prec == 0 else "fp32-compensated",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single-gpu",
+                   "l2": "state larger than L2 (no flush needed)",
+                   "tile": [info.tile_x, info.tile_y, info.seg_len]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     "bytes_per_site": bytes_site,
+                     "traffic": (lambda t: t * n3 if t else None)(profiled_traffic(args.workload))},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(params, cols, 10 if params.N <= 128 else 3)
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -206,8 +206,10 @@ def small_state(N: int, gauged: bool, seed: int = 7, L: float | None = None, **o
     """A small generic test state: two opposite balls plus noise on every
     field (and on the links when gauged), net charge removed."""
     L = L if L is not None else (N - 1) / 2.0 * 0.9
-    p = Params(N=N, L=L, dt_factor=0.2, bc_type=2, complex_gauge=1 if gauged else 0,
-               g_gauge=0.1 if gauged else 0.05, **over)
+    kw = dict(N=N, L=L, dt_factor=0.2, bc_type=2, complex_gauge=1 if gauged else 0,
+              g_gauge=0.1 if gauged else 0.05)
+    kw.update(over)
+    p = Params(**kw)
     st = State(p)
     w = 0.3 * p.L
     add_balls(st, [Ball(x0=-w, omega=-0.8, sigma=max(1.0, p.L / 4)),

@@ -1,0 +1,63 @@
+"""Regenerate the golden fixtures of tests/golden/ by running the reference
+CPU stepper itself (oracle/_ref/scp_sim, built from kardianos/scp
+sfa/sim/scp_sim.c by oracle/Makefile) on seeded inputs.
+
+Run in a checkout that has the reference tree:  python tests/golden/make_golden.py
+Each fixture stores the seed recipe, the reference's final FP64 frame (small
+grids) or a fixed sample of its sites (64^3), and its diag TSV rows.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from scp_b200 import seeds  # noqa: E402
+
+SAMPLE_SEED = 12345
+
+
+def sample_sites(n3: int, k: int = 2048) -> np.ndarray:
+    rng = np.random.default_rng(SAMPLE_SEED)
+    return np.sort(rng.choice(n3, size=k, replace=False))
+
+
+def small_case(name: str, N: int, gauged: bool, nsteps: int, diag_every: int, **over):
+    st = seeds.small_state(N, gauged, **over)
+    p = st.params
+    r = oracle.run_reference(p, st.cols(), nsteps, diag_every=diag_every, threads=os.cpu_count())
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        N=N, gauged=int(gauged), nsteps=nsteps, diag_every=diag_every, L=p.L,
+        bc_type=p.bc_type, damp_rate=p.damp_rate, damp_width=p.damp_width,
+        final=np.stack(r["cols"]), diag=r["diag"], diag_header=np.array(r["diag_header"]),
+        names=np.array(r["names"]))
+    print(name, "written", r["wall_ms_per_step"], "ms/step")
+
+
+def workload_case(name: str, wl: str, nsteps: int, diag_every: int):
+    st = seeds.make_state(wl)
+    p = st.params
+    r = oracle.run_reference(p, st.cols(), nsteps, diag_every=diag_every, threads=os.cpu_count())
+    idx = sample_sites(p.N ** 3)
+    fin = np.stack(r["cols"])
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        workload=wl, nsteps=nsteps, diag_every=diag_every, sites=idx,
+        sample=fin[:, idx], col_l2=np.linalg.norm(fin, axis=1), col_sum=fin.sum(axis=1),
+        diag=r["diag"], diag_header=np.array(r["diag_header"]), names=np.array(r["names"]))
+    print(name, "written", r["wall_ms_per_step"], "ms/step")
+
+
+if __name__ == "__main__":
+    small_case("ref_complex_n12", 12, False, 60, 10)
+    small_case("ref_gauged_n12", 12, True, 60, 10)
+    small_case("ref_gauged_n10_damped", 10, True, 40, 10, bc_type=0, damp_width=2.0, damp_rate=0.05)
+    small_case("ref_complex_n13_damped", 13, False, 40, 10, bc_type=0, damp_width=2.0, damp_rate=0.05)
+    workload_case("ref_c0_64_1000", "c0", 1000, 10)

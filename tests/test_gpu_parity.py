@@ -1,0 +1,177 @@
+"""Parity of the CUDA stepper (through the C ABI) with the CPU checker and
+with the reference's own recorded output."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from scp_b200 import Params, seeds
+from scp_b200.api import DTYPE_F16, DTYPE_F32, DTYPE_F64, Simulation
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / nb if nb > 0 else np.linalg.norm(a - b)
+
+
+def worst_rel(got, ref):
+    return max(rel_l2(np.asarray(g).reshape(-1), np.asarray(r).reshape(-1)) for g, r in zip(got, ref))
+
+
+@pytest.mark.parametrize("name", ["ref_complex_n12", "ref_gauged_n12", "ref_gauged_n10_damped",
+                                  "ref_complex_n13_damped"])
+def test_gpu_matches_reference_frames(gpu, name):
+    f = np.load(os.path.join(GOLD, name + ".npz"))
+    over = {}
+    if int(f["bc_type"]) != 2:
+        over = dict(bc_type=int(f["bc_type"]), damp_width=float(f["damp_width"]), damp_rate=float(f["damp_rate"]))
+    st = seeds.small_state(int(f["N"]), bool(int(f["gauged"])), **over)
+    with Simulation(st.params, st.cols()) as sim:
+        sim.step(int(f["nsteps"]))
+        got = sim.snapshot()
+    assert worst_rel(got, f["final"]) < 1e-11
+
+
+CASES = [(n, g, t) for n in (8, 13, 31, 33, 40) for g in (False, True) for t in (0, 2, 3, 4)]
+
+
+@pytest.mark.parametrize("N,gauged,tile", CASES)
+def test_gpu_matches_oracle_shapes(gpu, N, gauged, tile):
+    st = seeds.small_state(N, gauged, seed=N, tile_variant=tile)
+    o = oracle.Oracle(st.params, st.cols())
+    with Simulation(st.params, st.cols()) as sim:
+        for chunk in (1, 4, 7):
+            sim.step(chunk)
+            o.step(chunk)
+            assert worst_rel(sim.snapshot(), o.cols()) < 1e-11, chunk
+
+
+@pytest.mark.parametrize("gauged", [False, True])
+@pytest.mark.parametrize("bc", [2, 0])
+def test_gpu_diag_matches_oracle(gpu, gauged, bc):
+    over = dict(bc_type=0, damp_width=3.0, damp_rate=0.02) if bc == 0 else {}
+    st = seeds.small_state(24, gauged, seed=3, **over)
+    o = oracle.Oracle(st.params, st.cols())
+    with Simulation(st.params, st.cols()) as sim:
+        for n in (0, 5, 10):
+            if n:
+                sim.step(5)
+                o.step(5)
+            g = sim.diag_vector()
+            r = o.diag()
+            for q in range(31):
+                if not gauged and 24 <= q <= 27:
+                    continue
+                tol = 1e-9 * max(abs(r[q]), 1.0) if q in (7, 13, 14, 15, 19, 24, 25, 27, 28, 29, 30) \
+                    else 1e-11 * max(abs(r[q]), 1e-300)
+                assert abs(g[q] - r[q]) <= tol, (n, q, g[q], r[q])
+
+
+def test_gpu_diag_deterministic(gpu):
+    st = seeds.small_state(32, True, seed=5)
+    with Simulation(st.params, st.cols()) as a:
+        a.step(3)
+        d1 = a.diag_vector()
+        d2 = a.diag_vector()
+    with Simulation(st.params, st.cols()) as b:
+        b.step(3)
+        d3 = b.diag_vector()
+    assert np.array_equal(d1, d2) and np.array_equal(d1, d3)
+
+
+def _f16_trunc(x):
+    """The reference's f64_to_f16 (sfa/sim/scp_config.h:548-559) in numpy."""
+    f = x.astype(np.float32).view(np.uint32)
+    sign = ((f >> 16) & 0x8000).astype(np.uint16)
+    e = ((f >> 23) & 0xFF).astype(np.int32) - 127 + 15
+    mant = ((f >> 13) & 0x3FF).astype(np.uint16)
+    out = (sign | (np.clip(e, 0, 31).astype(np.uint16) << 10) | mant).astype(np.uint16)
+    out = np.where(e <= 0, sign, out)
+    out = np.where(e >= 31, sign | 0x7C00, out)
+    return out.astype(np.uint16)
+
+
+def test_gpu_snapshot_dtypes(gpu):
+    st = seeds.small_state(16, True, seed=9)
+    with Simulation(st.params, st.cols()) as sim:
+        sim.step(3)
+        f64 = sim.snapshot(DTYPE_F64)
+        f32 = sim.snapshot(DTYPE_F32)
+        f16 = sim.snapshot(DTYPE_F16)
+    for a, b, c in zip(f64, f32, f16):
+        assert np.array_equal(a.astype(np.float32), b)
+        assert np.array_equal(_f16_trunc(a), c)
+
+
+def test_gpu_initial_state_roundtrip(gpu):
+    st = seeds.small_state(12, False, seed=4)
+    with Simulation(st.params, st.cols()) as sim:
+        got = sim.snapshot()
+    for g, r in zip(got, st.cols()):
+        assert np.array_equal(g, r.reshape(-1))
+
+
+def test_gpu_gauss_projection_matches_oracle(gpu):
+    st = seeds.make_state("c1", seeds.params_for("c1", N=32, L=7.75))
+    o = oracle.Oracle(st.params, st.cols())
+    with Simulation(st.params, st.cols()) as sim:
+        inf = sim.info()
+        got = sim.snapshot()
+        d = sim.diag()
+    ref = o.cols()
+    for c in range(27, 30):   # E after projection
+        assert rel_l2(got[c], ref[c]) < 1e-10
+    assert abs(inf.G_offset - o.g_offset) < 1e-12
+    assert d["gauss_max"] < 1e-11
+
+
+def test_gpu_c0_64_1000_parity(gpu):
+    """Config-0 workload: 1000 FP64 steps within 1e-10 relative L2 per field of
+    the CPU checker, energy series identical to the printed precision, and
+    sampled sites within 1e-10 of the reference's own run."""
+    st = seeds.make_state("c0")
+    p = st.params
+    o = oracle.Oracle(p, st.cols())
+    e_gpu, e_orc = [], []
+    with Simulation(p, st.cols()) as sim:
+        for _ in range(100):
+            sim.step(10)
+            o.step(10)
+            e_gpu.append(sim.diag()["E_total"])
+            e_orc.append(o.diag()[8])
+        got = sim.snapshot()
+    ref = o.cols()
+    for c in range(24):
+        assert rel_l2(got[c], ref[c]) < 1e-10, c
+    e_gpu, e_orc = np.array(e_gpu), np.array(e_orc)
+    assert np.max(np.abs(e_gpu - e_orc) / np.abs(e_orc)) < 1e-11
+    f = np.load(os.path.join(GOLD, "ref_c0_64_1000.npz"))
+    idx = f["sites"]
+    for c in range(24):
+        assert rel_l2(got[c][idx], f["sample"][c]) < 1e-10
+
+
+def test_gpu_gauged_64_1000_parity(gpu):
+    """Gauged 64^3 (two opposite balls, g = 0.1): 1000 steps within 1e-10 per
+    field; the Gauss residual stays at roundoff."""
+    st = seeds.make_state("c1", seeds.params_for("c1", N=64, L=15.75))
+    p = st.params
+    o = oracle.Oracle(p, st.cols())
+    with Simulation(p, st.cols()) as sim:
+        gmax = []
+        for _ in range(10):
+            sim.step(100)
+            o.step(100)
+            gmax.append(sim.diag()["gauss_max"])
+        got = sim.snapshot()
+        d = sim.diag()
+    ref = o.cols()
+    for c in range(30):
+        assert rel_l2(got[c], ref[c]) < 1e-10, c
+    assert max(gmax) < 1e-10
+    r = o.diag()
+    assert abs(d["E_total"] - r[8]) < 1e-11 * abs(r[8])

@@ -1,0 +1,50 @@
+import math
+
+import numpy as np
+
+from scp_b200 import Params, seeds
+
+
+def test_splitmix64_known_answer():
+    # canonical SplitMix64 outputs for seed 1234567
+    assert [int(x) for x in seeds.splitmix64(1234567, 5)] == [
+        6457827717110365317, 3203168211198807973, 9817491932198370423,
+        4593380528125082431, 16408922859458223821]
+
+
+def test_normals_deterministic_and_standard():
+    a = seeds.normals(0, 3, 200001)
+    b = seeds.normals(0, 3, 200001)
+    assert np.array_equal(a, b)
+    assert abs(a.mean()) < 0.01 and abs(a.std() - 1.0) < 0.01
+    assert not np.array_equal(a[:100], seeds.normals(0, 4, 100))
+
+
+def test_workload_grids():
+    p = seeds.params_for("c1")
+    assert p.N == 128 and p.dx == 0.5 and abs(p.dt - 0.1) < 1e-15 and p.gauged
+    assert seeds.params_for("c0").ncols == 24 and p.ncols == 30
+
+
+def test_c1_is_net_neutral_and_c2_neutralised():
+    st = seeds.make_state("c1", seeds.params_for("c1", N=32, L=7.75))
+    rho = seeds.charge_density(st)
+    assert abs(rho.sum()) <= 1e-12 * np.abs(rho).sum()
+    st2 = seeds.State(st.params)
+    for k in st:
+        st2[k] = st[k].copy()
+    seeds.add_noise(st2, seeds.FIELD_COLS, 0.01, seed=1)
+    seeds.neutralise(st2)
+    rho2 = seeds.charge_density(st2)
+    assert abs(rho2.sum()) <= 1e-12 * np.abs(rho2).sum()
+
+
+def test_ball_is_phase_rotating():
+    p = Params(N=16, L=3.75)
+    st = seeds.State(p)
+    seeds.add_balls(st, [seeds.Ball(omega=0.8)])
+    # dPhi/dt = i omega Phi
+    assert np.allclose(st["phi_vx"], -0.8 * st["phiim_x"])
+    assert np.allclose(st["phiim_vy"], 0.8 * st["phi_y"])
+    c = st.params.N // 2
+    assert math.isclose(math.atan2(st["phiim_y"][c, c, c], st["phi_y"][c, c, c]), 2 * math.pi / 3, rel_tol=1e-12)
