@@ -137,6 +137,35 @@ const char *scp_gpu_errstr(int code);
 const char *scp_gpu_last_cuda_error(void);
 int  scp_gpu_abi_version(void);
 
+/* Diagnostics for callers that must not allocate device memory.
+ *
+ * No counterpart in the reference.  Some hosts of this library cannot call
+ * cudaMalloc while they run a simulation: a caller that replays captured
+ * work, a process whose device memory is carved up and owned by another
+ * framework, or a real-time loop that treats any allocation as a failure.
+ * This entry point computes the same diagnostics as scp_gpu_diag for a state
+ * that the caller already holds on the device, without a handle and without
+ * allocating: its reduction scratch is a fixed array that lives in the
+ * library (SCP_DIAG_STATIC_SCRATCH_BYTES, about 300 KB, held by every GPU
+ * that loads the library until the process exits).
+ *
+ *   p          grid and physics parameters (as for scp_gpu_init)
+ *   dev_cols   24 or 30 device pointers, FP64 columns in the SFA order above
+ *   G_offset   frozen Gauss offset to measure against (scp_gpu_info.G_offset)
+ *   stream     cudaStream_t to run on, or NULL for the legacy default stream
+ *   out        host result, slot order as scp_gpu_diag
+ *
+ * Grids larger than SCP_DIAG_STATIC_MAX_N per edge are rejected with
+ * SCP_EINVAL.  The first call on a device looks up the scratch array's
+ * device address (once per device); make that first call before any stream
+ * capture.  All calls share the one scratch array, so calls whose work
+ * overlaps on the GPU (two host threads, or two streams) race: serialise
+ * them.  The call synchronises on `stream` before it returns. */
+#define SCP_DIAG_STATIC_MAX_N 2048
+#define SCP_DIAG_STATIC_SCRATCH_BYTES (8 * (1184 * 32 + 64 + 8))
+int  scp_gpu_diag_noalloc(const scp_gpu_params *p, const double *const *dev_cols, double G_offset,
+                          void *stream, scp_gpu_diag_out *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -622,3 +622,156 @@ const char *scp_gpu_last_cuda_error(void) { return g_cuda_err; }
 int scp_gpu_abi_version(void) { return SCP_GPU_ABI_VERSION; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free diagnostics
+//
+// For callers that cannot allocate device memory (see scp_gpu_diag_noalloc
+// in include/scp_gpu.h).  The reduction scratch is this file-scope device
+// array: partial rows of the two reduction passes, the folded values and
+// the point reads.  Its name in host code is only a stand-in for the symbol,
+// so the device address is looked up with cudaGetSymbolAddress, once per
+// device with that device current, and passed to the kernels.
+
+namespace {
+
+constexpr int kStaticPartRows = kRedMaxBlocks;      // one row of 32 doubles per CTA
+constexpr size_t kStaticDoubles = (size_t)kStaticPartRows * 32 + 64 + 8;
+static_assert(kStaticDoubles * 8 == SCP_DIAG_STATIC_SCRATCH_BYTES, "scratch size in the header");
+
+__device__ __align__(256) double g_diag_scratch[kStaticDoubles];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double *g_scratch_addr[kMaxDevices] = {};
+
+// Device address of g_diag_scratch on the current device (looked up once).
+int static_scratch(int dev, double **out) {
+    if (dev < 0 || dev >= kMaxDevices) return SCP_ENODEV;
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_addr[dev]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_diag_scratch);
+        if (e != cudaSuccess || !ptr) {
+            snprintf(g_cuda_err, sizeof g_cuda_err, "cudaGetSymbolAddress(g_diag_scratch): %s",
+                     cudaGetErrorString(e));
+            return SCP_ECUDA;
+        }
+        g_scratch_addr[dev] = (double *)ptr;
+    }
+    *out = g_scratch_addr[dev];
+    return SCP_OK;
+}
+
+// State given as the caller's 24/30 device columns in SFA order.
+struct ViewCols {
+    const double *pos[15];   // packed field order u v tu tv th
+    const double *mom[15];   // du dv dtu dtv E
+    __device__ __forceinline__ double q(int f, long long i) const { return pos[f][i]; }
+    __device__ __forceinline__ double p(int f, long long i) const { return mom[f][i]; }
+};
+
+}  // namespace
+
+extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *const *dev_cols, double G_offset,
+                                    void *stream_ptr, scp_gpu_diag_out *out) {
+    int rc = validate(pp);
+    if (rc) return rc;
+    if (!dev_cols || !out) return SCP_EINVAL;
+    if (pp->N > SCP_DIAG_STATIC_MAX_N) {
+        snprintf(g_cuda_err, sizeof g_cuda_err, "scp_gpu_diag_noalloc: N=%d exceeds SCP_DIAG_STATIC_MAX_N=%d",
+                 pp->N, SCP_DIAG_STATIC_MAX_N);
+        return SCP_EINVAL;
+    }
+    const scp_gpu_params &p = *pp;
+    const int gauged = p.complex_gauge ? 1 : 0;
+    const int ncols = gauged ? 30 : 24;
+    ViewCols V;
+    for (int f = 0; f < 15; f++) { V.pos[f] = nullptr; V.mom[f] = nullptr; }
+    for (int c = 0; c < ncols; c++) {
+        if (!dev_cols[c]) return SCP_EINVAL;
+        int field, mom;
+        sfa_col_source(c, &field, &mom);
+        (mom ? V.mom : V.pos)[field] = dev_cols[c];
+    }
+    if (!gauged)   // ungauged diagnostics never read links or E; keep the pointers valid anyway
+        for (int f = FTH; f < FTH + 3; f++) { V.pos[f] = V.pos[FU]; V.mom[f] = V.mom[FU]; }
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    double *scratch = nullptr;
+    if ((rc = static_scratch(dev, &scratch))) return rc;
+    double *part = scratch, *fold = scratch + (size_t)kStaticPartRows * 32, *point = fold + 64;
+    cudaStream_t st = (cudaStream_t)stream_ptr;
+    const long long n3 = (long long)p.N * p.N * p.N;
+    const int nb = red_blocks(n3);
+    if (nb > kStaticPartRows) return SCP_EINVAL;
+    DiagConsts c;
+    c.N = p.N; c.N3 = n3; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx; c.idx1 = 1.0 / (2.0 * p.dx);
+    c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
+    c.gauged = gauged;
+    c.g = gauged ? p.g_gauge : 0.0;
+    c.bpre = gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
+    c.R2 = p.qdiag_radius * p.qdiag_radius;
+    c.Rcube = p.qdiag_radius;
+    const double Rint = (p.bc_type == 0) ? (p.L - p.damp_width - p.dx) : 1e300;
+    c.Rint2 = Rint * Rint;
+    c.G_offset = G_offset;
+    // every scratch word read below is written first in the same call (each
+    // CTA writes its whole partial row, the folds write their outputs), so
+    // no clearing is needed; the fold area is zeroed only so a failed launch
+    // cannot hand back the previous call's numbers
+    CK(cudaMemsetAsync(fold, 0, sizeof(double) * (64 + 8), st));
+    diag_pass1_kernel<ViewCols><<<nb, kRedThreads, 0, st>>>(V, c, part);
+    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, st>>>(part, nb, fold);
+    diag_pass2_kernel<ViewCols><<<nb, kRedThreads, 0, st>>>(V, c, fold, part);
+    fold_partials_kernel<1, 1><<<1, 1024, 0, st>>>(part, nb, fold + 40);
+    diag_point_kernel<ViewCols><<<1, 32, 0, st>>>(V, c, fold + 40, p.qdiag_probe1, p.qdiag_probe2, point);
+    CK(cudaGetLastError());
+    double h[53];
+    CK(cudaMemcpyAsync(h, fold, sizeof(double) * 42, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h + 48, point, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const double *f1 = h, *f2 = h + 40, *pt = h + 48;
+    const double dV = c.dV;
+    double *o = out->v;
+    for (int q = 0; q < SCP_DIAG_NSLOTS; q++) o[q] = 0.0;
+    o[SCP_DIAG_E_PHI_KIN] = f1[DS_EPK];
+    o[SCP_DIAG_E_THETA_KIN] = f1[DS_ETK];
+    o[SCP_DIAG_E_GRAD] = f1[DS_EG];
+    o[SCP_DIAG_E_MASS] = f1[DS_EM];
+    o[SCP_DIAG_E_POT] = f1[DS_EP];
+    o[SCP_DIAG_E_TGRAD] = f1[DS_ETG];
+    o[SCP_DIAG_E_TMASS] = f1[DS_ETM];
+    o[SCP_DIAG_E_COUPLING] = f1[DS_EC];
+    o[SCP_DIAG_E_TOTAL] = f1[DS_EPK] + f1[DS_ETK] + f1[DS_EG] + f1[DS_EM] + f1[DS_EP] + f1[DS_ETG] +
+                          f1[DS_ETM] + f1[DS_EC] + (gauged ? f1[DS_EEM] : 0.0);
+    o[SCP_DIAG_PHI_MAX] = f1[DS_NSUM + DM_PM];
+    o[SCP_DIAG_P_MAX] = f1[DS_NSUM + DM_PMAX];
+    o[SCP_DIAG_P_INT] = f1[DS_PINT];
+    o[SCP_DIAG_THETA_RMS] = sqrt(f1[DS_TRS] / (6.0 * (double)n3));
+    o[SCP_DIAG_Q_PHI] = f1[DS_QP] * dV;
+    o[SCP_DIAG_Q_THETA] = f1[DS_QT] * dV;
+    o[SCP_DIAG_Q_TOTAL] = f1[DS_QP] * dV + f1[DS_QT] * dV;
+    o[SCP_DIAG_S_MAX] = f1[DS_NSUM + DM_SMAX];
+    const double M0 = f1[DS_M0] * dV;
+    o[SCP_DIAG_R_CORE] = (M0 < 1e-30) ? 0.0 : sqrt(f2[0] * dV / M0);
+    o[SCP_DIAG_OMEGA_CORE] = pt[0];
+    o[SCP_DIAG_Q_CORE] = f1[DS_QC] * dV;
+    o[SCP_DIAG_THP1U] = pt[1]; o[SCP_DIAG_THP1V] = pt[2];
+    o[SCP_DIAG_THP2U] = pt[3]; o[SCP_DIAG_THP2V] = pt[4];
+    if (gauged) {
+        o[SCP_DIAG_GAUSS_MAX] = f1[DS_NSUM + DM_GMAX];
+        o[SCP_DIAG_GAUSS_L2] = f1[DS_NOM] > 0 ? sqrt(f1[DS_GL2] / f1[DS_NOM]) : 0.0;
+        o[SCP_DIAG_E_EM] = f1[DS_EEM];
+        o[SCP_DIAG_Q_FLUX] = (f1[DS_FSUM] - G_offset * f1[DS_NC] * dV) / p.g_gauge;
+    }
+    o[SCP_DIAG_Q_P0] = f1[DS_QP0] * dV;
+    o[SCP_DIAG_Q_P1] = f1[DS_QP1] * dV;
+    o[SCP_DIAG_Q_P2] = f1[DS_QP2] * dV;
+    if (!(M0 < 1e-30)) {
+        o[SCP_DIAG_CENTROID_X] = f1[DS_CX] * dV / M0;
+        o[SCP_DIAG_CENTROID_Y] = f1[DS_CY] * dV / M0;
+        o[SCP_DIAG_CENTROID_Z] = f1[DS_CZ] * dV / M0;
+    }
+    if (!isfinite(o[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
+    return SCP_OK;
+}
