@@ -157,6 +157,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--n", type=int, default=0, help="override the grid edge (profiling a smaller case)")
+    ap.add_argument("--tile", type=int, default=0, help="tile_variant (0 = library default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
@@ -180,7 +181,7 @@ def main():
     from scp_b200.api import Simulation
     seed, prec, desc = WORKLOADS[args.workload]
     over = dict(N=args.n, L=(args.n - 1) / 4.0) if args.n else {}
-    params = seeds.params_for(seed, precision=prec, device=local, **over)
+    params = seeds.params_for(seed, precision=prec, device=local, tile_variant=args.tile, **over)
     st = seeds.make_state(seed, params)
     cols = st.cols()
     n3 = params.N ** 3

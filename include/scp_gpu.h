@@ -136,6 +136,12 @@ void scp_gpu_free(scp_gpu *h);
 const char *scp_gpu_errstr(int code);
 const char *scp_gpu_last_cuda_error(void);
 int  scp_gpu_abi_version(void);
+/* Self-check of the library's bounded-argument sine/cosine (used by the
+ * gauged step in place of the CUDA math library) against CUDA's sin/cos on
+ * device: for the n host angles x[], err[0..3] receive the largest absolute
+ * difference of sin and cos in FP64 and of sin and cos in FP32.  Synchronous;
+ * allocates and frees its own device buffers. */
+int  scp_gpu_check_trig(int n, const double *x, double *err);
 
 /* Diagnostics for callers that must not allocate device memory.
  *

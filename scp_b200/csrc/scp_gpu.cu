@@ -10,14 +10,18 @@
 // After a scp_gpu_step call, X[cur^1] and S hold the state at the current
 // time (what diagnostics and snapshots read) and X[cur], W the drifted
 // positions and half-kicked momenta the next launch starts from.
+//
+// FP32-compensated mode keeps the same roles in FP32: positions as a
+// pair X32[b] (fp32 hi) + LO8[b] (int8 lo of the 12 matter fields) + TLO[b]
+// (fp32 lo of the 3 link angles), momenta W32, S32; the FP64 buffers
+// only stage the initial state (and its Gauss projection) and are released.
 #include "../../include/scp_gpu.h"
 #include "common.cuh"
 #include "diag.cuh"
-#include "fp32c.cuh"
 #include "gauss.cuh"
 #include "reduce.cuh"
 #include "snapshot.cuh"
-#include "step_f64.cuh"
+#include "step.cuh"
 
 #include <math.h>
 #include <stdio.h>
@@ -41,16 +45,17 @@ static thread_local char g_cuda_err[256] = "";
 
 namespace {
 
-using StepFn = void (*)(StepIO64, StepConsts, TileGrid);
+template <class P>
+using StepFnT = void (*)(StepIO<P>, StepConsts, TileGrid);
 
 struct TileShape { int tx, ty; };
 // tile_variant 1..: fixed shapes; 0 picks the default for the mode
 static const TileShape kShapes[] = {{32, 4}, {32, 4}, {32, 8}, {16, 8}, {64, 2}};
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
-template <int TX, int TY>
-StepFn pick_f64(bool g, bool f, bool s, bool d) {
-#define SCP_SEL(G, F, S, D) if (g == G && f == F && s == S && d == D) return step_f64_kernel<TX, TY, G, F, S, D>;
+template <class P, int TX, int TY>
+StepFnT<P> pick(bool g, bool f, bool s, bool d) {
+#define SCP_SEL(G, F, S, D) if (g == G && f == F && s == S && d == D) return step_kernel<P, TX, TY, G, F, S, D>;
     SCP_SEL(false, false, false, false) SCP_SEL(false, false, false, true)
     SCP_SEL(false, false, true, false)  SCP_SEL(false, false, true, true)
     SCP_SEL(false, true, false, false)  SCP_SEL(false, true, false, true)
@@ -63,18 +68,58 @@ StepFn pick_f64(bool g, bool f, bool s, bool d) {
     return nullptr;
 }
 
-template <int TX, int TY>
-size_t smem_f64(bool g) {
-    return g ? F64Layout<TX, TY, true>::smem_bytes : F64Layout<TX, TY, false>::smem_bytes;
+template <class P, int TX, int TY>
+size_t smem_of(bool g) {
+    return g ? StepLayout<P, TX, TY, true>::smem_bytes : StepLayout<P, TX, TY, false>::smem_bytes;
 }
 
-StepFn step_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
+template <class P>
+StepFnT<P> step_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
     switch (shape) {
-        case 2: *smem = smem_f64<32, 8>(g); return pick_f64<32, 8>(g, f, s, d);
-        case 3: *smem = smem_f64<16, 8>(g); return pick_f64<16, 8>(g, f, s, d);
-        case 4: *smem = smem_f64<64, 2>(g); return pick_f64<64, 2>(g, f, s, d);
-        default: *smem = smem_f64<32, 4>(g); return pick_f64<32, 4>(g, f, s, d);
+        case 2: *smem = smem_of<P, 32, 8>(g); return pick<P, 32, 8>(g, f, s, d);
+        case 3: *smem = smem_of<P, 16, 8>(g); return pick<P, 16, 8>(g, f, s, d);
+        case 4: *smem = smem_of<P, 64, 2>(g); return pick<P, 64, 2>(g, f, s, d);
+        default: *smem = smem_of<P, 32, 4>(g); return pick<P, 32, 4>(g, f, s, d);
     }
+}
+
+// FP32-compensated state from FP64 staging: hi = fp32(x), lo = bf16(x - hi),
+// momenta fp32
+__global__ void to_fp32c_kernel(const double *X, const double *S, int nf, long long n3, float *hi, int8_t *lo8,
+                                float *tlo, float *S32) {
+    const long long n = (long long)nf * n3;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double x = X[i];
+        const float h = (float)x;
+        const float l = (float)(x - (double)h);
+        hi[i] = h;
+        if (i < 12 * n3) lo8[i] = lo_encode(l, h);
+        else tlo[i - 12 * n3] = l;
+        S32[i] = (float)S[i];
+    }
+}
+
+// FP64 view of the FP32-compensated state for reductions and snapshots
+struct View32C {
+    const float *X;
+    const int8_t *LO;
+    const float *TLO;
+    const float *S;
+    long long N3;
+    __device__ __forceinline__ double q(int f, long long i) const {
+        const float h = X[f * N3 + i];
+        const float l = (f < 12) ? lo_decode(LO[f * N3 + i], h) : TLO[(f - 12) * N3 + i];
+        return (double)h + (double)l;
+    }
+    __device__ __forceinline__ double p(int f, long long i) const { return (double)S[f * N3 + i]; }
+};
+
+template <class View>
+__global__ void extract_col_kernel(View V, int field, int mom, long long n, double *out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = mom ? V.p(field, i) : V.q(field, i);
 }
 
 }  // namespace
@@ -93,7 +138,11 @@ struct scp_gpu {
     double *W = nullptr, *S = nullptr;
     int cur = 0;
     // FP32-compensated state
-    Fp32cState f32;
+    float *X32[2] = {nullptr, nullptr};
+    int8_t *LO[2] = {nullptr, nullptr};
+    float *TLO[2] = {nullptr, nullptr};
+    float *W32 = nullptr, *S32 = nullptr;
+    void *slab32 = nullptr;
     // scratch
     double *part = nullptr, *fold = nullptr, *cg = nullptr, *point = nullptr;
     int *flag = nullptr;
@@ -174,49 +223,68 @@ static void plan_tiles(scp_gpu *h, int tx, int ty, int slots) {
     h->grid = tg.nitems < slots ? tg.nitems : slots;
 }
 
+template <class P>
+static int occupancy_of(scp_gpu *h, int shape, int *occ) {
+    size_t smem = 0;
+    // raise the dynamic shared-memory cap of every variant of this shape
+    for (int v = 0; v < 8; v++) {
+        StepFnT<P> fn = step_fn<P>(shape, h->gauged, v & 1, (v >> 1) & 1, (v >> 2) & 1, &smem);
+        CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    StepFnT<P> fn = step_fn<P>(shape, h->gauged, false, false, false, &smem);
+    const TileShape ts = kShapes[shape];
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, (const void *)fn, ts.tx * ts.ty, smem));
+    return SCP_OK;
+}
+
 static int setup_launch(scp_gpu *h) {
     int shape = h->p.tile_variant;
-    if (shape == 0) shape = h->gauged ? 1 : 1;
+    if (shape == 0) shape = 1;
     h->shape = shape;
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
     const TileShape ts = kShapes[shape];
-    int slots = nsm;
-    if (h->prec == SCP_PREC_FP64) {
-        size_t smem = 0;
-        // raise the dynamic shared-memory cap of every variant of this shape
-        for (int v = 0; v < 16; v++) {
-            StepFn fn = step_fn(shape, h->gauged, v & 1, (v >> 1) & 1, (v >> 2) & 1, &smem);
-            if ((v >> 3) & 1) continue;
-            CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        }
-        StepFn fn = step_fn(shape, h->gauged, false, false, false, &smem);
-        int occ = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)fn, ts.tx * ts.ty, smem));
-        if (occ < 1) return SCP_EUNSUPPORTED;
-        slots = nsm * occ;
-    } else {
-        int occ = 0;
-        CK(fp32c_occupancy(h->gauged, ts.tx, ts.ty, &occ));
-        if (occ < 1) return SCP_EUNSUPPORTED;
-        slots = nsm * occ;
-    }
-    plan_tiles(h, ts.tx, ts.ty, slots);
+    int occ = 0, rc;
+    if (h->prec == SCP_PREC_FP64) rc = occupancy_of<F64>(h, shape, &occ);
+    else rc = occupancy_of<F32C>(h, shape, &occ);
+    if (rc) return rc;
+    if (occ < 1) return SCP_EUNSUPPORTED;
+    plan_tiles(h, ts.tx, ts.ty, nsm * occ);
     return SCP_OK;
 }
 
-static int launch_f64(scp_gpu *h, bool first, bool sync) {
+static int launch_step(scp_gpu *h, bool first, bool sync) {
     size_t smem = 0;
-    StepFn fn = step_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
     const TileShape ts = kShapes[h->shape];
-    StepIO64 io;
-    io.xin = h->X[h->cur];
-    io.xout = h->X[h->cur ^ 1];
-    io.win = first ? h->S : h->W;
-    io.wout = h->W;
-    io.sout = h->S;
-    io.flag = h->flag;
-    fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+    if (h->prec == SCP_PREC_FP64) {
+        StepFnT<F64> fn = step_fn<F64>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
+        StepIO<F64> io;
+        io.xin = h->X[h->cur];
+        io.xout = h->X[h->cur ^ 1];
+        io.loin = nullptr;
+        io.loout = nullptr;
+        io.tloin = nullptr;
+        io.tloout = nullptr;
+        io.win = first ? h->S : h->W;
+        io.wout = h->W;
+        io.sout = h->S;
+        io.flag = h->flag;
+        fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+    } else {
+        StepFnT<F32C> fn = step_fn<F32C>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
+        StepIO<F32C> io;
+        io.xin = h->X32[h->cur];
+        io.xout = h->X32[h->cur ^ 1];
+        io.loin = h->LO[h->cur];
+        io.loout = h->LO[h->cur ^ 1];
+        io.tloin = h->TLO[h->cur];
+        io.tloout = h->TLO[h->cur ^ 1];
+        io.win = first ? h->S32 : h->W32;
+        io.wout = h->W32;
+        io.sout = h->S32;
+        io.flag = h->flag;
+        fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+    }
     CK(cudaGetLastError());
     h->cur ^= 1;
     return SCP_OK;
@@ -318,6 +386,73 @@ static int alloc_common(scp_gpu *h) {
     return SCP_OK;
 }
 
+static size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
+    int rc;
+    if ((rc = alloc_common(h))) return rc;
+    const long long n3 = h->N3;
+    const int ncols = h->gauged ? 30 : 24;
+    const size_t nel = (size_t)h->nf * n3;
+    const size_t blk = sizeof(double) * nel;
+    // FP64 slab: X[0] = x_0 and S = v_0 stage the initial state in both modes;
+    // FP64 mode also keeps X[1] and W in it
+    const int nblk = (h->prec == SCP_PREC_FP64) ? 4 : 2;
+    CK(cudaMalloc(&h->slab, nblk * blk));
+    h->dev_bytes += nblk * blk;
+    h->X[0] = h->slab;
+    h->S = h->slab + nel;
+    if (h->prec == SCP_PREC_FP64) {
+        h->X[1] = h->slab + 2 * nel;
+        h->W = h->slab + 3 * nel;
+    }
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int c = 0; c < ncols; c++) {
+        int field, mom;
+        sfa_col_source(c, &field, &mom);
+        double *dst = (mom ? h->S : h->X[0]) + (size_t)field * n3;
+        cudaError_t e = cudaMemcpyAsync(dst, cols[c], sizeof(double) * n3, kind, h->stream);
+        if (e != cudaSuccess) {
+            snprintf(g_cuda_err, sizeof g_cuda_err, "%s (column %d upload)", cudaGetErrorString(e), c);
+            return SCP_ECUDA;
+        }
+    }
+    if (h->gauged && (rc = gauss_startup(h, h->X[0], h->S))) return rc;
+    if ((rc = setup_launch(h))) return rc;
+    CK(cudaMalloc(&h->stage, sizeof(double) * n3));
+    h->dev_bytes += sizeof(double) * n3;
+    h->cur = 0;
+    if (h->prec == SCP_PREC_FP64) return launch_step(h, true, false);
+    // FP32-compensated buffers: X32[0..1], W32, S32 (fp32, NF arrays), LO[0..1]
+    // (int8, 12 arrays), TLO[0..1] (fp32, 3 arrays, gauged only)
+    const size_t bf = round256(sizeof(float) * nel), bl = round256((size_t)12 * n3);
+    const size_t bt = h->gauged ? round256(sizeof(float) * 3 * (size_t)n3) : 0;
+    CK(cudaMalloc(&h->slab32, 4 * bf + 2 * bl + 2 * bt));
+    h->dev_bytes += 4 * bf + 2 * bl + 2 * bt;
+    char *b = (char *)h->slab32;
+    h->X32[0] = (float *)b; b += bf;
+    h->X32[1] = (float *)b; b += bf;
+    h->W32 = (float *)b; b += bf;
+    h->S32 = (float *)b; b += bf;
+    h->LO[0] = (int8_t *)b; b += bl;
+    h->LO[1] = (int8_t *)b; b += bl;
+    if (h->gauged) {
+        h->TLO[0] = (float *)b; b += bt;
+        h->TLO[1] = (float *)b;
+    }
+    to_fp32c_kernel<<<red_blocks((long long)nel), kRedThreads, 0, h->stream>>>(
+        h->X[0], h->S, h->nf, n3, h->X32[0], h->LO[0], h->TLO[0], h->S32);
+    CK(cudaGetLastError());
+    if ((rc = launch_step(h, true, false))) return rc;
+    // the FP64 staging is no longer needed: FP32C diagnostics read hi+lo directly
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaFree(h->slab));
+    h->dev_bytes -= nblk * blk;
+    h->slab = nullptr;
+    h->X[0] = h->X[1] = h->W = h->S = nullptr;
+    return SCP_OK;
+}
+
 static int init_common(const scp_gpu_params *p, const double *const *cols, bool on_device, scp_gpu **out) {
     if (!out) return SCP_EINVAL;
     *out = nullptr;
@@ -339,50 +474,18 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
     h->nf = h->gauged ? 15 : 12;
     h->prec = p->precision_mode;
     fill_consts(h);
-    auto fail = [&](int code) { scp_gpu_free(h); return code; };
-    if ((rc = alloc_common(h))) return fail(rc);
-    const long long n3 = h->N3;
-    const size_t blk = sizeof(double) * (size_t)h->nf * n3;
-    // FP64 staging of the initial state: X[0] = x_0, S = v_0 (also the
-    // working layout of FP64 mode)
-    {
-        cudaError_t e = cudaMalloc(&h->slab, 4 * blk);
-        if (e != cudaSuccess) { cudaGetLastError(); return fail(SCP_ENOMEM); }
-        h->dev_bytes += 4 * blk;
-    }
-    h->X[0] = h->slab;
-    h->X[1] = h->slab + (size_t)h->nf * n3;
-    h->W = h->slab + 2 * (size_t)h->nf * n3;
-    h->S = h->slab + 3 * (size_t)h->nf * n3;
-    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    for (int c = 0; c < ncols; c++) {
-        int field, mom;
-        sfa_col_source(c, &field, &mom);
-        double *dst = (mom ? h->S : h->X[0]) + (size_t)field * n3;
-        cudaError_t e = cudaMemcpyAsync(dst, cols[c], sizeof(double) * n3, kind, h->stream);
+    rc = init_body(h, cols, on_device);
+    if (rc == SCP_OK) {
+        cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
-            snprintf(g_cuda_err, sizeof g_cuda_err, "%s (column %d upload)", cudaGetErrorString(e), c);
-            return fail(SCP_ECUDA);
+            snprintf(g_cuda_err, sizeof g_cuda_err, "%s (init)", cudaGetErrorString(e));
+            rc = SCP_ECUDA;
         }
     }
-    if (h->gauged && (rc = gauss_startup(h, h->X[0], h->S))) return fail(rc);
-    if ((rc = setup_launch(h))) return fail(rc);
-    CK(cudaMalloc(&h->stage, sizeof(double) * n3));
-    h->dev_bytes += sizeof(double) * n3;
-    h->cur = 0;
-    if (h->prec == SCP_PREC_FP64) {
-        if ((rc = launch_f64(h, true, false))) return fail(rc);
-    } else {
-        if ((rc = fp32c_init(&h->f32, h->c, h->gauged, h->X[0], h->S, kShapes[h->shape].tx, kShapes[h->shape].ty,
-                             h->tg, h->grid, damping_on(h), h->flag, h->stream))) {
-            snprintf(g_cuda_err, sizeof g_cuda_err, "%s", fp32c_last_error());
-            return fail(rc);
-        }
-        h->dev_bytes += h->f32.bytes;
-        // the FP64 slab only staged the start; keep X[0]/S as the FP64 view
-        // buffers that diagnostics expand into (the other two are released)
+    if (rc) {
+        scp_gpu_free(h);
+        return rc;
     }
-    CK(cudaStreamSynchronize(h->stream));
     *out = h;
     return SCP_OK;
 }
@@ -404,9 +507,7 @@ int scp_gpu_step(scp_gpu *h, int nsteps) {
     int rc;
     for (int n = 0; n < nsteps; n++) {
         const bool last = (n == nsteps - 1);
-        if (h->prec == SCP_PREC_FP64) rc = launch_f64(h, false, last);
-        else rc = fp32c_step(&h->f32, last, h->stream);
-        if (rc) return rc;
+        if ((rc = launch_step(h, false, last))) return rc;
     }
     h->steps += nsteps;
     return SCP_OK;
@@ -422,27 +523,10 @@ int scp_gpu_sync(scp_gpu *h) {
     return f ? SCP_ENONFINITE : SCP_OK;
 }
 
-// FP64 view of the current state (FP32C expands into the staging slab first)
-static int current_view(scp_gpu *h, ViewF64 *v) {
-    v->N3 = h->N3;
-    if (h->prec == SCP_PREC_FP64) {
-        v->X = h->X[h->cur ^ 1];
-        v->S = h->S;
-        return SCP_OK;
-    }
-    int rc = fp32c_expand(&h->f32, h->X[0], h->S, h->stream);
-    if (rc) return rc;
-    v->X = h->X[0];
-    v->S = h->S;
-    return SCP_OK;
-}
+}  // extern "C"
 
-int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
-    if (!h || !out) return SCP_EINVAL;
-    CK(cudaSetDevice(h->device));
-    ViewF64 V;
-    int rc = current_view(h, &V);
-    if (rc) return rc;
+template <class View>
+static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
     const scp_gpu_params &p = h->p;
     DiagConsts c;
     c.N = h->N; c.N3 = h->N3; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx; c.idx1 = 1.0 / (2.0 * p.dx);
@@ -456,11 +540,11 @@ int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     c.Rint2 = Rint * Rint;
     c.G_offset = h->G_offset;
     const int nb = red_blocks(h->N3);
-    diag_pass1_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->part);
+    diag_pass1_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->part);
     fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-    diag_pass2_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->fold, h->part);
+    diag_pass2_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->fold, h->part);
     fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold + 40);
-    diag_point_kernel<ViewF64><<<1, 32, 0, h->stream>>>(V, c, h->fold + 40, p.qdiag_probe1, p.qdiag_probe2,
+    diag_point_kernel<View><<<1, 32, 0, h->stream>>>(V, c, h->fold + 40, p.qdiag_probe1, p.qdiag_probe2,
                                                         h->point);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * 42, cudaMemcpyDeviceToHost, h->stream));
@@ -512,35 +596,69 @@ int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     return SCP_OK;
 }
 
-int scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols) {
-    if (!h || !host_cols) return SCP_EINVAL;
-    if (dtype != SCP_DTYPE_F16 && dtype != SCP_DTYPE_F32 && dtype != SCP_DTYPE_F64) return SCP_EINVAL;
+extern "C" {
+
+int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
+    if (!h || !out) return SCP_EINVAL;
     CK(cudaSetDevice(h->device));
-    ViewF64 V;
-    int rc = current_view(h, &V);
-    if (rc) return rc;
+    if (h->prec == SCP_PREC_FP64) {
+        ViewF64 V{h->X[h->cur ^ 1], h->S, h->N3};
+        return diag_with(h, V, out);
+    }
+    View32C V{h->X32[h->cur ^ 1], h->LO[h->cur ^ 1], h->TLO[h->cur ^ 1], h->S32, h->N3};
+    return diag_with(h, V, out);
+}
+
+}  // extern "C"
+
+// one SFA column of the current state, converted to the snapshot dtype, into
+// the staging buffer (the f16 rule is the reference's, snapshot.cuh)
+template <class View>
+__global__ void snap_col_kernel(View V, int field, int mom, long long n, int dtype, void *out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double v = mom ? V.p(field, i) : V.q(field, i);
+        if (dtype == SCP_DTYPE_F64) ((double *)out)[i] = v;
+        else if (dtype == SCP_DTYPE_F32) ((float *)out)[i] = (float)v;
+        else ((uint16_t *)out)[i] = f64_to_f16_trunc(v);
+    }
+}
+
+template <class View>
+static int snapshot_with(scp_gpu *h, const View &V, int dtype, void *const *host_cols) {
     const int ncols = h->gauged ? 30 : 24;
     const long long n3 = h->N3;
     const int nb = red_blocks(n3);
+    const size_t es = dtype == SCP_DTYPE_F64 ? 8 : (dtype == SCP_DTYPE_F32 ? 4 : 2);
     for (int c = 0; c < ncols; c++) {
         if (!host_cols[c]) return SCP_EINVAL;
         int field, mom;
         sfa_col_source(c, &field, &mom);
-        const double *src = (mom ? V.S : V.X) + (size_t)field * n3;
-        if (dtype == SCP_DTYPE_F64) {
+        if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {   // straight copy of the FP64 column
+            const double *src = (mom ? h->S : h->X[h->cur ^ 1]) + (size_t)field * n3;
             CK(cudaMemcpyAsync(host_cols[c], src, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
-        } else if (dtype == SCP_DTYPE_F32) {
-            cast_f32_kernel<<<nb, kRedThreads, 0, h->stream>>>(src, (float *)h->stage, n3);
-            CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(host_cols[c], h->stage, sizeof(float) * n3, cudaMemcpyDeviceToHost, h->stream));
         } else {
-            cast_f16_kernel<<<nb, kRedThreads, 0, h->stream>>>(src, (uint16_t *)h->stage, n3);
+            snap_col_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, field, mom, n3, dtype, h->stage);
             CK(cudaGetLastError());
-            CK(cudaMemcpyAsync(host_cols[c], h->stage, sizeof(uint16_t) * n3, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaMemcpyAsync(host_cols[c], h->stage, es * n3, cudaMemcpyDeviceToHost, h->stream));
         }
         CK(cudaStreamSynchronize(h->stream));   // staging buffer reused per column
     }
     return SCP_OK;
+}
+
+extern "C" {
+
+int scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols) {
+    if (!h || !host_cols) return SCP_EINVAL;
+    if (dtype != SCP_DTYPE_F16 && dtype != SCP_DTYPE_F32 && dtype != SCP_DTYPE_F64) return SCP_EINVAL;
+    CK(cudaSetDevice(h->device));
+    if (h->prec == SCP_PREC_FP64) {
+        ViewF64 V{h->X[h->cur ^ 1], h->S, h->N3};
+        return snapshot_with(h, V, dtype, host_cols);
+    }
+    View32C V{h->X32[h->cur ^ 1], h->LO[h->cur ^ 1], h->TLO[h->cur ^ 1], h->S32, h->N3};
+    return snapshot_with(h, V, dtype, host_cols);
 }
 
 int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
@@ -552,13 +670,12 @@ int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
     info->cg_iterations = h->cg_iters;
     info->precision_mode = h->prec;
     info->device_bytes = h->dev_bytes;
-    if (h->prec == SCP_PREC_FP64) {
-        info->state_bytes_per_site = 2.0 * 8.0 * h->nf;   // x + w words
-        info->step_bytes_per_site = 2.0 * info->state_bytes_per_site;
-    } else {
-        info->state_bytes_per_site = h->f32.state_bytes_per_site;
-        info->step_bytes_per_site = 2.0 * h->f32.state_bytes_per_site;
-    }
+    // persistent bytes per site the step reads and writes: x and w (FP64);
+    // hi (fp32) + lo (int8 matter, fp32 links) + w (fp32) in FP32C
+    info->state_bytes_per_site = (h->prec == SCP_PREC_FP64)
+                                     ? 2.0 * 8.0 * h->nf
+                                     : 4.0 * h->nf + 12.0 * 1.0 + (h->gauged ? 3.0 * 4.0 : 0.0) + 4.0 * h->nf;
+    info->step_bytes_per_site = 2.0 * info->state_bytes_per_site;
     info->tile_x = kShapes[h->shape].tx;
     info->tile_y = kShapes[h->shape].ty;
     info->seg_len = h->tg.seg;
@@ -585,7 +702,7 @@ void scp_gpu_free(scp_gpu *h) {
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    fp32c_free(&h->f32);
+    cudaFree(h->slab32);
     cudaFree(h->slab);
     cudaFree(h->part);
     cudaFree(h->fold);
@@ -620,6 +737,51 @@ const char *scp_gpu_errstr(int code) {
 const char *scp_gpu_last_cuda_error(void) { return g_cuda_err; }
 
 int scp_gpu_abi_version(void) { return SCP_GPU_ABI_VERSION; }
+
+}  // extern "C"
+
+__global__ void trig_check_kernel(const double *x, int n, double *err) {
+    __shared__ double red[4][256];
+    double e[4] = {0, 0, 0, 0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double s, c, rs, rc;
+        sincos_bounded(x[i], &s, &c);
+        sincos(x[i], &rs, &rc);
+        e[0] = fmax(e[0], fabs(s - rs));
+        e[1] = fmax(e[1], fabs(c - rc));
+        float sf, cf, rsf, rcf;
+        sincos_bounded((float)x[i], &sf, &cf);
+        sincosf((float)x[i], &rsf, &rcf);
+        e[2] = fmax(e[2], (double)fabsf(sf - rsf));
+        e[3] = fmax(e[3], (double)fabsf(cf - rcf));
+    }
+    for (int q = 0; q < 4; q++) red[q][threadIdx.x] = e[q];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double m = 0;
+        for (int t = 0; t < (int)blockDim.x; t++) m = fmax(m, red[threadIdx.x][t]);
+        err[threadIdx.x] = m;
+    }
+}
+
+extern "C" int scp_gpu_check_trig(int n, const double *x, double *err) {
+    if (n < 1 || !x || !err) return SCP_EINVAL;
+    double *dx = nullptr, *de = nullptr;
+    CK(cudaMalloc(&dx, sizeof(double) * n));
+    cudaError_t e = cudaMalloc(&de, sizeof(double) * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        trig_check_kernel<<<1, 256>>>(dx, n, de);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(err, de, sizeof(double) * 4, cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(de);
+    CK(e);
+    return SCP_OK;
+}
+
+extern "C" {
 
 }  // extern "C"
 

@@ -1,0 +1,531 @@
+// step.cuh -- fused leapfrog step for the complex (v66) and gauged (v69)
+// Cosserat Q-ball lattice, one launch per time step, in two precisions:
+//   F64   all state and arithmetic in FP64 (the drop-in mode);
+//   F32C  FP32 state and arithmetic; positions carried as a compensated pair
+//         (hi: fp32, lo: int8 in units of ulp(hi)/256 for the matter fields,
+//         fp32 for the link angles) so the drift accumulates without loss.
+//         F32C evaluates Laplacians, currents and plaquette angles as sums of
+//         neighbour differences, which removes the cancellation that FP32
+//         would otherwise suffer against O(|f|) values.
+//
+// Time integration.  The reference runs kick / drift / force / kick as about
+// ten separate sweeps per step (sfa/sim/scp_sim.c:1583-1716, GPU launch
+// sequence sfa/sim/scp_sim.cu:2971-3208) and keeps an acceleration array.
+// Here the state between launches is (x_{n+1}, w_n) with the half-step
+// momentum w_n = v_n + hdt*a_n, and launch n+1 performs, per site,
+//     a_{n+1} = F(x_{n+1})                    (stencil of x_{n+1})
+//     v_{n+1} = w_n + hdt*a_{n+1}             (reference stage-4 kick)
+//     [v_{n+1} *= damp(r)]                    (reference stage 5, bc_type 0)
+//     w_{n+1} = v_{n+1} + hdt*a_{n+1}         (next step's stage-1 kick)
+//     x_{n+2} = x_{n+1} + dt*w_{n+1}          (next step's drift)
+// with the reference's arithmetic in the reference's order, so no
+// acceleration array exists and each state word is read once and written
+// once per step.  Links follow the same pattern with E and the wrapped drift
+// th += -g*dx*dt*E.  The launch that starts a run (FIRST) reads v_0 instead
+// of w and skips the stage-4 kick; a SYNC launch also stores v_{n+1} and
+// E_{n+1} for diagnostics and snapshots.
+//
+// Data movement.  Persistent CTAs walk work items = (TX x TY) columns in
+// (k, j) times segments of `seg` planes in i.  A CTA streams its column plane
+// by plane through a 3-slot shared-memory ring (plane i, plane i+1, and plane
+// i+2 in flight via cp.async), holding the x(i-1) centre values of its own
+// sites in registers.  Every thread copies its own site; the halo rows and
+// columns (periodic wrap) are spread over the CTA's threads so each thread
+// issues the same copies with no per-field branches.  In gauged mode the link
+// cos/sin and plaquette sines of each plane are computed once per site into
+// shared memory (plus the low-side halo row and column that the backward
+// transports and staples need) instead of once per use.
+#pragma once
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+#include "trig.cuh"
+
+namespace scp {
+
+struct F64 {
+    using T = double;
+    static constexpr bool COMP = false;
+};
+struct F32C {
+    using T = float;
+    static constexpr bool COMP = true;
+};
+
+template <class P>
+struct StepIO {
+    using T = typename P::T;
+    const T *xin;           // NF arrays of N^3: positions x_{n+1} (hi part in F32C)
+    T *xout;                // NF arrays: x_{n+2}
+    const int8_t *loin;     // F32C: scaled low parts of the 12 matter positions
+    int8_t *loout;
+    const float *tloin;     // F32C gauged: low parts of the 3 link angles
+    float *tloout;
+    const T *win;           // NF arrays: w_n (or v_0, E_0 when FIRST)
+    T *wout;                // NF arrays: w_{n+1} (may alias win)
+    T *sout;                // NF arrays: v_{n+1}, E_{n+1} (SYNC only)
+    int *flag;              // nonfinite flag (SYNC only)
+};
+
+// gauge-quantity slots of the per-plane shared array
+enum : int { GQ_C0 = 0, GQ_S0 = 3, GQ_P0 = 6, GQ_N = 9 };
+
+template <class P, int TX, int TY, bool GAUGED>
+struct StepLayout {
+    using T = typename P::T;
+    static constexpr int NF = GAUGED ? 15 : 12;
+    static constexpr int NR = NF + ((P::COMP && GAUGED) ? 3 : 0);   // ring fields (+ link lo parts)
+    static constexpr int PX = TX + 2, PY = TY + 2;
+    static constexpr int PLANE = NR * PY * PX;            // elements per ring slot
+    static constexpr int GX = TX + 1, GY = TY + 1;
+    static constexpr int GPLANE = GQ_N * GY * GX;
+    static constexpr int NT = TX * TY;
+    static constexpr int NHALO = 2 * TX + 2 * TY + (GAUGED ? 2 : 0);
+    static constexpr int HPT = (NHALO + NT - 1) / NT;      // halo sites per thread (max)
+    static constexpr size_t smem_bytes = sizeof(T) * (size_t)(3 * PLANE + (GAUGED ? 2 * GPLANE : 0));
+};
+
+__device__ __forceinline__ void cp_async_elem(double *s, const double *g) { cp_async8(s, g); }
+__device__ __forceinline__ void cp_async_elem(float *s, const float *g) { cp_async4(s, g); }
+
+__device__ __forceinline__ double ldg_t(const double *p) { return __ldg(p); }
+__device__ __forceinline__ float ldg_t(const float *p) { return __ldg(p); }
+
+__device__ __forceinline__ float bf16_to_f(uint16_t h) { return __uint_as_float((uint32_t)h << 16); }
+__device__ __forceinline__ uint16_t f_to_bf16(float f) {
+    return __bfloat16_as_ushort(__float2bfloat16_rn(f));
+}
+
+// Low part of a compensated fp32 pair stored as int8 in units of ulp(hi)/256
+// (|lo| <= ulp(hi)/2 after a two-sum, so the code stays within [-128, 128]).
+// The unit is a power of two taken from hi's exponent; below |hi| ~ 2^-95 it
+// is pinned to the smallest normal.
+__device__ __forceinline__ int lo_unit_exp(float hi) {
+    const int e = (int)((__float_as_uint(hi) >> 23) & 0xFF);
+    return max(e - 31, 1);
+}
+__device__ __forceinline__ float lo_decode(int8_t q, float hi) {
+    return (float)q * __int_as_float(lo_unit_exp(hi) << 23);
+}
+__device__ __forceinline__ int8_t lo_encode(float lo, float hi) {
+    const float r = rintf(lo * __int_as_float((254 - lo_unit_exp(hi)) << 23));
+    return (int8_t)fminf(fmaxf(r, -127.0f), 127.0f);
+}
+// exact sum: s + e = a + b (Knuth two-sum)
+__device__ __forceinline__ void two_sum(float a, float b, float *s, float *e) {
+    const float t = a + b;
+    const float bb = t - a;
+    *e = (a - (t - bb)) + (b - bb);
+    *s = t;
+}
+
+// link wrap into (-pi, pi] (reference: v - 2*pi*rint(v/(2*pi)), scp_sim.c:1647);
+// |v| < 3 never wraps, so the division only runs for the rare large angles
+__device__ __forceinline__ double link_wrap(double v) {
+    if (fabs(v) < 3.0) return v;
+    return wrap_angle(v);
+}
+
+template <class P, int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
+__global__ void __launch_bounds__(TX * TY)
+step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
+    using T = typename P::T;
+    using LY = StepLayout<P, TX, TY, GAUGED>;
+    constexpr int NF = LY::NF, PX = LY::PX, PY = LY::PY, NT = LY::NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *xs = reinterpret_cast<T *>(smem_raw);     // [3][NF][PY][PX]
+    T *gq = xs + 3 * LY::PLANE;                  // [2][GQ_N][GY][GX]
+    constexpr int NR = LY::NR;
+    auto XS = [&](int slot, int f, int r, int col) -> T & {
+        return xs[((slot * NR + f) * PY + r) * PX + col];
+    };
+    auto GQ = [&](int slot, int q, int r, int col) -> T & {
+        return gq[((slot * GQ_N + q) * LY::GY + r) * LY::GX + col];
+    };
+
+    const int N = c.N;
+    const long long N3 = c.N3;
+    const int tid = threadIdx.x;
+    const int tx = tid % TX, ty = tid / TX;
+    const T dt = (T)c.dt, hdt = (T)c.hdt, idx1 = (T)c.idx1, idx2 = (T)c.idx2;
+    const float dt_lo = (float)(c.dt - (double)(float)c.dt);
+
+    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) {
+        const int kt = item % tg.ntx;
+        const int jt = (item / tg.ntx) % tg.nty;
+        const int sg = item / (tg.ntx * tg.nty);
+        const int k0 = kt * TX, j0 = jt * TY;
+        const int i0 = sg * tg.seg, i1 = min(i0 + tg.seg, N);
+        const int k = k0 + tx, j = j0 + ty;
+        const int nk = min(k0 + TX, N) - k0, nj = min(j0 + TY, N) - j0;   // valid extent of the tile
+        const bool act = (tx < nk) && (ty < nj);
+        const int oc = j * N + k;                                          // in-plane offset (act only)
+        const int jlo = wrapi(j0 - 1, N), jhi = wrapi(j0 + nj, N);
+        const int klo = wrapi(k0 - 1, N), khi = wrapi(k0 + nk, N);
+
+        // halo copies of this thread: smem (row, col) and in-plane global offset
+        int h_s[LY::HPT], h_g[LY::HPT], h_nf[LY::HPT];
+#pragma unroll
+        for (int q = 0; q < LY::HPT; q++) {
+            const int h = tid + q * NT;
+            int r = 0, col = 0, gj = 0, gk = 0, nf = 0;
+            if (h < nk) { r = 0; col = h + 1; gj = jlo; gk = k0 + h; nf = NF; }
+            else if (h < 2 * nk) { r = nj + 1; col = h - nk + 1; gj = jhi; gk = k0 + h - nk; nf = NF; }
+            else if (h < 2 * nk + nj) { r = h - 2 * nk + 1; col = 0; gj = j0 + h - 2 * nk; gk = klo; nf = NF; }
+            else if (h < 2 * nk + 2 * nj) { r = h - 2 * nk - nj + 1; col = nk + 1; gj = j0 + h - 2 * nk - nj; gk = khi; nf = NF; }
+            else if (GAUGED && h == 2 * nk + 2 * nj) { r = nj + 1; col = 0; gj = jhi; gk = klo; nf = 3; }
+            else if (GAUGED && h == 2 * nk + 2 * nj + 1) { r = 0; col = nk + 1; gj = jlo; gk = khi; nf = 3; }
+            h_s[q] = r * PX + col;
+            h_g[q] = gj * N + gk;
+            h_nf[q] = nf;
+        }
+        const int c_s = (ty + 1) * PX + tx + 1;
+
+        auto issue_plane = [&](int p, int slot) {
+            const long long pb = (long long)wrapi(p, N) * N * N;
+            T *sbase = xs + slot * LY::PLANE;
+            const T *gbase = io.xin + pb;
+            if (act) {
+#pragma unroll
+                for (int f = 0; f < NF; f++)
+                    cp_async_elem(sbase + f * PY * PX + c_s, gbase + f * N3 + oc);
+                if constexpr (NR > NF) {
+#pragma unroll
+                    for (int f = NF; f < NR; f++)
+                        cp_async_elem(sbase + f * PY * PX + c_s, io.tloin + pb + (f - NF) * N3 + oc);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < LY::HPT; q++) {
+                const int nf = h_nf[q];
+                if (nf == 0) continue;
+                const int f0 = (nf == NF) ? 0 : FTH;   // corners carry only the link angles
+#pragma unroll
+                for (int f = 0; f < NF; f++)
+                    if (f >= f0) cp_async_elem(sbase + f * PY * PX + h_s[q], gbase + f * N3 + h_g[q]);
+                if constexpr (NR > NF) {
+#pragma unroll
+                    for (int f = NF; f < NR; f++)
+                        cp_async_elem(sbase + f * PY * PX + h_s[q], io.tloin + pb + (f - NF) * N3 + h_g[q]);
+                }
+            }
+        };
+
+        // gauge quantities of the plane in slot sc (next plane in slot sp) into gq slot gs
+        auto gauge_plane = [&](int sc, int sp, int gs) {
+            constexpr int NS = LY::GY * LY::GX;
+            for (int s = tid; s < NS; s += NT) {
+                const int r = s / LY::GX, col = s % LY::GX;
+                if ((r == 0 && col == 0) || r > nj || col > nk) continue;
+                const T t0 = XS(sc, FTH + 0, r, col), t1 = XS(sc, FTH + 1, r, col);
+                const T t2 = XS(sc, FTH + 2, r, col);
+                T sn, cs;
+                if (r > 0 && col > 0) {
+                    sincos_bounded(t0, &sn, &cs); GQ(gs, GQ_C0 + 0, r, col) = cs; GQ(gs, GQ_S0 + 0, r, col) = sn;
+                }
+                if (col > 0) {
+                    sincos_bounded(t1, &sn, &cs); GQ(gs, GQ_C0 + 1, r, col) = cs; GQ(gs, GQ_S0 + 1, r, col) = sn;
+                }
+                if (r > 0) {
+                    sincos_bounded(t2, &sn, &cs); GQ(gs, GQ_C0 + 2, r, col) = cs; GQ(gs, GQ_S0 + 2, r, col) = sn;
+                }
+                // plaquette angle th_a(y) + th_b(y+a) - th_a(y+b) - th_b(y), planes (0,1) (1,2) (2,0)
+                if constexpr (NR > NF) {
+                    // FP32C: (th_a(y) - th_a(y+b)) + (th_b(y+a) - th_b(y)), hi and lo parts
+                    auto TL = [&](int sl, int d, int rr, int cc) -> T { return XS(sl, NF + d, rr, cc); };
+                    if (col > 0) {
+                        const T a = (t0 - XS(sc, FTH + 0, r + 1, col)) + (XS(sp, FTH + 1, r, col) - t1);
+                        const T b = (TL(sc, 0, r, col) - TL(sc, 0, r + 1, col)) + (TL(sp, 1, r, col) - TL(sc, 1, r, col));
+                        GQ(gs, GQ_P0 + 0, r, col) = sin_bounded(a + b);
+                    }
+                    {
+                        const T a = (t1 - XS(sc, FTH + 1, r, col + 1)) + (XS(sc, FTH + 2, r + 1, col) - t2);
+                        const T b = (TL(sc, 1, r, col) - TL(sc, 1, r, col + 1)) + (TL(sc, 2, r + 1, col) - TL(sc, 2, r, col));
+                        GQ(gs, GQ_P0 + 1, r, col) = sin_bounded(a + b);
+                    }
+                    if (r > 0) {
+                        const T a = (t2 - XS(sp, FTH + 2, r, col)) + (XS(sc, FTH + 0, r, col + 1) - t0);
+                        const T b = (TL(sc, 2, r, col) - TL(sp, 2, r, col)) + (TL(sc, 0, r, col + 1) - TL(sc, 0, r, col));
+                        GQ(gs, GQ_P0 + 2, r, col) = sin_bounded(a + b);
+                    }
+                } else {
+                    if (col > 0)
+                        GQ(gs, GQ_P0 + 0, r, col) = sin_bounded(t0 + XS(sp, FTH + 1, r, col) - XS(sc, FTH + 0, r + 1, col) - t1);
+                    GQ(gs, GQ_P0 + 1, r, col) = sin_bounded(t1 + XS(sc, FTH + 2, r + 1, col) - XS(sc, FTH + 1, r, col + 1) - t2);
+                    if (r > 0)
+                        GQ(gs, GQ_P0 + 2, r, col) = sin_bounded(t2 + XS(sc, FTH + 0, r, col + 1) - XS(sp, FTH + 2, r, col) - t0);
+                }
+            }
+        };
+
+        __syncthreads();   // previous item finished reading the ring
+        issue_plane(i0 - 1, 0);
+        issue_plane(i0, 1);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        T xm[12];          // x(i-1) at this thread's site, matter fields
+#pragma unroll
+        for (int f = 0; f < 12; f++) xm[f] = act ? XS(0, f, ty + 1, tx + 1) : T(0);
+        if (GAUGED) gauge_plane(0, 1, 1);
+        issue_plane(i0 + 1, 2);
+        cp_async_commit();
+
+        for (int i = i0; i < i1; i++) {
+            const int sc = (i - i0 + 1) % 3, sp = (i - i0 + 2) % 3, sn = (i - i0) % 3;
+            const int gs = (i - i0) & 1, gm = gs ^ 1;
+            cp_async_wait<0>();
+            __syncthreads();
+            if (i + 2 <= i1) issue_plane(i + 2, sn);
+            cp_async_commit();
+            const long long site = (long long)i * N * N + oc;
+            T w[NF];
+            int8_t lo[P::COMP ? 12 : 1];
+            if (act) {
+#pragma unroll
+                for (int f = 0; f < NF; f++) w[f] = ldg_t(io.win + f * N3 + site);
+                if constexpr (P::COMP) {
+#pragma unroll
+                    for (int f = 0; f < 12; f++) lo[f] = (int8_t)__ldg((const char *)(io.loin + f * N3 + site));
+                }
+            }
+            if (GAUGED) {
+                gauge_plane(sc, sp, gs);
+                __syncthreads();
+            }
+            if (!act) continue;
+
+            T acc[12];
+            T K[3] = {T(0), T(0), T(0)};
+            T ctr[NF];
+#pragma unroll
+            for (int f = 0; f < NF; f++) ctr[f] = XS(sc, f, ty + 1, tx + 1);
+            // potential pieces (scp_sim.c:946-958)
+            const T s0 = ctr[FU + 0] * ctr[FU + 0] + ctr[FV + 0] * ctr[FV + 0];
+            const T s1 = ctr[FU + 1] * ctr[FU + 1] + ctr[FV + 1] * ctr[FV + 1];
+            const T s2 = ctr[FU + 2] * ctr[FU + 2] + ctr[FV + 2] * ctr[FV + 2];
+            const T sp3 = s0 * s1 * s2;
+            const T den = T(1) + (T)c.kappa * sp3;
+            const T Vp = T(0.5) * (T)c.mu / (den * den);
+            const T rest[3] = {s1 * s2, s0 * s2, s0 * s1};
+            const T m2 = (T)c.m2, mt2 = (T)c.mtheta2, eta = (T)c.eta;
+
+            if (!GAUGED) {
+                // compute_forces_complex, scp_sim.c:931-994
+                auto nb = [&](int f, int which) -> T {   // 0 ip 1 im 2 jp 3 jm 4 kp 5 km
+                    switch (which) {
+                        case 0: return XS(sp, f, ty + 1, tx + 1);
+                        case 1: return xm[f];
+                        case 2: return XS(sc, f, ty + 2, tx + 1);
+                        case 3: return XS(sc, f, ty, tx + 1);
+                        case 4: return XS(sc, f, ty + 1, tx + 2);
+                        default: return XS(sc, f, ty + 1, tx);
+                    }
+                };
+                auto lap = [&](int f) -> T {
+                    if constexpr (P::COMP) {   // neighbour differences: no cancellation against 6*centre
+                        const T x0 = ctr[f];
+                        return ((nb(f, 0) - x0) + (nb(f, 1) - x0) + (nb(f, 2) - x0) + (nb(f, 3) - x0) +
+                                (nb(f, 4) - x0) + (nb(f, 5) - x0)) * idx2;
+                    } else {
+                        return (nb(f, 0) + nb(f, 1) + nb(f, 2) + nb(f, 3) + nb(f, 4) + nb(f, 5) - T(6) * ctr[f]) * idx2;
+                    }
+                };
+                auto curl = [&](int g0, int a) -> T {
+                    if (a == 0) return (nb(g0 + 2, 2) - nb(g0 + 2, 3) - nb(g0 + 1, 4) + nb(g0 + 1, 5)) * idx1;
+                    if (a == 1) return (nb(g0 + 0, 4) - nb(g0 + 0, 5) - nb(g0 + 2, 0) + nb(g0 + 2, 1)) * idx1;
+                    return (nb(g0 + 1, 0) - nb(g0 + 1, 1) - nb(g0 + 0, 2) + nb(g0 + 0, 3)) * idx1;
+                };
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    T x = ctr[FU + a];
+                    acc[FU + a] = lap(FU + a) - m2 * x - T(2) * Vp * x * rest[a] + eta * curl(FTU, a);
+                    x = ctr[FV + a];
+                    acc[FV + a] = lap(FV + a) - m2 * x - T(2) * Vp * x * rest[a] + eta * curl(FTV, a);
+                    x = ctr[FTU + a];
+                    acc[FTU + a] = lap(FTU + a) - mt2 * x + eta * curl(FU, a);
+                    x = ctr[FTV + a];
+                    acc[FTV + a] = lap(FTV + a) - mt2 * x + eta * curl(FV, a);
+                }
+            } else {
+                // compute_forces_complex_gauge pass C, scp_sim.c:1112-1262
+                // complex fields q=0..2 Phi_a, q=3..5 Theta_a
+                const T fu[6] = {ctr[FU], ctr[FU + 1], ctr[FU + 2], ctr[FTU], ctr[FTU + 1], ctr[FTU + 2]};
+                const T fv[6] = {ctr[FV], ctr[FV + 1], ctr[FV + 2], ctr[FTV], ctr[FTV + 1], ctr[FTV + 2]};
+                T lapU[6], lapV[6];
+                T DcU[3][6], DcV[3][6];
+                T TRp_[3][3], TIp_[3][3];   // forward transports of Phi
+                T tup[3][3], tvp[3][3];     // raw Theta at x+d (current and seagull)
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    T cP, sP, cM, sM;
+                    cP = GQ(gs, GQ_C0 + d, ty + 1, tx + 1);
+                    sP = GQ(gs, GQ_S0 + d, ty + 1, tx + 1);
+                    if (d == 0) { cM = GQ(gm, GQ_C0, ty + 1, tx + 1); sM = GQ(gm, GQ_S0, ty + 1, tx + 1); }
+                    else if (d == 1) { cM = GQ(gs, GQ_C0 + 1, ty, tx + 1); sM = GQ(gs, GQ_S0 + 1, ty, tx + 1); }
+                    else { cM = GQ(gs, GQ_C0 + 2, ty + 1, tx); sM = GQ(gs, GQ_S0 + 2, ty + 1, tx); }
+#pragma unroll
+                    for (int q = 0; q < 6; q++) {
+                        const int fre = q < 3 ? FU + q : FTU + q - 3;
+                        const int fim = q < 3 ? FV + q : FTV + q - 3;
+                        T up, vp, um, vm;
+                        if (d == 0) {
+                            up = XS(sp, fre, ty + 1, tx + 1); vp = XS(sp, fim, ty + 1, tx + 1);
+                            um = xm[fre]; vm = xm[fim];
+                        } else if (d == 1) {
+                            up = XS(sc, fre, ty + 2, tx + 1); vp = XS(sc, fim, ty + 2, tx + 1);
+                            um = XS(sc, fre, ty, tx + 1);     vm = XS(sc, fim, ty, tx + 1);
+                        } else {
+                            up = XS(sc, fre, ty + 1, tx + 2); vp = XS(sc, fim, ty + 1, tx + 2);
+                            um = XS(sc, fre, ty + 1, tx);     vm = XS(sc, fim, ty + 1, tx);
+                        }
+                        const T TRp = cP * up - sP * vp, TIp = cP * vp + sP * up;
+                        const T TRm = cM * um + sM * vm, TIm = cM * vm - sM * um;
+                        if constexpr (P::COMP) {   // accumulate (transported - centre) differences
+                            const T cu = fu[q], cv = fv[q];
+                            if (d == 0) { lapU[q] = (TRp - cu) + (TRm - cu); lapV[q] = (TIp - cv) + (TIm - cv); }
+                            else { lapU[q] = lapU[q] + (TRp - cu) + (TRm - cu); lapV[q] = lapV[q] + (TIp - cv) + (TIm - cv); }
+                        } else {
+                            if (d == 0) { lapU[q] = TRp + TRm; lapV[q] = TIp + TIm; }
+                            else { lapU[q] = lapU[q] + TRp + TRm; lapV[q] = lapV[q] + TIp + TIm; }
+                        }
+                        DcU[d][q] = (TRp - TRm) * idx1;
+                        DcV[d][q] = (TIp - TIm) * idx1;
+                        if (q < 3) { TRp_[d][q] = TRp; TIp_[d][q] = TIp; }
+                        else { tup[d][q - 3] = up; tvp[d][q - 3] = vp; }
+                    }
+                    // lattice current J (scp_sim.c:1232-1249); the Theta transports are
+                    // recomputed from the cached raw neighbours to keep the live set small
+                    T Jg = T(0);
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        const T TIt = cP * tvp[d][a] + sP * tup[d][a];
+                        const T TRt = cP * tup[d][a] - sP * tvp[d][a];
+                        if constexpr (P::COMP) {
+                            // u*TI - v*TR = u*(TI - v) - v*(TR - u): differences of neighbouring
+                            // values instead of a difference of two O(|f|^2) products
+                            Jg += fu[a] * (TIp_[d][a] - fv[a]) - fv[a] * (TRp_[d][a] - fu[a]);
+                            Jg += fu[3 + a] * (TIt - fv[3 + a]) - fv[3 + a] * (TRt - fu[3 + a]);
+                        } else {
+                            Jg += fu[a] * TIp_[d][a] - fv[a] * TRp_[d][a];
+                            Jg += fu[3 + a] * TIt - fv[3 + a] * TRt;
+                        }
+                    }
+                    const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+                    const T WpR1 = cP * fu[d2] + sP * fv[d2], WpI1 = cP * fv[d2] - sP * fu[d2];
+                    const T WpR2 = cP * fu[d1] + sP * fv[d1], WpI2 = cP * fv[d1] - sP * fu[d1];
+                    const T T12 = (fu[3 + d1] * TIp_[d][d2] - fv[3 + d1] * TRp_[d][d2])
+                                + (tup[d][d1] * WpI1 - tvp[d][d1] * WpR1);
+                    const T T21 = (fu[3 + d2] * TIp_[d][d1] - fv[3 + d2] * TRp_[d][d1])
+                                + (tup[d][d2] * WpI2 - tvp[d][d2] * WpR2);
+                    K[d] = (T)c.inva * Jg - T(0.5) * eta * (T12 - T21);   // Jlat; staple added below
+                }
+                // staples (scp_sim.c:1214-1220)
+                const T P0 = GQ(gs, GQ_P0 + 0, ty + 1, tx + 1), P1 = GQ(gs, GQ_P0 + 1, ty + 1, tx + 1);
+                const T P2 = GQ(gs, GQ_P0 + 2, ty + 1, tx + 1);
+                const T st0 = (P0 - GQ(gs, GQ_P0 + 0, ty, tx + 1)) - (P2 - GQ(gs, GQ_P0 + 2, ty + 1, tx));
+                const T st1 = -(P0 - GQ(gm, GQ_P0 + 0, ty + 1, tx + 1)) + (P1 - GQ(gs, GQ_P0 + 1, ty + 1, tx));
+                const T st2 = (P2 - GQ(gm, GQ_P0 + 2, ty + 1, tx + 1)) - (P1 - GQ(gs, GQ_P0 + 1, ty, tx + 1));
+                const T stp = (T)c.stp, gg = (T)c.g;
+                K[0] = stp * st0 + gg * K[0];
+                K[1] = stp * st1 + gg * K[1];
+                K[2] = stp * st2 + gg * K[2];
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    const int d1 = (a + 1) % 3, d2 = (a + 2) % 3;
+                    const T reDxT = DcU[d1][3 + d2] - DcU[d2][3 + d1];
+                    const T imDxT = DcV[d1][3 + d2] - DcV[d2][3 + d1];
+                    const T reDxP = DcU[d1][d2] - DcU[d2][d1];
+                    const T imDxP = DcV[d1][d2] - DcV[d2][d1];
+                    const T c6 = P::COMP ? T(0) : T(6);   // FP32C accumulated differences already
+                    const T lUP = (lapU[a] - c6 * fu[a]) * idx2;
+                    const T lVP = (lapV[a] - c6 * fv[a]) * idx2;
+                    const T lUT = (lapU[3 + a] - c6 * fu[3 + a]) * idx2;
+                    const T lVT = (lapV[3 + a] - c6 * fv[3 + a]) * idx2;
+                    acc[FU + a] = lUP - m2 * fu[a] - T(2) * Vp * fu[a] * rest[a] + eta * reDxT;
+                    acc[FV + a] = lVP - m2 * fv[a] - T(2) * Vp * fv[a] * rest[a] + eta * imDxT;
+                    acc[FTU + a] = lUT - mt2 * fu[3 + a] + eta * reDxP;
+                    acc[FTV + a] = lVT - mt2 * fv[3 + a] + eta * imDxP;
+                }
+            }
+
+            // kicks, damping, drift (scp_sim.c:1591-1715, fused)
+            T dmp = T(1);
+            if (DAMP && !FIRST) {
+                const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
+                const double r = sqrt(x * x + y * y + z * z);
+                const double Rd = c.L - c.damp_width;
+                if (r > Rd) {
+                    double sc2 = (r - Rd) / c.damp_width;
+                    if (sc2 > 1) sc2 = 1;
+                    dmp = (T)(1.0 - c.damp_rate * sc2 * sc2);
+                }
+            }
+            bool bad = false;
+#pragma unroll
+            for (int f = 0; f < 12; f++) {
+                T v = FIRST ? w[f] : w[f] + hdt * acc[f];
+                if (DAMP && !FIRST) v *= dmp;
+                T wn, xn;
+                if constexpr (P::COMP) {
+                    // w_{n+1} = w_n + dt*a in one rounding (no damping), dt as an fp32 pair;
+                    // compensated drift (hi, lo) += dt*w_{n+1}
+                    if (DAMP || FIRST) wn = v + hdt * acc[f];
+                    else wn = fmaf((float)c.dt, acc[f], fmaf(dt_lo, acc[f], w[f]));
+                    const float y = fmaf((float)c.dt, wn, fmaf(dt_lo, wn, lo_decode(lo[f], ctr[f])));
+                    float e;
+                    two_sum(ctr[f], y, &xn, &e);
+                    io.loout[f * N3 + site] = lo_encode(e, xn);
+                } else {
+                    wn = v + hdt * acc[f];
+                    xn = ctr[f] + dt * wn;
+                }
+                st_cs(io.xout + f * N3 + site, xn);
+                io.wout[f * N3 + site] = wn;
+                if (SYNC && !FIRST) {
+                    st_cs(io.sout + f * N3 + site, v);
+                    bad |= !isfinite(xn) || !isfinite(v);
+                }
+            }
+            if (GAUGED) {
+                const T gad = (T)c.gad;
+#pragma unroll
+                for (int d = 0; d < 3; d++) {
+                    T E = FIRST ? w[FTH + d] : w[FTH + d] + hdt * K[d];
+                    if (DAMP && !FIRST) E *= dmp;
+                    T Eh, th;
+                    if constexpr (P::COMP) {
+                        if (DAMP || FIRST) Eh = E + hdt * K[d];
+                        else Eh = fmaf((float)c.dt, K[d], fmaf(dt_lo, K[d], w[FTH + d]));
+                        const float gad_lo = (float)(c.gad - (double)(float)c.gad);
+                        const float y = fmaf(gad, Eh, fmaf(gad_lo, Eh, XS(sc, NR - 3 + d, ty + 1, tx + 1)));
+                        float lnew;
+                        two_sum(ctr[FTH + d], y, &th, &lnew);
+                        if (fabsf(th) > 3.0f) {   // wrap by 2 pi, carried as an fp32 pair
+                            const float kq = rintf(th * 0.159154943091895336f);
+                            float t1, e1;
+                            two_sum(th, -kq * 6.28318548202514648f, &t1, &e1);   // 2 pi (fp32) times |kq| <= 1
+                            lnew = lnew + e1 + kq * 1.74845553e-7f;              // 2 pi = 6.2831855f - 1.748e-7
+                            two_sum(t1, lnew, &th, &lnew);
+                        }
+                        io.tloout[d * N3 + site] = lnew;
+                    } else {
+                        Eh = E + hdt * K[d];
+                        th = link_wrap(ctr[FTH + d] + gad * Eh);
+                    }
+                    st_cs(io.xout + (FTH + d) * N3 + site, th);
+                    io.wout[(FTH + d) * N3 + site] = Eh;
+                    if (SYNC && !FIRST) {
+                        st_cs(io.sout + (FTH + d) * N3 + site, E);
+                        bad |= !isfinite(E) || !isfinite(th);
+                    }
+                }
+            }
+            if (SYNC && bad) atomicOr(io.flag, 1);
+#pragma unroll
+            for (int f = 0; f < 12; f++) xm[f] = ctr[f];
+        }
+    }
+}
+
+}  // namespace scp

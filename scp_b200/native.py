@@ -19,7 +19,7 @@ EXPORTS = (
     "scp_gpu_init", "scp_gpu_init_device", "scp_gpu_step", "scp_gpu_sync", "scp_gpu_diag",
     "scp_gpu_snapshot", "scp_gpu_get_info", "scp_gpu_time_steps", "scp_gpu_stream",
     "scp_gpu_free", "scp_gpu_errstr", "scp_gpu_last_cuda_error", "scp_gpu_abi_version",
-    "scp_gpu_diag_noalloc",
+    "scp_gpu_diag_noalloc", "scp_gpu_check_trig",
 )
 
 DIAG_NSLOTS = 40
@@ -81,6 +81,7 @@ def lib() -> ctypes.CDLL:
     L.scp_gpu_errstr.argtypes = [ctypes.c_int]
     L.scp_gpu_errstr.restype = ctypes.c_char_p
     L.scp_gpu_last_cuda_error.restype = ctypes.c_char_p
+    L.scp_gpu_check_trig.argtypes = [ctypes.c_int, vp, vp]
     L.scp_gpu_diag_noalloc.argtypes = [ctypes.POINTER(CParams), ctypes.POINTER(vp), ctypes.c_double, vp,
                                        ctypes.POINTER(DiagOut)]
     _lib = L

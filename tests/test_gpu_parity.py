@@ -175,3 +175,28 @@ def test_gpu_gauged_64_1000_parity(gpu):
     assert max(gmax) < 1e-10
     r = o.diag()
     assert abs(d["E_total"] - r[8]) < 1e-11 * abs(r[8])
+
+
+@pytest.mark.parametrize("gauged", [False, True])
+def test_fp32c_tracks_fp64(gpu, gauged):
+    """FP32-compensated mode against FP64 on the same seed: field L2 error
+    and relative energy drift stay small over 400 steps."""
+    from scp_b200 import PREC_FP32C
+    if gauged:
+        st = seeds.make_state("c1", seeds.params_for("c1", N=48, L=11.75))
+    else:
+        st = seeds.make_state("c0", seeds.params_for("c0", N=48, L=11.75))
+    p64 = st.params
+    p32 = Params(**{**p64.__dict__, "precision": PREC_FP32C})
+    with Simulation(p64, st.cols()) as a, Simulation(p32, st.cols()) as b:
+        e0a, e0b = a.diag()["E_total"], b.diag()["E_total"]
+        a.step(400)
+        b.step(400)
+        da, db = a.diag(), b.diag()
+        A, B = a.snapshot(), b.snapshot()
+    assert abs(e0a - e0b) <= 1e-6 * abs(e0a)
+    worst = max(rel_l2(B[c], A[c]) for c in range(len(A)) if np.linalg.norm(A[c]) > 1e-3 * np.sqrt(len(A[c])))
+    assert worst < 1e-5, worst
+    assert abs(db["E_total"] - da["E_total"]) <= 1e-6 * abs(da["E_total"])
+    if gauged:
+        assert db["gauss_max"] < 1e-5
