@@ -172,6 +172,69 @@ int  scp_gpu_check_trig(int n, const double *x, double *err);
 int  scp_gpu_diag_noalloc(const scp_gpu_params *p, const double *const *dev_cols, double G_offset,
                           void *stream, scp_gpu_diag_out *out);
 
+/* ------------------------------------------------------------------ serving
+ *
+ * Continuous-batching server for many independent simulations on one GPU
+ * (no counterpart in the reference, which runs one simulation per process).
+ * Requests of any grid size are queued by scp_srv_submit, admitted by
+ * scp_srv_poll while active slots (max_active) and the HBM budget allow,
+ * and advanced together: every poll runs one chunk of chunk_steps steps in
+ * which one persistent launch per step advances every active request,
+ * replayed as a captured CUDA graph.  Requests that arrive while others run
+ * join at the next chunk boundary; a finished request is retired at the end
+ * of its chunk (final diagnostics, optional snapshot into the caller's
+ * out_cols, device memory freed).  The tile shape of each (grid size, gauge
+ * mode, precision) is picked by timing every compiled shape once (autotune).
+ * A request's state evolves exactly as it would through scp_gpu_step. */
+typedef struct scp_srv scp_srv;
+
+typedef struct {
+    int32_t device;
+    int32_t max_active;        /* concurrently admitted requests (<= 256 per group) */
+    int64_t mem_budget_bytes;  /* device bytes for admitted state; 0 = unlimited */
+    int32_t chunk_steps;       /* steps per poll (graph length) */
+    int32_t use_graph;         /* 1: replay chunks as a CUDA graph */
+    int32_t autotune;          /* 1: time the tile shapes per grid size */
+    int32_t admit_per_poll;    /* requests initialised per poll (0 = no cap); a cap lets
+                                  the first chunks start while later requests load */
+} scp_srv_config;
+
+#define SCP_SRV_QUEUED 0
+#define SCP_SRV_ACTIVE 1
+#define SCP_SRV_DONE   2
+#define SCP_SRV_FAILED 3
+
+typedef struct {
+    int32_t state, rc;
+    double  t_submit, t_admit, t_done;   /* host monotonic seconds */
+    int64_t nsteps;
+    int32_t N, tile_variant;
+} scp_srv_request_info;
+
+typedef struct {
+    int64_t step, chunks, mem_in_use;
+    int32_t n_active, n_queued, n_groups;
+    double  t_admit, t_autotune, t_run, t_retire;   /* host seconds spent per phase */
+} scp_srv_stats_t;
+
+int  scp_srv_create(const scp_srv_config *cfg, scp_srv **out);
+/* Queue a request.  The columns are copied, so host_cols may be released on
+ * return; scp_srv_submit_borrowed instead keeps the pointers, which must stay
+ * valid until the request is admitted (state no longer SCP_SRV_QUEUED).
+ * out_cols (optional, NULL for none) receive the final snapshot in out_dtype
+ * and must stay valid until the request is done. */
+int  scp_srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *host_cols, int64_t nsteps,
+                    void *const *out_cols, int out_dtype, int64_t *id_out);
+int  scp_srv_submit_borrowed(scp_srv *s, const scp_gpu_params *p, const double *const *host_cols, int64_t nsteps,
+                             void *const *out_cols, int out_dtype, int64_t *id_out);
+/* Admit, run one chunk, retire; reports the active and queued counts. */
+int  scp_srv_poll(scp_srv *s, int *n_active, int *n_queued);
+int  scp_srv_status(scp_srv *s, int64_t id, scp_srv_request_info *info);
+/* Final diagnostics of a finished request (SCP_EBUSY while queued/active). */
+int  scp_srv_result(scp_srv *s, int64_t id, scp_gpu_diag_out *diag);
+int  scp_srv_stats(scp_srv *s, scp_srv_stats_t *st);
+void scp_srv_free(scp_srv *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,7 +68,13 @@ __global__ void __launch_bounds__(kRedThreads) gauss_rhs_kernel(GaussArgs a, dou
 }
 
 // CG scalars kept on the device
-enum : int { CG_GBAR = 0, CG_GMAX0, CG_RZ, CG_PAP, CG_ALPHA, CG_BETA, CG_XBAR, CG_RMAX, CG_RZ2, CG_N };
+enum : int { CG_GBAR = 0, CG_GMAX0, CG_RZ, CG_PAP, CG_ALPHA, CG_BETA, CG_XBAR, CG_RMAX, CG_RZ2, CG_TOL, CG_DONE,
+             CG_IT, CG_N };
+
+// The iteration loop runs on the device in batches: every sweep returns at
+// once when CG_DONE is set (residual below tolerance or iteration cap), so the
+// host only checks after a batch and the iterations taken are exactly those
+// of the reference's while (rmax > tol && it < itmax) loop.
 
 // b -= gbar; r = p = b; chi = 0; partial sum r^2, max |b|
 __global__ void __launch_bounds__(kRedThreads) cg_start_kernel(long long n3, double *b, double *r, double *p,
@@ -88,9 +94,10 @@ __global__ void __launch_bounds__(kRedThreads) cg_start_kernel(long long n3, dou
 
 // Ap = -lap(p); partial sum p.Ap
 __global__ void __launch_bounds__(kRedThreads) cg_apply_kernel(int N, long long n3, double idx2, const double *p,
-                                                               double *Ap, double *part) {
+                                                               double *Ap, double *part, const double *cg) {
     __shared__ double scratch[32];
     double S[1] = {0.0}, M[1] = {0.0};
+    if (cg[CG_DONE] != 0.0) return;
     const long long NN = (long long)N * N;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
          idx += (long long)gridDim.x * blockDim.x) {
@@ -112,6 +119,7 @@ __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long long n3, do
                                                                 const double *Ap, const double *cg, double *part) {
     __shared__ double scratch[3 * 32];
     double S[2] = {0.0, 0.0}, M[1] = {0.0};
+    if (cg[CG_DONE] != 0.0) return;
     const double alpha = cg[CG_ALPHA];
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
          idx += (long long)gridDim.x * blockDim.x) {
@@ -127,6 +135,7 @@ __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long long n3, do
 
 // x -= xbar; p = r + beta p
 __global__ void cg_dir_kernel(long long n3, double *x, const double *r, double *p, const double *cg) {
+    if (cg[CG_DONE] != 0.0) return;
     const double xbar = cg[CG_XBAR], beta = cg[CG_BETA];
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
          idx += (long long)gridDim.x * blockDim.x) {
@@ -136,18 +145,32 @@ __global__ void cg_dir_kernel(long long n3, double *x, const double *r, double *
 }
 
 // single-thread scalar bookkeeping between CG sweeps
-__global__ void cg_scalar_kernel(int stage, double n3d, const double *fold, double *cg) {
+__global__ void cg_scalar_kernel(int stage, double n3d, const double *fold, double *cg, int itmax) {
     if (threadIdx.x | blockIdx.x) return;
     switch (stage) {
         case 0: cg[CG_GBAR] = fold[0] / n3d; break;                          // gbar
-        case 1: cg[CG_RZ] = fold[0]; cg[CG_GMAX0] = fold[1]; cg[CG_RMAX] = fold[1]; break;
-        case 2: cg[CG_PAP] = fold[0]; cg[CG_ALPHA] = cg[CG_RZ] / fold[0]; break;
+        case 1:
+            cg[CG_RZ] = fold[0]; cg[CG_GMAX0] = fold[1]; cg[CG_RMAX] = fold[1];
+            cg[CG_TOL] = 1e-13 * fmax(1.0, fold[1]);
+            cg[CG_IT] = 0.0;
+            cg[CG_DONE] = (fold[1] > cg[CG_TOL]) ? 0.0 : 1.0;
+            break;
+        case 2:
+            if (cg[CG_DONE] != 0.0) return;
+            cg[CG_PAP] = fold[0]; cg[CG_ALPHA] = cg[CG_RZ] / fold[0];
+            break;
         case 3:
+            if (cg[CG_DONE] != 0.0) return;
             cg[CG_RZ2] = fold[0];
             cg[CG_XBAR] = fold[1] / n3d;
             cg[CG_BETA] = fold[0] / cg[CG_RZ];
             cg[CG_RZ] = fold[0];
             cg[CG_RMAX] = fold[2];
+            break;
+        case 4:   // end of an iteration: count it and decide whether to go on
+            if (cg[CG_DONE] != 0.0) return;
+            cg[CG_IT] += 1.0;
+            if (!(cg[CG_RMAX] > cg[CG_TOL]) || cg[CG_IT] >= (double)itmax) cg[CG_DONE] = 1.0;
             break;
     }
 }

@@ -27,6 +27,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 
 using namespace scp;
@@ -146,7 +147,7 @@ struct scp_gpu {
     // scratch
     double *part = nullptr, *fold = nullptr, *cg = nullptr, *point = nullptr;
     int *flag = nullptr;
-    double *h_small = nullptr;   // pinned
+    double h_small[64];          // host landing area of the small device-to-host reads
     void *stage = nullptr;       // snapshot down-conversion staging (N3 doubles)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // launch geometry
@@ -309,6 +310,9 @@ static GaussArgs gauss_args(scp_gpu *h, const double *X, double *S) {
 }
 
 // net_charge_check + init_gauss_project on the state in (X, S)
+constexpr int kCgItMax = 20000;   // init_gauss_project's iteration cap (scp_sim.c:2337)
+constexpr int kCgBatch = 32;      // iterations enqueued between host checks
+
 static int gauss_startup(scp_gpu *h, const double *X, double *S) {
     const long long n3 = h->N3;
     const int nb = red_blocks(n3);
@@ -330,32 +334,30 @@ static int gauss_startup(scp_gpu *h, const double *X, double *S) {
     const double n3d = (double)n3, idx2 = 1.0 / (h->p.dx * h->p.dx);
     gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, b, h->part);
     fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(0, n3d, h->fold, h->cg);
+    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(0, n3d, h->fold, h->cg, kCgItMax);
     cg_start_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, b, r, p, x, h->cg, h->part);
     fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(1, n3d, h->fold, h->cg);
+    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(1, n3d, h->fold, h->cg, kCgItMax);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h->h_small, h->cg, sizeof(double) * CG_N, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaStreamSynchronize(h->stream));
-    const double tol = 1e-13 * fmax(1.0, h->h_small[CG_GMAX0]);
-    double rmax = h->h_small[CG_RMAX];
-    int it = 0;
-    while (rmax > tol && it < 20000) {
-        cg_apply_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->N, n3, idx2, p, Ap, h->part);
-        fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-        cg_scalar_kernel<<<1, 1, 0, h->stream>>>(2, n3d, h->fold, h->cg);
-        cg_update_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, p, Ap, h->cg, h->part);
-        fold_partials_kernel<2, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-        cg_scalar_kernel<<<1, 1, 0, h->stream>>>(3, n3d, h->fold, h->cg);
-        cg_dir_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, p, h->cg);
+    // iterations in device-checked batches (see gauss.cuh)
+    for (int batch = 0;; batch++) {
+        for (int k = 0; k < kCgBatch; k++) {
+            cg_apply_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->N, n3, idx2, p, Ap, h->part, h->cg);
+            fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+            cg_scalar_kernel<<<1, 1, 0, h->stream>>>(2, n3d, h->fold, h->cg, kCgItMax);
+            cg_update_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, p, Ap, h->cg, h->part);
+            fold_partials_kernel<2, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+            cg_scalar_kernel<<<1, 1, 0, h->stream>>>(3, n3d, h->fold, h->cg, kCgItMax);
+            cg_dir_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, p, h->cg);
+            cg_scalar_kernel<<<1, 1, 0, h->stream>>>(4, n3d, h->fold, h->cg, kCgItMax);
+        }
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(h->h_small, h->cg + CG_RMAX, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(h->h_small, h->cg, sizeof(double) * CG_N, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        rmax = h->h_small[0];
-        it++;
+        if (h->h_small[CG_DONE] != 0.0) break;
     }
-    h->cg_iters = it;
-    if (rmax > tol) {
+    h->cg_iters = (int)h->h_small[CG_IT];
+    if (h->h_small[CG_RMAX] > h->h_small[CG_TOL]) {
         cudaFreeAsync(tmp, h->stream);
         return SCP_EGAUSS;
     }
@@ -371,15 +373,30 @@ static int gauss_startup(scp_gpu *h, const double *X, double *S) {
 
 // ---------------------------------------------------------------- lifecycle
 
+// Device memory comes from the device's default stream-ordered pool, kept
+// instead of returned to the driver on synchronisation, so that handles made
+// and freed at a high rate (the server) neither block nor re-map memory.
+static std::once_flag g_pool_once[64];
+static void keep_pool(int dev) {
+    if (dev < 0 || dev >= 64) return;
+    std::call_once(g_pool_once[dev], [dev] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    });
+}
+
 static int alloc_common(scp_gpu *h) {
+    keep_pool(h->device);
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-    CK(cudaMalloc(&h->part, sizeof(double) * kRedMaxBlocks * 32));
-    CK(cudaMalloc(&h->fold, sizeof(double) * 64));
-    CK(cudaMalloc(&h->cg, sizeof(double) * 16));
-    CK(cudaMalloc(&h->point, sizeof(double) * 8));
-    CK(cudaMalloc(&h->flag, sizeof(int)));
+    CK(cudaMallocAsync(&h->part, sizeof(double) * kRedMaxBlocks * 32, h->stream));
+    CK(cudaMallocAsync(&h->fold, sizeof(double) * 64, h->stream));
+    CK(cudaMallocAsync(&h->cg, sizeof(double) * 16, h->stream));
+    CK(cudaMallocAsync(&h->point, sizeof(double) * 8, h->stream));
+    CK(cudaMallocAsync(&h->flag, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
-    CK(cudaMallocHost(&h->h_small, sizeof(double) * 64));
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
     h->dev_bytes += sizeof(double) * (kRedMaxBlocks * 32 + 64 + 16 + 8);
@@ -398,7 +415,7 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     // FP64 slab: X[0] = x_0 and S = v_0 stage the initial state in both modes;
     // FP64 mode also keeps X[1] and W in it
     const int nblk = (h->prec == SCP_PREC_FP64) ? 4 : 2;
-    CK(cudaMalloc(&h->slab, nblk * blk));
+    CK(cudaMallocAsync(&h->slab, nblk * blk, h->stream));
     h->dev_bytes += nblk * blk;
     h->X[0] = h->slab;
     h->S = h->slab + nel;
@@ -419,7 +436,7 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     }
     if (h->gauged && (rc = gauss_startup(h, h->X[0], h->S))) return rc;
     if ((rc = setup_launch(h))) return rc;
-    CK(cudaMalloc(&h->stage, sizeof(double) * n3));
+    CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
     h->dev_bytes += sizeof(double) * n3;
     h->cur = 0;
     if (h->prec == SCP_PREC_FP64) return launch_step(h, true, false);
@@ -427,7 +444,7 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     // (int8, 12 arrays), TLO[0..1] (fp32, 3 arrays, gauged only)
     const size_t bf = round256(sizeof(float) * nel), bl = round256((size_t)12 * n3);
     const size_t bt = h->gauged ? round256(sizeof(float) * 3 * (size_t)n3) : 0;
-    CK(cudaMalloc(&h->slab32, 4 * bf + 2 * bl + 2 * bt));
+    CK(cudaMallocAsync(&h->slab32, 4 * bf + 2 * bl + 2 * bt, h->stream));
     h->dev_bytes += 4 * bf + 2 * bl + 2 * bt;
     char *b = (char *)h->slab32;
     h->X32[0] = (float *)b; b += bf;
@@ -445,8 +462,7 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     CK(cudaGetLastError());
     if ((rc = launch_step(h, true, false))) return rc;
     // the FP64 staging is no longer needed: FP32C diagnostics read hi+lo directly
-    CK(cudaStreamSynchronize(h->stream));
-    CK(cudaFree(h->slab));
+    CK(cudaFreeAsync(h->slab, h->stream));
     h->dev_bytes -= nblk * blk;
     h->slab = nullptr;
     h->X[0] = h->X[1] = h->W = h->S = nullptr;
@@ -701,16 +717,12 @@ void *scp_gpu_stream(scp_gpu *h) { return h ? (void *)h->stream : nullptr; }
 void scp_gpu_free(scp_gpu *h) {
     if (!h) return;
     cudaSetDevice(h->device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
-    cudaFree(h->slab32);
-    cudaFree(h->slab);
-    cudaFree(h->part);
-    cudaFree(h->fold);
-    cudaFree(h->cg);
-    cudaFree(h->point);
-    cudaFree(h->flag);
-    cudaFree(h->stage);
-    if (h->h_small) cudaFreeHost(h->h_small);
+    if (h->stream) {
+        void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->stage};
+        for (void *b : bufs)
+            if (b) cudaFreeAsync(b, h->stream);
+        cudaStreamSynchronize(h->stream);
+    }
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -937,3 +949,5 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     if (!isfinite(o[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
     return SCP_OK;
 }
+
+#include "serve.cuh"

@@ -1,0 +1,551 @@
+// serve.cuh -- continuous-batching request server (C ABI scp_srv_*).
+//
+// Included at the end of scp_gpu.cu: a request is an ordinary scp_gpu handle
+// (its init does the upload, Gauss projection, precision conversion and the
+// first half step), but once admitted its steps are taken by the server's
+// multi-request launches instead of scp_gpu_step:
+//
+//   submit  -> queued (host copy of the columns; caller buffers may go)
+//   poll    -> admit queued requests while active slots and the HBM budget
+//              allow; rewrite the device request tables; replay one chunk of
+//              K steps as a CUDA graph (one persistent launch per step per
+//              group of requests sharing precision, gauge mode and tile
+//              shape; groups run on forked streams); retire finished
+//              requests (diagnostics, optional snapshot, free)
+//   result  -> final diagnostics (+ snapshot written at retirement)
+//
+// Requests that arrive while others run are admitted at the next chunk
+// boundary, so the work of old and new requests overlaps on the device.
+// The tile shape of each (grid size, gauge mode, precision) is chosen once by
+// timing every compiled shape on a scratch state (autotune).
+#pragma once
+
+#include <chrono>
+#include <deque>
+#include <map>
+#include <memory>
+#include <tuple>
+#include <vector>
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct SrvReq {
+    int64_t id = 0;
+    scp_gpu_params p{};
+    std::vector<double> cols;     // staged input, released at admission
+    std::vector<const double *> borrowed;   // caller's columns (scp_srv_submit_borrowed)
+    int64_t nsteps = 0;
+    int state = 0;                // SCP_SRV_QUEUED / ACTIVE / DONE / FAILED
+    int rc = 0;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    long long s0 = 0, s1 = 0;
+    scp_gpu *h = nullptr;
+    int64_t bytes = 0;
+    int group = -1;
+    scp_gpu_diag_out diag{};
+    void *const *out_cols = nullptr;
+    int out_dtype = SCP_DTYPE_F64;
+};
+
+struct SrvGroup {
+    int prec = 0, gauged = 0, shape = 1;
+    int grid = 0, threads = 0;
+    size_t smem = 0;
+    void *d_tab = nullptr;        // ReqTable<P> on the device
+    void *h_tab = nullptr;        // pinned staging copy
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<SrvReq *> members;
+};
+
+template <class P>
+size_t table_bytes() { return sizeof(ReqTable<P>); }
+
+template <class P>
+StepIO<P> req_io(scp_gpu *h, int par);
+
+template <>
+StepIO<F64> req_io<F64>(scp_gpu *h, int par) {
+    const int in = h->cur ^ par;
+    StepIO<F64> io;
+    io.xin = h->X[in];
+    io.xout = h->X[in ^ 1];
+    io.loin = nullptr; io.loout = nullptr; io.tloin = nullptr; io.tloout = nullptr;
+    io.win = h->W; io.wout = h->W; io.sout = h->S; io.flag = h->flag;
+    return io;
+}
+template <>
+StepIO<F32C> req_io<F32C>(scp_gpu *h, int par) {
+    const int in = h->cur ^ par;
+    StepIO<F32C> io;
+    io.xin = h->X32[in];
+    io.xout = h->X32[in ^ 1];
+    io.loin = h->LO[in]; io.loout = h->LO[in ^ 1];
+    io.tloin = h->TLO[in]; io.tloout = h->TLO[in ^ 1];
+    io.win = h->W32; io.wout = h->W32; io.sout = h->S32; io.flag = h->flag;
+    return io;
+}
+
+template <class P>
+using MultiFn = void (*)(const ReqTable<P> *, int);
+
+template <class P>
+MultiFn<P> multi_fn(int shape, bool g, size_t *smem) {
+    switch (shape) {
+        case 2: *smem = smem_of<P, 32, 8>(g);
+            return g ? step_multi_kernel<P, 32, 8, true> : step_multi_kernel<P, 32, 8, false>;
+        case 3: *smem = smem_of<P, 16, 8>(g);
+            return g ? step_multi_kernel<P, 16, 8, true> : step_multi_kernel<P, 16, 8, false>;
+        case 4: *smem = smem_of<P, 64, 2>(g);
+            return g ? step_multi_kernel<P, 64, 2, true> : step_multi_kernel<P, 64, 2, false>;
+        default: *smem = smem_of<P, 32, 4>(g);
+            return g ? step_multi_kernel<P, 32, 4, true> : step_multi_kernel<P, 32, 4, false>;
+    }
+}
+
+}  // namespace
+
+struct scp_srv {
+    scp_srv_config cfg{};
+    cudaStream_t stream = nullptr;
+    long long step = 0;
+    int64_t next_id = 1;
+    int64_t mem_in_use = 0;
+    std::deque<SrvReq *> queue;
+    std::vector<SrvReq *> active;
+    std::map<int64_t, std::unique_ptr<SrvReq>> all;
+    std::vector<std::unique_ptr<SrvGroup>> groups;
+    std::map<std::tuple<int, int, int>, int> group_of;        // (prec, gauged, shape) -> group
+    std::map<std::tuple<int, int, int>, int> tuned;           // (N, gauged, prec) -> shape
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_groups = -1;                                    // group count the graph was built for
+    int nsm = 0;
+    int64_t chunks = 0;
+    double t_admit = 0, t_autotune = 0, t_run = 0, t_retire = 0;
+    bool inflight = false;                                    // a chunk is running on the GPU
+};
+
+static int64_t srv_footprint(const scp_gpu_params &p) {
+    const int64_t n3 = (int64_t)p.N * p.N * p.N;
+    const int nf = p.complex_gauge ? 15 : 12;
+    int64_t b = (p.precision_mode == SCP_PREC_FP64) ? 4LL * 8 * nf * n3
+                                                   : 4LL * 4 * nf * n3 + 2LL * 12 * n3 + (p.complex_gauge ? 2LL * 12 * n3 : 0);
+    return b + 8 * n3 + (int64_t)kRedMaxBlocks * 32 * 8;   // + snapshot staging + reduction partials
+}
+
+// time each compiled tile shape on a scratch state and keep the fastest
+static int srv_autotune(scp_srv *s, const scp_gpu_params &p, int *shape_out) {
+    const auto key = std::make_tuple((int)p.N, (int)(p.complex_gauge != 0), (int)p.precision_mode);
+    auto it = s->tuned.find(key);
+    if (it != s->tuned.end()) { *shape_out = it->second; return SCP_OK; }
+    if (!s->cfg.autotune) { *shape_out = 1; s->tuned[key] = 1; return SCP_OK; }
+    const double t0 = now_s();
+    if (s->inflight) CK(cudaStreamSynchronize(s->stream));   // time the shapes on an idle GPU
+    const int64_t n3 = (int64_t)p.N * p.N * p.N;
+    const int ncols = p.complex_gauge ? 30 : 24;
+    std::vector<double> zero((size_t)n3, 0.0), bump((size_t)n3, 0.0);
+    for (int64_t i = 0; i < n3; i++) bump[(size_t)i] = 1e-3 * (double)((i * 2654435761LL) % 1000) / 1000.0;
+    std::vector<const double *> cols(ncols, zero.data());
+    for (int c = 0; c < 6; c++) cols[c] = bump.data();   // phi and theta real parts: a non-trivial state
+    double best = 1e300;
+    int best_shape = 1;
+    for (int shape = 1; shape < kNumShapes; shape++) {
+        scp_gpu_params q = p;
+        q.tile_variant = shape;
+        q.gauss_project = 0;
+        q.bc_type = 0;            // the scratch state need not be neutral
+        q.damp_rate = 0.0;
+        scp_gpu *h = nullptr;
+        if (scp_gpu_init(&q, cols.data(), &h) != SCP_OK) continue;
+        double ms = 0;
+        scp_gpu_step(h, 3);
+        const int rc = scp_gpu_time_steps(h, 10, &ms);
+        scp_gpu_free(h);
+        if (rc == SCP_OK && ms < best) { best = ms; best_shape = shape; }
+    }
+    s->tuned[key] = best_shape;
+    *shape_out = best_shape;
+    s->t_autotune += now_s() - t0;
+    return SCP_OK;
+}
+
+static int srv_group(scp_srv *s, int prec, int gauged, int shape, int *gidx) {
+    const auto key = std::make_tuple(prec, gauged, shape);
+    auto it = s->group_of.find(key);
+    if (it != s->group_of.end()) { *gidx = it->second; return SCP_OK; }
+    auto g = std::make_unique<SrvGroup>();
+    g->prec = prec; g->gauged = gauged; g->shape = shape;
+    g->threads = kShapes[shape].tx * kShapes[shape].ty;
+    const void *fn;
+    size_t tb;
+    if (prec == SCP_PREC_FP64) { fn = (const void *)multi_fn<F64>(shape, gauged, &g->smem); tb = table_bytes<F64>(); }
+    else { fn = (const void *)multi_fn<F32C>(shape, gauged, &g->smem); tb = table_bytes<F32C>(); }
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g->smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, g->threads, g->smem));
+    if (occ < 1) return SCP_EUNSUPPORTED;
+    g->grid = s->nsm * occ;
+    CK(cudaMalloc(&g->d_tab, tb));
+    CK(cudaMallocHost(&g->h_tab, tb));
+    memset(g->h_tab, 0, tb);
+    CK(cudaMemcpy(g->d_tab, g->h_tab, tb, cudaMemcpyHostToDevice));
+    CK(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming));
+    s->groups.push_back(std::move(g));
+    *gidx = (int)s->groups.size() - 1;
+    s->group_of[key] = *gidx;
+    return SCP_OK;
+}
+
+template <class P>
+static void fill_table(scp_srv *s, SrvGroup *g) {
+    ReqTable<P> *t = (ReqTable<P> *)g->h_tab;
+    t->step = s->step;
+    int items = 0, r = 0;
+    for (SrvReq *q : g->members) {
+        if (q->s1 <= s->step) continue;                  // finished, waiting to be retired
+        ReqSlot<P> &slot = t->r[r++];
+        slot.io[0] = req_io<P>(q->h, 0);
+        slot.io[1] = req_io<P>(q->h, 1);
+        slot.c = q->h->c;
+        slot.tg = q->h->tg;
+        slot.item0 = items;
+        slot.damp = damping_on(q->h) ? 1 : 0;
+        slot.s0 = q->s0;
+        slot.s1 = q->s1;
+        items += q->h->tg.nitems;
+    }
+    t->nreq = r;
+    t->nitems = items;
+}
+
+// Segment length for the next chunk.  One launch advances every request by a
+// step, so its duration is set by the slowest work item: cut every grid into
+// segments of about the same number of planes (16) so items of large and
+// small grids cost alike and the persistent CTAs stay balanced; split further
+// only when the active set is too small to fill the GPU.
+static void srv_plan(scp_srv *s) {
+    long long items = 0;
+    for (SrvReq *q : s->active)
+        if (q->s1 > s->step) {
+            const int N = q->h->N;
+            items += (long long)q->h->tg.ntx * q->h->tg.nty * ((N + 15) / 16);
+        }
+    const long long target = 6LL * s->nsm;
+    int seg_planes = 16;
+    while (items < target && seg_planes > 4) { seg_planes /= 2; items *= 2; }
+    for (SrvReq *q : s->active) {
+        TileGrid &tg = q->h->tg;
+        const int N = q->h->N;
+        const int seg = N < seg_planes ? N : seg_planes;
+        tg.seg = seg;
+        tg.nseg = (N + seg - 1) / seg;
+        tg.nitems = tg.ntx * tg.nty * tg.nseg;
+    }
+}
+
+static int srv_upload_tables(scp_srv *s) {
+    for (auto &g : s->groups) {
+        size_t tb;
+        if (g->prec == SCP_PREC_FP64) { fill_table<F64>(s, g.get()); tb = table_bytes<F64>(); }
+        else { fill_table<F32C>(s, g.get()); tb = table_bytes<F32C>(); }
+        CK(cudaMemcpyAsync(g->d_tab, g->h_tab, tb, cudaMemcpyHostToDevice, s->stream));
+    }
+    return SCP_OK;
+}
+
+// capture K steps of every group (each on its own forked stream) into a graph
+static int srv_build_graph(scp_srv *s) {
+    if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
+    if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+    cudaEvent_t fork;
+    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(fork, s->stream);
+    for (auto &g : s->groups) {
+        cudaStreamWaitEvent(g->st, fork, 0);
+        for (int k = 0; k < s->cfg.chunk_steps; k++) {
+            if (g->prec == SCP_PREC_FP64) {
+                size_t sm;
+                MultiFn<F64> fn = multi_fn<F64>(g->shape, g->gauged, &sm);
+                fn<<<g->grid, g->threads, g->smem, g->st>>>((const ReqTable<F64> *)g->d_tab, k);
+            } else {
+                size_t sm;
+                MultiFn<F32C> fn = multi_fn<F32C>(g->shape, g->gauged, &sm);
+                fn<<<g->grid, g->threads, g->smem, g->st>>>((const ReqTable<F32C> *)g->d_tab, k);
+            }
+        }
+        cudaEventRecord(g->done, g->st);
+        cudaStreamWaitEvent(s->stream, g->done, 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(s->stream, &s->graph);
+    cudaEventDestroy(fork);
+    CK(e);
+    CK(cudaGraphInstantiate(&s->exec, s->graph, 0));
+    s->graph_groups = (int)s->groups.size();
+    return SCP_OK;
+}
+
+static int srv_admit(scp_srv *s) {
+    int rc, admitted = 0;
+    while (!s->queue.empty() && (int)s->active.size() < s->cfg.max_active && s->active.size() < (size_t)kMaxReq &&
+           (s->cfg.admit_per_poll <= 0 || admitted < s->cfg.admit_per_poll || s->active.empty())) {
+        SrvReq *q = s->queue.front();
+        const int64_t need = srv_footprint(q->p);
+        if (s->cfg.mem_budget_bytes > 0 && s->mem_in_use + need > s->cfg.mem_budget_bytes && !s->active.empty())
+            break;                                             // wait for memory to free up
+        s->queue.pop_front();
+        int shape = 1;
+        if ((rc = srv_autotune(s, q->p, &shape))) return rc;
+        q->p.tile_variant = shape;
+        const int ncols = q->p.complex_gauge ? 30 : 24;
+        const int64_t n3 = (int64_t)q->p.N * q->p.N * q->p.N;
+        std::vector<const double *> cols(ncols);
+        for (int c = 0; c < ncols; c++)
+            cols[c] = q->borrowed.empty() ? q->cols.data() + (size_t)c * n3 : q->borrowed[c];
+        q->t_admit = now_s();
+        rc = scp_gpu_init(&q->p, cols.data(), &q->h);
+        std::vector<double>().swap(q->cols);
+        std::vector<const double *>().swap(q->borrowed);
+        admitted++;
+        if (rc != SCP_OK) {
+            q->state = SCP_SRV_FAILED; q->rc = rc; q->t_done = now_s();
+            continue;
+        }
+        int gi;
+        if ((rc = srv_group(s, q->p.precision_mode, q->p.complex_gauge ? 1 : 0, shape, &gi))) return rc;
+        if ((int)s->groups[gi]->members.size() >= kMaxReq) {    // table full: requeue for later
+            scp_gpu_free(q->h); q->h = nullptr;
+            s->queue.push_front(q);
+            break;
+        }
+        q->group = gi;
+        q->s0 = -1;                                           // set when its first chunk is launched
+        q->s1 = -1;
+        q->bytes = need;
+        q->state = SCP_SRV_ACTIVE;
+        s->mem_in_use += need;
+        s->groups[gi]->members.push_back(q);
+        s->active.push_back(q);
+    }
+    return SCP_OK;
+}
+
+static int srv_retire(scp_srv *s) {
+    std::vector<SrvReq *> keep;
+    for (SrvReq *q : s->active) {
+        if (q->s1 < 0 || q->s1 > s->step) { keep.push_back(q); continue; }
+        scp_gpu *h = q->h;
+        h->cur ^= (int)(q->nsteps & 1);
+        h->steps = q->nsteps;
+        q->rc = scp_gpu_sync(h);
+        int rc2 = scp_gpu_diag(h, &q->diag);
+        if (q->rc == SCP_OK) q->rc = rc2;
+        if (q->out_cols && q->rc == SCP_OK) q->rc = scp_gpu_snapshot(h, q->out_dtype, q->out_cols);
+        scp_gpu_free(h);
+        q->h = nullptr;
+        q->state = (q->rc == SCP_OK) ? SCP_SRV_DONE : SCP_SRV_FAILED;
+        q->t_done = now_s();
+        s->mem_in_use -= q->bytes;
+        auto &m = s->groups[q->group]->members;
+        m.erase(std::remove(m.begin(), m.end(), q), m.end());
+    }
+    s->active.swap(keep);
+    return SCP_OK;
+}
+
+extern "C" {
+
+int scp_srv_create(const scp_srv_config *cfg, scp_srv **out) {
+    if (!cfg || !out) return SCP_EINVAL;
+    *out = nullptr;
+    if (cfg->chunk_steps < 1 || cfg->chunk_steps > 4096 || cfg->max_active < 1) return SCP_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) return SCP_ENODEV;
+    CK(cudaSetDevice(cfg->device));
+    scp_srv *s = new scp_srv();
+    s->cfg = *cfg;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, cfg->device);
+    if (e != cudaSuccess) {
+        delete s;
+        snprintf(g_cuda_err, sizeof g_cuda_err, "%s", cudaGetErrorString(e));
+        return SCP_ECUDA;
+    }
+    *out = s;
+    return SCP_OK;
+}
+
+static int srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *host_cols, int64_t nsteps,
+                      void *const *out_cols, int out_dtype, int64_t *id_out, bool borrow) {
+    if (!s || !p || !host_cols || nsteps < 1 || !id_out) return SCP_EINVAL;
+    int rc = validate(p);
+    if (rc) return rc;
+    if (p->device != s->cfg.device) return SCP_EINVAL;
+    auto q = std::make_unique<SrvReq>();
+    q->id = s->next_id++;
+    q->p = *p;
+    q->nsteps = nsteps;
+    q->out_cols = out_cols;
+    q->out_dtype = out_dtype;
+    const int ncols = p->complex_gauge ? 30 : 24;
+    const int64_t n3 = (int64_t)p->N * p->N * p->N;
+    for (int c = 0; c < ncols; c++)
+        if (!host_cols[c]) return SCP_EINVAL;
+    if (borrow) {
+        q->borrowed.assign(host_cols, host_cols + ncols);
+    } else {
+        q->cols.resize((size_t)ncols * n3);
+        for (int c = 0; c < ncols; c++) memcpy(q->cols.data() + (size_t)c * n3, host_cols[c], sizeof(double) * n3);
+    }
+    q->state = SCP_SRV_QUEUED;
+    q->t_submit = now_s();
+    *id_out = q->id;
+    s->queue.push_back(q.get());
+    s->all[q->id] = std::move(q);
+    return SCP_OK;
+}
+
+int scp_srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *host_cols, int64_t nsteps,
+                   void *const *out_cols, int out_dtype, int64_t *id_out) {
+    return srv_submit(s, p, host_cols, nsteps, out_cols, out_dtype, id_out, false);
+}
+
+int scp_srv_submit_borrowed(scp_srv *s, const scp_gpu_params *p, const double *const *host_cols, int64_t nsteps,
+                            void *const *out_cols, int out_dtype, int64_t *id_out) {
+    return srv_submit(s, p, host_cols, nsteps, out_cols, out_dtype, id_out, true);
+}
+
+int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
+    if (!s) return SCP_EINVAL;
+    CK(cudaSetDevice(s->cfg.device));
+    int rc;
+    // 1. admit while the previous chunk (if any) is still running on the GPU
+    const double t0 = now_s();
+    if ((rc = srv_admit(s))) return rc;
+    const double t1 = now_s();
+    s->t_admit += t1 - t0;
+    // 2. finish the chunk in flight
+    if (s->inflight) {
+        CK(cudaStreamSynchronize(s->stream));
+        s->step += s->cfg.chunk_steps;
+        s->chunks++;
+        s->inflight = false;
+    }
+    const double t2 = now_s();
+    s->t_run += t2 - t1;
+    // 3. newly admitted requests start with the next chunk
+    bool work = false;
+    for (SrvReq *q : s->active) {
+        if (q->s0 < 0) { q->s0 = s->step; q->s1 = s->step + q->nsteps; }
+        if (q->s1 > s->step) work = true;
+    }
+    // 4. launch the next chunk
+    if (work) {
+        srv_plan(s);
+        if ((rc = srv_upload_tables(s))) return rc;
+        if (s->cfg.use_graph) {
+            if (s->graph_groups != (int)s->groups.size() && (rc = srv_build_graph(s))) return rc;
+            CK(cudaGraphLaunch(s->exec, s->stream));
+        } else {
+            cudaEvent_t fork;
+            CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+            cudaEventRecord(fork, s->stream);
+            for (auto &g : s->groups) {
+                cudaStreamWaitEvent(g->st, fork, 0);
+                for (int k = 0; k < s->cfg.chunk_steps; k++) {
+                    size_t sm;
+                    if (g->prec == SCP_PREC_FP64)
+                        multi_fn<F64>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
+                            (const ReqTable<F64> *)g->d_tab, k);
+                    else
+                        multi_fn<F32C>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
+                            (const ReqTable<F32C> *)g->d_tab, k);
+                }
+                cudaEventRecord(g->done, g->st);
+                cudaStreamWaitEvent(s->stream, g->done, 0);
+            }
+            cudaEventDestroy(fork);
+            CK(cudaGetLastError());
+        }
+        s->inflight = true;
+    }
+    // 5. retire the requests that finished in the chunk just completed, while
+    //    the next one runs (they are no longer in the tables)
+    const double t3 = now_s();
+    if ((rc = srv_retire(s))) return rc;
+    s->t_retire += now_s() - t3;
+    if (!s->inflight && s->active.empty() && s->queue.empty() && s->stream) CK(cudaStreamSynchronize(s->stream));
+    if (n_active) *n_active = (int)s->active.size();
+    if (n_queued) *n_queued = (int)s->queue.size();
+    return SCP_OK;
+}
+
+int scp_srv_status(scp_srv *s, int64_t id, scp_srv_request_info *info) {
+    if (!s || !info) return SCP_EINVAL;
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return SCP_EINVAL;
+    const SrvReq *q = it->second.get();
+    memset(info, 0, sizeof *info);
+    info->state = q->state;
+    info->rc = q->rc;
+    info->t_submit = q->t_submit;
+    info->t_admit = q->t_admit;
+    info->t_done = q->t_done;
+    info->nsteps = q->nsteps;
+    info->N = q->p.N;
+    info->tile_variant = q->p.tile_variant;
+    return SCP_OK;
+}
+
+int scp_srv_result(scp_srv *s, int64_t id, scp_gpu_diag_out *diag) {
+    if (!s || !diag) return SCP_EINVAL;
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return SCP_EINVAL;
+    const SrvReq *q = it->second.get();
+    if (q->state == SCP_SRV_QUEUED || q->state == SCP_SRV_ACTIVE) return SCP_EBUSY;
+    *diag = q->diag;
+    return q->rc;
+}
+
+int scp_srv_stats(scp_srv *s, scp_srv_stats_t *st) {
+    if (!s || !st) return SCP_EINVAL;
+    memset(st, 0, sizeof *st);
+    st->step = s->step;
+    st->chunks = s->chunks;
+    st->mem_in_use = s->mem_in_use;
+    st->n_active = (int)s->active.size();
+    st->n_queued = (int)s->queue.size();
+    st->n_groups = (int)s->groups.size();
+    st->t_admit = s->t_admit - s->t_autotune;
+    st->t_autotune = s->t_autotune;
+    st->t_run = s->t_run;
+    st->t_retire = s->t_retire;
+    return SCP_OK;
+}
+
+void scp_srv_free(scp_srv *s) {
+    if (!s) return;
+    cudaSetDevice(s->cfg.device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (SrvReq *q : s->active)
+        if (q->h) scp_gpu_free(q->h);
+    if (s->exec) cudaGraphExecDestroy(s->exec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    for (auto &g : s->groups) {
+        cudaFree(g->d_tab);
+        cudaFreeHost(g->h_tab);
+        if (g->st) cudaStreamDestroy(g->st);
+        if (g->done) cudaEventDestroy(g->done);
+    }
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+}  // extern "C"

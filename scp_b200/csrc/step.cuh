@@ -126,14 +126,16 @@ __device__ __forceinline__ double link_wrap(double v) {
     return wrap_angle(v);
 }
 
-template <class P, int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
-__global__ void __launch_bounds__(TX * TY)
-step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
+// One work item (a TX x TY column over one segment of planes) of one grid.
+// sync and damp are uniform per call; the single-grid kernel passes them as
+// constants, the multi-request kernel per request.
+template <class P, int TX, int TY, bool GAUGED, bool FIRST>
+__device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts &c, const TileGrid &tg, int item,
+                                          const bool SYNC, const bool DAMP, unsigned char *smem_raw) {
     using T = typename P::T;
     using LY = StepLayout<P, TX, TY, GAUGED>;
     constexpr int NF = LY::NF, PX = LY::PX, PY = LY::PY, NT = LY::NT;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *xs = reinterpret_cast<T *>(smem_raw);     // [3][NF][PY][PX]
+    T *xs = reinterpret_cast<T *>(smem_raw);     // [3][NR][PY][PX]
     T *gq = xs + 3 * LY::PLANE;                  // [2][GQ_N][GY][GX]
     constexpr int NR = LY::NR;
     auto XS = [&](int slot, int f, int r, int col) -> T & {
@@ -150,7 +152,7 @@ step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
     const T dt = (T)c.dt, hdt = (T)c.hdt, idx1 = (T)c.idx1, idx2 = (T)c.idx2;
     const float dt_lo = (float)(c.dt - (double)(float)c.dt);
 
-    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) {
+    {
         const int kt = item % tg.ntx;
         const int jt = (item / tg.ntx) % tg.nty;
         const int sg = item / (tg.ntx * tg.nty);
@@ -525,6 +527,65 @@ step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
 #pragma unroll
             for (int f = 0; f < 12; f++) xm[f] = ctr[f];
         }
+    }
+}
+
+// Single grid: persistent CTAs over the grid's work items.
+template <class P, int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
+__global__ void __launch_bounds__(TX * TY)
+step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x)
+        step_item<P, TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, smem_raw);
+}
+
+// ---------------------------------------------------------------- many grids per launch
+//
+// The serving loop advances every admitted request by one step per launch.
+// Requests live in a device-resident table; request r is active for global
+// steps s0 <= s < s1, its buffers swap roles by the parity of s - s0, and
+// its last step stores the synchronous momenta.  Because all of that is
+// derived from the step counter in the table, the launches can be captured
+// once in a CUDA graph and replayed while requests come and go: the host
+// only rewrites the table between replays.
+
+constexpr int kMaxReq = 256;
+
+template <class P>
+struct ReqSlot {
+    StepIO<P> io[2];      // io[p]: the step taken at parity p
+    StepConsts c;
+    TileGrid tg;
+    int item0;            // first global work item of this request
+    int damp;
+    long long s0, s1;     // active global steps [s0, s1)
+};
+
+template <class P>
+struct ReqTable {
+    int nreq;
+    int nitems;
+    long long step;       // global step of launch k = 0 of the current replay
+    ReqSlot<P> r[kMaxReq];
+};
+
+template <class P, int TX, int TY, bool GAUGED>
+__global__ void __launch_bounds__(TX * TY)
+step_multi_kernel(const ReqTable<P> *tab, int k) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nitems = tab->nitems, nreq = tab->nreq;
+    const long long s = tab->step + k;
+    for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+        int lo = 0, hi = nreq - 1;                 // last request with item0 <= item
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tab->r[mid].item0 <= item) lo = mid; else hi = mid - 1;
+        }
+        const ReqSlot<P> &q = tab->r[lo];
+        if (s < q.s0 || s >= q.s1) continue;       // uniform over the CTA
+        const int par = (int)((s - q.s0) & 1);
+        step_item<P, TX, TY, GAUGED, false>(q.io[par], q.c, q.tg, item - q.item0, s == q.s1 - 1, q.damp != 0,
+                                            smem_raw);
     }
 }
 

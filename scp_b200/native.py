@@ -20,6 +20,8 @@ EXPORTS = (
     "scp_gpu_snapshot", "scp_gpu_get_info", "scp_gpu_time_steps", "scp_gpu_stream",
     "scp_gpu_free", "scp_gpu_errstr", "scp_gpu_last_cuda_error", "scp_gpu_abi_version",
     "scp_gpu_diag_noalloc", "scp_gpu_check_trig",
+    "scp_srv_create", "scp_srv_submit", "scp_srv_submit_borrowed", "scp_srv_poll", "scp_srv_status", "scp_srv_result",
+    "scp_srv_stats", "scp_srv_free",
 )
 
 DIAG_NSLOTS = 40
@@ -42,6 +44,35 @@ class Info(ctypes.Structure):
         ("tile_x", ctypes.c_int32),
         ("tile_y", ctypes.c_int32),
         ("seg_len", ctypes.c_int32),
+    ]
+
+
+class SrvConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("max_active", ctypes.c_int32),
+        ("mem_budget_bytes", ctypes.c_int64),
+        ("chunk_steps", ctypes.c_int32),
+        ("use_graph", ctypes.c_int32),
+        ("autotune", ctypes.c_int32),
+        ("admit_per_poll", ctypes.c_int32),
+    ]
+
+
+class SrvRequestInfo(ctypes.Structure):
+    _fields_ = [
+        ("state", ctypes.c_int32), ("rc", ctypes.c_int32),
+        ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+        ("nsteps", ctypes.c_int64), ("N", ctypes.c_int32), ("tile_variant", ctypes.c_int32),
+    ]
+
+
+class SrvStats(ctypes.Structure):
+    _fields_ = [
+        ("step", ctypes.c_int64), ("chunks", ctypes.c_int64), ("mem_in_use", ctypes.c_int64),
+        ("n_active", ctypes.c_int32), ("n_queued", ctypes.c_int32), ("n_groups", ctypes.c_int32),
+        ("t_admit", ctypes.c_double), ("t_autotune", ctypes.c_double), ("t_run", ctypes.c_double),
+        ("t_retire", ctypes.c_double),
     ]
 
 
@@ -82,6 +113,17 @@ def lib() -> ctypes.CDLL:
     L.scp_gpu_errstr.restype = ctypes.c_char_p
     L.scp_gpu_last_cuda_error.restype = ctypes.c_char_p
     L.scp_gpu_check_trig.argtypes = [ctypes.c_int, vp, vp]
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.scp_srv_create.argtypes = [ctypes.POINTER(SrvConfig), ctypes.POINTER(vp)]
+    L.scp_srv_submit.argtypes = [vp, ctypes.POINTER(CParams), ctypes.POINTER(vp), ctypes.c_int64,
+                                 ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    L.scp_srv_submit_borrowed.argtypes = L.scp_srv_submit.argtypes
+    L.scp_srv_poll.argtypes = [vp, ip, ip]
+    L.scp_srv_status.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(SrvRequestInfo)]
+    L.scp_srv_result.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(DiagOut)]
+    L.scp_srv_stats.argtypes = [vp, ctypes.POINTER(SrvStats)]
+    L.scp_srv_free.argtypes = [vp]
+    L.scp_srv_free.restype = None
     L.scp_gpu_diag_noalloc.argtypes = [ctypes.POINTER(CParams), ctypes.POINTER(vp), ctypes.c_double, vp,
                                        ctypes.POINTER(DiagOut)]
     _lib = L
