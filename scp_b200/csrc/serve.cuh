@@ -135,7 +135,7 @@ static int64_t srv_footprint(const scp_gpu_params &p) {
     const int64_t n3 = (int64_t)p.N * p.N * p.N;
     const int nf = p.complex_gauge ? 15 : 12;
     int64_t b = (p.precision_mode == SCP_PREC_FP64) ? 4LL * 8 * nf * n3
-                                                   : 4LL * 4 * nf * n3 + 2LL * 12 * n3 + (p.complex_gauge ? 2LL * 12 * n3 : 0);
+                                                   : 4LL * 4 * nf * n3 + 2LL * 24 * n3 + (p.complex_gauge ? 2LL * 12 * n3 : 0);
     return b + 8 * n3 + (int64_t)kRedMaxBlocks * 32 * 8;   // + snapshot staging + reduction partials
 }
 

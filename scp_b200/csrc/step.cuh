@@ -2,8 +2,8 @@
 // Cosserat Q-ball lattice, one launch per time step, in two precisions:
 //   F64   all state and arithmetic in FP64 (the drop-in mode);
 //   F32C  FP32 state and arithmetic; positions carried as a compensated pair
-//         (hi: fp32, lo: int8 in units of ulp(hi)/256 for the matter fields,
-//         fp32 for the link angles) so the drift accumulates without loss.
+//         (hi: fp32, lo: bf16 for the matter fields, fp32 for the link
+//         angles) so the drift accumulates without loss.
 //         F32C evaluates Laplacians, currents and plaquette angles as sums of
 //         neighbour differences, which removes the cancellation that FP32
 //         would otherwise suffer against O(|f|) values.
@@ -31,10 +31,12 @@
 // i+2 in flight via cp.async), holding the x(i-1) centre values of its own
 // sites in registers.  Every thread copies its own site; the halo rows and
 // columns (periodic wrap) are spread over the CTA's threads so each thread
-// issues the same copies with no per-field branches.  In gauged mode the link
-// cos/sin and plaquette sines of each plane are computed once per site into
-// shared memory (plus the low-side halo row and column that the backward
-// transports and staples need) instead of once per use.
+// issues the same copies with no per-field branches.  In gauged mode every
+// thread evaluates the link cos/sin and plaquette sines it needs itself: its
+// own site, the j-1 and k-1 neighbours (recomputed from the ring), and the
+// i-1 values carried in registers from the previous plane -- more sines than
+// sharing them through shared memory, but no extra barrier per plane and no
+// shared array, which leaves room for more resident CTAs.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -57,8 +59,8 @@ struct StepIO {
     using T = typename P::T;
     const T *xin;           // NF arrays of N^3: positions x_{n+1} (hi part in F32C)
     T *xout;                // NF arrays: x_{n+2}
-    const int8_t *loin;     // F32C: scaled low parts of the 12 matter positions
-    int8_t *loout;
+    const uint16_t *loin;   // F32C: bf16 low parts of the 12 matter positions
+    uint16_t *loout;
     const float *tloin;     // F32C gauged: low parts of the 3 link angles
     float *tloout;
     const T *win;           // NF arrays: w_n (or v_0, E_0 when FIRST)
@@ -82,7 +84,7 @@ struct StepLayout {
     static constexpr int NT = TX * TY;
     static constexpr int NHALO = 2 * TX + 2 * TY + (GAUGED ? 2 : 0);
     static constexpr int HPT = (NHALO + NT - 1) / NT;      // halo sites per thread (max)
-    static constexpr size_t smem_bytes = sizeof(T) * (size_t)(3 * PLANE + (GAUGED ? 2 * GPLANE : 0));
+    static constexpr size_t smem_bytes = sizeof(T) * (size_t)(3 * PLANE);
 };
 
 __device__ __forceinline__ void cp_async_elem(double *s, const double *g) { cp_async8(s, g); }
@@ -96,21 +98,6 @@ __device__ __forceinline__ uint16_t f_to_bf16(float f) {
     return __bfloat16_as_ushort(__float2bfloat16_rn(f));
 }
 
-// Low part of a compensated fp32 pair stored as int8 in units of ulp(hi)/256
-// (|lo| <= ulp(hi)/2 after a two-sum, so the code stays within [-128, 128]).
-// The unit is a power of two taken from hi's exponent; below |hi| ~ 2^-95 it
-// is pinned to the smallest normal.
-__device__ __forceinline__ int lo_unit_exp(float hi) {
-    const int e = (int)((__float_as_uint(hi) >> 23) & 0xFF);
-    return max(e - 31, 1);
-}
-__device__ __forceinline__ float lo_decode(int8_t q, float hi) {
-    return (float)q * __int_as_float(lo_unit_exp(hi) << 23);
-}
-__device__ __forceinline__ int8_t lo_encode(float lo, float hi) {
-    const float r = rintf(lo * __int_as_float((254 - lo_unit_exp(hi)) << 23));
-    return (int8_t)fminf(fmaxf(r, -127.0f), 127.0f);
-}
 // exact sum: s + e = a + b (Knuth two-sum)
 __device__ __forceinline__ void two_sum(float a, float b, float *s, float *e) {
     const float t = a + b;
@@ -136,15 +123,10 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
     using LY = StepLayout<P, TX, TY, GAUGED>;
     constexpr int NF = LY::NF, PX = LY::PX, PY = LY::PY, NT = LY::NT;
     T *xs = reinterpret_cast<T *>(smem_raw);     // [3][NR][PY][PX]
-    T *gq = xs + 3 * LY::PLANE;                  // [2][GQ_N][GY][GX]
     constexpr int NR = LY::NR;
     auto XS = [&](int slot, int f, int r, int col) -> T & {
         return xs[((slot * NR + f) * PY + r) * PX + col];
     };
-    auto GQ = [&](int slot, int q, int r, int col) -> T & {
-        return gq[((slot * GQ_N + q) * LY::GY + r) * LY::GX + col];
-    };
-
     const int N = c.N;
     const long long N3 = c.N3;
     const int tid = threadIdx.x;
@@ -213,50 +195,23 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             }
         };
 
-        // gauge quantities of the plane in slot sc (next plane in slot sp) into gq slot gs
-        auto gauge_plane = [&](int sc, int sp, int gs) {
-            constexpr int NS = LY::GY * LY::GX;
-            for (int s = tid; s < NS; s += NT) {
-                const int r = s / LY::GX, col = s % LY::GX;
-                if ((r == 0 && col == 0) || r > nj || col > nk) continue;
-                const T t0 = XS(sc, FTH + 0, r, col), t1 = XS(sc, FTH + 1, r, col);
-                const T t2 = XS(sc, FTH + 2, r, col);
-                T sn, cs;
-                if (r > 0 && col > 0) {
-                    sincos_bounded(t0, &sn, &cs); GQ(gs, GQ_C0 + 0, r, col) = cs; GQ(gs, GQ_S0 + 0, r, col) = sn;
-                }
-                if (col > 0) {
-                    sincos_bounded(t1, &sn, &cs); GQ(gs, GQ_C0 + 1, r, col) = cs; GQ(gs, GQ_S0 + 1, r, col) = sn;
-                }
-                if (r > 0) {
-                    sincos_bounded(t2, &sn, &cs); GQ(gs, GQ_C0 + 2, r, col) = cs; GQ(gs, GQ_S0 + 2, r, col) = sn;
-                }
-                // plaquette angle th_a(y) + th_b(y+a) - th_a(y+b) - th_b(y), planes (0,1) (1,2) (2,0)
-                if constexpr (NR > NF) {
-                    // FP32C: (th_a(y) - th_a(y+b)) + (th_b(y+a) - th_b(y)), hi and lo parts
-                    auto TL = [&](int sl, int d, int rr, int cc) -> T { return XS(sl, NF + d, rr, cc); };
-                    if (col > 0) {
-                        const T a = (t0 - XS(sc, FTH + 0, r + 1, col)) + (XS(sp, FTH + 1, r, col) - t1);
-                        const T b = (TL(sc, 0, r, col) - TL(sc, 0, r + 1, col)) + (TL(sp, 1, r, col) - TL(sc, 1, r, col));
-                        GQ(gs, GQ_P0 + 0, r, col) = sin_bounded(a + b);
-                    }
-                    {
-                        const T a = (t1 - XS(sc, FTH + 1, r, col + 1)) + (XS(sc, FTH + 2, r + 1, col) - t2);
-                        const T b = (TL(sc, 1, r, col) - TL(sc, 1, r, col + 1)) + (TL(sc, 2, r + 1, col) - TL(sc, 2, r, col));
-                        GQ(gs, GQ_P0 + 1, r, col) = sin_bounded(a + b);
-                    }
-                    if (r > 0) {
-                        const T a = (t2 - XS(sp, FTH + 2, r, col)) + (XS(sc, FTH + 0, r, col + 1) - t0);
-                        const T b = (TL(sc, 2, r, col) - TL(sp, 2, r, col)) + (TL(sc, 0, r, col + 1) - TL(sc, 0, r, col));
-                        GQ(gs, GQ_P0 + 2, r, col) = sin_bounded(a + b);
-                    }
-                } else {
-                    if (col > 0)
-                        GQ(gs, GQ_P0 + 0, r, col) = sin_bounded(t0 + XS(sp, FTH + 1, r, col) - XS(sc, FTH + 0, r + 1, col) - t1);
-                    GQ(gs, GQ_P0 + 1, r, col) = sin_bounded(t1 + XS(sc, FTH + 2, r + 1, col) - XS(sc, FTH + 1, r, col + 1) - t2);
-                    if (r > 0)
-                        GQ(gs, GQ_P0 + 2, r, col) = sin_bounded(t2 + XS(sc, FTH + 0, r, col + 1) - XS(sp, FTH + 2, r, col) - t0);
-                }
+        // sine of the plaquette angle th_a(y) + th_b(y+a) - th_a(y+b) - th_b(y) of plane
+        // (a,b) = (0,1) (1,2) (2,0) [q = 0, 1, 2] at ring position (r, col) of slot sc,
+        // the next plane in slot sp (compute_forces_complex_gauge pass B, scp_sim.c:1090-1109)
+        auto plaq_sin = [&](int q, int sc, int sp, int r, int col) -> T {
+            const int a = q, b = (q + 1) % 3;
+            // th_b(y+a): the next plane for a = 0, else the neighbour row (a = 1) or column (a = 2)
+            const int sa = (a == 0) ? sp : sc, ra = r + (a == 1 ? 1 : 0), ca = col + (a == 2 ? 1 : 0);
+            const int sb = (b == 0) ? sp : sc, rb = r + (b == 1 ? 1 : 0), cb = col + (b == 2 ? 1 : 0);
+            const T tay = XS(sc, FTH + a, r, col), tby = XS(sc, FTH + b, r, col);
+            const T tbya = XS(sa, FTH + b, ra, ca), tayb = XS(sb, FTH + a, rb, cb);
+            if constexpr (NR > NF) {   // FP32C: hi differences plus lo differences
+                const T hi = (tay - tayb) + (tbya - tby);
+                const T lo = (XS(sc, NF + a, r, col) - XS(sb, NF + a, rb, cb)) +
+                             (XS(sa, NF + b, ra, ca) - XS(sc, NF + b, r, col));
+                return sin_bounded(hi + lo);
+            } else {
+                return sin_bounded(tay + tbya - tayb - tby);
             }
         };
 
@@ -269,31 +224,32 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
         T xm[12];          // x(i-1) at this thread's site, matter fields
 #pragma unroll
         for (int f = 0; f < 12; f++) xm[f] = act ? XS(0, f, ty + 1, tx + 1) : T(0);
-        if (GAUGED) gauge_plane(0, 1, 1);
+        // link 0 and the (0,1), (2,0) plaquettes at x - i (carried from plane to plane)
+        T c0m = T(1), s0m = T(0), P0m = T(0), P2m = T(0);
+        if (GAUGED && act) {
+            sincos_bounded(XS(0, FTH + 0, ty + 1, tx + 1), &s0m, &c0m);
+            P0m = plaq_sin(0, 0, 1, ty + 1, tx + 1);
+            P2m = plaq_sin(2, 0, 1, ty + 1, tx + 1);
+        }
         issue_plane(i0 + 1, 2);
         cp_async_commit();
 
         for (int i = i0; i < i1; i++) {
             const int sc = (i - i0 + 1) % 3, sp = (i - i0 + 2) % 3, sn = (i - i0) % 3;
-            const int gs = (i - i0) & 1, gm = gs ^ 1;
             cp_async_wait<0>();
             __syncthreads();
             if (i + 2 <= i1) issue_plane(i + 2, sn);
             cp_async_commit();
             const long long site = (long long)i * N * N + oc;
             T w[NF];
-            int8_t lo[P::COMP ? 12 : 1];
+            uint16_t lo[P::COMP ? 12 : 1];
             if (act) {
 #pragma unroll
                 for (int f = 0; f < NF; f++) w[f] = ldg_t(io.win + f * N3 + site);
                 if constexpr (P::COMP) {
 #pragma unroll
-                    for (int f = 0; f < 12; f++) lo[f] = (int8_t)__ldg((const char *)(io.loin + f * N3 + site));
+                    for (int f = 0; f < 12; f++) lo[f] = __ldg(io.loin + f * N3 + site);
                 }
-            }
-            if (GAUGED) {
-                gauge_plane(sc, sp, gs);
-                __syncthreads();
             }
             if (!act) continue;
 
@@ -358,14 +314,16 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 T DcU[3][6], DcV[3][6];
                 T TRp_[3][3], TIp_[3][3];   // forward transports of Phi
                 T tup[3][3], tvp[3][3];     // raw Theta at x+d (current and seagull)
+                // link cos/sin at x (pass A, scp_sim.c:1072-1079) and at x - d
+                T cPd[3], sPd[3], cMd[3], sMd[3];
+#pragma unroll
+                for (int d = 0; d < 3; d++) sincos_bounded(ctr[FTH + d], &sPd[d], &cPd[d]);
+                cMd[0] = c0m; sMd[0] = s0m;
+                sincos_bounded(XS(sc, FTH + 1, ty, tx + 1), &sMd[1], &cMd[1]);
+                sincos_bounded(XS(sc, FTH + 2, ty + 1, tx), &sMd[2], &cMd[2]);
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
-                    T cP, sP, cM, sM;
-                    cP = GQ(gs, GQ_C0 + d, ty + 1, tx + 1);
-                    sP = GQ(gs, GQ_S0 + d, ty + 1, tx + 1);
-                    if (d == 0) { cM = GQ(gm, GQ_C0, ty + 1, tx + 1); sM = GQ(gm, GQ_S0, ty + 1, tx + 1); }
-                    else if (d == 1) { cM = GQ(gs, GQ_C0 + 1, ty, tx + 1); sM = GQ(gs, GQ_S0 + 1, ty, tx + 1); }
-                    else { cM = GQ(gs, GQ_C0 + 2, ty + 1, tx); sM = GQ(gs, GQ_S0 + 2, ty + 1, tx); }
+                    const T cP = cPd[d], sP = sPd[d], cM = cMd[d], sM = sMd[d];
 #pragma unroll
                     for (int q = 0; q < 6; q++) {
                         const int fre = q < 3 ? FU + q : FTU + q - 3;
@@ -423,11 +381,14 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                     K[d] = (T)c.inva * Jg - T(0.5) * eta * (T12 - T21);   // Jlat; staple added below
                 }
                 // staples (scp_sim.c:1214-1220)
-                const T P0 = GQ(gs, GQ_P0 + 0, ty + 1, tx + 1), P1 = GQ(gs, GQ_P0 + 1, ty + 1, tx + 1);
-                const T P2 = GQ(gs, GQ_P0 + 2, ty + 1, tx + 1);
-                const T st0 = (P0 - GQ(gs, GQ_P0 + 0, ty, tx + 1)) - (P2 - GQ(gs, GQ_P0 + 2, ty + 1, tx));
-                const T st1 = -(P0 - GQ(gm, GQ_P0 + 0, ty + 1, tx + 1)) + (P1 - GQ(gs, GQ_P0 + 1, ty + 1, tx));
-                const T st2 = (P2 - GQ(gm, GQ_P0 + 2, ty + 1, tx + 1)) - (P1 - GQ(gs, GQ_P0 + 1, ty, tx + 1));
+                const T P0 = plaq_sin(0, sc, sp, ty + 1, tx + 1), P1 = plaq_sin(1, sc, sp, ty + 1, tx + 1);
+                const T P2 = plaq_sin(2, sc, sp, ty + 1, tx + 1);
+                const T P0jm = plaq_sin(0, sc, sp, ty, tx + 1), P1jm = plaq_sin(1, sc, sp, ty, tx + 1);
+                const T P1km = plaq_sin(1, sc, sp, ty + 1, tx), P2km = plaq_sin(2, sc, sp, ty + 1, tx);
+                const T st0 = (P0 - P0jm) - (P2 - P2km);
+                const T st1 = -(P0 - P0m) + (P1 - P1km);
+                const T st2 = (P2 - P2m) - (P1 - P1jm);
+                c0m = cPd[0]; s0m = sPd[0]; P0m = P0; P2m = P2;   // x - i of the next plane
                 const T stp = (T)c.stp, gg = (T)c.g;
                 K[0] = stp * st0 + gg * K[0];
                 K[1] = stp * st1 + gg * K[1];
@@ -474,10 +435,10 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                     // compensated drift (hi, lo) += dt*w_{n+1}
                     if (DAMP || FIRST) wn = v + hdt * acc[f];
                     else wn = fmaf((float)c.dt, acc[f], fmaf(dt_lo, acc[f], w[f]));
-                    const float y = fmaf((float)c.dt, wn, fmaf(dt_lo, wn, lo_decode(lo[f], ctr[f])));
+                    const float y = fmaf((float)c.dt, wn, fmaf(dt_lo, wn, bf16_to_f(lo[f])));
                     float e;
                     two_sum(ctr[f], y, &xn, &e);
-                    io.loout[f * N3 + site] = lo_encode(e, xn);
+                    io.loout[f * N3 + site] = f_to_bf16(e);
                 } else {
                     wn = v + hdt * acc[f];
                     xn = ctr[f] + dt * wn;
@@ -531,8 +492,15 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
 }
 
 // Single grid: persistent CTAs over the grid's work items.
+// resident CTAs per SM the register allocation is sized for
+// (FP64 at 3 CTAs of 128 threads would spill the gauged force; FP32C fits)
+template <class P, int TX, int TY, bool GAUGED>
+struct MinBlocks {
+    static constexpr int value = (TX * TY > 128) ? 1 : (P::COMP ? 3 : 2);
+};
+
 template <class P, int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
-__global__ void __launch_bounds__(TX * TY)
+__global__ void __launch_bounds__(TX * TY, (MinBlocks<P, TX, TY, GAUGED>::value))
 step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x)
@@ -570,7 +538,7 @@ struct ReqTable {
 };
 
 template <class P, int TX, int TY, bool GAUGED>
-__global__ void __launch_bounds__(TX * TY)
+__global__ void __launch_bounds__(TX * TY, (MinBlocks<P, TX, TY, GAUGED>::value))
 step_multi_kernel(const ReqTable<P> *tab, int k) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nitems = tab->nitems, nreq = tab->nreq;
