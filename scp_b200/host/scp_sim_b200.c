@@ -1,0 +1,293 @@
+/* scp_sim_b200.c -- config-driven host driver for the B200 stepper.
+ *
+ * The reference runs its complex / gauged simulations through `main` in
+ * sfa/sim/scp_sim.c (CPU) and sfa/sim/scp_sim.cu (CUDA): read a key = value
+ * config or resume from an .sfa file's KVMD, initialise the fields, write SFA
+ * snapshots and a diagnostic TSV while stepping.  This driver keeps that flow
+ * and those files -- it compiles the reference's own scp_config.h (Config,
+ * parser, validation), scp_init.h (initial states, KVMD embedding) and
+ * sfa/format/sfa.h (the archive) -- and replaces the stepper with the C ABI of
+ * libscpgpu.so (include/scp_gpu.h).
+ *
+ *   scp_sim_b200 config.cfg [-key value ...]
+ *   scp_sim_b200 run.sfa    [-key value ...]      resume from the last frame
+ *
+ * Extra keys read by this driver only (not passed to the reference parser):
+ *   gpu_precision = fp64 | fp32c   (default fp64)
+ *   gpu_device    = <ordinal>       (default 0)
+ * It covers the complex (complex_phi=1) and gauged (complex_gauge=1) stepper
+ * with bc_type 0 or 2; other modes are refused with a message.
+ *
+ * Build: make -C scp_b200/host REF=<kardianos/scp checkout>
+ */
+#define SFA_IMPLEMENTATION
+#include "sfa.h"
+#include "scp_config.h"
+
+#include <stdint.h>
+#include <time.h>
+
+#include "scp_gpu.h"
+
+/* Host staging grid with the members scp_init.h reads (sfa/sim/scp_init.h:1-8). */
+typedef struct {
+    double *mem;
+    double *phi[3], *phi_vel[3], *theta[3], *theta_vel[3];
+    double *phi_im[3], *phi_im_vel[3], *theta_im[3], *theta_im_vel[3];
+    double *th[3], *Efield[3];
+    int N;
+    long N3;
+    double L, dx, dt;
+} Grid;
+
+#define SCP_COMPLEX_FIELDS 1
+#include "scp_init.h"
+
+static double wall_now(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+/* Host arrays in SFA column order (24 or 30 columns of N^3 doubles). */
+static Grid *grid_new(const Config *c, double **cols, int ncols) {
+    Grid *g = calloc(1, sizeof(Grid));
+    if (!g) return NULL;
+    g->N = c->N;
+    g->N3 = (long)c->N * c->N * c->N;
+    g->L = c->L;
+    g->dx = 2.0 * c->L / (c->N - 1);
+    g->dt = c->dt_factor * g->dx;
+    g->mem = calloc((size_t)ncols * g->N3, sizeof(double));
+    if (!g->mem) { free(g); return NULL; }
+    for (int k = 0; k < ncols; k++) cols[k] = g->mem + (size_t)k * g->N3;
+    for (int a = 0; a < 3; a++) {
+        g->phi[a] = cols[0 + a];      g->theta[a] = cols[3 + a];
+        g->phi_vel[a] = cols[6 + a];  g->theta_vel[a] = cols[9 + a];
+        g->phi_im[a] = cols[12 + a];  g->theta_im[a] = cols[15 + a];
+        g->phi_im_vel[a] = cols[18 + a]; g->theta_im_vel[a] = cols[21 + a];
+        g->th[a] = ncols == 30 ? cols[24 + a] : NULL;
+        g->Efield[a] = ncols == 30 ? cols[27 + a] : NULL;
+    }
+    return g;
+}
+
+/* Column schema of the complex / gauged snapshot (sfa/sim/scp_sim.c:2862-2897). */
+static void add_columns(SFA *sfa, uint8_t dt, int gauged) {
+    static const char *names[30] = {
+        "phi_x", "phi_y", "phi_z", "theta_x", "theta_y", "theta_z",
+        "phi_vx", "phi_vy", "phi_vz", "theta_vx", "theta_vy", "theta_vz",
+        "phiim_x", "phiim_y", "phiim_z", "thetaim_x", "thetaim_y", "thetaim_z",
+        "phiim_vx", "phiim_vy", "phiim_vz", "thetaim_vx", "thetaim_vy", "thetaim_vz",
+        "th_x", "th_y", "th_z", "E_x", "E_y", "E_z"};
+    static const uint8_t sem[30] = {
+        SFA_POSITION, SFA_POSITION, SFA_POSITION, SFA_ANGLE, SFA_ANGLE, SFA_ANGLE,
+        SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY,
+        SFA_POSITION, SFA_POSITION, SFA_POSITION, SFA_ANGLE, SFA_ANGLE, SFA_ANGLE,
+        SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY,
+        SFA_ANGLE, SFA_ANGLE, SFA_ANGLE, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY};
+    static const uint8_t comp[30] = {0, 1, 2, 0, 1, 2, 0, 1, 2, 3, 4, 5, 3, 4, 5, 3, 4, 5,
+                                     6, 7, 8, 9, 10, 11, 6, 7, 8, 12, 13, 14};
+    const int n = gauged ? 30 : 24;
+    for (int k = 0; k < n; k++) sfa_add_column(sfa, names[k], dt, sem[k], comp[k]);
+}
+
+typedef struct {
+    scp_gpu *h;
+    int ncols, precision;
+    void *cols[30];       /* snapshot staging in the output dtype */
+} Snap;
+
+static int snap_write(SFA *sfa, Snap *s, double t) {
+    const int dt = s->precision == 0 ? SCP_DTYPE_F16 : (s->precision == 1 ? SCP_DTYPE_F32 : SCP_DTYPE_F64);
+    int rc = scp_gpu_snapshot(s->h, dt, s->cols);
+    if (rc) return rc;
+    sfa_write_frame(sfa, t, s->cols);
+    return 0;
+}
+
+/* One diag TSV row in the reference's column set and formats
+ * (sfa/sim/scp_sim.c:2993-3003, :3045-3066). */
+static void diag_row(FILE *fp, double t, const scp_gpu_diag_out *d, int gauged) {
+    const double *v = d->v;
+    fprintf(fp, "%.2f\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e", t,
+            v[SCP_DIAG_E_PHI_KIN], v[SCP_DIAG_E_THETA_KIN], v[SCP_DIAG_E_GRAD], v[SCP_DIAG_E_MASS],
+            v[SCP_DIAG_E_POT], v[SCP_DIAG_E_TGRAD], v[SCP_DIAG_E_TMASS], v[SCP_DIAG_E_COUPLING],
+            v[SCP_DIAG_E_TOTAL], v[SCP_DIAG_PHI_MAX], v[SCP_DIAG_P_MAX], v[SCP_DIAG_P_INT], v[SCP_DIAG_THETA_RMS]);
+    fprintf(fp, "\t%.12e\t%.12e\t%.12e\t%.6e\t%.6e\t%.12e\t%.12e\t%.6e\t%.6e\t%.6e\t%.6e",
+            v[SCP_DIAG_Q_PHI], v[SCP_DIAG_Q_THETA], v[SCP_DIAG_Q_TOTAL], v[SCP_DIAG_S_MAX], v[SCP_DIAG_R_CORE],
+            v[SCP_DIAG_OMEGA_CORE], v[SCP_DIAG_Q_CORE], v[SCP_DIAG_THP1U], v[SCP_DIAG_THP1V], v[SCP_DIAG_THP2U],
+            v[SCP_DIAG_THP2V]);
+    if (gauged)
+        fprintf(fp, "\t%.6e\t%.6e\t%.12e\t%.12e", v[SCP_DIAG_GAUSS_MAX], v[SCP_DIAG_GAUSS_L2], v[SCP_DIAG_E_EM],
+                v[SCP_DIAG_Q_FLUX]);
+    fprintf(fp, "\t%.12e\t%.12e\t%.12e\n", v[SCP_DIAG_Q_P0], v[SCP_DIAG_Q_P1], v[SCP_DIAG_Q_P2]);
+}
+
+static int fail(const char *what, int rc) {
+    fprintf(stderr, "FATAL: %s: %s (%d) %s\n", what, scp_gpu_errstr(rc), rc, scp_gpu_last_cuda_error());
+    return 1;
+}
+
+int main(int argc, char **argv) {
+    Config c = cfg_defaults();
+    if (argc < 2) {
+        fprintf(stderr, "Usage: %s config.cfg [-key value ...]\n", argv[0]);
+        fprintf(stderr, "       %s input.sfa [-key value ...]   (restart from SFA)\n", argv[0]);
+        return 1;
+    }
+    const char *arg1 = argv[1];
+    const size_t len1 = strlen(arg1);
+    if (len1 > 4 && !strcmp(arg1 + len1 - 4, ".sfa")) {
+        /* restart: KVMD set covering all frames as the base config, grid from the header */
+        SFA *in = sfa_open(arg1);
+        if (!in) { fprintf(stderr, "Cannot open SFA: %s\n", arg1); return 1; }
+        static SFA_KVMDSet kv[SFA_MAX_KVMD_SETS];
+        const int n_kv = sfa_read_kvmd(in, kv, SFA_MAX_KVMD_SETS);
+        if (n_kv > 0) {
+            SFA_KVMDSet *use = &kv[0];
+            for (int i = 0; i < n_kv; i++)
+                if (kv[i].first_frame == 0xFFFFFFFF) { use = &kv[i]; break; }
+            for (int i = 0; i < use->n_pairs; i++) cfg_set(&c, use->keys[i], use->values[i]);
+        }
+        char tmp[64];
+        snprintf(tmp, sizeof tmp, "%u", in->Nx); cfg_set(&c, "N", tmp);
+        snprintf(tmp, sizeof tmp, "%.6f", in->Lx); cfg_set(&c, "L", tmp);
+        cfg_set(&c, "init", "sfa");
+        strncpy(c.init_sfa, arg1, sizeof c.init_sfa - 1);
+        c.init_frame = -1;
+        sfa_close(in);
+    } else {
+        cfg_load(&c, arg1);
+    }
+    int gpu_prec = SCP_PREC_FP64, gpu_dev = 0;
+    for (int i = 2; i + 1 < argc; i += 2) {
+        const char *key = argv[i][0] == '-' ? argv[i] + 1 : argv[i];
+        if (!strcmp(key, "gpu_precision")) gpu_prec = !strcmp(argv[i + 1], "fp32c") ? SCP_PREC_FP32C : SCP_PREC_FP64;
+        else if (!strcmp(key, "gpu_device")) gpu_dev = atoi(argv[i + 1]);
+        else cfg_set(&c, key, argv[i + 1]);
+    }
+    cfg_print(&c);
+    cfg_validate(&c);
+    if (!c.complex_phi) { fprintf(stderr, "ERROR: scp_sim_b200 runs the complex/gauged stepper (complex_phi=1)\n"); return 1; }
+    if (c.bc_type == 1) { fprintf(stderr, "ERROR: bc_type=1 is not supported by scp_sim_b200\n"); return 1; }
+    if (c.n_fabrics != 1 || c.higgs_v > 0 || c.g_gauge2 != 0 || c.n_locks > 0 || c.test_gauge_xform) {
+        fprintf(stderr, "ERROR: multi-fabric, Higgs, second gauge, locks and test_gauge_xform are not supported\n");
+        return 1;
+    }
+    if (c.bc_type == 2) { c.damp_width = 0.0; c.damp_rate = 0.0; }   /* as the CUDA reference (scp_sim.cu:5170-5172) */
+    const int gauged = c.complex_gauge && c.g_gauge != 0.0;
+    const int ncols = c.complex_gauge ? 30 : 24;
+    double *cols[30] = {0};
+    Grid *g = grid_new(&c, cols, ncols);
+    if (!g) { fprintf(stderr, "FATAL: host allocation\n"); return 1; }
+    printf("dx=%.4f dt=%.6f device=%d precision=%s\n\n", g->dx, g->dt, gpu_dev,
+           gpu_prec == SCP_PREC_FP32C ? "fp32c" : "fp64");
+    do_init(g, &c);
+
+    scp_gpu_params p;
+    memset(&p, 0, sizeof p);
+    p.N = c.N; p.L = c.L; p.dx = g->dx; p.dt = g->dt;
+    p.m2 = c.m2; p.mtheta2 = c.mtheta2; p.eta = c.eta; p.mu = c.mu; p.kappa = c.kappa;
+    p.complex_gauge = gauged; p.g_gauge = c.g_gauge;
+    p.bc_type = c.bc_type; p.damp_width = c.damp_width; p.damp_rate = c.damp_rate;
+    p.precision_mode = gpu_prec;
+    p.qdiag_radius = c.qdiag_radius; p.qdiag_probe1 = c.qdiag_probe1; p.qdiag_probe2 = c.qdiag_probe2;
+    p.gauss_project = 1; p.device = gpu_dev; p.tile_variant = 0;
+    if (c.complex_gauge && !gauged) { fprintf(stderr, "ERROR: complex_gauge=1 with g_gauge=0 is not supported\n"); return 1; }
+    scp_gpu *h = NULL;
+    int rc = scp_gpu_init(&p, (const double *const *)cols, &h);
+    if (rc) return fail("scp_gpu_init", rc);
+    free(g->mem);
+    g->mem = NULL;
+    if (gauged) {
+        scp_gpu_info inf;
+        scp_gpu_get_info(h, &inf);
+        printf("Gauss projection: %d CG iters (offset %.3e)\n", inf.cg_iterations, inf.G_offset);
+    }
+
+    const uint8_t sdt = (c.precision == 0) ? SFA_F16 : (c.precision == 1) ? SFA_F32 : SFA_F64;
+    SFA *sfa = sfa_create(c.output, c.N, c.N, c.N, c.L, c.L, c.L, g->dt);
+    if (!sfa) { fprintf(stderr, "ERROR: cannot create output file '%s'\n", c.output); return 1; }
+    sfa->flags = SFA_CODEC_COLZSTD | SFA_FLAG_STREAMING;
+    sfa_embed_kvmd(sfa, &c);
+    add_columns(sfa, sdt, c.complex_gauge);
+    sfa_finalize_header(sfa);
+    Snap snap = {h, ncols, c.precision, {0}};
+    const size_t es = (size_t)sfa_dtype_size[sdt];
+    for (int k = 0; k < ncols; k++) snap.cols[k] = malloc(es * (size_t)g->N3);
+    if ((rc = snap_write(sfa, &snap, 0.0))) return fail("snapshot", rc);
+
+    FILE *fp = fopen(c.diag_file, "w");
+    if (!fp) { fprintf(stderr, "ERROR: cannot open %s\n", c.diag_file); return 1; }
+    fprintf(fp, "t\tE_phi_kin\tE_theta_kin\tE_grad\tE_mass\tE_pot\tE_tgrad\tE_tmass\t"
+                "E_coupling\tE_total\tphi_max\tP_max\tP_int\ttheta_rms");
+    fprintf(fp, "\tQ_phi\tQ_theta\tQ_total\ts_max\tr_core\tomega_core\tQ_core\tthp1u\tthp1v\tthp2u\tthp2v");
+    if (c.complex_gauge) fprintf(fp, "\tgauss_max\tgauss_l2\tE_em\tQ_flux");
+    fprintf(fp, "\tQ_p0\tQ_p1\tQ_p2\n");
+
+    const int n_steps = (int)lround(c.T / g->dt);
+    int diag_every = (int)lround(c.diag_dt / g->dt); if (diag_every < 1) diag_every = 1;
+    int snap_every = (int)lround(c.snap_dt / g->dt); if (snap_every < 1) snap_every = 1;
+    scp_gpu_diag_out d;
+    if ((rc = scp_gpu_diag(h, &d))) return fail("diag", rc);
+    const double E0 = d.v[SCP_DIAG_E_TOTAL];
+    printf("INIT: E_total=%.4e E_pot=%.4f phi_max=%.4f P_int=%.4e theta_rms=%.3e\n\n", E0, d.v[SCP_DIAG_E_POT],
+           d.v[SCP_DIAG_PHI_MAX], d.v[SCP_DIAG_P_INT], d.v[SCP_DIAG_THETA_RMS]);
+    diag_row(fp, 0.0, &d, c.complex_gauge);
+
+    int major = diag_every * 25;
+    if (major > n_steps / 10) { major = (n_steps / 10 / diag_every) * diag_every; if (major < diag_every) major = diag_every; }
+    const double wall0 = wall_now();
+    int step = 0;
+    while (step < n_steps) {
+        /* advance to the next diag or snapshot step in one call */
+        int next = n_steps;
+        const int nd = (step / diag_every + 1) * diag_every, ns = (step / snap_every + 1) * snap_every;
+        if (nd < next) next = nd;
+        if (ns < next) next = ns;
+        if ((rc = scp_gpu_step(h, next - step))) return fail("step", rc);
+        step = next;
+        const double t = step * g->dt;
+        if (step % snap_every == 0 && (rc = snap_write(sfa, &snap, t))) return fail("snapshot", rc);
+        if (step % diag_every == 0) {
+            if ((rc = scp_gpu_diag(h, &d))) return fail("diag", rc);
+            diag_row(fp, t, &d, c.complex_gauge);
+            fflush(fp);
+            if (step % major == 0) {
+                const double wall = wall_now() - wall0;
+                printf("t=%7.1f E=%.3e (drift %+.3f%%) Ep=%.1f phi=%.3f Q=%.6e ", t, d.v[SCP_DIAG_E_TOTAL],
+                       100 * (d.v[SCP_DIAG_E_TOTAL] - E0) / (fabs(E0) + 1e-30), d.v[SCP_DIAG_E_POT],
+                       d.v[SCP_DIAG_PHI_MAX], d.v[SCP_DIAG_Q_TOTAL]);
+                if (c.complex_gauge) printf("gauss=%.1e E_em=%.3e ", d.v[SCP_DIAG_GAUSS_MAX], d.v[SCP_DIAG_E_EM]);
+                printf("[%.0f%% %.1fs %.3fms/step]\n", 100.0 * step / n_steps, wall, 1000 * wall / step);
+                fflush(stdout);
+            }
+        }
+    }
+    if ((rc = scp_gpu_sync(h))) return fail("sync", rc);
+    const double wall = wall_now() - wall0;
+    {   /* final frame unless the last step was (nearly) a snapshot step (scp_sim.c:3254-3259) */
+        const int last = (n_steps / snap_every) * snap_every;
+        if (n_steps - last > snap_every / 2 && (rc = snap_write(sfa, &snap, n_steps * g->dt))) return fail("snapshot", rc);
+    }
+    const uint32_t nf = sfa->total_frames;
+    sfa_close(sfa);
+    if ((rc = scp_gpu_diag(h, &d))) return fail("diag", rc);
+    printf("\n=== COMPLETE ===\n");
+    printf("E_total=%.4e (drift %.3f%%) E_pot=%.4f\n", d.v[SCP_DIAG_E_TOTAL],
+           100 * (d.v[SCP_DIAG_E_TOTAL] - E0) / (fabs(E0) + 1e-30), d.v[SCP_DIAG_E_POT]);
+    printf("Q_phi=%.6e Q_theta=%.6e Q_total=%.6e s_max=%.4e r_core=%.3f omega_core=%.4f Q_core=%.6e\n",
+           d.v[SCP_DIAG_Q_PHI], d.v[SCP_DIAG_Q_THETA], d.v[SCP_DIAG_Q_TOTAL], d.v[SCP_DIAG_S_MAX],
+           d.v[SCP_DIAG_R_CORE], d.v[SCP_DIAG_OMEGA_CORE], d.v[SCP_DIAG_Q_CORE]);
+    if (c.complex_gauge)
+        printf("gauss_max=%.3e gauss_l2=%.3e E_em=%.6e Q_flux=%.6e\n", d.v[SCP_DIAG_GAUSS_MAX],
+               d.v[SCP_DIAG_GAUSS_L2], d.v[SCP_DIAG_E_EM], d.v[SCP_DIAG_Q_FLUX]);
+    printf("SFA: %s (%u frames)\n", c.output, nf);
+    printf("Wall: %.1fs (%.1f min) %.3fms/step\n", wall, wall / 60, n_steps ? 1000 * wall / n_steps : 0.0);
+    fclose(fp);
+    for (int k = 0; k < ncols; k++) free(snap.cols[k]);
+    scp_gpu_free(h);
+    free(g);
+    return 0;
+}

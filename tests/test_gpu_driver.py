@@ -1,0 +1,76 @@
+"""The config-driven host driver (scp_b200/host/scp_sim_b200, the reference's
+main flow on top of the C ABI) against the reference binary on the same
+config file and seed: same SFA schema, same frames, same diag TSV."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from scp_b200 import seeds
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "scp_b200", "host", "scp_sim_b200")
+
+
+def _run(binary, cfg, cwd):
+    env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1))
+    r = subprocess.run([binary, cfg], capture_output=True, text=True, cwd=cwd, env=env)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    return r.stdout
+
+
+@pytest.mark.parametrize("gauged", [False, True])
+def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
+    assert os.path.exists(DRIVER), "host driver not built (make -C scp_b200/host)"
+    st = seeds.small_state(16, gauged, seed=13)
+    p = st.params
+    seed = str(tmp_path / "seed.sfa")
+    oracle.write_seed(seed, p, st.cols())
+    nsteps = 40
+    outs = {}
+    for name, binary in (("ref", oracle.REF_BIN), ("b200", DRIVER)):
+        d = tmp_path / name
+        d.mkdir()
+        cfg = d / "run.cfg"
+        cfg.write_text(p.to_cfg(init="sfa", init_sfa=seed, init_frame=0, T=repr(nsteps * p.dt), precision="f64",
+                                output=str(d / "out.sfa"), diag_file=str(d / "diag.tsv"),
+                                snap_dt=repr(nsteps // 2 * p.dt), diag_dt=repr(10 * p.dt)))
+        _run(binary, str(cfg), str(d))
+        hdr, rows = oracle.read_diag(str(d / "diag.tsv"))
+        frames = [oracle.read_frame(str(d / "out.sfa"), f, p.N ** 3) for f in (0, 1, 2)]
+        outs[name] = (hdr, rows, frames)
+    (hr, rr, fr), (hb, rb, fb) = outs["ref"], outs["b200"]
+    assert hr == hb and rr.shape == rb.shape
+    for f in range(3):
+        assert fr[f][0] == fb[f][0]                                   # column names and order
+        for a, b in zip(fr[f][1], fb[f][1]):
+            nb = np.linalg.norm(a)
+            assert np.linalg.norm(a - b) <= 1e-11 * max(nb, 1e-30) + 1e-300
+    for ci, h in enumerate(hr):
+        ref, got = rr[:, ci], rb[:, ci]
+        scale = np.maximum(np.abs(ref), 1e-9)
+        if h in ("gauss_max", "gauss_l2", "Q_flux", "Q_phi", "Q_theta", "Q_total", "Q_core", "Q_p0", "Q_p1",
+                 "Q_p2", "E_coupling"):
+            assert np.all(np.abs(got - ref) <= np.maximum(1e-5 * scale, 1e-12)), h
+        else:
+            assert np.all(np.abs(got - ref) <= 2e-6 * scale), h
+
+
+def test_driver_restarts_from_its_snapshot(gpu, tmp_path):
+    st = seeds.small_state(12, True, seed=3)
+    p = st.params
+    seed = str(tmp_path / "seed.sfa")
+    oracle.write_seed(seed, p, st.cols())
+    cfg = tmp_path / "run.cfg"
+    cfg.write_text(p.to_cfg(init="sfa", init_sfa=seed, init_frame=0, T=repr(20 * p.dt), precision="f64",
+                            output=str(tmp_path / "a.sfa"), diag_file=str(tmp_path / "a.tsv"),
+                            snap_dt=repr(20 * p.dt), diag_dt=repr(10 * p.dt)))
+    _run(DRIVER, str(cfg), str(tmp_path))
+    r = subprocess.run([DRIVER, str(tmp_path / "a.sfa"), "-T", repr(10 * p.dt), "-output", str(tmp_path / "b.sfa"),
+                        "-diag_file", str(tmp_path / "b.tsv")], capture_output=True, text=True, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr[-2000:]
+    names, cols = oracle.read_frame(str(tmp_path / "b.sfa"), -1, p.N ** 3)
+    assert len(names) == 30 and all(np.all(np.isfinite(c)) for c in cols)
