@@ -1,13 +1,25 @@
-"""Benchmark of the B200 lattice stepper (see DESIGN.md for the accounting).
+"""Benchmark of the B200 lattice stepper.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c0|c2|c2f|c4f]
+                    [--workload c1|c0|c2|c2f|c4f|c3]
 
 One step = one leapfrog step over the whole grid of the workload.  The
 default workload is the gauged FP64 128^3 two-ball run (e = 0.1, dx = 0.5,
 dt = 0.1).  Under torchrun (N > 1) every rank runs an independent replica
 (the stepper does not shard); the reported value is the sum over ranks
 divided by the slowest rank's time.
+
+Roofline accounting: the algorithmic bytes of one site-update are every
+persistent state word read once and written once (FP64 gauged 2 x 30 x 8 =
+480 B, ungauged 384 B; FP32-compensated gauged 2 x 156 = 312 B, ungauged
+240 B), as reported by scp_gpu_get_info; achieved GB/s = those bytes x sites
+x steps / device time of the timed steps (CUDA events on the stepping
+stream).
+
+Workload c3 is the served mixed queue: R requests (default 512) of grid
+sizes 32..128 arriving as a Poisson process, run through the
+continuous-batching server in FP32-compensated mode, against the same
+requests run one after another in FP64 through scp_gpu handles.
 """
 from __future__ import annotations
 
@@ -33,6 +45,7 @@ WORKLOADS = {
     "c2": ("c2", 0, "gauged FP64 256^3 + N(0,0.01) thermal noise"),
     "c2f": ("c2", 1, "gauged FP32-compensated 256^3 + N(0,0.01) thermal noise"),
     "c4f": ("c4", 1, "gauged FP32-compensated 512^3, eight co-phase balls"),
+    "c3": (None, 1, "served mixed queue, FP32-compensated, Poisson arrivals, N in 32..128 (seed 2)"),
 }
 METRIC = "site-updates/s"
 
@@ -147,6 +160,71 @@ def run_reference_arm(args, rank, world):
     return line
 
 
+def step_bytes(params) -> float:
+    """Algorithmic bytes per site-update of the layout params select (the
+    figure scp_gpu_get_info reports)."""
+    nf = 15 if params.complex_gauge else 12
+    if params.precision == 0:
+        return 2.0 * 8.0 * nf
+    return 2.0 * (4.0 * nf + 24.0 + (12.0 if params.complex_gauge else 0.0) + 4.0 * nf)
+
+
+def run_served_mix(args) -> dict:
+    """Served mixed queue (c3): aggregate site-updates/s of the server over
+    the whole makespan (submission of the first request to completion of the
+    last), per-request latency percentiles, and the same requests one after
+    another in FP64 through scp_gpu handles."""
+    from scp_b200 import serve
+    reqs = serve.served_mix(n=args.requests, seed=2, rate=args.rate)
+    total = sum(r.site_updates for r in reqs)
+    algo = sum(step_bytes(r.params) * r.site_updates for r in reqs)
+    with serve.Server(device=0, max_active=args.max_active, chunk_steps=25) as srv:
+        clk = Clocks(0)
+        clk.start()
+        ids, makespan, lat = serve.run_served(reqs, srv, realtime=True)
+        clocks = clk.stop()
+        st = srv.stats()
+        bad = [i for i in ids if srv.status(i).state != serve.DONE]
+    if bad:
+        raise RuntimeError(f"{len(bad)} served requests failed")
+    value = total / makespan
+    seq = None
+    if not args.no_sequential:
+        nseq = len(reqs) if args.seq_sample <= 0 else min(args.seq_sample, len(reqs))
+        sub = reqs[:nseq]
+        t = serve.run_sequential(sub)
+        seq = {"value": sum(r.site_updates for r in sub) / t, "unit": METRIC, "requests": nseq,
+               "precision": "fp64", "wall_s": t}
+    peaks = measured_peaks()
+    achieved = algo / makespan / 1e9
+    sizes = {}
+    for r in reqs:
+        sizes[r.params.N] = sizes.get(r.params.N, 0) + 1
+    return {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": len(reqs), "warmup": 0,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32c", "data": "synthetic",
+        "config": {"workload": WORKLOADS["c3"][2], "requests": len(reqs), "rate_per_s": args.rate,
+                   "sizes": sizes, "site_updates": total, "max_active": args.max_active, "chunk_steps": 25,
+                   "parallelism": "single-gpu", "l2": "mixed sizes; makespan-level timing"},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "max": float(lat.max())},
+        "makespan_s": makespan,
+        "sequential_fp64": seq,
+        "served_over_sequential": (value / seq["value"]) if seq else None,
+        "server_phases_s": {"load": st.t_admit, "autotune": st.t_autotune, "run_wait": st.t_run,
+                            "retire": st.t_retire, "idle_wait": st.t_wait, "chunks": st.chunks},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"], "traffic": None,
+                     "note": "algorithmic bytes of all requests / makespan (host phases included)"},
+        "gpu_launches": int(st.chunks) * 25,
+        "clocks": clocks,
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "h2d_bytes_total": int(sum(sum(c.nbytes for c in r.state.cols()) for r in reqs)),
+                "includes": "submission from host columns, load, steps, final diagnostics"},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -158,6 +236,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--n", type=int, default=0, help="override the grid edge (profiling a smaller case)")
     ap.add_argument("--tile", type=int, default=0, help="tile_variant (0 = library default)")
+    ap.add_argument("--requests", type=int, default=512, help="c3: number of requests")
+    ap.add_argument("--rate", type=float, default=50.0, help="c3: Poisson arrival rate per second")
+    ap.add_argument("--max-active", type=int, default=128, help="c3: server slots")
+    ap.add_argument("--no-sequential", action="store_true", help="c3: skip the one-after-another FP64 run")
+    ap.add_argument("--seq-sample", type=int, default=0, help="c3: run only the first R requests sequentially")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
@@ -170,11 +253,22 @@ def main():
         dist = dist_mod
 
     if args.impl == "reference":
+        if args.workload == "c3":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no request server; "
+                                  "its CPU stepper is timed on the single-run workloads"}))
+            return
         line = run_reference_arm(args, rank, world)
         if rank == 0 and line:
             print(json.dumps(line))
         if dist:
             dist.destroy_process_group()
+        return
+
+    if args.workload == "c3":
+        if world > 1:
+            raise SystemExit("c3 runs on one GPU")
+        print(json.dumps(run_served_mix(args)))
         return
 
     from scp_b200 import seeds

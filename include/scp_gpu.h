@@ -214,7 +214,9 @@ typedef struct {
 typedef struct {
     int64_t step, chunks, mem_in_use;
     int32_t n_active, n_queued, n_groups;
-    double  t_admit, t_autotune, t_run, t_retire;   /* host seconds spent per phase */
+    double  t_admit, t_autotune, t_run, t_retire;   /* host seconds spent per phase; t_admit and
+                                                       t_autotune run on the loader thread */
+    double  t_wait;           /* poll time spent waiting for a first loaded request */
 } scp_srv_stats_t;
 
 int  scp_srv_create(const scp_srv_config *cfg, scp_srv **out);
@@ -227,7 +229,9 @@ int  scp_srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *ho
                     void *const *out_cols, int out_dtype, int64_t *id_out);
 int  scp_srv_submit_borrowed(scp_srv *s, const scp_gpu_params *p, const double *const *host_cols, int64_t nsteps,
                              void *const *out_cols, int out_dtype, int64_t *id_out);
-/* Admit, run one chunk, retire; reports the active and queued counts. */
+/* Take in the requests the loader thread has initialised, finish the chunk in
+ * flight, launch the next one, retire finished requests; reports the active
+ * count and the queued count (queued, loading or loaded but not yet taken). */
 int  scp_srv_poll(scp_srv *s, int *n_active, int *n_queued);
 int  scp_srv_status(scp_srv *s, int64_t id, scp_srv_request_info *info);
 /* Final diagnostics of a finished request (SCP_EBUSY while queued/active). */

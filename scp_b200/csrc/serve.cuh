@@ -6,8 +6,11 @@
 // multi-request launches instead of scp_gpu_step:
 //
 //   submit  -> queued (host copy of the columns; caller buffers may go)
-//   poll    -> admit queued requests while active slots and the HBM budget
-//              allow; rewrite the device request tables; replay one chunk of
+//   load    -> a loader thread initialises queued requests (upload, Gauss
+//              projection, precision conversion) while active slots and the
+//              HBM budget allow, concurrently with the running chunks
+//   poll    -> take the loaded requests in; rewrite the device request
+//              tables; replay one chunk of
 //              K steps as a CUDA graph (one persistent launch per step per
 //              group of requests sharing precision, gauge mode and tile
 //              shape; groups run on forked streams); retire finished
@@ -21,6 +24,9 @@
 #pragma once
 
 #include <chrono>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 #include <deque>
 #include <map>
 #include <memory>
@@ -127,8 +133,18 @@ struct scp_srv {
     int graph_groups = -1;                                    // group count the graph was built for
     int nsm = 0;
     int64_t chunks = 0;
-    double t_admit = 0, t_autotune = 0, t_run = 0, t_retire = 0;
+    double t_admit = 0, t_autotune = 0, t_run = 0, t_retire = 0, t_wait = 0;
     bool inflight = false;                                    // a chunk is running on the GPU
+    // loader thread: queue -> (init) -> ready.  queue, ready, all, the
+    // counters below and t_admit / t_autotune are guarded by mu.
+    std::thread loader;
+    std::mutex mu;
+    std::condition_variable cv;
+    bool stop = false;
+    std::deque<SrvReq *> ready;
+    int n_loading = 0;
+    int n_held = 0;                                           // loading + ready + active
+    int64_t mem_reserved = 0;                                 // footprint of the held requests
 };
 
 static int64_t srv_footprint(const scp_gpu_params &p) {
@@ -140,13 +156,14 @@ static int64_t srv_footprint(const scp_gpu_params &p) {
 }
 
 // time each compiled tile shape on a scratch state and keep the fastest
+// (loader thread; the chunks of the active requests run meanwhile, so the
+// shapes are compared under the same load)
 static int srv_autotune(scp_srv *s, const scp_gpu_params &p, int *shape_out) {
     const auto key = std::make_tuple((int)p.N, (int)(p.complex_gauge != 0), (int)p.precision_mode);
     auto it = s->tuned.find(key);
     if (it != s->tuned.end()) { *shape_out = it->second; return SCP_OK; }
     if (!s->cfg.autotune) { *shape_out = 1; s->tuned[key] = 1; return SCP_OK; }
     const double t0 = now_s();
-    if (s->inflight) CK(cudaStreamSynchronize(s->stream));   // time the shapes on an idle GPU
     const int64_t n3 = (int64_t)p.N * p.N * p.N;
     const int ncols = p.complex_gauge ? 30 : 24;
     std::vector<double> zero((size_t)n3, 0.0), bump((size_t)n3, 0.0);
@@ -171,6 +188,7 @@ static int srv_autotune(scp_srv *s, const scp_gpu_params &p, int *shape_out) {
     }
     s->tuned[key] = best_shape;
     *shape_out = best_shape;
+    std::lock_guard<std::mutex> lk(s->mu);
     s->t_autotune += now_s() - t0;
     return SCP_OK;
 }
@@ -260,30 +278,36 @@ static int srv_upload_tables(scp_srv *s) {
     return SCP_OK;
 }
 
-// capture K steps of every group (each on its own forked stream) into a graph
+static void srv_launch_group(const SrvGroup *g, int k) {
+    size_t sm;
+    if (g->prec == SCP_PREC_FP64)
+        multi_fn<F64>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
+            (const ReqTable<F64> *)g->d_tab, k);
+    else
+        multi_fn<F32C>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
+            (const ReqTable<F32C> *)g->d_tab, k);
+}
+
+// one chunk: every group's K steps on its own stream, forked from and joined
+// back to the server stream
+static void srv_enqueue_chunk(scp_srv *s, cudaEvent_t fork) {
+    cudaEventRecord(fork, s->stream);
+    for (auto &g : s->groups) {
+        cudaStreamWaitEvent(g->st, fork, 0);
+        for (int k = 0; k < s->cfg.chunk_steps; k++) srv_launch_group(g.get(), k);
+        cudaEventRecord(g->done, g->st);
+        cudaStreamWaitEvent(s->stream, g->done, 0);
+    }
+}
+
+// capture one chunk into a graph (rebuilt when the set of groups changes)
 static int srv_build_graph(scp_srv *s) {
     if (s->exec) { cudaGraphExecDestroy(s->exec); s->exec = nullptr; }
     if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
     cudaEvent_t fork;
     CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    cudaEventRecord(fork, s->stream);
-    for (auto &g : s->groups) {
-        cudaStreamWaitEvent(g->st, fork, 0);
-        for (int k = 0; k < s->cfg.chunk_steps; k++) {
-            if (g->prec == SCP_PREC_FP64) {
-                size_t sm;
-                MultiFn<F64> fn = multi_fn<F64>(g->shape, g->gauged, &sm);
-                fn<<<g->grid, g->threads, g->smem, g->st>>>((const ReqTable<F64> *)g->d_tab, k);
-            } else {
-                size_t sm;
-                MultiFn<F32C> fn = multi_fn<F32C>(g->shape, g->gauged, &sm);
-                fn<<<g->grid, g->threads, g->smem, g->st>>>((const ReqTable<F32C> *)g->d_tab, k);
-            }
-        }
-        cudaEventRecord(g->done, g->st);
-        cudaStreamWaitEvent(s->stream, g->done, 0);
-    }
+    srv_enqueue_chunk(s, fork);
     cudaError_t e = cudaStreamEndCapture(s->stream, &s->graph);
     cudaEventDestroy(fork);
     CK(e);
@@ -292,17 +316,35 @@ static int srv_build_graph(scp_srv *s) {
     return SCP_OK;
 }
 
-static int srv_admit(scp_srv *s) {
-    int rc, admitted = 0;
-    while (!s->queue.empty() && (int)s->active.size() < s->cfg.max_active && s->active.size() < (size_t)kMaxReq &&
-           (s->cfg.admit_per_poll <= 0 || admitted < s->cfg.admit_per_poll || s->active.empty())) {
+// may the loader take the next queued request?  (caller holds mu)  A request
+// larger than the whole budget still runs, alone.
+static bool srv_can_load(const scp_srv *s) {
+    if (s->queue.empty()) return false;
+    if (s->n_held >= s->cfg.max_active || s->n_held >= kMaxReq) return false;
+    const int64_t need = srv_footprint(s->queue.front()->p);
+    return s->cfg.mem_budget_bytes <= 0 || s->n_held == 0 || s->mem_reserved + need <= s->cfg.mem_budget_bytes;
+}
+
+// Loader thread: initialise queued requests (tile autotune, upload, Gauss
+// projection, conversion) on their own streams while the GPU runs chunks.
+// Slots and budget are reserved when a request leaves the queue and given
+// back at retirement.
+static void srv_loader(scp_srv *s) {
+    cudaSetDevice(s->cfg.device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv.wait(lk, [s] { return s->stop || srv_can_load(s); });
+        if (s->stop) return;
         SrvReq *q = s->queue.front();
-        const int64_t need = srv_footprint(q->p);
-        if (s->cfg.mem_budget_bytes > 0 && s->mem_in_use + need > s->cfg.mem_budget_bytes && !s->active.empty())
-            break;                                             // wait for memory to free up
         s->queue.pop_front();
+        const int64_t need = srv_footprint(q->p);
+        s->mem_reserved += need;
+        s->n_held++;
+        s->n_loading++;
+        lk.unlock();
+        const double t0 = now_s();
         int shape = 1;
-        if ((rc = srv_autotune(s, q->p, &shape))) return rc;
+        int rc = srv_autotune(s, q->p, &shape);
         q->p.tile_variant = shape;
         const int ncols = q->p.complex_gauge ? 30 : 24;
         const int64_t n3 = (int64_t)q->p.N * q->p.N * q->p.N;
@@ -310,27 +352,50 @@ static int srv_admit(scp_srv *s) {
         for (int c = 0; c < ncols; c++)
             cols[c] = q->borrowed.empty() ? q->cols.data() + (size_t)c * n3 : q->borrowed[c];
         q->t_admit = now_s();
-        rc = scp_gpu_init(&q->p, cols.data(), &q->h);
+        if (rc == SCP_OK) rc = scp_gpu_init(&q->p, cols.data(), &q->h);
         std::vector<double>().swap(q->cols);
         std::vector<const double *>().swap(q->borrowed);
-        admitted++;
+        lk.lock();
+        s->t_admit += now_s() - t0;
+        s->n_loading--;
+        q->bytes = need;
         if (rc != SCP_OK) {
             q->state = SCP_SRV_FAILED; q->rc = rc; q->t_done = now_s();
-            continue;
+            s->mem_reserved -= need;
+            s->n_held--;
+        } else {
+            s->ready.push_back(q);
         }
+        s->cv.notify_all();
+    }
+}
+
+// move loaded requests into the active set (poll thread), at most
+// admit_per_poll of them per poll when that is set
+static int srv_intake(scp_srv *s) {
+    std::vector<SrvReq *> got;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        const size_t cap = s->cfg.admit_per_poll > 0 ? (size_t)s->cfg.admit_per_poll : s->ready.size();
+        while (!s->ready.empty() && got.size() < cap) {
+            got.push_back(s->ready.front());
+            s->ready.pop_front();
+        }
+    }
+    int rc;
+    for (size_t n = 0; n < got.size(); n++) {
+        SrvReq *q = got[n];
         int gi;
-        if ((rc = srv_group(s, q->p.precision_mode, q->p.complex_gauge ? 1 : 0, shape, &gi))) return rc;
-        if ((int)s->groups[gi]->members.size() >= kMaxReq) {    // table full: requeue for later
-            scp_gpu_free(q->h); q->h = nullptr;
-            s->queue.push_front(q);
-            break;
+        if ((rc = srv_group(s, q->p.precision_mode, q->p.complex_gauge ? 1 : 0, q->h->shape, &gi))) {
+            std::lock_guard<std::mutex> lk(s->mu);    // hand the rest back; the caller sees the error
+            for (size_t m = got.size(); m-- > n;) s->ready.push_front(got[m]);
+            return rc;
         }
         q->group = gi;
         q->s0 = -1;                                           // set when its first chunk is launched
         q->s1 = -1;
-        q->bytes = need;
         q->state = SCP_SRV_ACTIVE;
-        s->mem_in_use += need;
+        s->mem_in_use += q->bytes;
         s->groups[gi]->members.push_back(q);
         s->active.push_back(q);
     }
@@ -350,9 +415,15 @@ static int srv_retire(scp_srv *s) {
         if (q->out_cols && q->rc == SCP_OK) q->rc = scp_gpu_snapshot(h, q->out_dtype, q->out_cols);
         scp_gpu_free(h);
         q->h = nullptr;
-        q->state = (q->rc == SCP_OK) ? SCP_SRV_DONE : SCP_SRV_FAILED;
         q->t_done = now_s();
         s->mem_in_use -= q->bytes;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            q->state = (q->rc == SCP_OK) ? SCP_SRV_DONE : SCP_SRV_FAILED;
+            s->mem_reserved -= q->bytes;
+            s->n_held--;
+        }
+        s->cv.notify_all();
         auto &m = s->groups[q->group]->members;
         m.erase(std::remove(m.begin(), m.end(), q), m.end());
     }
@@ -378,6 +449,7 @@ int scp_srv_create(const scp_srv_config *cfg, scp_srv **out) {
         snprintf(g_cuda_err, sizeof g_cuda_err, "%s", cudaGetErrorString(e));
         return SCP_ECUDA;
     }
+    s->loader = std::thread(srv_loader, s);
     *out = s;
     return SCP_OK;
 }
@@ -389,7 +461,6 @@ static int srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *
     if (rc) return rc;
     if (p->device != s->cfg.device) return SCP_EINVAL;
     auto q = std::make_unique<SrvReq>();
-    q->id = s->next_id++;
     q->p = *p;
     q->nsteps = nsteps;
     q->out_cols = out_cols;
@@ -406,9 +477,14 @@ static int srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *
     }
     q->state = SCP_SRV_QUEUED;
     q->t_submit = now_s();
-    *id_out = q->id;
-    s->queue.push_back(q.get());
-    s->all[q->id] = std::move(q);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        q->id = s->next_id++;
+        *id_out = q->id;
+        s->queue.push_back(q.get());
+        s->all[q->id] = std::move(q);
+    }
+    s->cv.notify_all();
     return SCP_OK;
 }
 
@@ -426,11 +502,17 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
     if (!s) return SCP_EINVAL;
     CK(cudaSetDevice(s->cfg.device));
     int rc;
-    // 1. admit while the previous chunk (if any) is still running on the GPU
+    // 1. take in the requests the loader has finished; with nothing to run
+    //    on the GPU, wait briefly for the first of them
     const double t0 = now_s();
-    if ((rc = srv_admit(s))) return rc;
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        if (!s->inflight && s->active.empty() && s->ready.empty() && (s->n_loading > 0 || srv_can_load(s)))
+            s->cv.wait_for(lk, std::chrono::milliseconds(2), [s] { return !s->ready.empty(); });
+    }
+    if ((rc = srv_intake(s))) return rc;
     const double t1 = now_s();
-    s->t_admit += t1 - t0;
+    s->t_wait += t1 - t0;
     // 2. finish the chunk in flight
     if (s->inflight) {
         CK(cudaStreamSynchronize(s->stream));
@@ -440,7 +522,7 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
     }
     const double t2 = now_s();
     s->t_run += t2 - t1;
-    // 3. newly admitted requests start with the next chunk
+    // 3. newly taken requests start with the next chunk
     bool work = false;
     for (SrvReq *q : s->active) {
         if (q->s0 < 0) { q->s0 = s->step; q->s1 = s->step + q->nsteps; }
@@ -456,21 +538,7 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
         } else {
             cudaEvent_t fork;
             CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-            cudaEventRecord(fork, s->stream);
-            for (auto &g : s->groups) {
-                cudaStreamWaitEvent(g->st, fork, 0);
-                for (int k = 0; k < s->cfg.chunk_steps; k++) {
-                    size_t sm;
-                    if (g->prec == SCP_PREC_FP64)
-                        multi_fn<F64>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
-                            (const ReqTable<F64> *)g->d_tab, k);
-                    else
-                        multi_fn<F32C>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
-                            (const ReqTable<F32C> *)g->d_tab, k);
-                }
-                cudaEventRecord(g->done, g->st);
-                cudaStreamWaitEvent(s->stream, g->done, 0);
-            }
+            srv_enqueue_chunk(s, fork);
             cudaEventDestroy(fork);
             CK(cudaGetLastError());
         }
@@ -481,14 +549,20 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
     const double t3 = now_s();
     if ((rc = srv_retire(s))) return rc;
     s->t_retire += now_s() - t3;
-    if (!s->inflight && s->active.empty() && s->queue.empty() && s->stream) CK(cudaStreamSynchronize(s->stream));
+    if (!s->inflight && s->active.empty() && s->stream) CK(cudaStreamSynchronize(s->stream));
+    int queued;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        queued = (int)(s->queue.size() + s->ready.size()) + s->n_loading;
+    }
     if (n_active) *n_active = (int)s->active.size();
-    if (n_queued) *n_queued = (int)s->queue.size();
+    if (n_queued) *n_queued = queued;
     return SCP_OK;
 }
 
 int scp_srv_status(scp_srv *s, int64_t id, scp_srv_request_info *info) {
     if (!s || !info) return SCP_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->all.find(id);
     if (it == s->all.end()) return SCP_EINVAL;
     const SrvReq *q = it->second.get();
@@ -506,6 +580,7 @@ int scp_srv_status(scp_srv *s, int64_t id, scp_srv_request_info *info) {
 
 int scp_srv_result(scp_srv *s, int64_t id, scp_gpu_diag_out *diag) {
     if (!s || !diag) return SCP_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->all.find(id);
     if (it == s->all.end()) return SCP_EINVAL;
     const SrvReq *q = it->second.get();
@@ -521,18 +596,30 @@ int scp_srv_stats(scp_srv *s, scp_srv_stats_t *st) {
     st->chunks = s->chunks;
     st->mem_in_use = s->mem_in_use;
     st->n_active = (int)s->active.size();
-    st->n_queued = (int)s->queue.size();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        st->n_queued = (int)(s->queue.size() + s->ready.size()) + s->n_loading;
+        st->t_admit = s->t_admit - s->t_autotune;   // loader thread, overlapped with the chunks
+        st->t_autotune = s->t_autotune;
+    }
     st->n_groups = (int)s->groups.size();
-    st->t_admit = s->t_admit - s->t_autotune;
-    st->t_autotune = s->t_autotune;
     st->t_run = s->t_run;
     st->t_retire = s->t_retire;
+    st->t_wait = s->t_wait;
     return SCP_OK;
 }
 
 void scp_srv_free(scp_srv *s) {
     if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    if (s->loader.joinable()) s->loader.join();
     cudaSetDevice(s->cfg.device);
+    for (SrvReq *q : s->ready)
+        if (q->h) scp_gpu_free(q->h);
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (SrvReq *q : s->active)
         if (q->h) scp_gpu_free(q->h);

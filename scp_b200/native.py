@@ -72,7 +72,7 @@ class SrvStats(ctypes.Structure):
         ("step", ctypes.c_int64), ("chunks", ctypes.c_int64), ("mem_in_use", ctypes.c_int64),
         ("n_active", ctypes.c_int32), ("n_queued", ctypes.c_int32), ("n_groups", ctypes.c_int32),
         ("t_admit", ctypes.c_double), ("t_autotune", ctypes.c_double), ("t_run", ctypes.c_double),
-        ("t_retire", ctypes.c_double),
+        ("t_retire", ctypes.c_double), ("t_wait", ctypes.c_double),
     ]
 
 
