@@ -213,7 +213,8 @@ def run_served_mix(args) -> dict:
         "sequential_fp64": seq,
         "served_over_sequential": (value / seq["value"]) if seq else None,
         "server_phases_s": {"load": st.t_admit, "autotune": st.t_autotune, "run_wait": st.t_run,
-                            "retire": st.t_retire, "idle_wait": st.t_wait, "chunks": st.chunks},
+                            "retire": st.t_retire, "idle_wait": st.t_wait, "launch": st.t_launch,
+                            "gpu_chunks": st.t_gpu, "chunks": st.chunks},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"], "traffic": None,
                      "note": "algorithmic bytes of all requests / makespan (host phases included)"},

@@ -107,6 +107,7 @@ typedef struct {
     double  state_bytes_per_site;   /* persistent bytes per site of the layout */
     double  step_bytes_per_site;    /* algorithmic bytes moved per site-update */
     int32_t tile_x, tile_y, seg_len; /* tile shape in use */
+    int32_t sites_per_thread; /* 2: two-site packed FP32C kernel (even N), else 1 */
 } scp_gpu_info;
 
 typedef struct scp_gpu scp_gpu;
@@ -217,6 +218,8 @@ typedef struct {
     double  t_admit, t_autotune, t_run, t_retire;   /* host seconds spent per phase; t_admit and
                                                        t_autotune run on the loader thread */
     double  t_wait;           /* poll time spent waiting for a first loaded request */
+    double  t_launch;         /* poll time spent planning, uploading tables, launching */
+    double  t_gpu;            /* device time of the chunks (CUDA events on the server stream) */
 } scp_srv_stats_t;
 
 int  scp_srv_create(const scp_srv_config *cfg, scp_srv **out);

@@ -21,7 +21,7 @@
 #include "gauss.cuh"
 #include "reduce.cuh"
 #include "snapshot.cuh"
-#include "step.cuh"
+#include "launch.cuh"
 
 #include <math.h>
 #include <stdio.h>
@@ -45,44 +45,6 @@ static thread_local char g_cuda_err[256] = "";
     } while (0)
 
 namespace {
-
-template <class P>
-using StepFnT = void (*)(StepIO<P>, StepConsts, TileGrid);
-
-struct TileShape { int tx, ty; };
-// tile_variant 1..: fixed shapes; 0 picks the default for the mode
-static const TileShape kShapes[] = {{32, 4}, {32, 4}, {32, 8}, {16, 8}, {64, 2}};
-constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
-
-template <class P, int TX, int TY>
-StepFnT<P> pick(bool g, bool f, bool s, bool d) {
-#define SCP_SEL(G, F, S, D) if (g == G && f == F && s == S && d == D) return step_kernel<P, TX, TY, G, F, S, D>;
-    SCP_SEL(false, false, false, false) SCP_SEL(false, false, false, true)
-    SCP_SEL(false, false, true, false)  SCP_SEL(false, false, true, true)
-    SCP_SEL(false, true, false, false)  SCP_SEL(false, true, false, true)
-    SCP_SEL(false, true, true, false)   SCP_SEL(false, true, true, true)
-    SCP_SEL(true, false, false, false)  SCP_SEL(true, false, false, true)
-    SCP_SEL(true, false, true, false)   SCP_SEL(true, false, true, true)
-    SCP_SEL(true, true, false, false)   SCP_SEL(true, true, false, true)
-    SCP_SEL(true, true, true, false)    SCP_SEL(true, true, true, true)
-#undef SCP_SEL
-    return nullptr;
-}
-
-template <class P, int TX, int TY>
-size_t smem_of(bool g) {
-    return g ? StepLayout<P, TX, TY, true>::smem_bytes : StepLayout<P, TX, TY, false>::smem_bytes;
-}
-
-template <class P>
-StepFnT<P> step_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
-    switch (shape) {
-        case 2: *smem = smem_of<P, 32, 8>(g); return pick<P, 32, 8>(g, f, s, d);
-        case 3: *smem = smem_of<P, 16, 8>(g); return pick<P, 16, 8>(g, f, s, d);
-        case 4: *smem = smem_of<P, 64, 2>(g); return pick<P, 64, 2>(g, f, s, d);
-        default: *smem = smem_of<P, 32, 4>(g); return pick<P, 32, 4>(g, f, s, d);
-    }
-}
 
 // FP32-compensated state from FP64 staging: hi = fp32(x), lo = bf16(x - hi),
 // momenta fp32
@@ -152,6 +114,8 @@ struct scp_gpu {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // launch geometry
     int shape;
+    int pairs = 0;               // 1: two-site packed FP32C kernel
+    int threads = 0;
     TileGrid tg;
     int grid;
     int64_t steps = 0;
@@ -238,15 +202,32 @@ static int occupancy_of(scp_gpu *h, int shape, int *occ) {
     return SCP_OK;
 }
 
+static int occupancy2_of(scp_gpu *h, int shape, int *occ) {
+    size_t smem = 0;
+    for (int v = 0; v < 8; v++) {
+        StepFnT<F32C> fn = step2_fn(shape, h->gauged, v & 1, (v >> 1) & 1, (v >> 2) & 1, &smem);
+        CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    StepFnT<F32C> fn = step2_fn(shape, h->gauged, false, false, false, &smem);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, (const void *)fn, h->threads, smem));
+    return SCP_OK;
+}
+
+// FP32C grids of even N run the two-site packed kernel; the default tile is
+// 32 x 4 (one site per thread) and 32 x 8 (site pairs: 128 threads)
 static int setup_launch(scp_gpu *h) {
+    const bool pairs = h->prec == SCP_PREC_FP32C && h->N % 2 == 0;
     int shape = h->p.tile_variant;
-    if (shape == 0) shape = 1;   // 32 x 4: fastest measured default in both precisions
+    if (shape == 0) shape = pairs ? 2 : 1;
     h->shape = shape;
+    h->pairs = pairs ? 1 : 0;
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
     const TileShape ts = kShapes[shape];
+    h->threads = ts.tx * ts.ty / (pairs ? 2 : 1);
     int occ = 0, rc;
-    if (h->prec == SCP_PREC_FP64) rc = occupancy_of<F64>(h, shape, &occ);
+    if (pairs) rc = occupancy2_of(h, shape, &occ);
+    else if (h->prec == SCP_PREC_FP64) rc = occupancy_of<F64>(h, shape, &occ);
     else rc = occupancy_of<F32C>(h, shape, &occ);
     if (rc) return rc;
     if (occ < 1) return SCP_EUNSUPPORTED;
@@ -272,7 +253,6 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         io.flag = h->flag;
         fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
     } else {
-        StepFnT<F32C> fn = step_fn<F32C>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
         StepIO<F32C> io;
         io.xin = h->X32[h->cur];
         io.xout = h->X32[h->cur ^ 1];
@@ -284,7 +264,13 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         io.wout = h->W32;
         io.sout = h->S32;
         io.flag = h->flag;
-        fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+        if (h->pairs) {
+            StepFnT<F32C> fn = step2_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
+            fn<<<h->grid, h->threads, smem, h->stream>>>(io, h->c, h->tg);
+        } else {
+            StepFnT<F32C> fn = step_fn<F32C>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
+            fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+        }
     }
     CK(cudaGetLastError());
     h->cur ^= 1;
@@ -695,6 +681,7 @@ int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
     info->tile_x = kShapes[h->shape].tx;
     info->tile_y = kShapes[h->shape].ty;
     info->seg_len = h->tg.seg;
+    info->sites_per_thread = h->pairs ? 2 : 1;
     return SCP_OK;
 }
 

@@ -59,7 +59,7 @@ struct SrvReq {
 };
 
 struct SrvGroup {
-    int prec = 0, gauged = 0, shape = 1;
+    int prec = 0, gauged = 0, shape = 1, pairs = 0;
     int grid = 0, threads = 0;
     size_t smem = 0;
     void *d_tab = nullptr;        // ReqTable<P> on the device
@@ -97,23 +97,6 @@ StepIO<F32C> req_io<F32C>(scp_gpu *h, int par) {
     return io;
 }
 
-template <class P>
-using MultiFn = void (*)(const ReqTable<P> *, int);
-
-template <class P>
-MultiFn<P> multi_fn(int shape, bool g, size_t *smem) {
-    switch (shape) {
-        case 2: *smem = smem_of<P, 32, 8>(g);
-            return g ? step_multi_kernel<P, 32, 8, true> : step_multi_kernel<P, 32, 8, false>;
-        case 3: *smem = smem_of<P, 16, 8>(g);
-            return g ? step_multi_kernel<P, 16, 8, true> : step_multi_kernel<P, 16, 8, false>;
-        case 4: *smem = smem_of<P, 64, 2>(g);
-            return g ? step_multi_kernel<P, 64, 2, true> : step_multi_kernel<P, 64, 2, false>;
-        default: *smem = smem_of<P, 32, 4>(g);
-            return g ? step_multi_kernel<P, 32, 4, true> : step_multi_kernel<P, 32, 4, false>;
-    }
-}
-
 }  // namespace
 
 struct scp_srv {
@@ -126,14 +109,16 @@ struct scp_srv {
     std::vector<SrvReq *> active;
     std::map<int64_t, std::unique_ptr<SrvReq>> all;
     std::vector<std::unique_ptr<SrvGroup>> groups;
-    std::map<std::tuple<int, int, int>, int> group_of;        // (prec, gauged, shape) -> group
+    std::map<std::tuple<int, int, int, int>, int> group_of;   // (prec, gauged, shape, pairs) -> group
     std::map<std::tuple<int, int, int>, int> tuned;           // (N, gauged, prec) -> shape
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int graph_groups = -1;                                    // group count the graph was built for
     int nsm = 0;
     int64_t chunks = 0;
-    double t_admit = 0, t_autotune = 0, t_run = 0, t_retire = 0, t_wait = 0;
+    double t_admit = 0, t_autotune = 0, t_run = 0, t_retire = 0, t_wait = 0, t_launch = 0;
+    double t_gpu = 0;                                         // device time of the chunks (events)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool inflight = false;                                    // a chunk is running on the GPU
     // loader thread: queue -> (init) -> ready.  queue, ready, all, the
     // counters below and t_admit / t_autotune are guarded by mu.
@@ -193,16 +178,17 @@ static int srv_autotune(scp_srv *s, const scp_gpu_params &p, int *shape_out) {
     return SCP_OK;
 }
 
-static int srv_group(scp_srv *s, int prec, int gauged, int shape, int *gidx) {
-    const auto key = std::make_tuple(prec, gauged, shape);
+static int srv_group(scp_srv *s, int prec, int gauged, int shape, int pairs, int *gidx) {
+    const auto key = std::make_tuple(prec, gauged, shape, pairs);
     auto it = s->group_of.find(key);
     if (it != s->group_of.end()) { *gidx = it->second; return SCP_OK; }
     auto g = std::make_unique<SrvGroup>();
-    g->prec = prec; g->gauged = gauged; g->shape = shape;
-    g->threads = kShapes[shape].tx * kShapes[shape].ty;
+    g->prec = prec; g->gauged = gauged; g->shape = shape; g->pairs = pairs;
+    g->threads = kShapes[shape].tx * kShapes[shape].ty / (pairs ? 2 : 1);
     const void *fn;
     size_t tb;
-    if (prec == SCP_PREC_FP64) { fn = (const void *)multi_fn<F64>(shape, gauged, &g->smem); tb = table_bytes<F64>(); }
+    if (pairs) { fn = (const void *)multi2_fn(shape, gauged, &g->smem); tb = table_bytes<F32C>(); }
+    else if (prec == SCP_PREC_FP64) { fn = (const void *)multi_fn<F64>(shape, gauged, &g->smem); tb = table_bytes<F64>(); }
     else { fn = (const void *)multi_fn<F32C>(shape, gauged, &g->smem); tb = table_bytes<F32C>(); }
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g->smem));
     int occ = 0;
@@ -280,7 +266,10 @@ static int srv_upload_tables(scp_srv *s) {
 
 static void srv_launch_group(const SrvGroup *g, int k) {
     size_t sm;
-    if (g->prec == SCP_PREC_FP64)
+    if (g->pairs)
+        multi2_fn(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
+            (const ReqTable<F32C> *)g->d_tab, k);
+    else if (g->prec == SCP_PREC_FP64)
         multi_fn<F64>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
             (const ReqTable<F64> *)g->d_tab, k);
     else
@@ -386,7 +375,7 @@ static int srv_intake(scp_srv *s) {
     for (size_t n = 0; n < got.size(); n++) {
         SrvReq *q = got[n];
         int gi;
-        if ((rc = srv_group(s, q->p.precision_mode, q->p.complex_gauge ? 1 : 0, q->h->shape, &gi))) {
+        if ((rc = srv_group(s, q->p.precision_mode, q->p.complex_gauge ? 1 : 0, q->h->shape, q->h->pairs, &gi))) {
             std::lock_guard<std::mutex> lk(s->mu);    // hand the rest back; the caller sees the error
             for (size_t m = got.size(); m-- > n;) s->ready.push_front(got[m]);
             return rc;
@@ -443,6 +432,8 @@ int scp_srv_create(const scp_srv_config *cfg, scp_srv **out) {
     scp_srv *s = new scp_srv();
     s->cfg = *cfg;
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev1);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, cfg->device);
     if (e != cudaSuccess) {
         delete s;
@@ -516,6 +507,8 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
     // 2. finish the chunk in flight
     if (s->inflight) {
         CK(cudaStreamSynchronize(s->stream));
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, s->ev0, s->ev1) == cudaSuccess) s->t_gpu += 1e-3 * ms;
         s->step += s->cfg.chunk_steps;
         s->chunks++;
         s->inflight = false;
@@ -532,8 +525,9 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
     if (work) {
         srv_plan(s);
         if ((rc = srv_upload_tables(s))) return rc;
+        if (s->cfg.use_graph && s->graph_groups != (int)s->groups.size() && (rc = srv_build_graph(s))) return rc;
+        CK(cudaEventRecord(s->ev0, s->stream));
         if (s->cfg.use_graph) {
-            if (s->graph_groups != (int)s->groups.size() && (rc = srv_build_graph(s))) return rc;
             CK(cudaGraphLaunch(s->exec, s->stream));
         } else {
             cudaEvent_t fork;
@@ -542,8 +536,10 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
             cudaEventDestroy(fork);
             CK(cudaGetLastError());
         }
+        CK(cudaEventRecord(s->ev1, s->stream));
         s->inflight = true;
     }
+    s->t_launch += now_s() - t2;
     // 5. retire the requests that finished in the chunk just completed, while
     //    the next one runs (they are no longer in the tables)
     const double t3 = now_s();
@@ -606,6 +602,8 @@ int scp_srv_stats(scp_srv *s, scp_srv_stats_t *st) {
     st->t_run = s->t_run;
     st->t_retire = s->t_retire;
     st->t_wait = s->t_wait;
+    st->t_launch = s->t_launch;
+    st->t_gpu = s->t_gpu;
     return SCP_OK;
 }
 
@@ -631,6 +629,8 @@ void scp_srv_free(scp_srv *s) {
         if (g->st) cudaStreamDestroy(g->st);
         if (g->done) cudaEventDestroy(g->done);
     }
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }

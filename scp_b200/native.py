@@ -44,6 +44,7 @@ class Info(ctypes.Structure):
         ("tile_x", ctypes.c_int32),
         ("tile_y", ctypes.c_int32),
         ("seg_len", ctypes.c_int32),
+        ("sites_per_thread", ctypes.c_int32),
     ]
 
 
@@ -73,6 +74,7 @@ class SrvStats(ctypes.Structure):
         ("n_active", ctypes.c_int32), ("n_queued", ctypes.c_int32), ("n_groups", ctypes.c_int32),
         ("t_admit", ctypes.c_double), ("t_autotune", ctypes.c_double), ("t_run", ctypes.c_double),
         ("t_retire", ctypes.c_double), ("t_wait", ctypes.c_double),
+        ("t_launch", ctypes.c_double), ("t_gpu", ctypes.c_double),
     ]
 
 

@@ -177,15 +177,40 @@ def test_gpu_gauged_64_1000_parity(gpu):
     assert abs(d["E_total"] - r[8]) < 1e-11 * abs(r[8])
 
 
-@pytest.mark.parametrize("gauged", [False, True])
-def test_fp32c_tracks_fp64(gpu, gauged):
-    """FP32-compensated mode against FP64 on the same seed: field L2 error
-    and relative energy drift stay small over 400 steps."""
+FP32C_CASES = [(n, g, t) for n in (13, 31, 32, 40) for g in (False, True) for t in (0, 1, 3, 4)]
+
+
+@pytest.mark.parametrize("N,gauged,tile", FP32C_CASES)
+def test_fp32c_shapes_match_oracle(gpu, N, gauged, tile):
+    """FP32-compensated mode on every tile shape, with the two-site packed
+    kernel (even N) and the one-site kernel (odd N), against the FP64 checker
+    after 1 and 7 steps."""
     from scp_b200 import PREC_FP32C
+    st = seeds.small_state(N, gauged, seed=N, tile_variant=tile)
+    o = oracle.Oracle(st.params, st.cols())
+    p32 = Params(**{**st.params.__dict__, "precision": PREC_FP32C})
+    with Simulation(p32, st.cols()) as sim:
+        assert sim.info().sites_per_thread == (2 if N % 2 == 0 else 1)
+        for chunk in (1, 6):
+            sim.step(chunk)
+            o.step(chunk)
+            got, want = sim.snapshot(), o.cols()
+            errs = [rel_l2(g, w) for g, w in zip(got, want) if np.linalg.norm(w) > 1e-3 * np.sqrt(len(w))]
+            assert max(errs) < 1e-5, (chunk, max(errs))
+
+
+@pytest.mark.parametrize("N", [48, 47])
+@pytest.mark.parametrize("gauged", [False, True])
+def test_fp32c_tracks_fp64(gpu, gauged, N):
+    """FP32-compensated mode against FP64 on the same seed: field L2 error
+    and relative energy drift stay small over 400 steps (even N runs the
+    two-site packed kernel, odd N the one-site kernel)."""
+    from scp_b200 import PREC_FP32C
+    L = (N - 1) / 4.0
     if gauged:
-        st = seeds.make_state("c1", seeds.params_for("c1", N=48, L=11.75))
+        st = seeds.make_state("c1", seeds.params_for("c1", N=N, L=L))
     else:
-        st = seeds.make_state("c0", seeds.params_for("c0", N=48, L=11.75))
+        st = seeds.make_state("c0", seeds.params_for("c0", N=N, L=L))
     p64 = st.params
     p32 = Params(**{**p64.__dict__, "precision": PREC_FP32C})
     with Simulation(p64, st.cols()) as a, Simulation(p32, st.cols()) as b:
