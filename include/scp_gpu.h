@@ -196,8 +196,11 @@ typedef struct {
     int32_t chunk_steps;       /* steps per poll (graph length) */
     int32_t use_graph;         /* 1: replay chunks as a CUDA graph */
     int32_t autotune;          /* 1: time the tile shapes per grid size */
-    int32_t admit_per_poll;    /* requests initialised per poll (0 = no cap); a cap lets
-                                  the first chunks start while later requests load */
+    int32_t admit_per_poll;    /* loaded requests taken into the active set per poll
+                                  (0 = no cap) */
+    int32_t loader_threads;    /* threads initialising queued requests (upload, Gauss
+                                  projection) while chunks run; 0 = 4.  Their work runs on
+                                  high-priority streams so it interleaves with the chunks. */
 } scp_srv_config;
 
 #define SCP_SRV_QUEUED 0

@@ -5,5 +5,7 @@ namespace scp {
 StepFnT<F64> step_fn_f64(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
     return select_one<F64>(shape, g, f, s, d, smem);
 }
-MultiFn<F64> multi_fn_f64(int shape, bool g, size_t *smem) { return select_multi<F64>(shape, g, smem); }
+MultiFn<F64> multi_fn_f64(int shape, bool g, bool d, size_t *smem) {
+    return select_multi<F64>(shape, g, d, smem);
+}
 }  // namespace scp

@@ -26,17 +26,18 @@ StepFnT<P> select_one(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
     }
 }
 
+template <class P, int TX, int TY>
+MultiFn<P> pick_multi(bool g, bool d) {
+    SCP_PICK4(step_multi_kernel, P, TX, TY);
+}
+
 template <class P>
-MultiFn<P> select_multi(int shape, bool g, size_t *smem) {
+MultiFn<P> select_multi(int shape, bool g, bool d, size_t *smem) {
     switch (shape) {
-        case 2: *smem = smem_one<P, 32, 8>(g);
-            return g ? step_multi_kernel<P, 32, 8, true> : step_multi_kernel<P, 32, 8, false>;
-        case 3: *smem = smem_one<P, 16, 8>(g);
-            return g ? step_multi_kernel<P, 16, 8, true> : step_multi_kernel<P, 16, 8, false>;
-        case 4: *smem = smem_one<P, 64, 2>(g);
-            return g ? step_multi_kernel<P, 64, 2, true> : step_multi_kernel<P, 64, 2, false>;
-        default: *smem = smem_one<P, 32, 4>(g);
-            return g ? step_multi_kernel<P, 32, 4, true> : step_multi_kernel<P, 32, 4, false>;
+        case 2: *smem = smem_one<P, 32, 8>(g); return pick_multi<P, 32, 8>(g, d);
+        case 3: *smem = smem_one<P, 16, 8>(g); return pick_multi<P, 16, 8>(g, d);
+        case 4: *smem = smem_one<P, 64, 2>(g); return pick_multi<P, 64, 2>(g, d);
+        default: *smem = smem_one<P, 32, 4>(g); return pick_multi<P, 32, 4>(g, d);
     }
 }
 

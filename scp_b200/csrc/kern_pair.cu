@@ -25,12 +25,17 @@ StepFnT<F32C> step2_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem) 
     }
 }
 
-MultiFn<F32C> multi2_fn(int shape, bool g, size_t *smem) {
+template <int TX, int TY>
+static MultiFn<F32C> pick_multi2(bool g, bool d) {
+    SCP_PICK4(step2_multi_kernel, TX, TY);
+}
+
+MultiFn<F32C> multi2_fn(int shape, bool g, bool d, size_t *smem) {
     switch (shape) {
-        case 2: *smem = smem_pair<32, 8>(g); return g ? step2_multi_kernel<32, 8, true> : step2_multi_kernel<32, 8, false>;
-        case 3: *smem = smem_pair<16, 8>(g); return g ? step2_multi_kernel<16, 8, true> : step2_multi_kernel<16, 8, false>;
-        case 4: *smem = smem_pair<64, 2>(g); return g ? step2_multi_kernel<64, 2, true> : step2_multi_kernel<64, 2, false>;
-        default: *smem = smem_pair<32, 4>(g); return g ? step2_multi_kernel<32, 4, true> : step2_multi_kernel<32, 4, false>;
+        case 2: *smem = smem_pair<32, 8>(g); return pick_multi2<32, 8>(g, d);
+        case 3: *smem = smem_pair<16, 8>(g); return pick_multi2<16, 8>(g, d);
+        case 4: *smem = smem_pair<64, 2>(g); return pick_multi2<64, 2>(g, d);
+        default: *smem = smem_pair<32, 4>(g); return pick_multi2<32, 4>(g, d);
     }
 }
 

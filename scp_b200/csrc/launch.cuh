@@ -25,11 +25,12 @@ constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 // one-site kernels: g gauged, f first step, s synchronous momenta, d damping
 StepFnT<F64> step_fn_f64(int shape, bool g, bool f, bool s, bool d, size_t *smem);
 StepFnT<F32C> step_fn_f32c(int shape, bool g, bool f, bool s, bool d, size_t *smem);
-MultiFn<F64> multi_fn_f64(int shape, bool g, size_t *smem);
-MultiFn<F32C> multi_fn_f32c(int shape, bool g, size_t *smem);
+// multi-request kernels: g gauged, d damping
+MultiFn<F64> multi_fn_f64(int shape, bool g, bool d, size_t *smem);
+MultiFn<F32C> multi_fn_f32c(int shape, bool g, bool d, size_t *smem);
 // two-site packed FP32C kernels (even N)
 StepFnT<F32C> step2_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
-MultiFn<F32C> multi2_fn(int shape, bool g, size_t *smem);
+MultiFn<F32C> multi2_fn(int shape, bool g, bool d, size_t *smem);
 
 template <class P>
 StepFnT<P> step_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
@@ -42,11 +43,17 @@ inline StepFnT<F32C> step_fn<F32C>(int shape, bool g, bool f, bool s, bool d, si
     return step_fn_f32c(shape, g, f, s, d, smem);
 }
 template <class P>
-MultiFn<P> multi_fn(int shape, bool g, size_t *smem);
+MultiFn<P> multi_fn(int shape, bool g, bool d, size_t *smem);
 template <>
-inline MultiFn<F64> multi_fn<F64>(int shape, bool g, size_t *smem) { return multi_fn_f64(shape, g, smem); }
+inline MultiFn<F64> multi_fn<F64>(int shape, bool g, bool d, size_t *smem) { return multi_fn_f64(shape, g, d, smem); }
 template <>
-inline MultiFn<F32C> multi_fn<F32C>(int shape, bool g, size_t *smem) { return multi_fn_f32c(shape, g, smem); }
+inline MultiFn<F32C> multi_fn<F32C>(int shape, bool g, bool d, size_t *smem) { return multi_fn_f32c(shape, g, d, smem); }
+
+#define SCP_PICK4(KERNEL, ...)                                                                     \
+    do {                                                                                           \
+        if (g) return d ? KERNEL<__VA_ARGS__, true, true> : KERNEL<__VA_ARGS__, true, false>;       \
+        return d ? KERNEL<__VA_ARGS__, false, true> : KERNEL<__VA_ARGS__, false, false>;            \
+    } while (0)
 
 // Instantiation helpers for the kern_*.cu units.
 #define SCP_PICK16(KERNEL, ...)                                                                        \

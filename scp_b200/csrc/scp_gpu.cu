@@ -166,6 +166,7 @@ static void plan_tiles(scp_gpu *h, int tx, int ty, int slots) {
     tg.ntx = (N + tx - 1) / tx;
     tg.nty = (N + ty - 1) / ty;
     const int ntiles = tg.ntx * tg.nty;
+
     double best = 1e300;
     int best_seg = N;
     const int cands[] = {4, 6, 8, 10, 12, 16, 20, 24, 32, 48, 64, 96, 128, 192, 256, 384, 512, 1024, 2048};
@@ -374,9 +375,14 @@ static void keep_pool(int dev) {
     });
 }
 
+// Priority of the streams of handles created by this thread (0: default).  The
+// server's loader threads raise it so that request start-up interleaves with
+// the running chunks instead of queueing behind them.
+static thread_local int t_stream_priority = 0;
+
 static int alloc_common(scp_gpu *h) {
     keep_pool(h->device);
-    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, t_stream_priority));
     CK(cudaMallocAsync(&h->part, sizeof(double) * kRedMaxBlocks * 32, h->stream));
     CK(cudaMallocAsync(&h->fold, sizeof(double) * 64, h->stream));
     CK(cudaMallocAsync(&h->cg, sizeof(double) * 16, h->stream));

@@ -35,6 +35,14 @@
 
 namespace {
 
+#ifndef SCP_SRV_OVERSUB
+#define SCP_SRV_OVERSUB 8
+#endif
+constexpr int kSrvOversub = SCP_SRV_OVERSUB;
+#ifndef SCP_SRV_SEG
+#define SCP_SRV_SEG 16      // planes per work item in the multi-request launches
+#endif
+
 double now_s() {
     using namespace std::chrono;
     return duration<double>(steady_clock::now().time_since_epoch()).count();
@@ -59,7 +67,7 @@ struct SrvReq {
 };
 
 struct SrvGroup {
-    int prec = 0, gauged = 0, shape = 1, pairs = 0;
+    int prec = 0, gauged = 0, shape = 1, pairs = 0, damp = 0;
     int grid = 0, threads = 0;
     size_t smem = 0;
     void *d_tab = nullptr;        // ReqTable<P> on the device
@@ -109,7 +117,7 @@ struct scp_srv {
     std::vector<SrvReq *> active;
     std::map<int64_t, std::unique_ptr<SrvReq>> all;
     std::vector<std::unique_ptr<SrvGroup>> groups;
-    std::map<std::tuple<int, int, int, int>, int> group_of;   // (prec, gauged, shape, pairs) -> group
+    std::map<std::tuple<int, int, int, int, int>, int> group_of;   // (prec, gauged, shape, pairs, damp) -> group
     std::map<std::tuple<int, int, int>, int> tuned;           // (N, gauged, prec) -> shape
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -120,9 +128,9 @@ struct scp_srv {
     double t_gpu = 0;                                         // device time of the chunks (events)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool inflight = false;                                    // a chunk is running on the GPU
-    // loader thread: queue -> (init) -> ready.  queue, ready, all, the
-    // counters below and t_admit / t_autotune are guarded by mu.
-    std::thread loader;
+    // loader threads: queue -> (init) -> ready.  queue, ready, all, tuned,
+    // the counters below and t_admit / t_autotune are guarded by mu.
+    std::vector<std::thread> loaders;
     std::mutex mu;
     std::condition_variable cv;
     bool stop = false;
@@ -145,9 +153,12 @@ static int64_t srv_footprint(const scp_gpu_params &p) {
 // shapes are compared under the same load)
 static int srv_autotune(scp_srv *s, const scp_gpu_params &p, int *shape_out) {
     const auto key = std::make_tuple((int)p.N, (int)(p.complex_gauge != 0), (int)p.precision_mode);
-    auto it = s->tuned.find(key);
-    if (it != s->tuned.end()) { *shape_out = it->second; return SCP_OK; }
-    if (!s->cfg.autotune) { *shape_out = 1; s->tuned[key] = 1; return SCP_OK; }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->tuned.find(key);
+        if (it != s->tuned.end()) { *shape_out = it->second; return SCP_OK; }
+    }
+    if (!s->cfg.autotune) { *shape_out = 0; return SCP_OK; }
     const double t0 = now_s();
     const int64_t n3 = (int64_t)p.N * p.N * p.N;
     const int ncols = p.complex_gauge ? 30 : 24;
@@ -171,30 +182,33 @@ static int srv_autotune(scp_srv *s, const scp_gpu_params &p, int *shape_out) {
         scp_gpu_free(h);
         if (rc == SCP_OK && ms < best) { best = ms; best_shape = shape; }
     }
-    s->tuned[key] = best_shape;
     *shape_out = best_shape;
     std::lock_guard<std::mutex> lk(s->mu);
+    s->tuned[key] = best_shape;
     s->t_autotune += now_s() - t0;
     return SCP_OK;
 }
 
-static int srv_group(scp_srv *s, int prec, int gauged, int shape, int pairs, int *gidx) {
-    const auto key = std::make_tuple(prec, gauged, shape, pairs);
+static int srv_group(scp_srv *s, int prec, int gauged, int shape, int pairs, int damp, int *gidx) {
+    const auto key = std::make_tuple(prec, gauged, shape, pairs, damp);
     auto it = s->group_of.find(key);
     if (it != s->group_of.end()) { *gidx = it->second; return SCP_OK; }
     auto g = std::make_unique<SrvGroup>();
-    g->prec = prec; g->gauged = gauged; g->shape = shape; g->pairs = pairs;
+    g->prec = prec; g->gauged = gauged; g->shape = shape; g->pairs = pairs; g->damp = damp;
     g->threads = kShapes[shape].tx * kShapes[shape].ty / (pairs ? 2 : 1);
     const void *fn;
     size_t tb;
-    if (pairs) { fn = (const void *)multi2_fn(shape, gauged, &g->smem); tb = table_bytes<F32C>(); }
-    else if (prec == SCP_PREC_FP64) { fn = (const void *)multi_fn<F64>(shape, gauged, &g->smem); tb = table_bytes<F64>(); }
-    else { fn = (const void *)multi_fn<F32C>(shape, gauged, &g->smem); tb = table_bytes<F32C>(); }
+    if (pairs) { fn = (const void *)multi2_fn(shape, gauged, damp, &g->smem); tb = table_bytes<F32C>(); }
+    else if (prec == SCP_PREC_FP64) { fn = (const void *)multi_fn<F64>(shape, gauged, damp, &g->smem); tb = table_bytes<F64>(); }
+    else { fn = (const void *)multi_fn<F32C>(shape, gauged, damp, &g->smem); tb = table_bytes<F32C>(); }
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g->smem));
     int occ = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, g->threads, g->smem));
     if (occ < 1) return SCP_EUNSUPPORTED;
-    g->grid = s->nsm * occ;
+    // 8 CTAs per resident slot: CTAs retire every few work items, so the
+    // start-up kernels of loading requests (higher stream priority) get SMs
+    // between them instead of waiting for the end of a step
+    g->grid = s->nsm * occ * kSrvOversub;
     CK(cudaMalloc(&g->d_tab, tb));
     CK(cudaMallocHost(&g->h_tab, tb));
     memset(g->h_tab, 0, tb);
@@ -220,7 +234,6 @@ static void fill_table(scp_srv *s, SrvGroup *g) {
         slot.c = q->h->c;
         slot.tg = q->h->tg;
         slot.item0 = items;
-        slot.damp = damping_on(q->h) ? 1 : 0;
         slot.s0 = q->s0;
         slot.s1 = q->s1;
         items += q->h->tg.nitems;
@@ -239,10 +252,10 @@ static void srv_plan(scp_srv *s) {
     for (SrvReq *q : s->active)
         if (q->s1 > s->step) {
             const int N = q->h->N;
-            items += (long long)q->h->tg.ntx * q->h->tg.nty * ((N + 15) / 16);
+            items += (long long)q->h->tg.ntx * q->h->tg.nty * ((N + SCP_SRV_SEG - 1) / SCP_SRV_SEG);
         }
     const long long target = 6LL * s->nsm;
-    int seg_planes = 16;
+    int seg_planes = SCP_SRV_SEG;
     while (items < target && seg_planes > 4) { seg_planes /= 2; items *= 2; }
     for (SrvReq *q : s->active) {
         TileGrid &tg = q->h->tg;
@@ -267,13 +280,13 @@ static int srv_upload_tables(scp_srv *s) {
 static void srv_launch_group(const SrvGroup *g, int k) {
     size_t sm;
     if (g->pairs)
-        multi2_fn(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
+        multi2_fn(g->shape, g->gauged, g->damp, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
             (const ReqTable<F32C> *)g->d_tab, k);
     else if (g->prec == SCP_PREC_FP64)
-        multi_fn<F64>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
+        multi_fn<F64>(g->shape, g->gauged, g->damp, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
             (const ReqTable<F64> *)g->d_tab, k);
     else
-        multi_fn<F32C>(g->shape, g->gauged, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
+        multi_fn<F32C>(g->shape, g->gauged, g->damp, &sm)<<<g->grid, g->threads, g->smem, g->st>>>(
             (const ReqTable<F32C> *)g->d_tab, k);
 }
 
@@ -320,6 +333,8 @@ static bool srv_can_load(const scp_srv *s) {
 // back at retirement.
 static void srv_loader(scp_srv *s) {
     cudaSetDevice(s->cfg.device);
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) t_stream_priority = greatest;
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
         s->cv.wait(lk, [s] { return s->stop || srv_can_load(s); });
@@ -332,7 +347,7 @@ static void srv_loader(scp_srv *s) {
         s->n_loading++;
         lk.unlock();
         const double t0 = now_s();
-        int shape = 1;
+        int shape = 0;
         int rc = srv_autotune(s, q->p, &shape);
         q->p.tile_variant = shape;
         const int ncols = q->p.complex_gauge ? 30 : 24;
@@ -375,7 +390,8 @@ static int srv_intake(scp_srv *s) {
     for (size_t n = 0; n < got.size(); n++) {
         SrvReq *q = got[n];
         int gi;
-        if ((rc = srv_group(s, q->p.precision_mode, q->p.complex_gauge ? 1 : 0, q->h->shape, q->h->pairs, &gi))) {
+        if ((rc = srv_group(s, q->p.precision_mode, q->p.complex_gauge ? 1 : 0, q->h->shape, q->h->pairs,
+                             damping_on(q->h) ? 1 : 0, &gi))) {
             std::lock_guard<std::mutex> lk(s->mu);    // hand the rest back; the caller sees the error
             for (size_t m = got.size(); m-- > n;) s->ready.push_front(got[m]);
             return rc;
@@ -396,9 +412,10 @@ static int srv_retire(scp_srv *s) {
     for (SrvReq *q : s->active) {
         if (q->s1 < 0 || q->s1 > s->step) { keep.push_back(q); continue; }
         scp_gpu *h = q->h;
-        h->cur ^= (int)(q->nsteps & 1);
-        h->steps = q->nsteps;
-        q->rc = scp_gpu_sync(h);
+        h->cur ^= (int)((q->nsteps - 1) & 1);
+        h->steps = q->nsteps - 1;
+        q->rc = scp_gpu_step(h, 1);
+        if (q->rc == SCP_OK) q->rc = scp_gpu_sync(h);
         int rc2 = scp_gpu_diag(h, &q->diag);
         if (q->rc == SCP_OK) q->rc = rc2;
         if (q->out_cols && q->rc == SCP_OK) q->rc = scp_gpu_snapshot(h, q->out_dtype, q->out_cols);
@@ -426,6 +443,7 @@ int scp_srv_create(const scp_srv_config *cfg, scp_srv **out) {
     if (!cfg || !out) return SCP_EINVAL;
     *out = nullptr;
     if (cfg->chunk_steps < 1 || cfg->chunk_steps > 4096 || cfg->max_active < 1) return SCP_EINVAL;
+    if (cfg->loader_threads < 0 || cfg->loader_threads > 64) return SCP_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || cfg->device < 0 || cfg->device >= ndev) return SCP_ENODEV;
     CK(cudaSetDevice(cfg->device));
@@ -440,7 +458,8 @@ int scp_srv_create(const scp_srv_config *cfg, scp_srv **out) {
         snprintf(g_cuda_err, sizeof g_cuda_err, "%s", cudaGetErrorString(e));
         return SCP_ECUDA;
     }
-    s->loader = std::thread(srv_loader, s);
+    const int nload = cfg->loader_threads > 0 ? cfg->loader_threads : 4;
+    for (int t = 0; t < nload; t++) s->loaders.emplace_back(srv_loader, s);
     *out = s;
     return SCP_OK;
 }
@@ -518,7 +537,9 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
     // 3. newly taken requests start with the next chunk
     bool work = false;
     for (SrvReq *q : s->active) {
-        if (q->s0 < 0) { q->s0 = s->step; q->s1 = s->step + q->nsteps; }
+        // the tables take all but the final step, which stores the synchronous
+        // momenta and runs through the single-grid kernel at retirement
+        if (q->s0 < 0) { q->s0 = s->step; q->s1 = s->step + q->nsteps - 1; }
         if (q->s1 > s->step) work = true;
     }
     // 4. launch the next chunk
@@ -614,7 +635,8 @@ void scp_srv_free(scp_srv *s) {
         s->stop = true;
     }
     s->cv.notify_all();
-    if (s->loader.joinable()) s->loader.join();
+    for (auto &t : s->loaders)
+        if (t.joinable()) t.join();
     cudaSetDevice(s->cfg.device);
     for (SrvReq *q : s->ready)
         if (q->h) scp_gpu_free(q->h);

@@ -511,11 +511,13 @@ step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
 //
 // The serving loop advances every admitted request by one step per launch.
 // Requests live in a device-resident table; request r is active for global
-// steps s0 <= s < s1, its buffers swap roles by the parity of s - s0, and
-// its last step stores the synchronous momenta.  Because all of that is
-// derived from the step counter in the table, the launches can be captured
-// once in a CUDA graph and replayed while requests come and go: the host
-// only rewrites the table between replays.
+// steps s0 <= s < s1 and its buffers swap roles by the parity of s - s0.
+// Because all of that is derived from the step counter in the table, the
+// launches can be captured once in a CUDA graph and replayed while requests
+// come and go: the host only rewrites the table between replays.  These
+// launches never store the synchronous momenta: a request's final step (the
+// one that does) runs through the single-grid kernel when it retires.  All
+// requests of one launch share the damping mode (a template parameter).
 
 constexpr int kMaxReq = 256;
 
@@ -525,7 +527,7 @@ struct ReqSlot {
     StepConsts c;
     TileGrid tg;
     int item0;            // first global work item of this request
-    int damp;
+    int pad;
     long long s0, s1;     // active global steps [s0, s1)
 };
 
@@ -537,23 +539,32 @@ struct ReqTable {
     ReqSlot<P> r[kMaxReq];
 };
 
-template <class P, int TX, int TY, bool GAUGED>
+// last request of the table whose first item is <= item
+template <class P>
+__device__ __forceinline__ int req_of_item(const ReqTable<P> *tab, int nreq, int item) {
+    int lo = 0, hi = nreq - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tab->r[mid].item0 <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <class P, int TX, int TY, bool GAUGED, bool DAMP>
 __global__ void __launch_bounds__(TX * TY, (MinBlocks<P, TX, TY, GAUGED>::value))
 step_multi_kernel(const ReqTable<P> *tab, int k) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nitems = tab->nitems, nreq = tab->nreq;
     const long long s = tab->step + k;
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-        int lo = 0, hi = nreq - 1;                 // last request with item0 <= item
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (tab->r[mid].item0 <= item) lo = mid; else hi = mid - 1;
-        }
-        const ReqSlot<P> &q = tab->r[lo];
+        const ReqSlot<P> &q = tab->r[req_of_item(tab, nreq, item)];
         if (s < q.s0 || s >= q.s1) continue;       // uniform over the CTA
-        const int par = (int)((s - q.s0) & 1);
-        step_item<P, TX, TY, GAUGED, false>(q.io[par], q.c, q.tg, item - q.item0, s == q.s1 - 1, q.damp != 0,
-                                            smem_raw);
+        // the request's arguments in registers: the table is global memory the
+        // stores of the step could alias, so reading it in place reloads it
+        const StepIO<P> io = q.io[(int)((s - q.s0) & 1)];
+        const StepConsts c = q.c;
+        const TileGrid tg = q.tg;
+        step_item<P, TX, TY, GAUGED, false>(io, c, tg, item - q.item0, false, DAMP, smem_raw);
     }
 }
 

@@ -22,6 +22,10 @@
 #include "step.cuh"
 #include "vec2.cuh"
 
+#ifndef SCP_PAIR_THREADS_PER_SM
+#define SCP_PAIR_THREADS_PER_SM 256
+#endif
+
 namespace scp {
 
 template <int TX, int TY, bool GAUGED>
@@ -35,8 +39,9 @@ struct Step2Layout {
     static constexpr int NHALO = TX + 2 * TY + (GAUGED ? 2 : 0);   // pair rows + single columns + corners
     static constexpr int HPT = (NHALO + NT - 1) / NT;
     static constexpr size_t smem_bytes = sizeof(float) * (size_t)(3 * PLANE);
-    // resident threads per SM the register allocation is sized for (255 registers)
-    static constexpr int MIN_BLOCKS = (256 / NT) > 0 ? 256 / NT : 1;
+    // resident threads per SM the register allocation is sized for
+    // (256: up to 255 registers a thread)
+    static constexpr int MIN_BLOCKS = (SCP_PAIR_THREADS_PER_SM / NT) > 0 ? SCP_PAIR_THREADS_PER_SM / NT : 1;
 };
 
 __device__ __forceinline__ V2 bf16x2_to_v2(uint32_t u) {
@@ -426,23 +431,19 @@ step2_kernel(StepIO<F32C> io, StepConsts c, TileGrid tg) {
 }
 
 // many FP32C requests of even N per launch (table semantics as step_multi_kernel)
-template <int TX, int TY, bool GAUGED>
+template <int TX, int TY, bool GAUGED, bool DAMP>
 __global__ void __launch_bounds__(Step2Layout<TX, TY, GAUGED>::NT, Step2Layout<TX, TY, GAUGED>::MIN_BLOCKS)
 step2_multi_kernel(const ReqTable<F32C> *tab, int k) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nitems = tab->nitems, nreq = tab->nreq;
     const long long s = tab->step + k;
     for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-        int lo = 0, hi = nreq - 1;                 // last request with item0 <= item
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (tab->r[mid].item0 <= item) lo = mid; else hi = mid - 1;
-        }
-        const ReqSlot<F32C> &q = tab->r[lo];
+        const ReqSlot<F32C> &q = tab->r[req_of_item(tab, nreq, item)];
         if (s < q.s0 || s >= q.s1) continue;       // uniform over the CTA
-        const int par = (int)((s - q.s0) & 1);
-        step_item2<TX, TY, GAUGED, false>(q.io[par], q.c, q.tg, item - q.item0, s == q.s1 - 1, q.damp != 0,
-                                          smem_raw);
+        const StepIO<F32C> io = q.io[(int)((s - q.s0) & 1)];
+        const StepConsts c = q.c;
+        const TileGrid tg = q.tg;
+        step_item2<TX, TY, GAUGED, false>(io, c, tg, item - q.item0, false, DAMP, smem_raw);
     }
 }
 

@@ -57,6 +57,7 @@ class SrvConfig(ctypes.Structure):
         ("use_graph", ctypes.c_int32),
         ("autotune", ctypes.c_int32),
         ("admit_per_poll", ctypes.c_int32),
+        ("loader_threads", ctypes.c_int32),
     ]
 
 

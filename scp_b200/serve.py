@@ -23,10 +23,10 @@ class Server:
     """One scp_srv instance on one device."""
 
     def __init__(self, device: int = 0, max_active: int = 64, mem_budget_bytes: int = 0, chunk_steps: int = 25,
-                 use_graph: bool = True, autotune: bool = True, admit_per_poll: int = 8):
+                 use_graph: bool = True, autotune: bool = True, admit_per_poll: int = 0, loader_threads: int = 4):
         L = native.lib()
         cfg = native.SrvConfig(device, max_active, mem_budget_bytes, chunk_steps, 1 if use_graph else 0,
-                               1 if autotune else 0, admit_per_poll)
+                               1 if autotune else 0, admit_per_poll, loader_threads)
         h = ctypes.c_void_p()
         native.check(L.scp_srv_create(ctypes.byref(cfg), ctypes.byref(h)), "scp_srv_create")
         self._h = h

@@ -54,7 +54,9 @@ def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
         scale = np.maximum(np.abs(ref), 1e-9)
         if h in ("gauss_max", "gauss_l2", "Q_flux", "Q_phi", "Q_theta", "Q_total", "Q_core", "Q_p0", "Q_p1",
                  "Q_p2", "E_coupling"):
-            assert np.all(np.abs(got - ref) <= np.maximum(1e-5 * scale, 1e-12)), h
+            # roundoff-level sums (Q_flux ~ 1e-13 in a periodic box): the floor is
+            # 1e-11, well above the summation-order noise and far below O(1) values
+            assert np.all(np.abs(got - ref) <= np.maximum(1e-5 * scale, 1e-11)), h
         else:
             assert np.all(np.abs(got - ref) <= 2e-6 * scale), h
 
