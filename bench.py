@@ -46,6 +46,7 @@ WORKLOADS = {
     "c2f": ("c2", 1, "gauged FP32-compensated 256^3 + N(0,0.01) thermal noise"),
     "c4f": ("c4", 1, "gauged FP32-compensated 512^3, eight co-phase balls"),
     "c3": (None, 1, "served mixed queue, FP32-compensated, Poisson arrivals, N in 32..128 (seed 2)"),
+    "c2acc": ("c2", 1, "gauged 256^3 + N(0,0.01) thermal noise: FP32-compensated against FP64, side by side"),
 }
 METRIC = "site-updates/s"
 
@@ -226,6 +227,107 @@ def run_served_mix(args) -> dict:
     }
 
 
+def _half_centroids(cols, params) -> np.ndarray:
+    """rho^2-weighted centroids of the x < 0 and x >= 0 halves of the box
+    (the two opposite-charge balls of the c1/c2 seeds), rho the Noether
+    charge density u*dv - v*du + tu*dtv - tv*dtu summed over components."""
+    from scp_b200 import COLUMN_NAMES
+    N = params.N
+    c = {k: np.asarray(v).reshape(-1) for k, v in zip(COLUMN_NAMES, cols)}
+    rho = np.zeros(N ** 3)
+    for a in "xyz":
+        rho += c[f"phi_{a}"] * c[f"phiim_v{a}"] - c[f"phiim_{a}"] * c[f"phi_v{a}"]
+        rho += c[f"theta_{a}"] * c[f"thetaim_v{a}"] - c[f"thetaim_{a}"] * c[f"theta_v{a}"]
+    w = (rho * rho).reshape(N, N, N)
+    x = -params.L + np.arange(N) * params.dx
+    out = []
+    for half in (slice(0, N // 2), slice(N // 2, N)):
+        wh = w[half]
+        tot = wh.sum()
+        xi = x[half]
+        out.append([float((wh.sum(axis=(1, 2)) * xi).sum() / tot), float((wh.sum(axis=(0, 2)) * x).sum() / tot),
+                    float((wh.sum(axis=(0, 1)) * x).sum() / tot)])
+    return np.array(out)
+
+
+def run_precision_compare(args) -> dict:
+    """c2acc: the c2 seed (gauged, thermal background) stepped in FP64 and in
+    FP32-compensated mode side by side; per-observable error of the FP32C run
+    against the FP64 run: energy drift, Noether charge, Gauss residual,
+    per-field relative L2 and the two half-box charge centroids."""
+    import dataclasses
+    from scp_b200 import seeds, PREC_FP32C
+    from scp_b200.api import Simulation
+    over = dict(N=args.n, L=(args.n - 1) / 4.0) if args.n else {}
+    p64 = seeds.params_for("c2", **over)
+    p32 = dataclasses.replace(p64, precision=PREC_FP32C)
+    st = seeds.make_state("c2", p64)
+    cols = st.cols()
+    del st
+    total = args.steps
+    every, snap_every = 50, max(50, total // 4)
+    series = {"fp64": [], "fp32c": []}
+    cent = {"fp64": [], "fp32c": []}
+    field_l2 = []
+    walls = {"fp64": 0.0, "fp32c": 0.0}
+    with Simulation(p64, cols) as a, Simulation(p32, cols) as b:
+        del cols
+        sims = {"fp64": a, "fp32c": b}
+        for k, sim in sims.items():
+            series[k].append(sim.diag_vector())
+        done = 0
+        while done < total:
+            n = min(every, total - done)
+            for k, sim in sims.items():
+                t0 = time.perf_counter()
+                sim.step(n)
+                sim.sync()
+                walls[k] += time.perf_counter() - t0
+                series[k].append(sim.diag_vector())
+            done += n
+            if done % snap_every == 0 or done == total:
+                snaps = {k: sim.snapshot() for k, sim in sims.items()}
+                for k in sims:
+                    cent[k].append(_half_centroids(snaps[k], p64))
+                l2 = []
+                for ca, cb in zip(snaps["fp64"], snaps["fp32c"]):
+                    na = np.linalg.norm(ca)
+                    if na > 1e-3 * np.sqrt(len(ca)):
+                        l2.append(float(np.linalg.norm(cb - ca) / na))
+                field_l2.append((done, max(l2)))
+                del snaps
+    from scp_b200 import DIAG_NAMES
+    ix = {n: i for i, n in enumerate(DIAG_NAMES)}
+    A, B = np.array(series["fp64"]), np.array(series["fp32c"])
+    e0a = A[0, ix["E_total"]]
+    drift_a = (A[:, ix["E_total"]] - e0a) / abs(e0a)
+    drift_b = (B[:, ix["E_total"]] - B[0, ix["E_total"]]) / abs(B[0, ix["E_total"]])
+    q = ix["Q_total"]
+    ca, cb = np.array(cent["fp64"]), np.array(cent["fp32c"])
+    n3 = p64.N ** 3
+    return {
+        "metric": "FP32-compensated error vs FP64", "workload": WORKLOADS["c2acc"][2], "N": p64.N, "steps": total,
+        "diag_every": every, "data": "synthetic",
+        "energy": {"rel_drift_fp64_end": float(drift_a[-1]), "rel_drift_fp32c_end": float(drift_b[-1]),
+                   "max_abs_drift_difference": float(np.max(np.abs(drift_b - drift_a))),
+                   "rel_E_total_difference_end": float(abs(B[-1, ix["E_total"]] - A[-1, ix["E_total"]]) / abs(e0a))},
+        "energy_terms_rel_difference_end": {
+            n: float(abs(B[-1, ix[n]] - A[-1, ix[n]]) / abs(e0a))
+            for n in ("E_phi_kin", "E_theta_kin", "E_grad", "E_mass", "E_pot", "E_tgrad", "E_tmass", "E_coupling",
+                      "E_em")},
+        "energy_difference_series": [float(x) for x in (B[::8, ix["E_total"]] - A[::8, ix["E_total"]]) / abs(e0a)],
+        "charge": {"Q_total_fp64_end": float(A[-1, q]), "Q_total_fp32c_end": float(B[-1, q]),
+                   "sum_abs_Q_phi_fp64_end": float(abs(A[-1, ix["Q_phi"]])),
+                   "max_abs_difference": float(np.max(np.abs(B[:, q] - A[:, q])))},
+        "gauss": {"gauss_max_fp64_max": float(A[:, ix["gauss_max"]].max()),
+                  "gauss_max_fp32c_max": float(B[:, ix["gauss_max"]].max())},
+        "field_rel_l2_max_over_columns": field_l2,
+        "centroids": {"steps": [s for s, _ in field_l2], "fp64": ca.tolist(),
+                      "max_abs_difference": float(np.max(np.abs(cb - ca)))},
+        "throughput_incl_diag": {k: n3 * total / walls[k] for k in walls},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -254,10 +356,11 @@ def main():
         dist = dist_mod
 
     if args.impl == "reference":
-        if args.workload == "c3":
+        if args.workload in ("c3", "c2acc"):
             if rank == 0:
-                print(json.dumps({"impl": "reference", "unavailable": "the reference has no request server; "
-                                  "its CPU stepper is timed on the single-run workloads"}))
+                print(json.dumps({"impl": "reference", "unavailable": "this workload exercises the library's "
+                                  "server or its two precisions, which the reference does not have; its CPU "
+                                  "stepper is timed on the single-run workloads"}))
             return
         line = run_reference_arm(args, rank, world)
         if rank == 0 and line:
@@ -270,6 +373,11 @@ def main():
         if world > 1:
             raise SystemExit("c3 runs on one GPU")
         print(json.dumps(run_served_mix(args)))
+        return
+    if args.workload == "c2acc":
+        if world > 1:
+            raise SystemExit("c2acc runs on one GPU")
+        print(json.dumps(run_precision_compare(args)))
         return
 
     from scp_b200 import seeds

@@ -133,6 +133,7 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
     const int tx = tid % TX, ty = tid / TX;
     const T dt = (T)c.dt, hdt = (T)c.hdt, idx1 = (T)c.idx1, idx2 = (T)c.idx2;
     const float dt_lo = (float)(c.dt - (double)(float)c.dt);
+    const float hdt_lo = (float)(c.hdt - (double)(float)c.hdt);
 
     {
         const int kt = item % tg.ntx;
@@ -427,19 +428,25 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             bool bad = false;
 #pragma unroll
             for (int f = 0; f < 12; f++) {
-                T v = FIRST ? w[f] : w[f] + hdt * acc[f];
-                if (DAMP && !FIRST) v *= dmp;
-                T wn, xn;
+                T v, wn, xn;
                 if constexpr (P::COMP) {
-                    // w_{n+1} = w_n + dt*a in one rounding (no damping), dt as an fp32 pair;
+                    // kicks with dt and dt/2 as fp32 pairs: the increment h*a is formed
+                    // first (hi*a + lo*a), then added to the momentum in one rounding --
+                    // folding lo*a into the momentum first would lose it below half an
+                    // ulp and run the kick with fp32(dt), a systematic energy drift
+                    const float ha = fmaf(hdt, acc[f], hdt_lo * acc[f]);
+                    v = FIRST ? w[f] : w[f] + ha;
+                    if (DAMP && !FIRST) v *= dmp;
+                    if (DAMP || FIRST) wn = v + ha;
+                    else wn = w[f] + fmaf((float)c.dt, acc[f], dt_lo * acc[f]);   // w_n + dt*a, no damping
                     // compensated drift (hi, lo) += dt*w_{n+1}
-                    if (DAMP || FIRST) wn = v + hdt * acc[f];
-                    else wn = fmaf((float)c.dt, acc[f], fmaf(dt_lo, acc[f], w[f]));
                     const float y = fmaf((float)c.dt, wn, fmaf(dt_lo, wn, bf16_to_f(lo[f])));
                     float e;
                     two_sum(ctr[f], y, &xn, &e);
                     io.loout[f * N3 + site] = f_to_bf16(e);
                 } else {
+                    v = FIRST ? w[f] : w[f] + hdt * acc[f];
+                    if (DAMP && !FIRST) v *= dmp;
                     wn = v + hdt * acc[f];
                     xn = ctr[f] + dt * wn;
                 }
@@ -454,12 +461,13 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 const T gad = (T)c.gad;
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
-                    T E = FIRST ? w[FTH + d] : w[FTH + d] + hdt * K[d];
-                    if (DAMP && !FIRST) E *= dmp;
-                    T Eh, th;
+                    T E, Eh, th;
                     if constexpr (P::COMP) {
-                        if (DAMP || FIRST) Eh = E + hdt * K[d];
-                        else Eh = fmaf((float)c.dt, K[d], fmaf(dt_lo, K[d], w[FTH + d]));
+                        const float hK = fmaf(hdt, K[d], hdt_lo * K[d]);
+                        E = FIRST ? w[FTH + d] : w[FTH + d] + hK;
+                        if (DAMP && !FIRST) E *= dmp;
+                        if (DAMP || FIRST) Eh = E + hK;
+                        else Eh = w[FTH + d] + fmaf((float)c.dt, K[d], dt_lo * K[d]);
                         const float gad_lo = (float)(c.gad - (double)(float)c.gad);
                         const float y = fmaf(gad, Eh, fmaf(gad_lo, Eh, XS(sc, NR - 3 + d, ty + 1, tx + 1)));
                         float lnew;
@@ -473,6 +481,8 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                         }
                         io.tloout[d * N3 + site] = lnew;
                     } else {
+                        E = FIRST ? w[FTH + d] : w[FTH + d] + hdt * K[d];
+                        if (DAMP && !FIRST) E *= dmp;
                         Eh = E + hdt * K[d];
                         th = link_wrap(ctr[FTH + d] + gad * Eh);
                     }

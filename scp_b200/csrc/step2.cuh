@@ -80,7 +80,7 @@ __device__ __forceinline__ void step_item2(const StepIO<F32C> &io, const StepCon
     const int tid = threadIdx.x;
     const int tx2 = tid % HX, ty = tid / HX;
     const V2 dt((float)c.dt), hdt((float)c.hdt), idx1((float)c.idx1), idx2((float)c.idx2);
-    const V2 dt_lo((float)(c.dt - (double)(float)c.dt));
+    const V2 dt_lo((float)(c.dt - (double)(float)c.dt)), hdt_lo((float)(c.hdt - (double)(float)c.hdt));
 
     const int kt = item % tg.ntx;
     const int jt = (item / tg.ntx) % tg.nty;
@@ -379,11 +379,14 @@ __device__ __forceinline__ void step_item2(const StepIO<F32C> &io, const StepCon
         bool bad = false;
 #pragma unroll
         for (int f = 0; f < 12; f++) {
-            V2 v = FIRST ? w[f] : fma2(hdt, acc[f], w[f]);
+            // kicks with dt and dt/2 as fp32 pairs: the increment is formed first and
+            // added in one rounding (lo*a folded into w first would be lost below
+            // half an ulp and run the kick with fp32(dt))
+            const V2 ha = fma2(hdt, acc[f], hdt_lo * acc[f]);
+            V2 v = FIRST ? w[f] : w[f] + ha;
             if (DAMP && !FIRST) v = v * dmp;
-            // w_{n+1} = w_n + dt*a in one rounding (no damping), dt as an fp32 pair;
+            const V2 wn = (DAMP || FIRST) ? v + ha : w[f] + fma2(dt, acc[f], dt_lo * acc[f]);
             // compensated drift (hi, lo) += dt*w_{n+1}
-            const V2 wn = (DAMP || FIRST) ? fma2(hdt, acc[f], v) : fma2(dt, acc[f], fma2(dt_lo, acc[f], w[f]));
             const V2 y = fma2(dt, wn, fma2(dt_lo, wn, bf16x2_to_v2(lo[f])));
             V2 xn, e;
             two_sum2(ctr[f], y, &xn, &e);
@@ -399,9 +402,10 @@ __device__ __forceinline__ void step_item2(const StepIO<F32C> &io, const StepCon
             const V2 gad((float)c.gad), gad_lo((float)(c.gad - (double)(float)c.gad));
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-                V2 E = FIRST ? w[FTH + d] : fma2(hdt, K[d], w[FTH + d]);
+                const V2 hK = fma2(hdt, K[d], hdt_lo * K[d]);
+                V2 E = FIRST ? w[FTH + d] : w[FTH + d] + hK;
                 if (DAMP && !FIRST) E = E * dmp;
-                const V2 Eh = (DAMP || FIRST) ? fma2(hdt, K[d], E) : fma2(dt, K[d], fma2(dt_lo, K[d], w[FTH + d]));
+                const V2 Eh = (DAMP || FIRST) ? E + hK : w[FTH + d] + fma2(dt, K[d], dt_lo * K[d]);
                 const V2 y = fma2(gad, Eh, fma2(gad_lo, Eh, S2(sc, NF + d, r0, cc)));
                 V2 th, lnew;
                 two_sum2(ctr[FTH + d], y, &th, &lnew);
