@@ -312,19 +312,21 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 const T fu[6] = {ctr[FU], ctr[FU + 1], ctr[FU + 2], ctr[FTU], ctr[FTU + 1], ctr[FTU + 2]};
                 const T fv[6] = {ctr[FV], ctr[FV + 1], ctr[FV + 2], ctr[FTV], ctr[FTV + 1], ctr[FTV + 2]};
                 T lapU[6], lapV[6];
-                T DcU[3][6], DcV[3][6];
-                T TRp_[3][3], TIp_[3][3];   // forward transports of Phi
-                T tup[3][3], tvp[3][3];     // raw Theta at x+d (current and seagull)
-                // link cos/sin at x (pass A, scp_sim.c:1072-1079) and at x - d
-                T cPd[3], sPd[3], cMd[3], sMd[3];
-#pragma unroll
-                for (int d = 0; d < 3; d++) sincos_bounded(ctr[FTH + d], &sPd[d], &cPd[d]);
-                cMd[0] = c0m; sMd[0] = s0m;
-                sincos_bounded(XS(sc, FTH + 1, ty, tx + 1), &sMd[1], &cMd[1]);
-                sincos_bounded(XS(sc, FTH + 2, ty + 1, tx), &sMd[2], &cMd[2]);
+                // covariant curls, built as the directions come in: component a is
+                // D[d = a+1][field a+2] - D[d = a+2][field a+1] (indices mod 3) of the
+                // central differences D = (transported(x+d) - transported(x-d))/(2dx);
+                // one subtraction either way round, as the reference forms it
+                T crT[3], ciT[3], crP[3], ciP[3];
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
-                    const T cP = cPd[d], sP = sPd[d], cM = cMd[d], sM = sMd[d];
+                    // link d at x (pass A, scp_sim.c:1072-1079) and at x - d
+                    T cP, sP, cM, sM;
+                    sincos_bounded(ctr[FTH + d], &sP, &cP);
+                    if (d == 0) { cM = c0m; sM = s0m; c0m = cP; s0m = sP; }
+                    else if (d == 1) sincos_bounded(XS(sc, FTH + 1, ty, tx + 1), &sM, &cM);
+                    else sincos_bounded(XS(sc, FTH + 2, ty + 1, tx), &sM, &cM);
+                    T TRpP[3], TIpP[3];   // forward transports of Phi
+                    T tup[3], tvp[3];     // raw Theta at x+d (current and seagull)
 #pragma unroll
                     for (int q = 0; q < 6; q++) {
                         const int fre = q < 3 ? FU + q : FTU + q - 3;
@@ -350,35 +352,47 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                             if (d == 0) { lapU[q] = TRp + TRm; lapV[q] = TIp + TIm; }
                             else { lapU[q] = lapU[q] + TRp + TRm; lapV[q] = lapV[q] + TIp + TIm; }
                         }
-                        DcU[d][q] = (TRp - TRm) * idx1;
-                        DcV[d][q] = (TIp - TIm) * idx1;
-                        if (q < 3) { TRp_[d][q] = TRp; TIp_[d][q] = TIp; }
-                        else { tup[d][q - 3] = up; tvp[d][q - 3] = vp; }
+                        const int qa = q < 3 ? q : q - 3;
+                        if (qa != d) {
+                            const T DR = (TRp - TRm) * idx1, DI = (TIp - TIm) * idx1;
+                            T *cr = q < 3 ? crP : crT, *ci = q < 3 ? ciP : ciT;
+                            if (qa == (d + 1) % 3) {            // plus term of a = d + 2
+                                const int a = (d + 2) % 3;
+                                if (d < (a + 2) % 3) { cr[a] = DR; ci[a] = DI; }
+                                else { cr[a] = DR - cr[a]; ci[a] = DI - ci[a]; }
+                            } else {                            // minus term of a = d + 1
+                                const int a = (d + 1) % 3;
+                                if (d < (a + 1) % 3) { cr[a] = DR; ci[a] = DI; }
+                                else { cr[a] = cr[a] - DR; ci[a] = ci[a] - DI; }
+                            }
+                        }
+                        if (q < 3) { TRpP[q] = TRp; TIpP[q] = TIp; }
+                        else { tup[q - 3] = up; tvp[q - 3] = vp; }
                     }
                     // lattice current J (scp_sim.c:1232-1249); the Theta transports are
                     // recomputed from the cached raw neighbours to keep the live set small
                     T Jg = T(0);
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
-                        const T TIt = cP * tvp[d][a] + sP * tup[d][a];
-                        const T TRt = cP * tup[d][a] - sP * tvp[d][a];
+                        const T TIt = cP * tvp[a] + sP * tup[a];
+                        const T TRt = cP * tup[a] - sP * tvp[a];
                         if constexpr (P::COMP) {
                             // u*TI - v*TR = u*(TI - v) - v*(TR - u): differences of neighbouring
                             // values instead of a difference of two O(|f|^2) products
-                            Jg += fu[a] * (TIp_[d][a] - fv[a]) - fv[a] * (TRp_[d][a] - fu[a]);
+                            Jg += fu[a] * (TIpP[a] - fv[a]) - fv[a] * (TRpP[a] - fu[a]);
                             Jg += fu[3 + a] * (TIt - fv[3 + a]) - fv[3 + a] * (TRt - fu[3 + a]);
                         } else {
-                            Jg += fu[a] * TIp_[d][a] - fv[a] * TRp_[d][a];
+                            Jg += fu[a] * TIpP[a] - fv[a] * TRpP[a];
                             Jg += fu[3 + a] * TIt - fv[3 + a] * TRt;
                         }
                     }
                     const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
                     const T WpR1 = cP * fu[d2] + sP * fv[d2], WpI1 = cP * fv[d2] - sP * fu[d2];
                     const T WpR2 = cP * fu[d1] + sP * fv[d1], WpI2 = cP * fv[d1] - sP * fu[d1];
-                    const T T12 = (fu[3 + d1] * TIp_[d][d2] - fv[3 + d1] * TRp_[d][d2])
-                                + (tup[d][d1] * WpI1 - tvp[d][d1] * WpR1);
-                    const T T21 = (fu[3 + d2] * TIp_[d][d1] - fv[3 + d2] * TRp_[d][d1])
-                                + (tup[d][d2] * WpI2 - tvp[d][d2] * WpR2);
+                    const T T12 = (fu[3 + d1] * TIpP[d2] - fv[3 + d1] * TRpP[d2])
+                                + (tup[d1] * WpI1 - tvp[d1] * WpR1);
+                    const T T21 = (fu[3 + d2] * TIpP[d1] - fv[3 + d2] * TRpP[d1])
+                                + (tup[d2] * WpI2 - tvp[d2] * WpR2);
                     K[d] = (T)c.inva * Jg - T(0.5) * eta * (T12 - T21);   // Jlat; staple added below
                 }
                 // staples (scp_sim.c:1214-1220)
@@ -389,27 +403,22 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 const T st0 = (P0 - P0jm) - (P2 - P2km);
                 const T st1 = -(P0 - P0m) + (P1 - P1km);
                 const T st2 = (P2 - P2m) - (P1 - P1jm);
-                c0m = cPd[0]; s0m = sPd[0]; P0m = P0; P2m = P2;   // x - i of the next plane
+                P0m = P0; P2m = P2;   // x - i of the next plane
                 const T stp = (T)c.stp, gg = (T)c.g;
                 K[0] = stp * st0 + gg * K[0];
                 K[1] = stp * st1 + gg * K[1];
                 K[2] = stp * st2 + gg * K[2];
 #pragma unroll
                 for (int a = 0; a < 3; a++) {
-                    const int d1 = (a + 1) % 3, d2 = (a + 2) % 3;
-                    const T reDxT = DcU[d1][3 + d2] - DcU[d2][3 + d1];
-                    const T imDxT = DcV[d1][3 + d2] - DcV[d2][3 + d1];
-                    const T reDxP = DcU[d1][d2] - DcU[d2][d1];
-                    const T imDxP = DcV[d1][d2] - DcV[d2][d1];
                     const T c6 = P::COMP ? T(0) : T(6);   // FP32C accumulated differences already
                     const T lUP = (lapU[a] - c6 * fu[a]) * idx2;
                     const T lVP = (lapV[a] - c6 * fv[a]) * idx2;
                     const T lUT = (lapU[3 + a] - c6 * fu[3 + a]) * idx2;
                     const T lVT = (lapV[3 + a] - c6 * fv[3 + a]) * idx2;
-                    acc[FU + a] = lUP - m2 * fu[a] - T(2) * Vp * fu[a] * rest[a] + eta * reDxT;
-                    acc[FV + a] = lVP - m2 * fv[a] - T(2) * Vp * fv[a] * rest[a] + eta * imDxT;
-                    acc[FTU + a] = lUT - mt2 * fu[3 + a] + eta * reDxP;
-                    acc[FTV + a] = lVT - mt2 * fv[3 + a] + eta * imDxP;
+                    acc[FU + a] = lUP - m2 * fu[a] - T(2) * Vp * fu[a] * rest[a] + eta * crT[a];
+                    acc[FV + a] = lVP - m2 * fv[a] - T(2) * Vp * fv[a] * rest[a] + eta * ciT[a];
+                    acc[FTU + a] = lUT - mt2 * fu[3 + a] + eta * crP[a];
+                    acc[FTV + a] = lVT - mt2 * fv[3 + a] + eta * ciP[a];
                 }
             }
 
