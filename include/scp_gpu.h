@@ -72,7 +72,9 @@ typedef struct {
     double  dx, dt;           /* dt = dt_factor*dx (scp_sim.c:204-205) */
     double  m2, mtheta2, eta, mu, kappa;
     int32_t complex_gauge;    /* 1: compact U(1) links on every link */
-    double  g_gauge;          /* gauge coupling; must be > 0 when complex_gauge=1 */
+    double  g_gauge;          /* gauge coupling >= 0; with complex_gauge=1 and g_gauge=0 the
+                                 ungauged dynamics run and th / E are carried unchanged, as
+                                 the reference dispatches (scp_sim.c:1586, :2820) */
     int32_t bc_type;          /* 0 absorbing sphere, 2 periodic (1 unsupported) */
     double  damp_width, damp_rate;
     int32_t precision_mode;   /* SCP_PREC_FP64 or SCP_PREC_FP32C */

@@ -23,7 +23,8 @@ struct DiagConsts {
     long long N3;
     double L, dx, dV, idx1;
     double m2, mtheta2, eta, mu, kappa;
-    int gauged;
+    int gauged;               // covariant energy, plaquette energy (g != 0)
+    int links;                // th / E columns present: Gauss residual, E_em, Q_flux
     double g, bpre;           // bpre = 1/(g^2 dx^4)
     double R2;                // qdiag_radius^2
     double Rcube;             // qdiag_radius (Q_flux cube half width)
@@ -139,8 +140,9 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagCon
         M[DM_SMAX] = fmax(M[DM_SMAX], sprod);
         S[DS_M0] += rho2;
         S[DS_CX] += x * rho2; S[DS_CY] += y * rho2; S[DS_CZ] += z * rho2;
-        // ---- Gauss law and E_em
-        if (c.gauged) {
+        // ---- Gauss law and E_em (compute_gauss: also with g = 0, where the
+        //      links are carried unchanged and only 1/2 E^2 enters E_em)
+        if (c.links) {
             const double E0 = V.p(FTH + 0, idx), E1 = V.p(FTH + 1, idx), E2 = V.p(FTH + 2, idx);
             const double divE = (E0 - V.p(FTH + 0, nm[0]) + E1 - V.p(FTH + 1, nm[1])
                                  + E2 - V.p(FTH + 2, nm[2])) / c.dx;
@@ -154,13 +156,16 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagCon
                 S[DS_GL2] += (G - c.G_offset) * (G - c.G_offset);
                 S[DS_NOM] += 1.0;
             }
-            const double ee = 0.5 * (E0 * E0 + E1 * E1 + E2 * E2);
-            const double th0 = V.q(FTH + 0, idx), th1 = V.q(FTH + 1, idx), th2 = V.q(FTH + 2, idx);
-            double bb = 0.0;
-            bb += 1.0 - cos(th0 + V.q(FTH + 1, np[0]) - V.q(FTH + 0, np[1]) - th1);
-            bb += 1.0 - cos(th1 + V.q(FTH + 2, np[1]) - V.q(FTH + 1, np[2]) - th2);
-            bb += 1.0 - cos(th2 + V.q(FTH + 0, np[2]) - V.q(FTH + 2, np[0]) - th0);
-            S[DS_EEM] += (ee + c.bpre * bb) * dV;
+            double ee = 0.5 * (E0 * E0 + E1 * E1 + E2 * E2);
+            if (c.gauged) {
+                const double th0 = V.q(FTH + 0, idx), th1 = V.q(FTH + 1, idx), th2 = V.q(FTH + 2, idx);
+                double bb = 0.0;
+                bb += 1.0 - cos(th0 + V.q(FTH + 1, np[0]) - V.q(FTH + 0, np[1]) - th1);
+                bb += 1.0 - cos(th1 + V.q(FTH + 2, np[1]) - V.q(FTH + 1, np[2]) - th2);
+                bb += 1.0 - cos(th2 + V.q(FTH + 0, np[2]) - V.q(FTH + 2, np[0]) - th0);
+                ee += c.bpre * bb;
+            }
+            S[DS_EEM] += ee * dV;
             if (fabs(x) <= c.Rcube && fabs(y) <= c.Rcube && fabs(z) <= c.Rcube) {
                 S[DS_FSUM] += divE * dV;
                 S[DS_NC] += 1.0;

@@ -93,6 +93,7 @@ struct scp_gpu {
     int N;
     long long N3;
     int gauged, nf, prec;
+    int links;                   // th / E columns carried (complex_gauge; with g = 0 they stay constant)
     int device;
     cudaStream_t stream = nullptr;
     // FP64 state
@@ -128,7 +129,7 @@ static int validate(const scp_gpu_params *p) {
     if (!p) return SCP_EINVAL;
     if (p->N < 4 || p->N > 2048) return SCP_EINVAL;
     if (!(p->dx > 0) || !(p->dt > 0)) return SCP_EINVAL;
-    if (p->complex_gauge && !(p->g_gauge > 0)) return SCP_EINVAL;
+    if (p->complex_gauge && !(p->g_gauge >= 0)) return SCP_EINVAL;
     if (p->bc_type != 0 && p->bc_type != 2) return SCP_EUNSUPPORTED;
     if (p->precision_mode != SCP_PREC_FP64 && p->precision_mode != SCP_PREC_FP32C) return SCP_EINVAL;
     if (p->tile_variant < 0 || p->tile_variant >= kNumShapes) return SCP_EINVAL;
@@ -146,9 +147,10 @@ static void fill_consts(scp_gpu *h) {
     c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
     c.dt = p.dt;
     c.hdt = 0.5 * p.dt;
-    c.g = p.complex_gauge ? p.g_gauge : 0.0;
+    const bool gauged = p.complex_gauge && p.g_gauge != 0.0;
+    c.g = gauged ? p.g_gauge : 0.0;
     c.gad = -c.g * p.dx * p.dt;
-    c.stp = p.complex_gauge ? 1.0 / (p.g_gauge * p.dx * p.dx * p.dx) : 0.0;
+    c.stp = gauged ? 1.0 / (p.g_gauge * p.dx * p.dx * p.dx) : 0.0;
     c.L = p.L; c.dx = p.dx;
     c.damp_width = p.damp_width;
     c.damp_rate = p.damp_rate;
@@ -401,7 +403,7 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     int rc;
     if ((rc = alloc_common(h))) return rc;
     const long long n3 = h->N3;
-    const int ncols = h->gauged ? 30 : 24;
+    const int ncols = h->links ? 30 : 24;
     const size_t nel = (size_t)h->nf * n3;
     const size_t blk = sizeof(double) * nel;
     // FP64 slab: X[0] = x_0 and S = v_0 stage the initial state in both modes;
@@ -427,6 +429,11 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
         }
     }
     if (h->gauged && (rc = gauss_startup(h, h->X[0], h->S))) return rc;
+    // g = 0 with link columns: the ungauged step never writes th, so both
+    // position buffers carry the same constant angles (E lives in S)
+    if (h->links && !h->gauged && h->prec == SCP_PREC_FP64)
+        CK(cudaMemcpyAsync(h->X[1] + (size_t)FTH * n3, h->X[0] + (size_t)FTH * n3, sizeof(double) * 3 * n3,
+                           cudaMemcpyDeviceToDevice, h->stream));
     if ((rc = setup_launch(h))) return rc;
     CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
     h->dev_bytes += sizeof(double) * n3;
@@ -435,7 +442,7 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     // FP32-compensated buffers: X32[0..1], W32, S32 (fp32, NF arrays), LO[0..1]
     // (bf16, 12 arrays), TLO[0..1] (fp32, 3 arrays, gauged only)
     const size_t bf = round256(sizeof(float) * nel), bl = round256(sizeof(uint16_t) * 12 * (size_t)n3);
-    const size_t bt = h->gauged ? round256(sizeof(float) * 3 * (size_t)n3) : 0;
+    const size_t bt = h->links ? round256(sizeof(float) * 3 * (size_t)n3) : 0;
     CK(cudaMallocAsync(&h->slab32, 4 * bf + 2 * bl + 2 * bt, h->stream));
     h->dev_bytes += 4 * bf + 2 * bl + 2 * bt;
     char *b = (char *)h->slab32;
@@ -445,13 +452,18 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     h->S32 = (float *)b; b += bf;
     h->LO[0] = (uint16_t *)b; b += bl;
     h->LO[1] = (uint16_t *)b; b += bl;
-    if (h->gauged) {
+    if (h->links) {
         h->TLO[0] = (float *)b; b += bt;
         h->TLO[1] = (float *)b;
     }
     to_fp32c_kernel<<<red_blocks((long long)nel), kRedThreads, 0, h->stream>>>(
         h->X[0], h->S, h->nf, n3, h->X32[0], h->LO[0], h->TLO[0], h->S32);
     CK(cudaGetLastError());
+    if (h->links && !h->gauged) {   // constant angles in both position buffers (see above)
+        CK(cudaMemcpyAsync(h->X32[1] + (size_t)FTH * n3, h->X32[0] + (size_t)FTH * n3, sizeof(float) * 3 * n3,
+                           cudaMemcpyDeviceToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->TLO[1], h->TLO[0], sizeof(float) * 3 * n3, cudaMemcpyDeviceToDevice, h->stream));
+    }
     if ((rc = launch_step(h, true, false))) return rc;
     // the FP64 staging is no longer needed: FP32C diagnostics read hi+lo directly
     CK(cudaFreeAsync(h->slab, h->stream));
@@ -478,8 +490,11 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
     h->device = p->device;
     h->N = p->N;
     h->N3 = (long long)p->N * p->N * p->N;
-    h->gauged = p->complex_gauge ? 1 : 0;
-    h->nf = h->gauged ? 15 : 12;
+    // the reference dispatches on complex_gauge && g != 0 (scp_sim.c:1586, :2820):
+    // with g = 0 it runs the ungauged dynamics and carries th / E unchanged
+    h->links = p->complex_gauge ? 1 : 0;
+    h->gauged = (p->complex_gauge && p->g_gauge != 0.0) ? 1 : 0;
+    h->nf = h->links ? 15 : 12;
     h->prec = p->precision_mode;
     fill_consts(h);
     rc = init_body(h, cols, on_device);
@@ -533,6 +548,55 @@ int scp_gpu_sync(scp_gpu *h) {
 
 }  // extern "C"
 
+// Diagnostic slots from the folded reductions: f1 = pass-1 sums then maxima,
+// f2 = pass-2 sums, pt = point values (omega_core, theta probes).
+static void diag_assemble(const double *f1, const double *f2, const double *pt, const DiagConsts &c,
+                          long long n3, double g_gauge, scp_gpu_diag_out *out) {
+    const double dV = c.dV;
+    double *o = out->v;
+    for (int q = 0; q < SCP_DIAG_NSLOTS; q++) o[q] = 0.0;
+    o[SCP_DIAG_E_PHI_KIN] = f1[DS_EPK];
+    o[SCP_DIAG_E_THETA_KIN] = f1[DS_ETK];
+    o[SCP_DIAG_E_GRAD] = f1[DS_EG];
+    o[SCP_DIAG_E_MASS] = f1[DS_EM];
+    o[SCP_DIAG_E_POT] = f1[DS_EP];
+    o[SCP_DIAG_E_TGRAD] = f1[DS_ETG];
+    o[SCP_DIAG_E_TMASS] = f1[DS_ETM];
+    o[SCP_DIAG_E_COUPLING] = f1[DS_EC];
+    // the gauged energy counts E_em (compute_energy_complex_gauge); with g = 0 the
+    // reference evaluates the ungauged energy and reports E_em separately
+    o[SCP_DIAG_E_TOTAL] = f1[DS_EPK] + f1[DS_ETK] + f1[DS_EG] + f1[DS_EM] + f1[DS_EP] + f1[DS_ETG] +
+                          f1[DS_ETM] + f1[DS_EC] + (c.gauged ? f1[DS_EEM] : 0.0);
+    o[SCP_DIAG_PHI_MAX] = f1[DS_NSUM + DM_PM];
+    o[SCP_DIAG_P_MAX] = f1[DS_NSUM + DM_PMAX];
+    o[SCP_DIAG_P_INT] = f1[DS_PINT];
+    o[SCP_DIAG_THETA_RMS] = sqrt(f1[DS_TRS] / (6.0 * (double)n3));
+    o[SCP_DIAG_Q_PHI] = f1[DS_QP] * dV;
+    o[SCP_DIAG_Q_THETA] = f1[DS_QT] * dV;
+    o[SCP_DIAG_Q_TOTAL] = f1[DS_QP] * dV + f1[DS_QT] * dV;
+    o[SCP_DIAG_S_MAX] = f1[DS_NSUM + DM_SMAX];
+    const double M0 = f1[DS_M0] * dV;
+    o[SCP_DIAG_R_CORE] = (M0 < 1e-30) ? 0.0 : sqrt(f2[0] * dV / M0);
+    o[SCP_DIAG_OMEGA_CORE] = pt[0];
+    o[SCP_DIAG_Q_CORE] = f1[DS_QC] * dV;
+    o[SCP_DIAG_THP1U] = pt[1]; o[SCP_DIAG_THP1V] = pt[2];
+    o[SCP_DIAG_THP2U] = pt[3]; o[SCP_DIAG_THP2V] = pt[4];
+    if (c.links) {   // compute_gauss (scp_sim.c:2186-2243)
+        o[SCP_DIAG_GAUSS_MAX] = f1[DS_NSUM + DM_GMAX];
+        o[SCP_DIAG_GAUSS_L2] = f1[DS_NOM] > 0 ? sqrt(f1[DS_GL2] / f1[DS_NOM]) : 0.0;
+        o[SCP_DIAG_E_EM] = f1[DS_EEM];
+        o[SCP_DIAG_Q_FLUX] = (g_gauge != 0.0) ? (f1[DS_FSUM] - c.G_offset * f1[DS_NC] * dV) / g_gauge : 0.0;
+    }
+    o[SCP_DIAG_Q_P0] = f1[DS_QP0] * dV;
+    o[SCP_DIAG_Q_P1] = f1[DS_QP1] * dV;
+    o[SCP_DIAG_Q_P2] = f1[DS_QP2] * dV;
+    if (!(M0 < 1e-30)) {
+        o[SCP_DIAG_CENTROID_X] = f1[DS_CX] * dV / M0;
+        o[SCP_DIAG_CENTROID_Y] = f1[DS_CY] * dV / M0;
+        o[SCP_DIAG_CENTROID_Z] = f1[DS_CZ] * dV / M0;
+    }
+}
+
 template <class View>
 static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
     const scp_gpu_params &p = h->p;
@@ -540,6 +604,7 @@ static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
     c.N = h->N; c.N3 = h->N3; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx; c.idx1 = 1.0 / (2.0 * p.dx);
     c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
     c.gauged = h->gauged;
+    c.links = h->links;
     c.g = h->gauged ? p.g_gauge : 0.0;
     c.bpre = h->gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
     c.R2 = p.qdiag_radius * p.qdiag_radius;
@@ -558,49 +623,8 @@ static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
     CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * 42, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(h->h_small + 48, h->point, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    const double *f1 = h->h_small, *f2 = h->h_small + 40, *pt = h->h_small + 48;
-    const double dV = c.dV;
-    double *o = out->v;
-    for (int q = 0; q < SCP_DIAG_NSLOTS; q++) o[q] = 0.0;
-    o[SCP_DIAG_E_PHI_KIN] = f1[DS_EPK];
-    o[SCP_DIAG_E_THETA_KIN] = f1[DS_ETK];
-    o[SCP_DIAG_E_GRAD] = f1[DS_EG];
-    o[SCP_DIAG_E_MASS] = f1[DS_EM];
-    o[SCP_DIAG_E_POT] = f1[DS_EP];
-    o[SCP_DIAG_E_TGRAD] = f1[DS_ETG];
-    o[SCP_DIAG_E_TMASS] = f1[DS_ETM];
-    o[SCP_DIAG_E_COUPLING] = f1[DS_EC];
-    o[SCP_DIAG_E_TOTAL] = f1[DS_EPK] + f1[DS_ETK] + f1[DS_EG] + f1[DS_EM] + f1[DS_EP] + f1[DS_ETG] +
-                          f1[DS_ETM] + f1[DS_EC] + (h->gauged ? f1[DS_EEM] : 0.0);
-    o[SCP_DIAG_PHI_MAX] = f1[DS_NSUM + DM_PM];
-    o[SCP_DIAG_P_MAX] = f1[DS_NSUM + DM_PMAX];
-    o[SCP_DIAG_P_INT] = f1[DS_PINT];
-    o[SCP_DIAG_THETA_RMS] = sqrt(f1[DS_TRS] / (6.0 * (double)h->N3));
-    o[SCP_DIAG_Q_PHI] = f1[DS_QP] * dV;
-    o[SCP_DIAG_Q_THETA] = f1[DS_QT] * dV;
-    o[SCP_DIAG_Q_TOTAL] = f1[DS_QP] * dV + f1[DS_QT] * dV;
-    o[SCP_DIAG_S_MAX] = f1[DS_NSUM + DM_SMAX];
-    const double M0 = f1[DS_M0] * dV;
-    o[SCP_DIAG_R_CORE] = (M0 < 1e-30) ? 0.0 : sqrt(f2[0] * dV / M0);
-    o[SCP_DIAG_OMEGA_CORE] = pt[0];
-    o[SCP_DIAG_Q_CORE] = f1[DS_QC] * dV;
-    o[SCP_DIAG_THP1U] = pt[1]; o[SCP_DIAG_THP1V] = pt[2];
-    o[SCP_DIAG_THP2U] = pt[3]; o[SCP_DIAG_THP2V] = pt[4];
-    if (h->gauged) {
-        o[SCP_DIAG_GAUSS_MAX] = f1[DS_NSUM + DM_GMAX];
-        o[SCP_DIAG_GAUSS_L2] = f1[DS_NOM] > 0 ? sqrt(f1[DS_GL2] / f1[DS_NOM]) : 0.0;
-        o[SCP_DIAG_E_EM] = f1[DS_EEM];
-        o[SCP_DIAG_Q_FLUX] = (f1[DS_FSUM] - h->G_offset * f1[DS_NC] * dV) / p.g_gauge;
-    }
-    o[SCP_DIAG_Q_P0] = f1[DS_QP0] * dV;
-    o[SCP_DIAG_Q_P1] = f1[DS_QP1] * dV;
-    o[SCP_DIAG_Q_P2] = f1[DS_QP2] * dV;
-    if (!(M0 < 1e-30)) {
-        o[SCP_DIAG_CENTROID_X] = f1[DS_CX] * dV / M0;
-        o[SCP_DIAG_CENTROID_Y] = f1[DS_CY] * dV / M0;
-        o[SCP_DIAG_CENTROID_Z] = f1[DS_CZ] * dV / M0;
-    }
-    if (!isfinite(o[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
+    diag_assemble(h->h_small, h->h_small + 40, h->h_small + 48, c, h->N3, p.g_gauge, out);
+    if (!isfinite(out->v[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
     return SCP_OK;
 }
 
@@ -634,7 +658,7 @@ __global__ void snap_col_kernel(View V, int field, int mom, long long n, int dty
 
 template <class View>
 static int snapshot_with(scp_gpu *h, const View &V, int dtype, void *const *host_cols) {
-    const int ncols = h->gauged ? 30 : 24;
+    const int ncols = h->links ? 30 : 24;
     const long long n3 = h->N3;
     const int nb = red_blocks(n3);
     const size_t es = dtype == SCP_DTYPE_F64 ? 8 : (dtype == SCP_DTYPE_F32 ? 4 : 2);
@@ -850,8 +874,9 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
         return SCP_EINVAL;
     }
     const scp_gpu_params &p = *pp;
-    const int gauged = p.complex_gauge ? 1 : 0;
-    const int ncols = gauged ? 30 : 24;
+    const int links = p.complex_gauge ? 1 : 0;
+    const int gauged = (p.complex_gauge && p.g_gauge != 0.0) ? 1 : 0;
+    const int ncols = links ? 30 : 24;
     ViewCols V;
     for (int f = 0; f < 15; f++) { V.pos[f] = nullptr; V.mom[f] = nullptr; }
     for (int c = 0; c < ncols; c++) {
@@ -860,7 +885,7 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
         sfa_col_source(c, &field, &mom);
         (mom ? V.mom : V.pos)[field] = dev_cols[c];
     }
-    if (!gauged)   // ungauged diagnostics never read links or E; keep the pointers valid anyway
+    if (!links)   // ungauged diagnostics never read links or E; keep the pointers valid anyway
         for (int f = FTH; f < FTH + 3; f++) { V.pos[f] = V.pos[FU]; V.mom[f] = V.mom[FU]; }
     int dev = 0;
     CK(cudaGetDevice(&dev));
@@ -875,6 +900,7 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     c.N = p.N; c.N3 = n3; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx; c.idx1 = 1.0 / (2.0 * p.dx);
     c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
     c.gauged = gauged;
+    c.links = links;
     c.g = gauged ? p.g_gauge : 0.0;
     c.bpre = gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
     c.R2 = p.qdiag_radius * p.qdiag_radius;
@@ -897,49 +923,8 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     CK(cudaMemcpyAsync(h, fold, sizeof(double) * 42, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(h + 48, point, sizeof(double) * 5, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    const double *f1 = h, *f2 = h + 40, *pt = h + 48;
-    const double dV = c.dV;
-    double *o = out->v;
-    for (int q = 0; q < SCP_DIAG_NSLOTS; q++) o[q] = 0.0;
-    o[SCP_DIAG_E_PHI_KIN] = f1[DS_EPK];
-    o[SCP_DIAG_E_THETA_KIN] = f1[DS_ETK];
-    o[SCP_DIAG_E_GRAD] = f1[DS_EG];
-    o[SCP_DIAG_E_MASS] = f1[DS_EM];
-    o[SCP_DIAG_E_POT] = f1[DS_EP];
-    o[SCP_DIAG_E_TGRAD] = f1[DS_ETG];
-    o[SCP_DIAG_E_TMASS] = f1[DS_ETM];
-    o[SCP_DIAG_E_COUPLING] = f1[DS_EC];
-    o[SCP_DIAG_E_TOTAL] = f1[DS_EPK] + f1[DS_ETK] + f1[DS_EG] + f1[DS_EM] + f1[DS_EP] + f1[DS_ETG] +
-                          f1[DS_ETM] + f1[DS_EC] + (gauged ? f1[DS_EEM] : 0.0);
-    o[SCP_DIAG_PHI_MAX] = f1[DS_NSUM + DM_PM];
-    o[SCP_DIAG_P_MAX] = f1[DS_NSUM + DM_PMAX];
-    o[SCP_DIAG_P_INT] = f1[DS_PINT];
-    o[SCP_DIAG_THETA_RMS] = sqrt(f1[DS_TRS] / (6.0 * (double)n3));
-    o[SCP_DIAG_Q_PHI] = f1[DS_QP] * dV;
-    o[SCP_DIAG_Q_THETA] = f1[DS_QT] * dV;
-    o[SCP_DIAG_Q_TOTAL] = f1[DS_QP] * dV + f1[DS_QT] * dV;
-    o[SCP_DIAG_S_MAX] = f1[DS_NSUM + DM_SMAX];
-    const double M0 = f1[DS_M0] * dV;
-    o[SCP_DIAG_R_CORE] = (M0 < 1e-30) ? 0.0 : sqrt(f2[0] * dV / M0);
-    o[SCP_DIAG_OMEGA_CORE] = pt[0];
-    o[SCP_DIAG_Q_CORE] = f1[DS_QC] * dV;
-    o[SCP_DIAG_THP1U] = pt[1]; o[SCP_DIAG_THP1V] = pt[2];
-    o[SCP_DIAG_THP2U] = pt[3]; o[SCP_DIAG_THP2V] = pt[4];
-    if (gauged) {
-        o[SCP_DIAG_GAUSS_MAX] = f1[DS_NSUM + DM_GMAX];
-        o[SCP_DIAG_GAUSS_L2] = f1[DS_NOM] > 0 ? sqrt(f1[DS_GL2] / f1[DS_NOM]) : 0.0;
-        o[SCP_DIAG_E_EM] = f1[DS_EEM];
-        o[SCP_DIAG_Q_FLUX] = (f1[DS_FSUM] - G_offset * f1[DS_NC] * dV) / p.g_gauge;
-    }
-    o[SCP_DIAG_Q_P0] = f1[DS_QP0] * dV;
-    o[SCP_DIAG_Q_P1] = f1[DS_QP1] * dV;
-    o[SCP_DIAG_Q_P2] = f1[DS_QP2] * dV;
-    if (!(M0 < 1e-30)) {
-        o[SCP_DIAG_CENTROID_X] = f1[DS_CX] * dV / M0;
-        o[SCP_DIAG_CENTROID_Y] = f1[DS_CY] * dV / M0;
-        o[SCP_DIAG_CENTROID_Z] = f1[DS_CZ] * dV / M0;
-    }
-    if (!isfinite(o[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
+    diag_assemble(h, h + 40, h + 48, c, n3, p.g_gauge, out);
+    if (!isfinite(out->v[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
     return SCP_OK;
 }
 

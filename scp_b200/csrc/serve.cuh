@@ -152,7 +152,7 @@ static int64_t srv_footprint(const scp_gpu_params &p) {
 // (loader thread; the chunks of the active requests run meanwhile, so the
 // shapes are compared under the same load)
 static int srv_autotune(scp_srv *s, const scp_gpu_params &p, int *shape_out) {
-    const auto key = std::make_tuple((int)p.N, (int)(p.complex_gauge != 0), (int)p.precision_mode);
+    const auto key = std::make_tuple((int)p.N, (int)(p.complex_gauge != 0 && p.g_gauge != 0.0), (int)p.precision_mode);
     {
         std::lock_guard<std::mutex> lk(s->mu);
         auto it = s->tuned.find(key);
@@ -390,7 +390,7 @@ static int srv_intake(scp_srv *s) {
     for (size_t n = 0; n < got.size(); n++) {
         SrvReq *q = got[n];
         int gi;
-        if ((rc = srv_group(s, q->p.precision_mode, q->p.complex_gauge ? 1 : 0, q->h->shape, q->h->pairs,
+        if ((rc = srv_group(s, q->p.precision_mode, q->h->gauged, q->h->shape, q->h->pairs,
                              damping_on(q->h) ? 1 : 0, &gi))) {
             std::lock_guard<std::mutex> lk(s->mu);    // hand the rest back; the caller sees the error
             for (size_t m = got.size(); m-- > n;) s->ready.push_front(got[m]);

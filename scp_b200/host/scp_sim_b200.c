@@ -189,12 +189,11 @@ int main(int argc, char **argv) {
     memset(&p, 0, sizeof p);
     p.N = c.N; p.L = c.L; p.dx = g->dx; p.dt = g->dt;
     p.m2 = c.m2; p.mtheta2 = c.mtheta2; p.eta = c.eta; p.mu = c.mu; p.kappa = c.kappa;
-    p.complex_gauge = gauged; p.g_gauge = c.g_gauge;
+    p.complex_gauge = c.complex_gauge; p.g_gauge = c.g_gauge;   /* g_gauge = 0: ungauged dynamics, links carried */
     p.bc_type = c.bc_type; p.damp_width = c.damp_width; p.damp_rate = c.damp_rate;
     p.precision_mode = gpu_prec;
     p.qdiag_radius = c.qdiag_radius; p.qdiag_probe1 = c.qdiag_probe1; p.qdiag_probe2 = c.qdiag_probe2;
     p.gauss_project = 1; p.device = gpu_dev; p.tile_variant = 0;
-    if (c.complex_gauge && !gauged) { fprintf(stderr, "ERROR: complex_gauge=1 with g_gauge=0 is not supported\n"); return 1; }
     scp_gpu *h = NULL;
     int rc = scp_gpu_init(&p, (const double *const *)cols, &h);
     if (rc) return fail("scp_gpu_init", rc);

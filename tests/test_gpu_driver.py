@@ -22,10 +22,15 @@ def _run(binary, cfg, cwd):
     return r.stdout
 
 
-@pytest.mark.parametrize("gauged", [False, True])
+@pytest.mark.parametrize("gauged", [False, True, "g0"])
 def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
+    """gauged="g0": complex_gauge=1 with g_gauge=0, the reference's ungauged
+    dispatch with the link columns carried."""
     assert os.path.exists(DRIVER), "host driver not built (make -C scp_b200/host)"
-    st = seeds.small_state(16, gauged, seed=13)
+    if gauged == "g0":
+        st = seeds.small_state(16, True, seed=13, g_gauge=0.0)
+    else:
+        st = seeds.small_state(16, gauged, seed=13)
     p = st.params
     seed = str(tmp_path / "seed.sfa")
     oracle.write_seed(seed, p, st.cols())

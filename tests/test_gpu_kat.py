@@ -49,6 +49,40 @@ def test_gauge_covariance(gpu):
         assert abs(da[key] - db[key]) <= 1e-10 * max(abs(da[key]), 1.0), key
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_zero_coupling_runs_the_ungauged_stepper(gpu, prec):
+    """complex_gauge=1 with g_gauge=0 is the reference's ungauged dispatch
+    (scp_sim.c:1586, :2820): the 24 matter columns evolve bit for bit as in
+    the ungauged run, th and E are carried unchanged, the energy is the
+    ungauged one, and compute_gauss reports div E, 1/2 E^2 and Q_flux = 0."""
+    st = seeds.small_state(16, True, seed=17, g_gauge=0.0, precision=prec)
+    p = st.params
+    pu = Params(**{**p.__dict__, "complex_gauge": 0})
+    cols = st.cols()
+    with Simulation(p, cols) as a, Simulation(pu, cols[:24]) as b:
+        a.step(7)
+        b.step(7)
+        A, B = a.snapshot(), b.snapshot()
+        da, db = a.diag(), b.diag()
+    for c in range(24):
+        assert np.array_equal(A[c], B[c]), c
+    for c in range(24, 30):   # FP64 exactly; FP32C holds E in fp32 and th as an fp32 pair
+        want = np.asarray(cols[c]).reshape(-1)
+        if prec == 0:
+            assert np.array_equal(A[c], want), c
+        else:
+            assert np.max(np.abs(A[c] - want)) <= 1e-7 * max(np.max(np.abs(want)), 1e-30), c
+    for key in ("E_total", "E_grad", "Q_total", "s_max", "r_core"):
+        assert da[key] == db[key], key
+    N, dx = p.N, p.dx
+    E = [A[27 + d].reshape(N, N, N) for d in range(3)]
+    div = sum(E[d] - np.roll(E[d], 1, axis=d) for d in range(3)) / dx
+    assert abs(da["gauss_max"] - np.abs(div).max()) <= 1e-12 * max(np.abs(div).max(), 1.0)
+    eem = 0.5 * sum((e ** 2).sum() for e in E) * dx ** 3
+    assert abs(da["E_em"] - eem) <= 1e-12 * max(eem, 1.0)
+    assert da["Q_flux"] == 0.0
+
+
 def test_real_limit_keeps_imaginary_sector_zero(gpu):
     """v = tv = 0 with zero imaginary momenta stays exactly zero
     (the complex kernel's real limit, v66 reg_harness)."""
@@ -112,7 +146,7 @@ def test_charged_periodic_gauged_seed_refused(gpu):
 def test_bad_parameters(gpu):
     L = native.lib()
     h = ctypes.c_void_p()
-    for bad in (dict(N=3), dict(bc_type=1), dict(complex_gauge=1, g_gauge=0.0), dict(tile_variant=99)):
+    for bad in (dict(N=3), dict(bc_type=1), dict(complex_gauge=1, g_gauge=-0.1), dict(tile_variant=99)):
         p = Params(**bad)
         cols = [np.zeros(p.N ** 3) for _ in range(p.ncols)]
         arr = (ctypes.c_void_p * p.ncols)(*[c.ctypes.data for c in cols])
