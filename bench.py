@@ -47,6 +47,8 @@ WORKLOADS = {
     "c4f": ("c4", 1, "gauged FP32-compensated 512^3, eight co-phase balls"),
     "c3": (None, 1, "served mixed queue, FP32-compensated, Poisson arrivals, N in 32..128 (seed 2)"),
     "c2acc": ("c2", 1, "gauged 256^3 + N(0,0.01) thermal noise: FP32-compensated against FP64, side by side"),
+    "snap": (None, 1, "host driver scp_sim_b200, gauged FP32C two-ball qball init, f32 SFA snapshots: "
+                      "none / synchronous / pipelined"),
 }
 METRIC = "site-updates/s"
 
@@ -328,6 +330,59 @@ def run_precision_compare(args) -> dict:
     }
 
 
+def run_snapshot_pipeline(args) -> dict:
+    """snap: the config-driven host driver (scp_b200/host/scp_sim_b200) on a
+    gauged FP32C run initialised by the reference's own qball init (two
+    opposite balls from a Gaussian radial profile), writing f32 SFA frames
+    every --snap-every steps: wall ms/step without snapshots, with the
+    synchronous snapshot path and with the pipelined one (device
+    down-conversion, copy stream, writer thread)."""
+    import tempfile
+    driver = os.path.join(ROOT, "scp_b200", "host", "scp_sim_b200")
+    if not os.path.exists(driver):
+        raise SystemExit("scp_b200/host/scp_sim_b200 is not built")
+    N = args.n or 128
+    L = (N - 1) / 4.0
+    dx = 2 * L / (N - 1)
+    dt = 0.2 * dx
+    steps, every = args.steps, args.snap_every
+    out = {}
+    with tempfile.TemporaryDirectory() as d:
+        prof = os.path.join(d, "profile.txt")
+        with open(prof, "w") as f:
+            for r in np.arange(0.0, 4 * L, 0.05):
+                f.write(f"{r:.4f} {np.exp(-r * r / 18.0):.12e}\n")
+        base = {"N": N, "L": L, "dt_factor": 0.2, "complex_phi": 1, "complex_gauge": 1, "g_gauge": 0.1,
+                "bc_type": 2, "init": "qball", "qball_profile": prof, "qball_omega": 1.45, "qball_x0": -L / 3,
+                "qball_y0": 0.0, "qball_z0": 0.0, "qball2_x0": L / 3, "qball2_y0": 0.0, "qball2_z0": 0.0,
+                "qball2_sign": -1, "precision": "f32", "T": steps * dt, "diag_dt": every * dt}
+        for name, snap_dt, asyn in (("no_snapshots", 10 * steps * dt, 1), ("synchronous", every * dt, 0),
+                                    ("pipelined", every * dt, 1)):
+            cfg = os.path.join(d, f"{name}.cfg")
+            kv = dict(base, snap_dt=snap_dt, output=os.path.join(d, f"{name}.sfa"),
+                      diag_file=os.path.join(d, f"{name}.tsv"))
+            with open(cfg, "w") as f:
+                f.write("".join(f"{k} = {v}\n" for k, v in kv.items()))
+            t0 = time.perf_counter()
+            r = subprocess.run([driver, cfg, "-gpu_precision", "fp32c", "-gpu_async_snap", str(asyn)],
+                               capture_output=True, text=True, cwd=d)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                raise RuntimeError(f"driver failed ({name}): {r.stderr[-800:]}")
+            m = re.search(r"Wall: ([0-9.]+)s .* ([0-9.]+)ms/step", r.stdout)
+            m2 = re.search(r"SFA: .* \((\d+) frames\)", r.stdout)
+            out[name] = {"loop_ms_per_step": float(m.group(2)), "loop_s": float(m.group(1)),
+                         "process_s": wall, "frames": int(m2.group(1)) if m2 else None,
+                         "sfa_bytes": os.path.getsize(kv["output"])}
+    frame_bytes = 30 * N ** 3 * 4
+    nframes = steps // every
+    extra = {k: (out[k]["loop_s"] - out["no_snapshots"]["loop_s"]) / max(nframes, 1)
+             for k in ("synchronous", "pipelined")}
+    return {"metric": "driver loop ms/step with f32 snapshots", "workload": WORKLOADS["snap"][2], "N": N,
+            "steps": steps, "snapshot_every": every, "frame_bytes": frame_bytes, "runs": out,
+            "snapshot_cost_s_per_frame": extra, "data": "synthetic"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,6 +399,7 @@ def main():
     ap.add_argument("--max-active", type=int, default=128, help="c3: server slots")
     ap.add_argument("--no-sequential", action="store_true", help="c3: skip the one-after-another FP64 run")
     ap.add_argument("--seq-sample", type=int, default=0, help="c3: run only the first R requests sequentially")
+    ap.add_argument("--snap-every", type=int, default=100, help="snap: steps between SFA frames")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
@@ -356,7 +412,7 @@ def main():
         dist = dist_mod
 
     if args.impl == "reference":
-        if args.workload in ("c3", "c2acc"):
+        if args.workload in ("c3", "c2acc", "snap"):
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "this workload exercises the library's "
                                   "server or its two precisions, which the reference does not have; its CPU "
@@ -373,6 +429,9 @@ def main():
         if world > 1:
             raise SystemExit("c3 runs on one GPU")
         print(json.dumps(run_served_mix(args)))
+        return
+    if args.workload == "snap":
+        print(json.dumps(run_snapshot_pipeline(args)))
         return
     if args.workload == "c2acc":
         if world > 1:

@@ -129,6 +129,22 @@ int  scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out);
 /* Copy the current state to host columns in dtype (SCP_DTYPE_*); the f32/f16
  * casts are done on the device with the reference's conversion rules. */
 int  scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols);
+/* Asynchronous snapshot, the overlapped form of the reference's snap_hook
+ * (scp_sim.cu:3496-3691: down-cast kernels, pinned buffers, async D2H).  The
+ * down-conversion into device staging runs on the handle's stream, so steps
+ * enqueued after this call see it finished before they overwrite the state;
+ * the copies into host_cols run on a separate copy stream and overlap with
+ * those steps.  host_cols must stay valid until scp_gpu_snapshot_wait
+ * returns (page-locked memory from scp_gpu_host_alloc makes the copies truly
+ * asynchronous).  One snapshot is in flight per handle: a second call first
+ * waits for the previous one.  The staging (ncols x N^3 x dtype size) is
+ * allocated on first use and kept until scp_gpu_free. */
+int  scp_gpu_snapshot_async(scp_gpu *h, int dtype, void *const *host_cols);
+/* Wait until the snapshot in flight (if any) has landed in host memory. */
+int  scp_gpu_snapshot_wait(scp_gpu *h);
+/* Page-locked host memory for snapshot buffers (NULL on failure). */
+void *scp_gpu_host_alloc(size_t bytes);
+void scp_gpu_host_free(void *p);
 int  scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info);
 /* Time nsteps on the handle's stream with CUDA events recorded on that
  * stream; *ms_out receives the device time of the whole batch. */

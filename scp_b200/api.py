@@ -71,6 +71,18 @@ class Simulation:
         native.check(native.lib().scp_gpu_snapshot(self._h, int(dtype), arr), "scp_gpu_snapshot")
         return cols
 
+    def snapshot_async(self, cols: list[np.ndarray], dtype: int = DTYPE_F64) -> None:
+        """Start a snapshot into caller-owned arrays (N^3 each, of the dtype's
+        numpy type); they must stay alive until snapshot_wait() returns."""
+        p = self.params
+        if len(cols) < p.ncols or any(c.dtype != _NP_DTYPE[dtype] or c.size != p.N ** 3 for c in cols[:p.ncols]):
+            raise ValueError("snapshot_async: need ncols arrays of N^3 values of the dtype")
+        arr = (ctypes.c_void_p * p.ncols)(*[c.ctypes.data for c in cols[:p.ncols]])
+        native.check(native.lib().scp_gpu_snapshot_async(self._h, int(dtype), arr), "scp_gpu_snapshot_async")
+
+    def snapshot_wait(self) -> None:
+        native.check(native.lib().scp_gpu_snapshot_wait(self._h), "scp_gpu_snapshot_wait")
+
     def snapshot_dict(self, dtype: int = DTYPE_F64) -> dict:
         return dict(zip(COLUMN_NAMES, self.snapshot(dtype)))
 

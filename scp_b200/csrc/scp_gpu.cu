@@ -113,6 +113,12 @@ struct scp_gpu {
     double h_small[64];          // host landing area of the small device-to-host reads
     void *stage = nullptr;       // snapshot down-conversion staging (N3 doubles)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // asynchronous snapshots: device staging of every column, copies on their own stream
+    cudaStream_t copy_stream = nullptr;
+    void *snap_dev = nullptr;
+    size_t snap_dev_bytes = 0;
+    cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
+    int snap_pending = 0;
     // launch geometry
     int shape;
     int pairs = 0;               // 1: two-site packed FP32C kernel
@@ -693,6 +699,92 @@ int scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols) {
     return snapshot_with(h, V, dtype, host_cols);
 }
 
+}  // extern "C"
+
+// Down-convert every column of the current state into device staging on the
+// handle's stream (later steps overwrite the state, so this part is ordered
+// with them), then copy the staging to the host on the copy stream.
+template <class View>
+static int snapshot_async_with(scp_gpu *h, const View &V, int dtype, void *const *host_cols) {
+    const int ncols = h->links ? 30 : 24;
+    const long long n3 = h->N3;
+    const size_t es = dtype == SCP_DTYPE_F64 ? 8 : (dtype == SCP_DTYPE_F32 ? 4 : 2);
+    const size_t col = es * (size_t)n3, need = col * ncols;
+    for (int c = 0; c < ncols; c++)
+        if (!host_cols[c]) return SCP_EINVAL;
+    if (!h->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->snap_ready, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->snap_done, cudaEventDisableTiming));
+    }
+    if (h->snap_dev_bytes < need) {
+        if (h->snap_dev) {
+            CK(cudaFreeAsync(h->snap_dev, h->stream));
+            h->dev_bytes -= h->snap_dev_bytes;
+            h->snap_dev = nullptr;
+            h->snap_dev_bytes = 0;
+        }
+        CK(cudaMallocAsync(&h->snap_dev, need, h->stream));
+        h->snap_dev_bytes = need;
+        h->dev_bytes += need;
+    }
+    char *stage = (char *)h->snap_dev;
+    const int nb = red_blocks(n3);
+    for (int c = 0; c < ncols; c++) {
+        int field, mom;
+        sfa_col_source(c, &field, &mom);
+        if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {
+            const double *src = (mom ? h->S : h->X[h->cur ^ 1]) + (size_t)field * n3;
+            CK(cudaMemcpyAsync(stage + c * col, src, col, cudaMemcpyDeviceToDevice, h->stream));
+        } else {
+            snap_col_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, field, mom, n3, dtype, stage + c * col);
+        }
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(h->snap_ready, h->stream));
+    CK(cudaStreamWaitEvent(h->copy_stream, h->snap_ready, 0));
+    for (int c = 0; c < ncols; c++)
+        CK(cudaMemcpyAsync(host_cols[c], stage + c * col, col, cudaMemcpyDeviceToHost, h->copy_stream));
+    CK(cudaEventRecord(h->snap_done, h->copy_stream));
+    h->snap_pending = 1;
+    return SCP_OK;
+}
+
+extern "C" {
+
+int scp_gpu_snapshot_wait(scp_gpu *h) {
+    if (!h) return SCP_EINVAL;
+    if (!h->snap_pending) return SCP_OK;
+    CK(cudaSetDevice(h->device));
+    h->snap_pending = 0;
+    CK(cudaEventSynchronize(h->snap_done));
+    return SCP_OK;
+}
+
+int scp_gpu_snapshot_async(scp_gpu *h, int dtype, void *const *host_cols) {
+    if (!h || !host_cols) return SCP_EINVAL;
+    if (dtype != SCP_DTYPE_F16 && dtype != SCP_DTYPE_F32 && dtype != SCP_DTYPE_F64) return SCP_EINVAL;
+    int rc;
+    if ((rc = scp_gpu_snapshot_wait(h))) return rc;   // one snapshot in flight per handle
+    CK(cudaSetDevice(h->device));
+    if (h->prec == SCP_PREC_FP64) {
+        ViewF64 V{h->X[h->cur ^ 1], h->S, h->N3};
+        return snapshot_async_with(h, V, dtype, host_cols);
+    }
+    View32C V{h->X32[h->cur ^ 1], h->LO[h->cur ^ 1], h->TLO[h->cur ^ 1], h->S32, h->N3};
+    return snapshot_async_with(h, V, dtype, host_cols);
+}
+
+void *scp_gpu_host_alloc(size_t bytes) {
+    void *p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void scp_gpu_host_free(void *p) {
+    if (p) cudaFreeHost(p);
+}
+
 int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
     if (!h || !info) return SCP_EINVAL;
     memset(info, 0, sizeof *info);
@@ -704,9 +796,12 @@ int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
     info->device_bytes = h->dev_bytes;
     // persistent bytes per site the step reads and writes: x and w (FP64);
     // hi (fp32) + lo (bf16 matter, fp32 links) + w (fp32) in FP32C
+    // (the fields the step touches: 15 gauged, 12 otherwise, links carried
+    // unchanged with g = 0 included in neither)
+    const double nfs = h->gauged ? 15.0 : 12.0;
     info->state_bytes_per_site = (h->prec == SCP_PREC_FP64)
-                                     ? 2.0 * 8.0 * h->nf
-                                     : 4.0 * h->nf + 12.0 * 2.0 + (h->gauged ? 3.0 * 4.0 : 0.0) + 4.0 * h->nf;
+                                     ? 2.0 * 8.0 * nfs
+                                     : 4.0 * nfs + 12.0 * 2.0 + (h->gauged ? 3.0 * 4.0 : 0.0) + 4.0 * nfs;
     info->step_bytes_per_site = 2.0 * info->state_bytes_per_site;
     info->tile_x = kShapes[h->shape].tx;
     info->tile_y = kShapes[h->shape].ty;
@@ -734,14 +829,19 @@ void *scp_gpu_stream(scp_gpu *h) { return h ? (void *)h->stream : nullptr; }
 void scp_gpu_free(scp_gpu *h) {
     if (!h) return;
     cudaSetDevice(h->device);
+    if (h->snap_pending) cudaEventSynchronize(h->snap_done);
+    if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->stream) {
-        void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->stage};
+        void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->stage, h->snap_dev};
         for (void *b : bufs)
             if (b) cudaFreeAsync(b, h->stream);
         cudaStreamSynchronize(h->stream);
     }
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->snap_ready) cudaEventDestroy(h->snap_ready);
+    if (h->snap_done) cudaEventDestroy(h->snap_done);
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }

@@ -13,8 +13,10 @@
  *   scp_sim_b200 run.sfa    [-key value ...]      resume from the last frame
  *
  * Extra keys read by this driver only (not passed to the reference parser):
- *   gpu_precision = fp64 | fp32c   (default fp64)
- *   gpu_device    = <ordinal>       (default 0)
+ *   gpu_precision  = fp64 | fp32c   (default fp64)
+ *   gpu_device     = <ordinal>       (default 0)
+ *   gpu_async_snap = 1 | 0          (default 1: snapshots copied and written
+ *                                     while the GPU keeps stepping)
  * It covers the complex (complex_phi=1) and gauged (complex_gauge=1) stepper
  * with bc_type 0 or 2; other modes are refused with a message.
  *
@@ -24,6 +26,7 @@
 #include "sfa.h"
 #include "scp_config.h"
 
+#include <pthread.h>
 #include <stdint.h>
 #include <time.h>
 
@@ -92,18 +95,118 @@ static void add_columns(SFA *sfa, uint8_t dt, int gauged) {
     for (int k = 0; k < n; k++) sfa_add_column(sfa, names[k], dt, sem[k], comp[k]);
 }
 
+/* Snapshot pipeline: two host buffer sets (page-locked when available).
+ * snap_start begins a device snapshot into a free set (down-conversion on the
+ * stepping stream, copy on the library's copy stream); snap_flush, called
+ * right after the next steps are enqueued, waits for the copy and queues the
+ * set to a writer thread that compresses and appends the frame
+ * (sfa_write_frame) while the GPU keeps stepping.  With async = 0 every frame
+ * is taken and written synchronously, as the reference's CPU path does. */
 typedef struct {
     scp_gpu *h;
-    int ncols, precision;
-    void *cols[30];       /* snapshot staging in the output dtype */
+    SFA *sfa;
+    int ncols, dtype, async;
+    size_t col_bytes;
+    void *cols[2][30];
+    int pinned[2];
+    double t[2];
+    int busy[2];          /* set queued to or being written by the writer */
+    int queue[2], qn;     /* FIFO of sets to write */
+    int next, pending;    /* next set to fill; set whose copy is in flight (-1 none) */
+    int stop, werr;
+    pthread_t thr;
+    pthread_mutex_t mu;
+    pthread_cond_t cv;
 } Snap;
 
-static int snap_write(SFA *sfa, Snap *s, double t) {
-    const int dt = s->precision == 0 ? SCP_DTYPE_F16 : (s->precision == 1 ? SCP_DTYPE_F32 : SCP_DTYPE_F64);
-    int rc = scp_gpu_snapshot(s->h, dt, s->cols);
-    if (rc) return rc;
-    sfa_write_frame(sfa, t, s->cols);
+static void *snap_writer(void *arg) {
+    Snap *s = arg;
+    pthread_mutex_lock(&s->mu);
+    for (;;) {
+        while (!s->stop && s->qn == 0) pthread_cond_wait(&s->cv, &s->mu);
+        if (s->qn == 0) break;
+        const int k = s->queue[0];
+        s->queue[0] = s->queue[1];
+        s->qn--;
+        pthread_mutex_unlock(&s->mu);
+        sfa_write_frame(s->sfa, s->t[k], s->cols[k]);
+        pthread_mutex_lock(&s->mu);
+        s->busy[k] = 0;
+        pthread_cond_broadcast(&s->cv);
+    }
+    pthread_mutex_unlock(&s->mu);
+    return NULL;
+}
+
+static int snap_open(Snap *s, scp_gpu *h, SFA *sfa, int ncols, int precision, long n3, int async) {
+    memset(s, 0, sizeof *s);
+    s->h = h; s->sfa = sfa; s->ncols = ncols; s->async = async;
+    s->dtype = precision == 0 ? SCP_DTYPE_F16 : (precision == 1 ? SCP_DTYPE_F32 : SCP_DTYPE_F64);
+    s->col_bytes = (size_t)(precision == 0 ? 2 : (precision == 1 ? 4 : 8)) * (size_t)n3;
+    s->pending = -1;
+    for (int b = 0; b < (async ? 2 : 1); b++) {
+        void *blk = async ? scp_gpu_host_alloc(s->col_bytes * ncols) : NULL;
+        s->pinned[b] = blk != NULL;
+        if (!blk) blk = malloc(s->col_bytes * ncols);
+        if (!blk) return -1;
+        for (int k = 0; k < ncols; k++) s->cols[b][k] = (char *)blk + (size_t)k * s->col_bytes;
+    }
+    pthread_mutex_init(&s->mu, NULL);
+    pthread_cond_init(&s->cv, NULL);
+    if (async && pthread_create(&s->thr, NULL, snap_writer, s)) return -1;
     return 0;
+}
+
+/* hand the frame whose copy is in flight to the writer */
+static int snap_flush(Snap *s) {
+    if (s->pending < 0) return 0;
+    int rc = scp_gpu_snapshot_wait(s->h);
+    if (rc) return rc;
+    pthread_mutex_lock(&s->mu);
+    s->queue[s->qn++] = s->pending;
+    s->pending = -1;
+    pthread_cond_broadcast(&s->cv);
+    pthread_mutex_unlock(&s->mu);
+    return 0;
+}
+
+static int snap_start(Snap *s, double t) {
+    if (!s->async) {
+        int rc = scp_gpu_snapshot(s->h, s->dtype, s->cols[0]);
+        if (rc) return rc;
+        sfa_write_frame(s->sfa, t, s->cols[0]);
+        return 0;
+    }
+    int rc = snap_flush(s);
+    if (rc) return rc;
+    const int k = s->next;
+    pthread_mutex_lock(&s->mu);
+    while (s->busy[k]) pthread_cond_wait(&s->cv, &s->mu);
+    s->busy[k] = 1;
+    pthread_mutex_unlock(&s->mu);
+    s->t[k] = t;
+    if ((rc = scp_gpu_snapshot_async(s->h, s->dtype, s->cols[k]))) return rc;
+    s->pending = k;
+    s->next ^= 1;
+    return 0;
+}
+
+/* flush the last frame, stop the writer, release the buffers */
+static int snap_close(Snap *s) {
+    int rc = 0;
+    if (s->async) {
+        rc = snap_flush(s);
+        pthread_mutex_lock(&s->mu);
+        s->stop = 1;
+        pthread_cond_broadcast(&s->cv);
+        pthread_mutex_unlock(&s->mu);
+        pthread_join(s->thr, NULL);
+    }
+    for (int b = 0; b < (s->async ? 2 : 1); b++) {
+        if (s->pinned[b]) scp_gpu_host_free(s->cols[b][0]);
+        else free(s->cols[b][0]);
+    }
+    return rc;
 }
 
 /* One diag TSV row in the reference's column set and formats
@@ -160,11 +263,12 @@ int main(int argc, char **argv) {
     } else {
         cfg_load(&c, arg1);
     }
-    int gpu_prec = SCP_PREC_FP64, gpu_dev = 0;
+    int gpu_prec = SCP_PREC_FP64, gpu_dev = 0, gpu_async_snap = 1;
     for (int i = 2; i + 1 < argc; i += 2) {
         const char *key = argv[i][0] == '-' ? argv[i] + 1 : argv[i];
         if (!strcmp(key, "gpu_precision")) gpu_prec = !strcmp(argv[i + 1], "fp32c") ? SCP_PREC_FP32C : SCP_PREC_FP64;
         else if (!strcmp(key, "gpu_device")) gpu_dev = atoi(argv[i + 1]);
+        else if (!strcmp(key, "gpu_async_snap")) gpu_async_snap = atoi(argv[i + 1]);
         else cfg_set(&c, key, argv[i + 1]);
     }
     cfg_print(&c);
@@ -212,10 +316,12 @@ int main(int argc, char **argv) {
     sfa_embed_kvmd(sfa, &c);
     add_columns(sfa, sdt, c.complex_gauge);
     sfa_finalize_header(sfa);
-    Snap snap = {h, ncols, c.precision, {0}};
-    const size_t es = (size_t)sfa_dtype_size[sdt];
-    for (int k = 0; k < ncols; k++) snap.cols[k] = malloc(es * (size_t)g->N3);
-    if ((rc = snap_write(sfa, &snap, 0.0))) return fail("snapshot", rc);
+    static Snap snap;
+    if (snap_open(&snap, h, sfa, ncols, c.precision, g->N3, gpu_async_snap)) {
+        fprintf(stderr, "FATAL: snapshot buffers\n");
+        return 1;
+    }
+    if ((rc = snap_start(&snap, 0.0))) return fail("snapshot", rc);
 
     FILE *fp = fopen(c.diag_file, "w");
     if (!fp) { fprintf(stderr, "ERROR: cannot open %s\n", c.diag_file); return 1; }
@@ -246,9 +352,10 @@ int main(int argc, char **argv) {
         if (nd < next) next = nd;
         if (ns < next) next = ns;
         if ((rc = scp_gpu_step(h, next - step))) return fail("step", rc);
+        if ((rc = snap_flush(&snap))) return fail("snapshot", rc);   /* its copy overlapped these steps */
         step = next;
         const double t = step * g->dt;
-        if (step % snap_every == 0 && (rc = snap_write(sfa, &snap, t))) return fail("snapshot", rc);
+        if (step % snap_every == 0 && (rc = snap_start(&snap, t))) return fail("snapshot", rc);
         if (step % diag_every == 0) {
             if ((rc = scp_gpu_diag(h, &d))) return fail("diag", rc);
             diag_row(fp, t, &d, c.complex_gauge);
@@ -268,8 +375,9 @@ int main(int argc, char **argv) {
     const double wall = wall_now() - wall0;
     {   /* final frame unless the last step was (nearly) a snapshot step (scp_sim.c:3254-3259) */
         const int last = (n_steps / snap_every) * snap_every;
-        if (n_steps - last > snap_every / 2 && (rc = snap_write(sfa, &snap, n_steps * g->dt))) return fail("snapshot", rc);
+        if (n_steps - last > snap_every / 2 && (rc = snap_start(&snap, n_steps * g->dt))) return fail("snapshot", rc);
     }
+    if ((rc = snap_close(&snap))) return fail("snapshot", rc);
     const uint32_t nf = sfa->total_frames;
     sfa_close(sfa);
     if ((rc = scp_gpu_diag(h, &d))) return fail("diag", rc);
@@ -285,7 +393,6 @@ int main(int argc, char **argv) {
     printf("SFA: %s (%u frames)\n", c.output, nf);
     printf("Wall: %.1fs (%.1f min) %.3fms/step\n", wall, wall / 60, n_steps ? 1000 * wall / n_steps : 0.0);
     fclose(fp);
-    for (int k = 0; k < ncols; k++) free(snap.cols[k]);
     scp_gpu_free(h);
     free(g);
     return 0;

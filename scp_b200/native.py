@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 # every symbol declared in include/scp_gpu.h
 EXPORTS = (
     "scp_gpu_init", "scp_gpu_init_device", "scp_gpu_step", "scp_gpu_sync", "scp_gpu_diag",
-    "scp_gpu_snapshot", "scp_gpu_get_info", "scp_gpu_time_steps", "scp_gpu_stream",
+    "scp_gpu_snapshot", "scp_gpu_snapshot_async", "scp_gpu_snapshot_wait", "scp_gpu_host_alloc",
+    "scp_gpu_host_free", "scp_gpu_get_info", "scp_gpu_time_steps", "scp_gpu_stream",
     "scp_gpu_free", "scp_gpu_errstr", "scp_gpu_last_cuda_error", "scp_gpu_abi_version",
     "scp_gpu_diag_noalloc", "scp_gpu_check_trig",
     "scp_srv_create", "scp_srv_submit", "scp_srv_submit_borrowed", "scp_srv_poll", "scp_srv_status", "scp_srv_result",
@@ -106,6 +107,12 @@ def lib() -> ctypes.CDLL:
     L.scp_gpu_sync.argtypes = [vp]
     L.scp_gpu_diag.argtypes = [vp, ctypes.POINTER(DiagOut)]
     L.scp_gpu_snapshot.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+    L.scp_gpu_snapshot_async.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp)]
+    L.scp_gpu_snapshot_wait.argtypes = [vp]
+    L.scp_gpu_host_alloc.argtypes = [ctypes.c_size_t]
+    L.scp_gpu_host_alloc.restype = vp
+    L.scp_gpu_host_free.argtypes = [vp]
+    L.scp_gpu_host_free.restype = None
     L.scp_gpu_get_info.argtypes = [vp, ctypes.POINTER(Info)]
     L.scp_gpu_time_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.scp_gpu_stream.argtypes = [vp]

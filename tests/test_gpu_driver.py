@@ -15,22 +15,23 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DRIVER = os.path.join(ROOT, "scp_b200", "host", "scp_sim_b200")
 
 
-def _run(binary, cfg, cwd):
+def _run(binary, cfg, cwd, extra=()):
     env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1))
-    r = subprocess.run([binary, cfg], capture_output=True, text=True, cwd=cwd, env=env)
+    r = subprocess.run([binary, cfg, *extra], capture_output=True, text=True, cwd=cwd, env=env)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     return r.stdout
 
 
-@pytest.mark.parametrize("gauged", [False, True, "g0"])
+@pytest.mark.parametrize("gauged", [False, True, "g0", "sync"])
 def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
     """gauged="g0": complex_gauge=1 with g_gauge=0, the reference's ungauged
-    dispatch with the link columns carried."""
+    dispatch with the link columns carried; "sync": gauged with the
+    synchronous snapshot path (gpu_async_snap = 0) instead of the pipelined one."""
     assert os.path.exists(DRIVER), "host driver not built (make -C scp_b200/host)"
     if gauged == "g0":
         st = seeds.small_state(16, True, seed=13, g_gauge=0.0)
     else:
-        st = seeds.small_state(16, gauged, seed=13)
+        st = seeds.small_state(16, bool(gauged), seed=13)
     p = st.params
     seed = str(tmp_path / "seed.sfa")
     oracle.write_seed(seed, p, st.cols())
@@ -43,7 +44,8 @@ def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
         cfg.write_text(p.to_cfg(init="sfa", init_sfa=seed, init_frame=0, T=repr(nsteps * p.dt), precision="f64",
                                 output=str(d / "out.sfa"), diag_file=str(d / "diag.tsv"),
                                 snap_dt=repr(nsteps // 2 * p.dt), diag_dt=repr(10 * p.dt)))
-        _run(binary, str(cfg), str(d))
+        extra = ("-gpu_async_snap", "0") if (name == "b200" and gauged == "sync") else ()
+        _run(binary, str(cfg), str(d), extra)
         hdr, rows = oracle.read_diag(str(d / "diag.tsv"))
         frames = [oracle.read_frame(str(d / "out.sfa"), f, p.N ** 3) for f in (0, 1, 2)]
         outs[name] = (hdr, rows, frames)
