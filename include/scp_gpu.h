@@ -237,7 +237,9 @@ typedef struct {
     int64_t step, chunks, mem_in_use;
     int32_t n_active, n_queued, n_groups;
     double  t_admit, t_autotune, t_run, t_retire;   /* host seconds spent per phase; t_admit and
-                                                       t_autotune run on the loader thread */
+                                                       t_autotune are summed over the loader
+                                                       threads, t_retire over the two retire
+                                                       threads (final step, diagnostics, free) */
     double  t_wait;           /* poll time spent waiting for a first loaded request */
     double  t_launch;         /* poll time spent planning, uploading tables, launching */
     double  t_gpu;            /* device time of the chunks (CUDA events on the server stream) */
@@ -253,9 +255,10 @@ int  scp_srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *ho
                     void *const *out_cols, int out_dtype, int64_t *id_out);
 int  scp_srv_submit_borrowed(scp_srv *s, const scp_gpu_params *p, const double *const *host_cols, int64_t nsteps,
                              void *const *out_cols, int out_dtype, int64_t *id_out);
-/* Take in the requests the loader thread has initialised, finish the chunk in
- * flight, launch the next one, retire finished requests; reports the active
- * count and the queued count (queued, loading or loaded but not yet taken). */
+/* Take in the requests the loader threads have initialised, finish the chunk
+ * in flight, launch the next one, hand finished requests to the retire
+ * threads; reports the active count (running or retiring) and the queued
+ * count (queued, loading or loaded but not yet taken). */
 int  scp_srv_poll(scp_srv *s, int *n_active, int *n_queued);
 int  scp_srv_status(scp_srv *s, int64_t id, scp_srv_request_info *info);
 /* Final diagnostics of a finished request (SCP_EBUSY while queued/active). */

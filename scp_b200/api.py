@@ -64,9 +64,17 @@ class Simulation:
         native.check(native.lib().scp_gpu_diag(self._h, ctypes.byref(out)), "scp_gpu_diag")
         return np.array(out.v[: len(DIAG_NAMES)])
 
-    def snapshot(self, dtype: int = DTYPE_F64) -> list[np.ndarray]:
+    def snapshot(self, dtype: int = DTYPE_F64, out: list[np.ndarray] | None = None) -> list[np.ndarray]:
+        """Current state as host columns (SFA order) in dtype; into `out`
+        (ncols arrays of N^3 values of the dtype) when given."""
         p = self.params
-        cols = [np.empty(p.N ** 3, dtype=_NP_DTYPE[dtype]) for _ in range(p.ncols)]
+        if out is not None:
+            if len(out) < p.ncols or any(c.dtype != _NP_DTYPE[dtype] or c.size != p.N ** 3 or not c.flags.c_contiguous
+                                         for c in out[:p.ncols]):
+                raise ValueError("snapshot: out needs ncols contiguous arrays of N^3 values of the dtype")
+            cols = list(out[:p.ncols])
+        else:
+            cols = [np.empty(p.N ** 3, dtype=_NP_DTYPE[dtype]) for _ in range(p.ncols)]
         arr = (ctypes.c_void_p * p.ncols)(*[c.ctypes.data for c in cols])
         native.check(native.lib().scp_gpu_snapshot(self._h, int(dtype), arr), "scp_gpu_snapshot")
         return cols
@@ -111,3 +119,17 @@ class Simulation:
             self.close()
         except Exception:
             pass
+
+
+def pinned_empty(n: int, dtype=np.float64) -> np.ndarray:
+    """A 1-D numpy array of n values in page-locked host memory
+    (scp_gpu_host_alloc), released when the array is garbage collected."""
+    import weakref
+    L = native.lib()
+    nbytes = int(n) * np.dtype(dtype).itemsize
+    ptr = L.scp_gpu_host_alloc(max(nbytes, 1))
+    if not ptr:
+        raise MemoryError(f"scp_gpu_host_alloc({nbytes}) failed")
+    base = np.frombuffer((ctypes.c_char * max(nbytes, 1)).from_address(ptr), dtype=np.uint8)
+    weakref.finalize(base, L.scp_gpu_host_free, ptr)
+    return base[:nbytes].view(dtype)

@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(kRedThreads) gauss_rhs_kernel(GaussArgs a, dou
 enum : int { CG_GBAR = 0, CG_GMAX0, CG_RZ, CG_PAP, CG_ALPHA, CG_BETA, CG_XBAR, CG_RMAX, CG_RZ2, CG_TOL, CG_DONE,
              CG_IT, CG_N };
 
-// The iteration loop runs on the device in batches: every sweep returns at
+// The iteration loop runs on the device in batches: every launch returns at
 // once when CG_DONE is set (residual below tolerance or iteration cap), so the
 // host only checks after a batch and the iterations taken are exactly those
 // of the reference's while (rmax > tol && it < itmax) loop.
@@ -92,31 +92,58 @@ __global__ void __launch_bounds__(kRedThreads) cg_start_kernel(long long n3, dou
     block_fold<1, 1>(S, M, scratch, part);
 }
 
-// Ap = -lap(p); partial sum p.Ap
-__global__ void __launch_bounds__(kRedThreads) cg_apply_kernel(int N, long long n3, double idx2, const double *p,
-                                                               double *Ap, double *part, const double *cg) {
+// One CG iteration is two launches.  The last CTA to finish each launch folds
+// the per-CTA partials (fold_partials_block, the same fixed-order fold as
+// everywhere else) and updates the scalars, so no separate fold or scalar
+// launches are needed; the arithmetic and its order are those of the
+// reference loop (init_gauss_project, scp_sim.c:2330-2364).
+
+// p_new = r + beta*p_old (the reference's direction update, applied here at
+// the start of the next iteration), x -= xbar, Ap = -lap(p_new); p_new at the
+// six neighbours is formed on the fly with the same expression, so it equals
+// what their owners store.  The last CTA sets alpha = rz / (p.Ap).
+__global__ void __launch_bounds__(kRedThreads) cg_dirapply_kernel(int N, long long n3, double idx2, const double *r,
+                                                                  const double *pold, double *pnew, double *x,
+                                                                  double *Ap, double *part, unsigned *count,
+                                                                  double *fold, double *cg) {
     __shared__ double scratch[32];
     double S[1] = {0.0}, M[1] = {0.0};
-    if (cg[CG_DONE] != 0.0) return;
+    if (cg[CG_DONE] != 0.0) return;              // uniform: set by an earlier launch
+    const double beta = cg[CG_BETA], xbar = cg[CG_XBAR];
     const long long NN = (long long)N * N;
+    auto P = [&](long long y) { return fma(beta, pold[y], r[y]); };
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
          idx += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
-        const double lap = (p[(long long)wrapi(i + 1, N) * NN + (long long)j * N + k]
-                            + p[(long long)wrapi(i - 1, N) * NN + (long long)j * N + k]
-                            + p[(long long)i * NN + (long long)wrapi(j + 1, N) * N + k]
-                            + p[(long long)i * NN + (long long)wrapi(j - 1, N) * N + k]
-                            + p[(long long)i * NN + (long long)j * N + wrapi(k + 1, N)]
-                            + p[(long long)i * NN + (long long)j * N + wrapi(k - 1, N)] - 6.0 * p[idx]) * idx2;
-        Ap[idx] = -lap;
-        S[0] += p[idx] * Ap[idx];
+        const double pc = P(idx);
+        const double lap = (P((long long)wrapi(i + 1, N) * NN + (long long)j * N + k)
+                            + P((long long)wrapi(i - 1, N) * NN + (long long)j * N + k)
+                            + P((long long)i * NN + (long long)wrapi(j + 1, N) * N + k)
+                            + P((long long)i * NN + (long long)wrapi(j - 1, N) * N + k)
+                            + P((long long)i * NN + (long long)j * N + wrapi(k + 1, N))
+                            + P((long long)i * NN + (long long)j * N + wrapi(k - 1, N)) - 6.0 * pc) * idx2;
+        pnew[idx] = pc;
+        x[idx] -= xbar;
+        const double ap = -lap;
+        Ap[idx] = ap;
+        S[0] += pc * ap;
     }
     block_fold<1, 0>(S, M, scratch, part);
+    if (last_block_done(count)) {
+        fold_partials_block<1, 0>(part, gridDim.x, fold);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            cg[CG_PAP] = fold[0];
+            cg[CG_ALPHA] = cg[CG_RZ] / fold[0];
+        }
+    }
 }
 
-// x += alpha p; r -= alpha Ap; partial sums r.r, sum x, max |r|
+// x += alpha p; r -= alpha Ap; the last CTA sets rz, xbar, beta, max|r|,
+// counts the iteration and decides whether to go on.
 __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long long n3, double *x, double *r, const double *p,
-                                                                const double *Ap, const double *cg, double *part) {
+                                                                const double *Ap, double *part, unsigned *count,
+                                                                double *fold, double *cg, double n3d, int itmax) {
     __shared__ double scratch[3 * 32];
     double S[2] = {0.0, 0.0}, M[1] = {0.0};
     if (cg[CG_DONE] != 0.0) return;
@@ -131,21 +158,23 @@ __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long long n3, do
         M[0] = fmax(M[0], fabs(rv));
     }
     block_fold<2, 1>(S, M, scratch, part);
-}
-
-// x -= xbar; p = r + beta p
-__global__ void cg_dir_kernel(long long n3, double *x, const double *r, double *p, const double *cg) {
-    if (cg[CG_DONE] != 0.0) return;
-    const double xbar = cg[CG_XBAR], beta = cg[CG_BETA];
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
-         idx += (long long)gridDim.x * blockDim.x) {
-        x[idx] -= xbar;
-        p[idx] = r[idx] + beta * p[idx];
+    if (last_block_done(count)) {
+        fold_partials_block<2, 1>(part, gridDim.x, fold);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            cg[CG_RZ2] = fold[0];
+            cg[CG_XBAR] = fold[1] / n3d;
+            cg[CG_BETA] = fold[0] / cg[CG_RZ];
+            cg[CG_RZ] = fold[0];
+            cg[CG_RMAX] = fold[2];
+            cg[CG_IT] += 1.0;
+            if (!(cg[CG_RMAX] > cg[CG_TOL]) || cg[CG_IT] >= (double)itmax) cg[CG_DONE] = 1.0;
+        }
     }
 }
 
-// single-thread scalar bookkeeping between CG sweeps
-__global__ void cg_scalar_kernel(int stage, double n3d, const double *fold, double *cg, int itmax) {
+// single-thread scalar bookkeeping of the start-up
+__global__ void cg_scalar_kernel(int stage, double n3d, const double *fold, double *cg) {
     if (threadIdx.x | blockIdx.x) return;
     switch (stage) {
         case 0: cg[CG_GBAR] = fold[0] / n3d; break;                          // gbar
@@ -153,39 +182,27 @@ __global__ void cg_scalar_kernel(int stage, double n3d, const double *fold, doub
             cg[CG_RZ] = fold[0]; cg[CG_GMAX0] = fold[1]; cg[CG_RMAX] = fold[1];
             cg[CG_TOL] = 1e-13 * fmax(1.0, fold[1]);
             cg[CG_IT] = 0.0;
+            cg[CG_BETA] = 0.0;     // first direction p = r
+            cg[CG_XBAR] = 0.0;
             cg[CG_DONE] = (fold[1] > cg[CG_TOL]) ? 0.0 : 1.0;
-            break;
-        case 2:
-            if (cg[CG_DONE] != 0.0) return;
-            cg[CG_PAP] = fold[0]; cg[CG_ALPHA] = cg[CG_RZ] / fold[0];
-            break;
-        case 3:
-            if (cg[CG_DONE] != 0.0) return;
-            cg[CG_RZ2] = fold[0];
-            cg[CG_XBAR] = fold[1] / n3d;
-            cg[CG_BETA] = fold[0] / cg[CG_RZ];
-            cg[CG_RZ] = fold[0];
-            cg[CG_RMAX] = fold[2];
-            break;
-        case 4:   // end of an iteration: count it and decide whether to go on
-            if (cg[CG_DONE] != 0.0) return;
-            cg[CG_IT] += 1.0;
-            if (!(cg[CG_RMAX] > cg[CG_TOL]) || cg[CG_IT] >= (double)itmax) cg[CG_DONE] = 1.0;
             break;
     }
 }
 
-// E_d += (chi(x+d) - chi(x))/dx
-__global__ void gauss_correct_kernel(GaussArgs a, const double *chi) {
+// E_d += (chi(x+d) - chi(x))/dx with chi = x - xbar: the reference's last
+// iteration subtracts xbar in its direction step, which the next
+// cg_dirapply_kernel would have done here
+__global__ void gauss_correct_kernel(GaussArgs a, const double *x, const double *cg) {
     const int N = a.N;
     const long long NN = (long long)N * N;
+    const double xbar = cg[CG_XBAR];
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.N3;
          idx += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
-        const double c0 = chi[idx];
-        a.S[(FTH + 0) * a.N3 + idx] += (chi[(long long)wrapi(i + 1, N) * NN + (long long)j * N + k] - c0) / a.dx;
-        a.S[(FTH + 1) * a.N3 + idx] += (chi[(long long)i * NN + (long long)wrapi(j + 1, N) * N + k] - c0) / a.dx;
-        a.S[(FTH + 2) * a.N3 + idx] += (chi[(long long)i * NN + (long long)j * N + wrapi(k + 1, N)] - c0) / a.dx;
+        const double c0 = x[idx] - xbar;
+        a.S[(FTH + 0) * a.N3 + idx] += ((x[(long long)wrapi(i + 1, N) * NN + (long long)j * N + k] - xbar) - c0) / a.dx;
+        a.S[(FTH + 1) * a.N3 + idx] += ((x[(long long)i * NN + (long long)wrapi(j + 1, N) * N + k] - xbar) - c0) / a.dx;
+        a.S[(FTH + 2) * a.N3 + idx] += ((x[(long long)i * NN + (long long)j * N + wrapi(k + 1, N)] - xbar) - c0) / a.dx;
     }
 }
 

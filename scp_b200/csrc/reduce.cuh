@@ -71,6 +71,43 @@ __global__ void fold_partials_kernel(const double *part, int nb, double *out) {
     }
 }
 
+// The same fold as fold_partials_kernel, run by the last CTA of a grid to
+// finish (threads of one CTA, one warp per slot): the result is bit for bit
+// the one fold_partials_kernel gives.  part is read through L2 (__ldcg) since
+// it was written by other CTAs during this launch.
+template <int NS, int NM>
+__device__ __forceinline__ void fold_partials_block(const double *part, int nb, double *out) {
+    constexpr int NQ = NS + NM;
+    const int lane = threadIdx.x & 31;
+    for (int q = threadIdx.x >> 5; q < NQ; q += blockDim.x >> 5) {
+        const bool is_max = q >= NS;
+        double acc = is_max ? -INFINITY : 0.0;
+        for (int b = lane; b < nb; b += 32) {
+            const double v = __ldcg(part + (size_t)b * NQ + q);
+            acc = is_max ? fmax(acc, v) : acc + v;
+        }
+        acc = is_max ? warp_max(acc) : warp_sum(acc);
+        if (lane == 0) out[q] = acc;
+    }
+}
+
+// After block_fold: true in exactly one CTA, the last to finish, once every
+// CTA's partial is visible to it.  count is reset by that CTA for the next
+// launch.  No CTA waits for another.
+__device__ __forceinline__ bool last_block_done(unsigned *count) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(count, 1u);
+        last = (t == gridDim.x - 1);
+        if (last) *count = 0;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
 inline int red_blocks(long long n3) {
     long long b = (n3 + kRedThreads - 1) / kRedThreads;
     return (int)(b < kRedMaxBlocks ? (b < 1 ? 1 : b) : kRedMaxBlocks);

@@ -110,6 +110,7 @@ struct scp_gpu {
     // scratch
     double *part = nullptr, *fold = nullptr, *cg = nullptr, *point = nullptr;
     int *flag = nullptr;
+    unsigned *count = nullptr;   // last-CTA counter of the fused CG launches
     double h_small[64];          // host landing area of the small device-to-host reads
     void *stage = nullptr;       // snapshot down-conversion staging (N3 doubles)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -329,22 +330,21 @@ static int gauss_startup(scp_gpu *h, const double *X, double *S) {
     const double n3d = (double)n3, idx2 = 1.0 / (h->p.dx * h->p.dx);
     gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, b, h->part);
     fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(0, n3d, h->fold, h->cg, kCgItMax);
+    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(0, n3d, h->fold, h->cg);
     cg_start_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, b, r, p, x, h->cg, h->part);
     fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(1, n3d, h->fold, h->cg, kCgItMax);
+    cg_scalar_kernel<<<1, 1, 0, h->stream>>>(1, n3d, h->fold, h->cg);
     CK(cudaGetLastError());
-    // iterations in device-checked batches (see gauss.cuh)
-    for (int batch = 0;; batch++) {
-        for (int k = 0; k < kCgBatch; k++) {
-            cg_apply_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->N, n3, idx2, p, Ap, h->part, h->cg);
-            fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-            cg_scalar_kernel<<<1, 1, 0, h->stream>>>(2, n3d, h->fold, h->cg, kCgItMax);
-            cg_update_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, p, Ap, h->cg, h->part);
-            fold_partials_kernel<2, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-            cg_scalar_kernel<<<1, 1, 0, h->stream>>>(3, n3d, h->fold, h->cg, kCgItMax);
-            cg_dir_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, p, h->cg);
-            cg_scalar_kernel<<<1, 1, 0, h->stream>>>(4, n3d, h->fold, h->cg, kCgItMax);
+    // the right-hand side is not needed any more: b is the second direction buffer
+    double *dirs[2] = {p, b};
+    // iterations in device-checked batches (see gauss.cuh); two launches each
+    for (int batch = 0, it = 0;; batch++) {
+        for (int k = 0; k < kCgBatch; k++, it++) {
+            double *pold = dirs[it & 1], *pnew = dirs[(it + 1) & 1];
+            cg_dirapply_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->N, n3, idx2, r, pold, pnew, x, Ap, h->part,
+                                                                  h->count, h->fold, h->cg);
+            cg_update_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, x, r, pnew, Ap, h->part, h->count, h->fold,
+                                                                h->cg, n3d, kCgItMax);
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(h->h_small, h->cg, sizeof(double) * CG_N, cudaMemcpyDeviceToHost, h->stream));
@@ -356,7 +356,7 @@ static int gauss_startup(scp_gpu *h, const double *X, double *S) {
         cudaFreeAsync(tmp, h->stream);
         return SCP_EGAUSS;
     }
-    gauss_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, x);
+    gauss_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, x, h->cg);
     gauss_sum_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, h->part);
     fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
     CK(cudaGetLastError());
@@ -397,6 +397,8 @@ static int alloc_common(scp_gpu *h) {
     CK(cudaMallocAsync(&h->point, sizeof(double) * 8, h->stream));
     CK(cudaMallocAsync(&h->flag, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->flag, 0, sizeof(int), h->stream));
+    CK(cudaMallocAsync(&h->count, sizeof(unsigned), h->stream));
+    CK(cudaMemsetAsync(h->count, 0, sizeof(unsigned), h->stream));
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
     h->dev_bytes += sizeof(double) * (kRedMaxBlocks * 32 + 64 + 16 + 8);
@@ -832,7 +834,8 @@ void scp_gpu_free(scp_gpu *h) {
     if (h->snap_pending) cudaEventSynchronize(h->snap_done);
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->stream) {
-        void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->stage, h->snap_dev};
+        void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->count, h->stage,
+                        h->snap_dev};
         for (void *b : bufs)
             if (b) cudaFreeAsync(b, h->stream);
         cudaStreamSynchronize(h->stream);

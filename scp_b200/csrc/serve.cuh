@@ -135,6 +135,9 @@ struct scp_srv {
     std::condition_variable cv;
     bool stop = false;
     std::deque<SrvReq *> ready;
+    std::deque<SrvReq *> retiring;                            // finished, waiting for a retire thread
+    std::vector<std::thread> retirers;
+    int n_retiring = 0;                                       // queued or being retired
     int n_loading = 0;
     int n_held = 0;                                           // loading + ready + active
     int64_t mem_reserved = 0;                                 // footprint of the held requests
@@ -399,41 +402,75 @@ static int srv_intake(scp_srv *s) {
         q->group = gi;
         q->s0 = -1;                                           // set when its first chunk is launched
         q->s1 = -1;
-        q->state = SCP_SRV_ACTIVE;
-        s->mem_in_use += q->bytes;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            q->state = SCP_SRV_ACTIVE;
+            s->mem_in_use += q->bytes;
+        }
         s->groups[gi]->members.push_back(q);
         s->active.push_back(q);
     }
     return SCP_OK;
 }
 
-static int srv_retire(scp_srv *s) {
-    std::vector<SrvReq *> keep;
-    for (SrvReq *q : s->active) {
-        if (q->s1 < 0 || q->s1 > s->step) { keep.push_back(q); continue; }
+// Retire thread: a finished request's final (synchronous-momenta) step
+// through the single-grid kernel, diagnostics, optional snapshot, free -- all
+// on the request's own stream, while the poll thread keeps the chunks going.
+static void srv_retirer(scp_srv *s) {
+    cudaSetDevice(s->cfg.device);
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) t_stream_priority = greatest;
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv.wait(lk, [s] { return s->stop || !s->retiring.empty(); });
+        if (s->retiring.empty()) return;                 // stop, nothing left
+        SrvReq *q = s->retiring.front();
+        s->retiring.pop_front();
+        lk.unlock();
+        const double t0 = now_s();
         scp_gpu *h = q->h;
         h->cur ^= (int)((q->nsteps - 1) & 1);
         h->steps = q->nsteps - 1;
-        q->rc = scp_gpu_step(h, 1);
-        if (q->rc == SCP_OK) q->rc = scp_gpu_sync(h);
-        int rc2 = scp_gpu_diag(h, &q->diag);
-        if (q->rc == SCP_OK) q->rc = rc2;
-        if (q->out_cols && q->rc == SCP_OK) q->rc = scp_gpu_snapshot(h, q->out_dtype, q->out_cols);
+        int rc = scp_gpu_step(h, 1);
+        if (rc == SCP_OK) rc = scp_gpu_sync(h);
+        const int rc2 = scp_gpu_diag(h, &q->diag);
+        if (rc == SCP_OK) rc = rc2;
+        if (q->out_cols && rc == SCP_OK) rc = scp_gpu_snapshot(h, q->out_dtype, q->out_cols);
         scp_gpu_free(h);
         q->h = nullptr;
+        lk.lock();
+        q->rc = rc;
         q->t_done = now_s();
+        q->state = (rc == SCP_OK) ? SCP_SRV_DONE : SCP_SRV_FAILED;
         s->mem_in_use -= q->bytes;
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            q->state = (q->rc == SCP_OK) ? SCP_SRV_DONE : SCP_SRV_FAILED;
-            s->mem_reserved -= q->bytes;
-            s->n_held--;
-        }
+        s->mem_reserved -= q->bytes;
+        s->n_held--;
+        s->n_retiring--;
+        s->t_retire += now_s() - t0;
         s->cv.notify_all();
+    }
+}
+
+// hand the requests whose table steps are done to the retire threads (they
+// are no longer in the tables of the chunk in flight)
+static int srv_retire(scp_srv *s) {
+    std::vector<SrvReq *> keep, done;
+    for (SrvReq *q : s->active) {
+        if (q->s1 < 0 || q->s1 > s->step) keep.push_back(q);
+        else done.push_back(q);
+    }
+    if (done.empty()) return SCP_OK;
+    for (SrvReq *q : done) {
         auto &m = s->groups[q->group]->members;
         m.erase(std::remove(m.begin(), m.end(), q), m.end());
     }
     s->active.swap(keep);
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (SrvReq *q : done) s->retiring.push_back(q);
+        s->n_retiring += (int)done.size();
+    }
+    s->cv.notify_all();
     return SCP_OK;
 }
 
@@ -460,6 +497,7 @@ int scp_srv_create(const scp_srv_config *cfg, scp_srv **out) {
     }
     const int nload = cfg->loader_threads > 0 ? cfg->loader_threads : 4;
     for (int t = 0; t < nload; t++) s->loaders.emplace_back(srv_loader, s);
+    for (int t = 0; t < 2; t++) s->retirers.emplace_back(srv_retirer, s);
     *out = s;
     return SCP_OK;
 }
@@ -563,16 +601,18 @@ int scp_srv_poll(scp_srv *s, int *n_active, int *n_queued) {
     s->t_launch += now_s() - t2;
     // 5. retire the requests that finished in the chunk just completed, while
     //    the next one runs (they are no longer in the tables)
-    const double t3 = now_s();
     if ((rc = srv_retire(s))) return rc;
-    s->t_retire += now_s() - t3;
     if (!s->inflight && s->active.empty() && s->stream) CK(cudaStreamSynchronize(s->stream));
-    int queued;
+    int queued, retiring;
     {
-        std::lock_guard<std::mutex> lk(s->mu);
+        std::unique_lock<std::mutex> lk(s->mu);
+        // nothing else to do: let the retire threads finish before reporting
+        if (!s->inflight && s->active.empty() && s->n_retiring > 0)
+            s->cv.wait_for(lk, std::chrono::milliseconds(2), [s] { return s->n_retiring == 0; });
         queued = (int)(s->queue.size() + s->ready.size()) + s->n_loading;
+        retiring = s->n_retiring;
     }
-    if (n_active) *n_active = (int)s->active.size();
+    if (n_active) *n_active = (int)s->active.size() + retiring;   // retiring requests still count as active
     if (n_queued) *n_queued = queued;
     return SCP_OK;
 }
@@ -611,17 +651,18 @@ int scp_srv_stats(scp_srv *s, scp_srv_stats_t *st) {
     memset(st, 0, sizeof *st);
     st->step = s->step;
     st->chunks = s->chunks;
-    st->mem_in_use = s->mem_in_use;
     st->n_active = (int)s->active.size();
     {
         std::lock_guard<std::mutex> lk(s->mu);
+        st->mem_in_use = s->mem_in_use;
+        st->n_active += s->n_retiring;
+        st->t_retire = s->t_retire;
         st->n_queued = (int)(s->queue.size() + s->ready.size()) + s->n_loading;
         st->t_admit = s->t_admit - s->t_autotune;   // loader thread, overlapped with the chunks
         st->t_autotune = s->t_autotune;
     }
     st->n_groups = (int)s->groups.size();
     st->t_run = s->t_run;
-    st->t_retire = s->t_retire;
     st->t_wait = s->t_wait;
     st->t_launch = s->t_launch;
     st->t_gpu = s->t_gpu;
@@ -636,6 +677,8 @@ void scp_srv_free(scp_srv *s) {
     }
     s->cv.notify_all();
     for (auto &t : s->loaders)
+        if (t.joinable()) t.join();
+    for (auto &t : s->retirers)   // they drain the retire queue before leaving
         if (t.joinable()) t.join();
     cudaSetDevice(s->cfg.device);
     for (SrvReq *q : s->ready)
