@@ -57,6 +57,35 @@ def test_mix_equals_alone(gpu, prec):
             assert np.linalg.norm(a - b) <= tol * max(nb, 1e-30)
 
 
+@pytest.mark.parametrize("prec", [PREC_FP32C, PREC_FP64])
+def test_damped_and_zero_coupling_requests(gpu, prec):
+    """Requests with the absorbing sponge (their own damped group) and with
+    complex_gauge=1, g_gauge=0 (ungauged dynamics, links carried) in one mix:
+    each matches the single-grid path within the mode's tolerance."""
+    rng = np.random.default_rng(21)
+    reqs = []
+    for k, N in enumerate((16, 20, 24, 18)):
+        p, st, _ = serve.make_request(rng, N, prec, (10, 20))
+        if k % 2 == 0:
+            p = dataclasses.replace(p, bc_type=0, damp_width=2.0, damp_rate=0.05)
+        reqs.append((p, st, 30 + 7 * k))
+    p, st, _ = serve.make_request(rng, 16, prec, (10, 20))
+    while not p.complex_gauge:
+        p, st, _ = serve.make_request(rng, 16, prec, (10, 20))
+    reqs.append((dataclasses.replace(p, g_gauge=0.0), st, 33))
+    mixed = _run_mix(reqs)
+    tol = 1e-11 if prec == PREC_FP64 else 1e-5
+    for (p, st, n), (snap, diag, info) in zip(reqs, mixed):
+        assert info.state == serve.DONE
+        assert len(snap) == p.ncols
+        with Simulation(dataclasses.replace(p, tile_variant=info.tile_variant), st.cols()) as sim:
+            sim.step(n)
+            alone = sim.snapshot()
+        for a, b in zip(snap, alone):
+            nb = np.linalg.norm(b)
+            assert np.linalg.norm(a - b) <= tol * max(nb, 1e-30)
+
+
 def test_budget_limits_admission(gpu):
     reqs = _requests(PREC_FP32C, seed=9)
     with serve.Server(chunk_steps=10, autotune=False, mem_budget_bytes=1) as srv:   # room for one at a time
