@@ -111,6 +111,23 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x: float, dist, device: str) -> float:
+    """The largest x over all ranks (the slowest replica's time); x itself
+    without a process group."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job rate of N independent replicas: every rank did the same work,
+    and the job took as long as the slowest rank."""
+    return units_per_rank * world / seconds_max
+
+
 def measured_peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -465,14 +482,9 @@ def main():
     clocks = clk.stop()
     barrier()
     info = sim.info()
-    ms_max = ms
-    if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist, f"cuda:{local}")
     ms_step = ms_max / args.steps
-    value = n3 * args.steps * world / (ms_max * 1e-3)
+    value = replica_throughput(n3 * args.steps, world, ms_max * 1e-3)
     bytes_site = info.step_bytes_per_site
     achieved = bytes_site * n3 / (ms / args.steps * 1e-3) / 1e9
     peaks = measured_peaks()
@@ -503,15 +515,10 @@ def main():
         sim2.snapshot(out=snap)
         t1 = time.perf_counter()
         sim2.close()
-        wall = t1 - t0
-        if dist:
-            import torch
-            t = torch.tensor([wall], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        wall = max_over_ranks(t1 - t0, dist, f"cuda:{local}")
         h2d = sum(c.nbytes for c in cols)
         d2h = sum(c.nbytes for c in snap) + nd * 8 * 53
-        e2e = {"value": n3 * args.steps * world / wall, "unit": METRIC,
+        e2e = {"value": replica_throughput(n3 * args.steps, world, wall), "unit": METRIC,
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "wall_s": wall, "includes": "init upload from page-locked host columns, Gauss projection, "
                                            "steps, diag every 10 steps, final f64 snapshot into page-locked "

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SCP_GPU_ABI_VERSION 1
+#define SCP_GPU_ABI_VERSION 2
 #define SCP_GPU_MAX_COLS 30
 
 /* status codes */
