@@ -161,6 +161,19 @@ def cpu_baseline(params, cols, nsteps: int) -> dict:
                       f"loop wall time {ms:.2f} ms/step"}
 
 
+def reference_gpu(params, cols, nsteps: int) -> dict:
+    """The reference's own CUDA stepper (sfa/sim/scp_sim.cu, recompiled
+    unmodified for sm_100a into oracle/_ref/scp_sim_cuda) on the same
+    workload, timed by its own loop clock."""
+    import oracle
+    if not os.path.exists(oracle.REF_GPU_BIN):
+        return {"value": None, "unit": METRIC, "note": "reference CUDA binary not built"}
+    r = oracle.run_reference(params, cols, nsteps, diag_every=nsteps, read_final=False, binary=oracle.REF_GPU_BIN)
+    ms = r["wall_ms_per_step"]
+    return {"value": params.N ** 3 / (ms * 1e-3), "unit": METRIC, "ms_per_step": ms, "steps": nsteps,
+            "kind": "reference sfa/sim/scp_sim.cu recompiled for sm_100a, FP64, its own loop clock"}
+
+
 def run_reference_arm(args, rank, world):
     from scp_b200 import seeds
     seed, prec, desc = WORKLOADS[args.workload]
@@ -417,6 +430,8 @@ def main():
     ap.add_argument("--no-sequential", action="store_true", help="c3: skip the one-after-another FP64 run")
     ap.add_argument("--seq-sample", type=int, default=0, help="c3: run only the first R requests sequentially")
     ap.add_argument("--snap-every", type=int, default=100, help="snap: steps between SFA frames")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="also time the reference's own CUDA stepper on the same FP64 workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
@@ -543,6 +558,11 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(params, cols, 10 if params.N <= 128 else 3)
+    if rank == 0 and world == 1 and args.ref_gpu and prec == 0:
+        rg = reference_gpu(params, cols, 50)
+        if rg.get("value"):
+            rg["ours_over_reference_gpu"] = value / rg["value"]
+        line["reference_gpu"] = rg
     if rank == 0:
         print(json.dumps(line))
     if dist:

@@ -23,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_BIN = os.path.join(HERE, "_ref", "scp_sim")
+REF_GPU_BIN = os.path.join(HERE, "_ref", "scp_sim_cuda")   # the reference's CUDA stepper (sm_100a)
 SFA_TOOL = os.path.join(HERE, "_ref", "sfa_tool")
 NDIAG = 31
 
@@ -177,8 +178,9 @@ def read_diag(path: str) -> tuple[list[str], np.ndarray]:
 
 def run_reference(params, cols: Sequence[np.ndarray], nsteps: int, diag_every: int | None = None,
                   threads: int | None = None, workdir: str | None = None, extra_cfg: dict | None = None,
-                  read_final: bool = True) -> dict:
-    """Run the reference binary on the given initial columns for nsteps.
+                  read_final: bool = True, binary: str | None = None) -> dict:
+    """Run the reference binary (CPU by default, or `binary`, e.g. REF_GPU_BIN)
+    on the given initial columns for nsteps.
 
     Returns {'cols': final columns (SFA order) or None, 'names', 'diag_header',
     'diag' rows, 'wall_ms_per_step', 'stdout'}.
@@ -200,7 +202,7 @@ def run_reference(params, cols: Sequence[np.ndarray], nsteps: int, diag_every: i
         f.write(params.to_cfg(**kv))
     env = dict(os.environ)
     env["OMP_NUM_THREADS"] = str(threads or os.cpu_count() or 1)
-    res = subprocess.run([REF_BIN, cfg], capture_output=True, text=True, env=env, cwd=tmp)
+    res = subprocess.run([binary or REF_BIN, cfg], capture_output=True, text=True, env=env, cwd=tmp)
     if res.returncode != 0:
         raise RuntimeError(f"reference run failed ({res.returncode}): {res.stderr[-2000:]}")
     wall = None
