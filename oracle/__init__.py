@@ -170,9 +170,13 @@ def read_frame(path: str, frame: int, n3: int) -> tuple[list[str], list[np.ndarr
 
 
 def read_diag(path: str) -> tuple[list[str], np.ndarray]:
+    """Header and rows of a diag TSV (a list of rows when their lengths
+    differ, as in the reference CUDA build's file)."""
     with open(path) as f:
         header = f.readline().rstrip("\n").split("\t")
-        rows = [[float(x) for x in ln.split("\t")] for ln in f if ln.strip()]
+        rows = [[float(x) for x in ln.split("\t") if x.strip()] for ln in f if ln.strip()]
+    if len({len(r) for r in rows}) > 1:
+        return header, rows
     return header, np.array(rows)
 
 

@@ -124,3 +124,21 @@ def test_small_served_mix(gpu):
             d = srv.result(i)
             assert np.isfinite(d[8])
     assert np.all(lat > 0) and makespan > 0
+
+
+def test_free_with_requests_in_flight(gpu):
+    """Closing the server while requests are queued, loading, running and
+    retiring returns cleanly (loader and retire threads are joined, every
+    handle freed) and the device stays usable."""
+    reqs = _requests(PREC_FP64, seed=31) + _requests(PREC_FP32C, seed=32)
+    srv = serve.Server(chunk_steps=4, autotune=False, loader_threads=2)
+    for p, st, n in reqs:
+        srv.submit(p, st.cols(), n)
+    srv.poll()
+    srv.poll()
+    srv.close()
+    p, st, n = reqs[0]
+    with Simulation(p, st.cols()) as sim:
+        sim.step(3)
+        assert np.isfinite(sim.diag()["E_total"])
+
