@@ -47,6 +47,8 @@ WORKLOADS = {
     "c4f": ("c4", 1, "gauged FP32-compensated 512^3, eight co-phase balls"),
     "c3": (None, 1, "served mixed queue, FP32-compensated, Poisson arrivals, N in 32..128 (seed 2)"),
     "c2acc": ("c2", 1, "gauged 256^3 + N(0,0.01) thermal noise: FP32-compensated against FP64, side by side"),
+    "c4acc": ("c4", 1, "gauged 512^3, eight co-phase balls: FP32-compensated against FP64 at full size, "
+                       "diagnostics every 50 steps"),
     "snap": (None, 1, "host driver scp_sim_b200, gauged FP32C two-ball qball init, f32 SFA snapshots: "
                       "none / synchronous / pipelined"),
 }
@@ -289,18 +291,23 @@ def _half_centroids(cols, params) -> np.ndarray:
     return np.array(out)
 
 
-def run_precision_compare(args) -> dict:
-    """c2acc: the c2 seed (gauged, thermal background) stepped in FP64 and in
-    FP32-compensated mode side by side; per-observable error of the FP32C run
-    against the FP64 run: energy drift, Noether charge, Gauss residual,
-    per-field relative L2 and the two half-box charge centroids."""
+def run_precision_compare(args, name: str = "c2acc") -> dict:
+    """c2acc: the c2 seed (gauged, thermal background, 256^3) stepped in FP64
+    and in FP32-compensated mode side by side; per-observable error of the
+    FP32C run against the FP64 run: energy drift, Noether charge, Gauss
+    residual, per-field relative L2 and the two half-box charge centroids.
+    c4acc: the same comparison for the c4 seed (eight co-phase balls, 512^3,
+    FP64 at full size as the reference run) on the diagnostics alone (a
+    512^3 snapshot is 32 GB of host memory per run)."""
     import dataclasses
     from scp_b200 import seeds, PREC_FP32C
     from scp_b200.api import Simulation
+    seed = "c2" if name == "c2acc" else "c4"
+    snapshots = name == "c2acc"
     over = dict(N=args.n, L=(args.n - 1) / 4.0) if args.n else {}
-    p64 = seeds.params_for("c2", **over)
+    p64 = seeds.params_for(seed, **over)
     p32 = dataclasses.replace(p64, precision=PREC_FP32C)
-    st = seeds.make_state("c2", p64)
+    st = seeds.make_state(seed, p64)
     cols = st.cols()
     del st
     total = args.steps
@@ -324,7 +331,7 @@ def run_precision_compare(args) -> dict:
                 walls[k] += time.perf_counter() - t0
                 series[k].append(sim.diag_vector())
             done += n
-            if done % snap_every == 0 or done == total:
+            if snapshots and (done % snap_every == 0 or done == total):
                 snaps = {k: sim.snapshot() for k, sim in sims.items()}
                 for k in sims:
                     cent[k].append(_half_centroids(snaps[k], p64))
@@ -342,10 +349,16 @@ def run_precision_compare(args) -> dict:
     drift_a = (A[:, ix["E_total"]] - e0a) / abs(e0a)
     drift_b = (B[:, ix["E_total"]] - B[0, ix["E_total"]]) / abs(B[0, ix["E_total"]])
     q = ix["Q_total"]
-    ca, cb = np.array(cent["fp64"]), np.array(cent["fp32c"])
+    if snapshots:
+        ca, cb = np.array(cent["fp64"]), np.array(cent["fp32c"])
+        csteps = [s for s, _ in field_l2]
+    else:   # the rho^2-weighted centroid of the diagnostics, every diag step
+        cols3 = [ix["centroid_x"], ix["centroid_y"], ix["centroid_z"]]
+        ca, cb = A[:, cols3], B[:, cols3]
+        csteps = list(range(0, total + 1, every))
     n3 = p64.N ** 3
     return {
-        "metric": "FP32-compensated error vs FP64", "workload": WORKLOADS["c2acc"][2], "N": p64.N, "steps": total,
+        "metric": "FP32-compensated error vs FP64", "workload": WORKLOADS[name][2], "N": p64.N, "steps": total,
         "diag_every": every, "data": "synthetic",
         "energy": {"rel_drift_fp64_end": float(drift_a[-1]), "rel_drift_fp32c_end": float(drift_b[-1]),
                    "max_abs_drift_difference": float(np.max(np.abs(drift_b - drift_a))),
@@ -361,8 +374,12 @@ def run_precision_compare(args) -> dict:
         "gauss": {"gauss_max_fp64_max": float(A[:, ix["gauss_max"]].max()),
                   "gauss_max_fp32c_max": float(B[:, ix["gauss_max"]].max())},
         "field_rel_l2_max_over_columns": field_l2,
-        "centroids": {"steps": [s for s, _ in field_l2], "fp64": ca.tolist(),
+        "centroids": {"steps": csteps[:: max(1, len(csteps) // 8)],
+                      "fp64": ca[:: max(1, len(csteps) // 8)].tolist(),
                       "max_abs_difference": float(np.max(np.abs(cb - ca)))},
+        "other_diagnostics_max_rel_difference": {
+            n: float(np.max(np.abs(B[:, ix[n]] - A[:, ix[n]])) / max(np.max(np.abs(A[:, ix[n]])), 1e-300))
+            for n in ("phi_max", "P_max", "s_max", "r_core", "Q_core", "E_em")},
         "throughput_incl_diag": {k: n3 * total / walls[k] for k in walls},
     }
 
@@ -451,7 +468,7 @@ def main():
         dist = dist_mod
 
     if args.impl == "reference":
-        if args.workload in ("c3", "c2acc", "snap"):
+        if args.workload in ("c3", "c2acc", "c4acc", "snap"):
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "this workload exercises the library's "
                                   "server or its two precisions, which the reference does not have; its CPU "
@@ -472,10 +489,10 @@ def main():
     if args.workload == "snap":
         print(json.dumps(run_snapshot_pipeline(args)))
         return
-    if args.workload == "c2acc":
+    if args.workload in ("c2acc", "c4acc"):
         if world > 1:
-            raise SystemExit("c2acc runs on one GPU")
-        print(json.dumps(run_precision_compare(args)))
+            raise SystemExit(f"{args.workload} runs on one GPU")
+        print(json.dumps(run_precision_compare(args, args.workload)))
         return
 
     from scp_b200 import seeds
