@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SCP_GPU_ABI_VERSION 2
+#define SCP_GPU_ABI_VERSION 3
 #define SCP_GPU_MAX_COLS 30
 
 /* status codes */
@@ -82,6 +82,11 @@ typedef struct {
     int32_t gauss_project;    /* 1: one-time Gauss projection at init (reference default) */
     int32_t device;           /* CUDA device ordinal */
     int32_t tile_variant;     /* 0: autotuned default; >0 selects a fixed tile shape */
+    int32_t real_fields;      /* 1: the reference's real 6-field mode (complex_phi=0,
+                                 compute_forces scp_sim.c:743-929 with its default terms):
+                                 12 host columns (0-11 of the order above), run as the
+                                 complex dynamics with a zero imaginary sector, which is the
+                                 same equation of motion; not with complex_gauge */
 } scp_gpu_params;
 
 /* Diagnostic slots: the reference diag TSV columns after "t"

@@ -8,7 +8,7 @@
  *
  *   sfa_tool write OUT.sfa N L dt NCOLS RAW.f64
  *       RAW.f64 holds NCOLS*N^3 little-endian doubles, columns in the
- *       stepper's registration order (24 complex or 30 gauged columns,
+ *       stepper's registration order (12 real, 24 complex or 30 gauged columns,
  *       sfa/sim/scp_sim.c:2862-2897).  Writes one F64 frame at t=0, raw codec.
  *
  *   sfa_tool read IN.sfa FRAME OUT.f64
@@ -45,7 +45,7 @@ static int do_write(int argc, char **argv) {
     int N = atoi(argv[3]);
     double L = atof(argv[4]), dt = atof(argv[5]);
     int ncols = atoi(argv[6]);
-    if (N < 2 || (ncols != 24 && ncols != 30)) { fprintf(stderr, "bad N/NCOLS\n"); return 2; }
+    if (N < 2 || (ncols != 12 && ncols != 24 && ncols != 30)) { fprintf(stderr, "bad N/NCOLS\n"); return 2; }
     size_t n3 = (size_t)N * N * N;
     double *raw = malloc(sizeof(double) * n3 * ncols);
     FILE *fp = fopen(argv[7], "rb");

@@ -25,6 +25,7 @@ struct DiagConsts {
     double m2, mtheta2, eta, mu, kappa;
     int gauged;               // covariant energy, plaquette energy (g != 0)
     int links;                // th / E columns present: Gauss residual, E_em, Q_flux
+    int real;                 // real 6-field mode (imaginary sector zero): theta_rms over 3 components
     double g, bpre;           // bpre = 1/(g^2 dx^4)
     double R2;                // qdiag_radius^2
     double Rcube;             // qdiag_radius (Q_flux cube half width)

@@ -94,6 +94,7 @@ struct scp_gpu {
     long long N3;
     int gauged, nf, prec;
     int links;                   // th / E columns carried (complex_gauge; with g = 0 they stay constant)
+    int real;                    // real 6-field mode: 12 host columns, imaginary sector held at zero
     int device;
     cudaStream_t stream = nullptr;
     // FP64 state
@@ -140,6 +141,8 @@ static int validate(const scp_gpu_params *p) {
     if (p->bc_type != 0 && p->bc_type != 2) return SCP_EUNSUPPORTED;
     if (p->precision_mode != SCP_PREC_FP64 && p->precision_mode != SCP_PREC_FP32C) return SCP_EINVAL;
     if (p->tile_variant < 0 || p->tile_variant >= kNumShapes) return SCP_EINVAL;
+    if (p->real_fields != 0 && p->real_fields != 1) return SCP_EINVAL;
+    if (p->real_fields && p->complex_gauge) return SCP_EUNSUPPORTED;   // links need the complex fields
     return SCP_OK;
 }
 
@@ -411,7 +414,7 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     int rc;
     if ((rc = alloc_common(h))) return rc;
     const long long n3 = h->N3;
-    const int ncols = h->links ? 30 : 24;
+    const int ncols = h->links ? 30 : 24;   // device columns (the real mode's imaginary ones are zero)
     const size_t nel = (size_t)h->nf * n3;
     const size_t blk = sizeof(double) * nel;
     // FP64 slab: X[0] = x_0 and S = v_0 stage the initial state in both modes;
@@ -430,7 +433,10 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
         int field, mom;
         sfa_col_source(c, &field, &mom);
         double *dst = (mom ? h->S : h->X[0]) + (size_t)field * n3;
-        cudaError_t e = cudaMemcpyAsync(dst, cols[c], sizeof(double) * n3, kind, h->stream);
+        // real 6-field mode: the caller passes columns 0-11 only; v = tv = 0 exactly,
+        // and the complex step keeps them zero (its real limit)
+        cudaError_t e = (h->real && c >= 12) ? cudaMemsetAsync(dst, 0, sizeof(double) * n3, h->stream)
+                                             : cudaMemcpyAsync(dst, cols[c], sizeof(double) * n3, kind, h->stream);
         if (e != cudaSuccess) {
             snprintf(g_cuda_err, sizeof g_cuda_err, "%s (column %d upload)", cudaGetErrorString(e), c);
             return SCP_ECUDA;
@@ -487,7 +493,7 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
     int rc = validate(p);
     if (rc) return rc;
     if (!cols) return SCP_EINVAL;
-    const int ncols = p->complex_gauge ? 30 : 24;
+    const int ncols = p->complex_gauge ? 30 : (p->real_fields ? 12 : 24);
     for (int c = 0; c < ncols; c++)
         if (!cols[c]) return SCP_EINVAL;
     int ndev = 0;
@@ -501,6 +507,7 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
     // the reference dispatches on complex_gauge && g != 0 (scp_sim.c:1586, :2820):
     // with g = 0 it runs the ungauged dynamics and carries th / E unchanged
     h->links = p->complex_gauge ? 1 : 0;
+    h->real = p->real_fields ? 1 : 0;
     h->gauged = (p->complex_gauge && p->g_gauge != 0.0) ? 1 : 0;
     h->nf = h->links ? 15 : 12;
     h->prec = p->precision_mode;
@@ -578,7 +585,9 @@ static void diag_assemble(const double *f1, const double *f2, const double *pt, 
     o[SCP_DIAG_PHI_MAX] = f1[DS_NSUM + DM_PM];
     o[SCP_DIAG_P_MAX] = f1[DS_NSUM + DM_PMAX];
     o[SCP_DIAG_P_INT] = f1[DS_PINT];
-    o[SCP_DIAG_THETA_RMS] = sqrt(f1[DS_TRS] / (6.0 * (double)n3));
+    // complex: over 6 real components per site (theta_rms_complex); real mode: over
+    // the 3 real angles (theta_rms, scp_sim.c:1803-1809), the imaginary parts being zero
+    o[SCP_DIAG_THETA_RMS] = sqrt(f1[DS_TRS] / ((c.real ? 3.0 : 6.0) * (double)n3));
     o[SCP_DIAG_Q_PHI] = f1[DS_QP] * dV;
     o[SCP_DIAG_Q_THETA] = f1[DS_QT] * dV;
     o[SCP_DIAG_Q_TOTAL] = f1[DS_QP] * dV + f1[DS_QT] * dV;
@@ -613,6 +622,7 @@ static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
     c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
     c.gauged = h->gauged;
     c.links = h->links;
+    c.real = h->real;
     c.g = h->gauged ? p.g_gauge : 0.0;
     c.bpre = h->gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
     c.R2 = p.qdiag_radius * p.qdiag_radius;
@@ -666,7 +676,7 @@ __global__ void snap_col_kernel(View V, int field, int mom, long long n, int dty
 
 template <class View>
 static int snapshot_with(scp_gpu *h, const View &V, int dtype, void *const *host_cols) {
-    const int ncols = h->links ? 30 : 24;
+    const int ncols = h->links ? 30 : (h->real ? 12 : 24);
     const long long n3 = h->N3;
     const int nb = red_blocks(n3);
     const size_t es = dtype == SCP_DTYPE_F64 ? 8 : (dtype == SCP_DTYPE_F32 ? 4 : 2);
@@ -708,7 +718,7 @@ int scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols) {
 // with them), then copy the staging to the host on the copy stream.
 template <class View>
 static int snapshot_async_with(scp_gpu *h, const View &V, int dtype, void *const *host_cols) {
-    const int ncols = h->links ? 30 : 24;
+    const int ncols = h->links ? 30 : (h->real ? 12 : 24);
     const long long n3 = h->N3;
     const size_t es = dtype == SCP_DTYPE_F64 ? 8 : (dtype == SCP_DTYPE_F32 ? 4 : 2);
     const size_t col = es * (size_t)n3, need = col * ncols;
@@ -971,6 +981,7 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     int rc = validate(pp);
     if (rc) return rc;
     if (!dev_cols || !out) return SCP_EINVAL;
+    if (pp->real_fields) return SCP_EUNSUPPORTED;   // takes the complex column set
     if (pp->N > SCP_DIAG_STATIC_MAX_N) {
         snprintf(g_cuda_err, sizeof g_cuda_err, "scp_gpu_diag_noalloc: N=%d exceeds SCP_DIAG_STATIC_MAX_N=%d",
                  pp->N, SCP_DIAG_STATIC_MAX_N);
@@ -1004,6 +1015,7 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
     c.gauged = gauged;
     c.links = links;
+    c.real = 0;
     c.g = gauged ? p.g_gauge : 0.0;
     c.bpre = gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
     c.R2 = p.qdiag_radius * p.qdiag_radius;

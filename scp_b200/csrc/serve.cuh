@@ -508,6 +508,7 @@ static int srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *
     int rc = validate(p);
     if (rc) return rc;
     if (p->device != s->cfg.device) return SCP_EINVAL;
+    if (p->real_fields) return SCP_EUNSUPPORTED;   // the server takes complex and gauged requests
     auto q = std::make_unique<SrvReq>();
     q->p = *p;
     q->nsteps = nsteps;

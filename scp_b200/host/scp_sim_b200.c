@@ -17,7 +17,8 @@
  *   gpu_device     = <ordinal>       (default 0)
  *   gpu_async_snap = 1 | 0          (default 1: snapshots copied and written
  *                                     while the GPU keeps stepping)
- * It covers the complex (complex_phi=1) and gauged (complex_gauge=1) stepper
+ * It covers the complex (complex_phi=1), gauged (complex_gauge=1) and real
+ * 6-field (complex_phi=0, default terms) stepper
  * with bc_type 0 or 2; other modes are refused with a message.
  *
  * Build: make -C scp_b200/host REF=<kardianos/scp checkout>
@@ -76,7 +77,7 @@ static Grid *grid_new(const Config *c, double **cols, int ncols) {
 }
 
 /* Column schema of the complex / gauged snapshot (sfa/sim/scp_sim.c:2862-2897). */
-static void add_columns(SFA *sfa, uint8_t dt, int gauged) {
+static void add_columns(SFA *sfa, uint8_t dt, int n) {
     static const char *names[30] = {
         "phi_x", "phi_y", "phi_z", "theta_x", "theta_y", "theta_z",
         "phi_vx", "phi_vy", "phi_vz", "theta_vx", "theta_vy", "theta_vz",
@@ -91,7 +92,6 @@ static void add_columns(SFA *sfa, uint8_t dt, int gauged) {
         SFA_ANGLE, SFA_ANGLE, SFA_ANGLE, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY};
     static const uint8_t comp[30] = {0, 1, 2, 0, 1, 2, 0, 1, 2, 3, 4, 5, 3, 4, 5, 3, 4, 5,
                                      6, 7, 8, 9, 10, 11, 6, 7, 8, 12, 13, 14};
-    const int n = gauged ? 30 : 24;
     for (int k = 0; k < n; k++) sfa_add_column(sfa, names[k], dt, sem[k], comp[k]);
 }
 
@@ -211,12 +211,16 @@ static int snap_close(Snap *s) {
 
 /* One diag TSV row in the reference's column set and formats
  * (sfa/sim/scp_sim.c:2993-3003, :3045-3066). */
-static void diag_row(FILE *fp, double t, const scp_gpu_diag_out *d, int gauged) {
+static void diag_row(FILE *fp, double t, const scp_gpu_diag_out *d, int gauged, int complex) {
     const double *v = d->v;
     fprintf(fp, "%.2f\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e", t,
             v[SCP_DIAG_E_PHI_KIN], v[SCP_DIAG_E_THETA_KIN], v[SCP_DIAG_E_GRAD], v[SCP_DIAG_E_MASS],
             v[SCP_DIAG_E_POT], v[SCP_DIAG_E_TGRAD], v[SCP_DIAG_E_TMASS], v[SCP_DIAG_E_COUPLING],
             v[SCP_DIAG_E_TOTAL], v[SCP_DIAG_PHI_MAX], v[SCP_DIAG_P_MAX], v[SCP_DIAG_P_INT], v[SCP_DIAG_THETA_RMS]);
+    if (!complex) {   /* real 6-field mode: energies and amplitudes only */
+        fprintf(fp, "\n");
+        return;
+    }
     fprintf(fp, "\t%.12e\t%.12e\t%.12e\t%.6e\t%.6e\t%.12e\t%.12e\t%.6e\t%.6e\t%.6e\t%.6e",
             v[SCP_DIAG_Q_PHI], v[SCP_DIAG_Q_THETA], v[SCP_DIAG_Q_TOTAL], v[SCP_DIAG_S_MAX], v[SCP_DIAG_R_CORE],
             v[SCP_DIAG_OMEGA_CORE], v[SCP_DIAG_Q_CORE], v[SCP_DIAG_THP1U], v[SCP_DIAG_THP1V], v[SCP_DIAG_THP2U],
@@ -273,7 +277,11 @@ int main(int argc, char **argv) {
     }
     cfg_print(&c);
     cfg_validate(&c);
-    if (!c.complex_phi) { fprintf(stderr, "ERROR: scp_sim_b200 runs the complex/gauged stepper (complex_phi=1)\n"); return 1; }
+    if (!c.complex_phi && (c.complex_gauge || c.mode != 0 || c.alpha_cs != 0 || c.beta_h != 0 || c.kappa_h != 0)) {
+        fprintf(stderr, "ERROR: the real 6-field mode runs with its default terms only "
+                        "(mode=0, alpha_cs=beta_h=kappa_h=0, no gauge)\n");
+        return 1;
+    }
     if (c.bc_type == 1) { fprintf(stderr, "ERROR: bc_type=1 is not supported by scp_sim_b200\n"); return 1; }
     if (c.n_fabrics != 1 || c.higgs_v > 0 || c.g_gauge2 != 0 || c.n_locks > 0 || c.test_gauge_xform) {
         fprintf(stderr, "ERROR: multi-fabric, Higgs, second gauge, locks and test_gauge_xform are not supported\n");
@@ -281,7 +289,7 @@ int main(int argc, char **argv) {
     }
     if (c.bc_type == 2) { c.damp_width = 0.0; c.damp_rate = 0.0; }   /* as the CUDA reference (scp_sim.cu:5170-5172) */
     const int gauged = c.complex_gauge && c.g_gauge != 0.0;
-    const int ncols = c.complex_gauge ? 30 : 24;
+    const int ncols = c.complex_gauge ? 30 : (c.complex_phi ? 24 : 12);
     double *cols[30] = {0};
     Grid *g = grid_new(&c, cols, ncols);
     if (!g) { fprintf(stderr, "FATAL: host allocation\n"); return 1; }
@@ -298,6 +306,7 @@ int main(int argc, char **argv) {
     p.precision_mode = gpu_prec;
     p.qdiag_radius = c.qdiag_radius; p.qdiag_probe1 = c.qdiag_probe1; p.qdiag_probe2 = c.qdiag_probe2;
     p.gauss_project = 1; p.device = gpu_dev; p.tile_variant = 0;
+    p.real_fields = c.complex_phi ? 0 : 1;
     scp_gpu *h = NULL;
     int rc = scp_gpu_init(&p, (const double *const *)cols, &h);
     if (rc) return fail("scp_gpu_init", rc);
@@ -314,7 +323,7 @@ int main(int argc, char **argv) {
     if (!sfa) { fprintf(stderr, "ERROR: cannot create output file '%s'\n", c.output); return 1; }
     sfa->flags = SFA_CODEC_COLZSTD | SFA_FLAG_STREAMING;
     sfa_embed_kvmd(sfa, &c);
-    add_columns(sfa, sdt, c.complex_gauge);
+    add_columns(sfa, sdt, ncols);
     sfa_finalize_header(sfa);
     static Snap snap;
     if (snap_open(&snap, h, sfa, ncols, c.precision, g->N3, gpu_async_snap)) {
@@ -327,9 +336,11 @@ int main(int argc, char **argv) {
     if (!fp) { fprintf(stderr, "ERROR: cannot open %s\n", c.diag_file); return 1; }
     fprintf(fp, "t\tE_phi_kin\tE_theta_kin\tE_grad\tE_mass\tE_pot\tE_tgrad\tE_tmass\t"
                 "E_coupling\tE_total\tphi_max\tP_max\tP_int\ttheta_rms");
-    fprintf(fp, "\tQ_phi\tQ_theta\tQ_total\ts_max\tr_core\tomega_core\tQ_core\tthp1u\tthp1v\tthp2u\tthp2v");
+    if (c.complex_phi)
+        fprintf(fp, "\tQ_phi\tQ_theta\tQ_total\ts_max\tr_core\tomega_core\tQ_core\tthp1u\tthp1v\tthp2u\tthp2v");
     if (c.complex_gauge) fprintf(fp, "\tgauss_max\tgauss_l2\tE_em\tQ_flux");
-    fprintf(fp, "\tQ_p0\tQ_p1\tQ_p2\n");
+    if (c.complex_phi) fprintf(fp, "\tQ_p0\tQ_p1\tQ_p2");
+    fprintf(fp, "\n");
 
     const int n_steps = (int)lround(c.T / g->dt);
     int diag_every = (int)lround(c.diag_dt / g->dt); if (diag_every < 1) diag_every = 1;
@@ -339,7 +350,7 @@ int main(int argc, char **argv) {
     const double E0 = d.v[SCP_DIAG_E_TOTAL];
     printf("INIT: E_total=%.4e E_pot=%.4f phi_max=%.4f P_int=%.4e theta_rms=%.3e\n\n", E0, d.v[SCP_DIAG_E_POT],
            d.v[SCP_DIAG_PHI_MAX], d.v[SCP_DIAG_P_INT], d.v[SCP_DIAG_THETA_RMS]);
-    diag_row(fp, 0.0, &d, c.complex_gauge);
+    diag_row(fp, 0.0, &d, c.complex_gauge, c.complex_phi);
 
     int major = diag_every * 25;
     if (major > n_steps / 10) { major = (n_steps / 10 / diag_every) * diag_every; if (major < diag_every) major = diag_every; }
@@ -358,7 +369,7 @@ int main(int argc, char **argv) {
         if (step % snap_every == 0 && (rc = snap_start(&snap, t))) return fail("snapshot", rc);
         if (step % diag_every == 0) {
             if ((rc = scp_gpu_diag(h, &d))) return fail("diag", rc);
-            diag_row(fp, t, &d, c.complex_gauge);
+            diag_row(fp, t, &d, c.complex_gauge, c.complex_phi);
             fflush(fp);
             if (step % major == 0) {
                 const double wall = wall_now() - wall0;
@@ -384,7 +395,8 @@ int main(int argc, char **argv) {
     printf("\n=== COMPLETE ===\n");
     printf("E_total=%.4e (drift %.3f%%) E_pot=%.4f\n", d.v[SCP_DIAG_E_TOTAL],
            100 * (d.v[SCP_DIAG_E_TOTAL] - E0) / (fabs(E0) + 1e-30), d.v[SCP_DIAG_E_POT]);
-    printf("Q_phi=%.6e Q_theta=%.6e Q_total=%.6e s_max=%.4e r_core=%.3f omega_core=%.4f Q_core=%.6e\n",
+    if (c.complex_phi)
+        printf("Q_phi=%.6e Q_theta=%.6e Q_total=%.6e s_max=%.4e r_core=%.3f omega_core=%.4f Q_core=%.6e\n",
            d.v[SCP_DIAG_Q_PHI], d.v[SCP_DIAG_Q_THETA], d.v[SCP_DIAG_Q_TOTAL], d.v[SCP_DIAG_S_MAX],
            d.v[SCP_DIAG_R_CORE], d.v[SCP_DIAG_OMEGA_CORE], d.v[SCP_DIAG_Q_CORE]);
     if (c.complex_gauge)

@@ -41,6 +41,7 @@ class CParams(ctypes.Structure):
         ("gauss_project", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("tile_variant", ctypes.c_int32),
+        ("real_fields", ctypes.c_int32),
     ]
 
 
@@ -72,6 +73,7 @@ class Params:
     gauss_project: int = 1
     device: int = 0
     tile_variant: int = 0
+    real_fields: int = 0      # 1: the reference's real 6-field mode (complex_phi = 0)
 
     @property
     def dx(self) -> float:
@@ -95,6 +97,8 @@ class Params:
 
     @property
     def ncols(self) -> int:
+        if self.real_fields:
+            return 12
         return 30 if self.complex_gauge else 24
 
     def steps_for(self, T: float) -> int:
@@ -124,6 +128,7 @@ class Params:
         c.gauss_project = self.gauss_project
         c.device = self.device
         c.tile_variant = self.tile_variant
+        c.real_fields = 1 if self.real_fields else 0
         return c
 
     def to_cfg(self, **extra) -> str:
@@ -131,7 +136,7 @@ class Params:
         kv = {
             "N": self.N, "L": repr(self.L), "dt_factor": repr(self.dt_factor),
             "m": repr(self.m), "m_theta": repr(self.m_theta), "eta": repr(self.eta),
-            "mu": repr(self.mu), "kappa": repr(self.kappa), "complex_phi": 1,
+            "mu": repr(self.mu), "kappa": repr(self.kappa), "complex_phi": 0 if self.real_fields else 1,
             "complex_gauge": int(self.complex_gauge), "g_gauge": repr(self.g_gauge),
             "bc_type": self.bc_type, "damp_width": repr(self.damp_width),
             "damp_rate": repr(self.damp_rate), "qdiag_radius": repr(self.qdiag_radius),

@@ -125,6 +125,29 @@ def add_noise(st: State, names: Sequence[str], var: float, seed: int) -> None:
         st[name] += sd * normals(seed, j, n3).reshape(st[name].shape)
 
 
+def real_state(N: int, seed: int = 5, L: float | None = None, **over) -> State:
+    """A test state of the real 6-field mode (complex_phi = 0): two Gaussian
+    blobs with different amplitudes per component on phi (the triple product
+    P = phi_x phi_y phi_z is non-zero in their cores), a breathing velocity
+    phi_v = -0.3 phi, and N(0, 1e-3) noise on theta and on every velocity."""
+    L = L if L is not None else (N - 1) / 2.0 * 0.9
+    kw = dict(N=N, L=L, dt_factor=0.2, bc_type=2, complex_gauge=0, real_fields=1)
+    kw.update(over)
+    p = Params(**kw)
+    st = State(p)
+    x = coords(p)
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    sig = max(1.0, p.L / 4)
+    for cx, amps in ((-0.3 * p.L, (1.0, 0.9, 1.1)), (0.3 * p.L, (0.8, 1.2, 1.0))):
+        env = np.exp(-((X - cx) ** 2 + Y ** 2 + Z ** 2) / (2 * sig * sig))
+        for a, ax in enumerate("xyz"):
+            st["phi_" + ax] += amps[a] * env
+            st["phi_v" + ax] += -0.3 * amps[a] * env
+    add_noise(st, ("theta_x", "theta_y", "theta_z"), 1e-3, seed=seed)
+    add_noise(st, ("phi_vx", "phi_vy", "phi_vz", "theta_vx", "theta_vy", "theta_vz"), 1e-3, seed=seed + 1)
+    return st
+
+
 def charge_density(st: State) -> np.ndarray:
     """rho = sum_a u v' - v u' + tu tv' - tv tu' (sfa/sim/scp_sim.c:153-160)."""
     rho = np.zeros_like(st["phi_x"])

@@ -127,6 +127,42 @@ def test_snapshot_async_matches_sync_while_stepping(gpu, prec, dtype):
     assert not np.array_equal(later[0], want[0])
 
 
+def test_real_mode_matches_reference_binary(gpu):
+    """The reference's real 6-field mode (complex_phi = 0, compute_forces with
+    its default terms) run by the reference CPU binary and by this library on
+    the same seed: final frame per column and every diag TSV column."""
+    st = seeds.real_state(16, seed=9)
+    p = st.params
+    ref = oracle.run_reference(p, st.cols(), 40, diag_every=10)
+    rows = []
+    with Simulation(p, st.cols()) as sim:
+        rows.append(sim.diag_vector())
+        for _ in range(4):
+            sim.step(10)
+            rows.append(sim.diag_vector())
+        got = sim.snapshot()
+    assert len(got) == 12 and len(ref["cols"]) == 12
+    assert worst_rel(got, ref["cols"]) < 1e-11
+    want = np.asarray(ref["diag"])[:, 1:]                 # drop t; %.6e columns in the reference's TSV
+    have = np.array(rows)[:, :want.shape[1]]
+    assert np.all(np.abs(have - want) <= 2e-6 * np.abs(want) + 1e-12)
+
+
+def test_real_mode_fp32c_tracks_fp64(gpu):
+    """FP32-compensated real mode against the FP64 real mode after 100 steps."""
+    from scp_b200 import PREC_FP32C
+    st = seeds.real_state(24, seed=12)
+    p64 = st.params
+    p32 = Params(**{**p64.__dict__, "precision": PREC_FP32C})
+    with Simulation(p64, st.cols()) as a, Simulation(p32, st.cols()) as b:
+        a.step(100)
+        b.step(100)
+        A, B = a.snapshot(), b.snapshot()
+    assert len(A) == len(B) == 12
+    worst = max(rel_l2(B[c], A[c]) for c in range(12) if np.linalg.norm(A[c]) > 1e-3 * np.sqrt(len(A[c])))
+    assert worst < 1e-5, worst
+
+
 def test_gpu_initial_state_roundtrip(gpu):
     st = seeds.small_state(12, False, seed=4)
     with Simulation(st.params, st.cols()) as sim:
