@@ -127,18 +127,22 @@ def test_snapshot_async_matches_sync_while_stepping(gpu, prec, dtype):
     assert not np.array_equal(later[0], want[0])
 
 
-def test_real_mode_matches_reference_binary(gpu):
+@pytest.mark.parametrize("N,nsteps,damped", [(16, 40, False), (33, 60, True), (64, 200, False)])
+def test_real_mode_matches_reference_binary(gpu, N, nsteps, damped):
     """The reference's real 6-field mode (complex_phi = 0, compute_forces with
     its default terms) run by the reference CPU binary and by this library on
-    the same seed: final frame per column and every diag TSV column."""
-    st = seeds.real_state(16, seed=9)
+    the same seed: final frame per column and every diag TSV column; odd N and
+    the absorbing sponge included."""
+    over = dict(bc_type=0, damp_width=3.0, damp_rate=0.02) if damped else {}
+    st = seeds.real_state(N, seed=9, **over)
     p = st.params
-    ref = oracle.run_reference(p, st.cols(), 40, diag_every=10)
+    every = nsteps // 4
+    ref = oracle.run_reference(p, st.cols(), nsteps, diag_every=every)
     rows = []
     with Simulation(p, st.cols()) as sim:
         rows.append(sim.diag_vector())
         for _ in range(4):
-            sim.step(10)
+            sim.step(every)
             rows.append(sim.diag_vector())
         got = sim.snapshot()
     assert len(got) == 12 and len(ref["cols"]) == 12
