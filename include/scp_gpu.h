@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define SCP_GPU_ABI_VERSION 3
+#define SCP_GPU_ABI_VERSION 4
 #define SCP_GPU_MAX_COLS 30
 
 /* status codes */
@@ -87,6 +87,13 @@ typedef struct {
                                  12 host columns (0-11 of the order above), run as the
                                  complex dynamics with a zero imaginary sector, which is the
                                  same equation of motion; not with complex_gauge */
+    /* Optional terms of the real 6-field mode (compute_forces, scp_sim.c:743-929; all
+     * zero = the default terms): mass mode 1 (m_eff^2 = inv_alpha/(1+inv_beta|phi|^2))
+     * or 3 (kappa_eff = kappa/(1+kappa_gamma|phi|^2)), Cosserat strain alpha_cs,
+     * curl-squared hardening beta_h, chiral helicity kappa_h.  With any of them set the
+     * real mode runs on separate FP64 per-site kernels (FP32C refused). */
+    int32_t mode;
+    double  inv_alpha, inv_beta, kappa_gamma, alpha_cs, beta_h, kappa_h;
 } scp_gpu_params;
 
 /* Diagnostic slots: the reference diag TSV columns after "t"

@@ -22,6 +22,7 @@
 #include "reduce.cuh"
 #include "snapshot.cuh"
 #include "launch.cuh"
+#include "real.cuh"
 
 #include <math.h>
 #include <stdio.h>
@@ -95,6 +96,10 @@ struct scp_gpu {
     int gauged, nf, prec;
     int links;                   // th / E columns carried (complex_gauge; with g = 0 they stay constant)
     int real;                    // real 6-field mode: 12 host columns, imaginary sector held at zero
+    // real 6-field mode with optional terms: separate per-site kernels (real.cuh)
+    int rp = 0;
+    double *rbuf = nullptr, *rx = nullptr, *rv = nullptr, *ra = nullptr, *rmq = nullptr;
+    RealConsts rc{};
     int device;
     cudaStream_t stream = nullptr;
     // FP64 state
@@ -143,6 +148,10 @@ static int validate(const scp_gpu_params *p) {
     if (p->tile_variant < 0 || p->tile_variant >= kNumShapes) return SCP_EINVAL;
     if (p->real_fields != 0 && p->real_fields != 1) return SCP_EINVAL;
     if (p->real_fields && p->complex_gauge) return SCP_EUNSUPPORTED;   // links need the complex fields
+    const bool optional = p->mode != 0 || p->alpha_cs != 0 || p->beta_h != 0 || p->kappa_h != 0;
+    if (p->mode != 0 && p->mode != 1 && p->mode != 3) return SCP_EUNSUPPORTED;
+    if (optional && !p->real_fields) return SCP_EINVAL;   // the reference allows them in the real mode only
+    if (optional && p->precision_mode != SCP_PREC_FP64) return SCP_EUNSUPPORTED;
     return SCP_OK;
 }
 
@@ -487,6 +496,97 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     return SCP_OK;
 }
 
+// ---------------------------------------------------------------- real mode with optional terms
+
+static bool real_optional(const scp_gpu_params *p) {
+    return p->real_fields && (p->mode != 0 || p->alpha_cs != 0 || p->beta_h != 0 || p->kappa_h != 0);
+}
+
+static void real_forces(scp_gpu *h) {
+    const int nb = red_blocks(h->N3);
+    if (h->rc.acs != 0 || h->rc.bh != 0) real_pass1_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->rx, h->rmq, h->rc);
+    real_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->rx, h->rmq, h->ra, h->rc);
+}
+
+// one verlet_step (scp_sim.c:1583-1716): kick, drift, forces, kick, sponge
+static int real_step(scp_gpu *h) {
+    const int nb = red_blocks(h->N3);
+    real_kick_drift_kernel<<<red_blocks(6 * h->N3), kRedThreads, 0, h->stream>>>(h->rx, h->rv, h->ra, h->rc);
+    real_forces(h);
+    real_kick_damp_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->rv, h->ra, h->rc);
+    CK(cudaGetLastError());
+    return SCP_OK;
+}
+
+static int init_real(scp_gpu *h, const double *const *cols, bool on_device) {
+    int rc;
+    if ((rc = alloc_common(h))) return rc;
+    const long long n3 = h->N3;
+    CK(cudaMallocAsync(&h->rbuf, sizeof(double) * 24 * (size_t)n3, h->stream));
+    CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
+    h->dev_bytes += sizeof(double) * 25 * (size_t)n3;
+    h->rx = h->rbuf;
+    h->rv = h->rbuf + 6 * n3;
+    h->ra = h->rbuf + 12 * n3;
+    h->rmq = h->rbuf + 18 * n3;
+    CK(cudaMemsetAsync(h->rmq, 0, sizeof(double) * 6 * (size_t)n3, h->stream));
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int c = 0; c < 12; c++)
+        CK(cudaMemcpyAsync((c < 6 ? h->rx + c * n3 : h->rv + (c - 6) * n3), cols[c], sizeof(double) * n3, kind,
+                           h->stream));
+    const scp_gpu_params &p = h->p;
+    RealConsts &r = h->rc;
+    r.N = p.N; r.N3 = n3; r.L = p.L; r.dx = p.dx; r.dV = p.dx * p.dx * p.dx;
+    r.idx1 = 1.0 / (2.0 * p.dx); r.idx2 = 1.0 / (p.dx * p.dx); r.hdt = 0.5 * p.dt; r.dt = p.dt;
+    r.mu = p.mu; r.kappa = p.kappa; r.m2 = p.m2; r.mtheta2 = p.mtheta2; r.eta = p.eta;
+    r.kh = p.kappa_h; r.acs = p.alpha_cs; r.bh = p.beta_h; r.kg = p.kappa_gamma; r.ia = p.inv_alpha; r.ib = p.inv_beta;
+    r.mode = p.mode;
+    r.damp = damping_on(h) ? 1 : 0;
+    r.damp_width = p.damp_width; r.damp_rate = p.damp_rate;
+    real_forces(h);                                  // the reference computes forces before its loop
+    CK(cudaGetLastError());
+    // the generic snapshot and info code reads these
+    h->X[0] = h->X[1] = h->rx;
+    h->S = h->rv;
+    h->cur = 0;
+    h->shape = 1;
+    return SCP_OK;
+}
+
+static int real_diag(scp_gpu *h, scp_gpu_diag_out *out) {
+    const int nb = red_blocks(h->N3);
+    real_energy_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->rx, h->rv, h->rc, h->part);
+    fold_partials_kernel<RS_NSUM, RM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * (RS_NSUM + RM_NMAX), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    const double *f = h->h_small;
+    double *o = out->v;
+    for (int q = 0; q < SCP_DIAG_NSLOTS; q++) o[q] = 0.0;
+    o[SCP_DIAG_E_PHI_KIN] = f[RS_EPK];
+    o[SCP_DIAG_E_THETA_KIN] = f[RS_ETK];
+    o[SCP_DIAG_E_GRAD] = f[RS_EG];
+    o[SCP_DIAG_E_MASS] = f[RS_EM];
+    o[SCP_DIAG_E_POT] = f[RS_EP];
+    o[SCP_DIAG_E_TGRAD] = f[RS_ETG];
+    o[SCP_DIAG_E_TMASS] = f[RS_ETM];
+    o[SCP_DIAG_E_COUPLING] = f[RS_EC];
+    o[SCP_DIAG_E_TOTAL] = f[RS_EPK] + f[RS_ETK] + f[RS_EG] + f[RS_EM] + f[RS_EP] + f[RS_ETG] + f[RS_ETM] + f[RS_EC];
+    o[SCP_DIAG_PHI_MAX] = f[RS_NSUM + RM_PM];
+    o[SCP_DIAG_P_MAX] = f[RS_NSUM + RM_PMAX];
+    o[SCP_DIAG_P_INT] = f[RS_PINT];
+    o[SCP_DIAG_THETA_RMS] = sqrt(f[RS_TH2] / (3.0 * (double)h->N3));
+    if (!isfinite(o[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
+    return SCP_OK;
+}
+
+// source slot of host column c: the packed complex layout, or the 6-field one
+static void col_source(const scp_gpu *h, int c, int *field, int *mom) {
+    if (h->rp) { *field = c % 6; *mom = c >= 6; return; }
+    sfa_col_source(c, field, mom);
+}
+
 static int init_common(const scp_gpu_params *p, const double *const *cols, bool on_device, scp_gpu **out) {
     if (!out) return SCP_EINVAL;
     *out = nullptr;
@@ -512,7 +612,8 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
     h->nf = h->links ? 15 : 12;
     h->prec = p->precision_mode;
     fill_consts(h);
-    rc = init_body(h, cols, on_device);
+    h->rp = real_optional(p) ? 1 : 0;
+    rc = h->rp ? init_real(h, cols, on_device) : init_body(h, cols, on_device);
     if (rc == SCP_OK) {
         cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
@@ -543,6 +644,12 @@ int scp_gpu_step(scp_gpu *h, int nsteps) {
     if (nsteps == 0) return SCP_OK;
     CK(cudaSetDevice(h->device));
     int rc;
+    if (h->rp) {
+        for (int n = 0; n < nsteps; n++)
+            if ((rc = real_step(h))) return rc;
+        h->steps += nsteps;
+        return SCP_OK;
+    }
     for (int n = 0; n < nsteps; n++) {
         const bool last = (n == nsteps - 1);
         if ((rc = launch_step(h, false, last))) return rc;
@@ -651,6 +758,7 @@ extern "C" {
 int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     if (!h || !out) return SCP_EINVAL;
     CK(cudaSetDevice(h->device));
+    if (h->rp) return real_diag(h, out);
     if (h->prec == SCP_PREC_FP64) {
         ViewF64 V{h->X[h->cur ^ 1], h->S, h->N3};
         return diag_with(h, V, out);
@@ -683,7 +791,7 @@ static int snapshot_with(scp_gpu *h, const View &V, int dtype, void *const *host
     for (int c = 0; c < ncols; c++) {
         if (!host_cols[c]) return SCP_EINVAL;
         int field, mom;
-        sfa_col_source(c, &field, &mom);
+        col_source(h, c, &field, &mom);
         if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {   // straight copy of the FP64 column
             const double *src = (mom ? h->S : h->X[h->cur ^ 1]) + (size_t)field * n3;
             CK(cudaMemcpyAsync(host_cols[c], src, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
@@ -744,7 +852,7 @@ static int snapshot_async_with(scp_gpu *h, const View &V, int dtype, void *const
     const int nb = red_blocks(n3);
     for (int c = 0; c < ncols; c++) {
         int field, mom;
-        sfa_col_source(c, &field, &mom);
+        col_source(h, c, &field, &mom);
         if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {
             const double *src = (mom ? h->S : h->X[h->cur ^ 1]) + (size_t)field * n3;
             CK(cudaMemcpyAsync(stage + c * col, src, col, cudaMemcpyDeviceToDevice, h->stream));
@@ -845,7 +953,7 @@ void scp_gpu_free(scp_gpu *h) {
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->stream) {
         void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->count, h->stage,
-                        h->snap_dev};
+                        h->snap_dev, h->rbuf};
         for (void *b : bufs)
             if (b) cudaFreeAsync(b, h->stream);
         cudaStreamSynchronize(h->stream);

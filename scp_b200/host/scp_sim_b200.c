@@ -18,7 +18,7 @@
  *   gpu_async_snap = 1 | 0          (default 1: snapshots copied and written
  *                                     while the GPU keeps stepping)
  * It covers the complex (complex_phi=1), gauged (complex_gauge=1) and real
- * 6-field (complex_phi=0, default terms) stepper
+ * 6-field (complex_phi=0, with its optional terms) stepper
  * with bc_type 0 or 2; other modes are refused with a message.
  *
  * Build: make -C scp_b200/host REF=<kardianos/scp checkout>
@@ -277,9 +277,8 @@ int main(int argc, char **argv) {
     }
     cfg_print(&c);
     cfg_validate(&c);
-    if (!c.complex_phi && (c.complex_gauge || c.mode != 0 || c.alpha_cs != 0 || c.beta_h != 0 || c.kappa_h != 0)) {
-        fprintf(stderr, "ERROR: the real 6-field mode runs with its default terms only "
-                        "(mode=0, alpha_cs=beta_h=kappa_h=0, no gauge)\n");
+    if (!c.complex_phi && c.complex_gauge) {
+        fprintf(stderr, "ERROR: the gauge links need the complex fields (complex_phi=1)\n");
         return 1;
     }
     if (c.bc_type == 1) { fprintf(stderr, "ERROR: bc_type=1 is not supported by scp_sim_b200\n"); return 1; }
@@ -307,6 +306,8 @@ int main(int argc, char **argv) {
     p.qdiag_radius = c.qdiag_radius; p.qdiag_probe1 = c.qdiag_probe1; p.qdiag_probe2 = c.qdiag_probe2;
     p.gauss_project = 1; p.device = gpu_dev; p.tile_variant = 0;
     p.real_fields = c.complex_phi ? 0 : 1;
+    p.mode = c.mode; p.inv_alpha = c.inv_alpha; p.inv_beta = c.inv_beta; p.kappa_gamma = c.kappa_gamma;
+    p.alpha_cs = c.alpha_cs; p.beta_h = c.beta_h; p.kappa_h = c.kappa_h;
     scp_gpu *h = NULL;
     int rc = scp_gpu_init(&p, (const double *const *)cols, &h);
     if (rc) return fail("scp_gpu_init", rc);

@@ -42,6 +42,13 @@ class CParams(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("tile_variant", ctypes.c_int32),
         ("real_fields", ctypes.c_int32),
+        ("mode", ctypes.c_int32),
+        ("inv_alpha", ctypes.c_double),
+        ("inv_beta", ctypes.c_double),
+        ("kappa_gamma", ctypes.c_double),
+        ("alpha_cs", ctypes.c_double),
+        ("beta_h", ctypes.c_double),
+        ("kappa_h", ctypes.c_double),
     ]
 
 
@@ -74,6 +81,14 @@ class Params:
     device: int = 0
     tile_variant: int = 0
     real_fields: int = 0      # 1: the reference's real 6-field mode (complex_phi = 0)
+    # optional terms of the real mode (scp_config.h defaults)
+    mode: int = 0
+    inv_alpha: float = 2.25
+    inv_beta: float = 5.0
+    kappa_gamma: float = 2.0
+    alpha_cs: float = 0.0
+    beta_h: float = 0.0
+    kappa_h: float = 0.0
 
     @property
     def dx(self) -> float:
@@ -129,6 +144,13 @@ class Params:
         c.device = self.device
         c.tile_variant = self.tile_variant
         c.real_fields = 1 if self.real_fields else 0
+        c.mode = self.mode
+        c.inv_alpha = self.inv_alpha
+        c.inv_beta = self.inv_beta
+        c.kappa_gamma = self.kappa_gamma
+        c.alpha_cs = self.alpha_cs
+        c.beta_h = self.beta_h
+        c.kappa_h = self.kappa_h
         return c
 
     def to_cfg(self, **extra) -> str:
@@ -141,6 +163,9 @@ class Params:
             "bc_type": self.bc_type, "damp_width": repr(self.damp_width),
             "damp_rate": repr(self.damp_rate), "qdiag_radius": repr(self.qdiag_radius),
             "qdiag_probe1": repr(self.qdiag_probe1), "qdiag_probe2": repr(self.qdiag_probe2),
+            "mode": self.mode, "inv_alpha": repr(self.inv_alpha), "inv_beta": repr(self.inv_beta),
+            "kappa_gamma": repr(self.kappa_gamma), "alpha_cs": repr(self.alpha_cs), "beta_h": repr(self.beta_h),
+            "kappa_h": repr(self.kappa_h),
         }
         kv.update(extra)
         return "".join(f"{k} = {v}\n" for k, v in kv.items())

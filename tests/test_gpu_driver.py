@@ -22,17 +22,19 @@ def _run(binary, cfg, cwd, extra=()):
     return r.stdout
 
 
-@pytest.mark.parametrize("gauged", [False, True, "g0", "sync", "real"])
+@pytest.mark.parametrize("gauged", [False, True, "g0", "sync", "real", "real_terms"])
 def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
     """gauged="g0": complex_gauge=1 with g_gauge=0, the reference's ungauged
     dispatch with the link columns carried; "sync": gauged with the
     synchronous snapshot path (gpu_async_snap = 0) instead of the pipelined one;
-    "real": the real 6-field mode (complex_phi = 0)."""
+    "real": the real 6-field mode (complex_phi = 0); "real_terms": with optional terms."""
     assert os.path.exists(DRIVER), "host driver not built (make -C scp_b200/host)"
     if gauged == "g0":
         st = seeds.small_state(16, True, seed=13, g_gauge=0.0)
     elif gauged == "real":
         st = seeds.real_state(16, seed=13)
+    elif gauged == "real_terms":
+        st = seeds.real_state(16, seed=13, mode=3, alpha_cs=0.2, kappa_h=0.1)
     else:
         st = seeds.small_state(16, bool(gauged), seed=13)
     p = st.params

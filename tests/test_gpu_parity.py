@@ -152,6 +152,33 @@ def test_real_mode_matches_reference_binary(gpu, N, nsteps, damped):
     assert np.all(np.abs(have - want) <= 2e-6 * np.abs(want) + 1e-12)
 
 
+REAL_TERMS = [dict(mode=1), dict(mode=3), dict(alpha_cs=0.3), dict(beta_h=0.5), dict(kappa_h=0.2),
+              dict(mode=3, alpha_cs=0.2, beta_h=0.3, kappa_h=0.1, bc_type=0, damp_width=3.0, damp_rate=0.02)]
+
+
+@pytest.mark.parametrize("terms", REAL_TERMS, ids=lambda t: "-".join(f"{k}{v}" for k, v in t.items()))
+def test_real_mode_optional_terms_match_reference_binary(gpu, terms):
+    """The real mode's optional terms (mass modes 1 and 3, Cosserat strain,
+    curl-squared hardening, chiral helicity; compute_forces, scp_sim.c:743-929)
+    on the separate real-mode kernels, against the reference CPU binary: final
+    frame per column and every diag TSV column."""
+    st = seeds.real_state(17, seed=21, **terms)
+    p = st.params
+    ref = oracle.run_reference(p, st.cols(), 40, diag_every=10)
+    rows = []
+    with Simulation(p, st.cols()) as sim:
+        rows.append(sim.diag_vector())
+        for _ in range(4):
+            sim.step(10)
+            rows.append(sim.diag_vector())
+        got = sim.snapshot()
+    assert len(got) == 12 and len(ref["cols"]) == 12
+    assert worst_rel(got, ref["cols"]) < 1e-11
+    want = np.asarray(ref["diag"])[:, 1:]
+    have = np.array(rows)[:, :want.shape[1]]
+    assert np.all(np.abs(have - want) <= 2e-6 * np.abs(want) + 1e-12)
+
+
 def test_real_mode_fp32c_tracks_fp64(gpu):
     """FP32-compensated real mode against the FP64 real mode after 100 steps."""
     from scp_b200 import PREC_FP32C
