@@ -51,7 +51,11 @@ WORKLOADS = {
                        "diagnostics every 50 steps"),
     "snap": (None, 1, "host driver scp_sim_b200, gauged FP32C two-ball qball init, f32 SFA snapshots: "
                       "none / synchronous / pipelined"),
+    "c1x": ("c1", 0, "gauged FP64 128^3 two balls + Higgs condensate (v=1, lambda=1, kappa_H=2, cavity r=4) "
+                     "+ second U(1) gauge (g2=0.1, charges 1,1,-2): per-site FP64 kernels"),
 }
+# parameters a workload adds to its seed's
+WORKLOAD_OVER = {"c1x": dict(higgs_v=1.0, higgs_rvoid=4.0, g_gauge2=0.1)}
 METRIC = "site-updates/s"
 
 
@@ -186,7 +190,7 @@ def reference_gpu(params, cols, n_short: int = 50, n_long: int = 250) -> dict:
 def run_reference_arm(args, rank, world):
     from scp_b200 import seeds
     seed, prec, desc = WORKLOADS[args.workload]
-    params = seeds.params_for(seed)
+    params = seeds.params_for(seed, **WORKLOAD_OVER.get(args.workload, {}))
     cfg = {"workload": desc, "N": params.N, "steps_sample": args.warmup + args.steps,
            "parallelism": "cpu-openmp"}
     if rank != 0:
@@ -499,7 +503,10 @@ def main():
     from scp_b200.api import Simulation
     seed, prec, desc = WORKLOADS[args.workload]
     over = dict(N=args.n, L=(args.n - 1) / 4.0) if args.n else {}
-    params = seeds.params_for(seed, precision=prec, device=local, tile_variant=args.tile, **over)
+    params = seeds.params_for(seed, precision=prec, device=local, tile_variant=args.tile, **over,
+                              **WORKLOAD_OVER.get(args.workload, {}))
+    # kernels per step: one fused launch, or the six per-site passes of the extensions
+    launches_per_step = 6 if (params.complex_gauge and (params.higgs_v > 0 or params.g_gauge2 != 0)) else 1
     st = seeds.make_state(seed, params)
     cols = st.cols()
     n3 = params.N ** 3
@@ -539,7 +546,7 @@ def main():
         pin_in = [pinned_empty(n3) for _ in cols]
         for dst, src in zip(pin_in, cols):
             dst[:] = np.asarray(src).reshape(-1)
-        snap = [pinned_empty(n3) for _ in cols]
+        snap = [pinned_empty(n3) for _ in range(params.snap_ncols)]   # + th2, E2 with the second gauge
         barrier()
         nd = 0
         t0 = time.perf_counter()
@@ -576,7 +583,7 @@ def main():
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "bytes_per_site": bytes_site,
                      "traffic": (lambda t: t * n3 if t else None)(profiled_traffic(args.workload))},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * launches_per_step,
         "clocks": clocks,
         "e2e": e2e,
     }

@@ -22,6 +22,9 @@
  *    0- 2 phi_x..z   3- 5 theta_x..z   6- 8 phi_vx..vz   9-11 theta_vx..vz
  *   12-14 phiim_*   15-17 thetaim_*   18-20 phiim_v*    21-23 thetaim_v*
  *   24-26 th_x..z   27-29 E_x..z      (24-29 only when complex_gauge=1)
+ *   30-32 th2_x..z  33-35 E2_x..z     (snapshots only, when g_gauge2 != 0:
+ *                                      the second gauge starts at zero, as the
+ *                                      reference's SFA seed loader leaves it)
  * Each column is N^3 values, site index (i*N + j)*N + k, k fastest.
  *
  * Threading: one handle is driven by one host thread at a time.  Every handle
@@ -37,8 +40,8 @@
 extern "C" {
 #endif
 
-#define SCP_GPU_ABI_VERSION 4
-#define SCP_GPU_MAX_COLS 30
+#define SCP_GPU_ABI_VERSION 5
+#define SCP_GPU_MAX_COLS 36
 
 /* status codes */
 #define SCP_OK              0
@@ -94,6 +97,17 @@ typedef struct {
      * real mode runs on separate FP64 per-site kernels (FP32C refused). */
     int32_t mode;
     double  inv_alpha, inv_beta, kappa_gamma, alpha_cs, beta_h, kappa_h;
+    /* Extensions of the gauged stepper (complex_gauge=1 and g_gauge != 0; ignored
+     * without complex_gauge, as the reference ignores them; refused with g_gauge = 0
+     * and in FP32C).  Higgs condensate (higgs_v > 0): V_H = (higgs_lam/4)(H^2 - v^2)^2
+     * + (higgs_kap/2) s H^2, H starting at v, or with a tanh cavity of radius
+     * higgs_rvoid (scp_sim.c:2802-2817).  Second compact U(1) gauge (g_gauge2 != 0)
+     * with per-component charges gauge2_q[3] (scp_config.h:97-103); its links and
+     * field start at zero and are Gauss-projected at init.  Either runs on separate
+     * FP64 per-site kernels in the reference's three-pass form. */
+    double  higgs_v, higgs_lam, higgs_kap, higgs_rvoid;
+    double  g_gauge2;
+    double  gauge2_q[3];
 } scp_gpu_params;
 
 /* Diagnostic slots: the reference diag TSV columns after "t"
@@ -126,7 +140,7 @@ typedef struct {
 
 typedef struct scp_gpu scp_gpu;
 
-/* Allocate device state, upload the host columns (24 complex or 30 gauged),
+/* Allocate device state, upload the host columns (12 real, 24 complex or 30 gauged),
  * and run the start-up sequence of the reference main (scp_sim.cu:5151-5245):
  * net-charge check (gauged, periodic), Gauss projection, first force. */
 int  scp_gpu_init(const scp_gpu_params *p, const double *const *host_cols, scp_gpu **out);

@@ -68,14 +68,15 @@ class Simulation:
         """Current state as host columns (SFA order) in dtype; into `out`
         (ncols arrays of N^3 values of the dtype) when given."""
         p = self.params
+        nc = p.snap_ncols
         if out is not None:
-            if len(out) < p.ncols or any(c.dtype != _NP_DTYPE[dtype] or c.size != p.N ** 3 or not c.flags.c_contiguous
-                                         for c in out[:p.ncols]):
+            if len(out) < nc or any(c.dtype != _NP_DTYPE[dtype] or c.size != p.N ** 3 or not c.flags.c_contiguous
+                                         for c in out[:nc]):
                 raise ValueError("snapshot: out needs ncols contiguous arrays of N^3 values of the dtype")
-            cols = list(out[:p.ncols])
+            cols = list(out[:nc])
         else:
-            cols = [np.empty(p.N ** 3, dtype=_NP_DTYPE[dtype]) for _ in range(p.ncols)]
-        arr = (ctypes.c_void_p * p.ncols)(*[c.ctypes.data for c in cols])
+            cols = [np.empty(p.N ** 3, dtype=_NP_DTYPE[dtype]) for _ in range(nc)]
+        arr = (ctypes.c_void_p * nc)(*[c.ctypes.data for c in cols])
         native.check(native.lib().scp_gpu_snapshot(self._h, int(dtype), arr), "scp_gpu_snapshot")
         return cols
 
@@ -83,9 +84,10 @@ class Simulation:
         """Start a snapshot into caller-owned arrays (N^3 each, of the dtype's
         numpy type); they must stay alive until snapshot_wait() returns."""
         p = self.params
-        if len(cols) < p.ncols or any(c.dtype != _NP_DTYPE[dtype] or c.size != p.N ** 3 for c in cols[:p.ncols]):
+        nc = p.snap_ncols
+        if len(cols) < nc or any(c.dtype != _NP_DTYPE[dtype] or c.size != p.N ** 3 for c in cols[:nc]):
             raise ValueError("snapshot_async: need ncols arrays of N^3 values of the dtype")
-        arr = (ctypes.c_void_p * p.ncols)(*[c.ctypes.data for c in cols[:p.ncols]])
+        arr = (ctypes.c_void_p * nc)(*[c.ctypes.data for c in cols[:nc]])
         native.check(native.lib().scp_gpu_snapshot_async(self._h, int(dtype), arr), "scp_gpu_snapshot_async")
 
     def snapshot_wait(self) -> None:

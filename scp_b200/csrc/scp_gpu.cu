@@ -23,6 +23,7 @@
 #include "snapshot.cuh"
 #include "launch.cuh"
 #include "real.cuh"
+#include "gext.cuh"
 
 #include <math.h>
 #include <stdio.h>
@@ -100,6 +101,12 @@ struct scp_gpu {
     int rp = 0;
     double *rbuf = nullptr, *rx = nullptr, *rv = nullptr, *ra = nullptr, *rmq = nullptr;
     RealConsts rc{};
+    // gauged stepper with the Higgs condensate and/or the second gauge: separate
+    // per-site FP64 kernels (gext.cuh)
+    int gx = 0, g2 = 0, higgs = 0;
+    double *gbuf = nullptr;
+    GextState gs{};
+    GextConsts gc{};
     int device;
     cudaStream_t stream = nullptr;
     // FP64 state
@@ -152,6 +159,12 @@ static int validate(const scp_gpu_params *p) {
     if (p->mode != 0 && p->mode != 1 && p->mode != 3) return SCP_EUNSUPPORTED;
     if (optional && !p->real_fields) return SCP_EINVAL;   // the reference allows them in the real mode only
     if (optional && p->precision_mode != SCP_PREC_FP64) return SCP_EUNSUPPORTED;
+    // the reference ignores the gauged extensions without complex_gauge (scp_sim.c:229-238)
+    if (p->complex_gauge && (p->higgs_v > 0 || p->g_gauge2 != 0)) {
+        if (p->g_gauge == 0) return SCP_EUNSUPPORTED;   // the ungauged dispatch never evolves them
+        if (p->precision_mode != SCP_PREC_FP64) return SCP_EUNSUPPORTED;
+        if (!isfinite(p->g_gauge2) || !isfinite(p->higgs_v)) return SCP_EINVAL;
+    }
     return SCP_OK;
 }
 
@@ -321,26 +334,12 @@ static GaussArgs gauss_args(scp_gpu *h, const double *X, double *S) {
 constexpr int kCgItMax = 20000;   // init_gauss_project's iteration cap (scp_sim.c:2337)
 constexpr int kCgBatch = 32;      // iterations enqueued between host checks
 
-static int gauss_startup(scp_gpu *h, const double *X, double *S) {
+// Conjugate gradients on -lap(chi) = b - mean(b) (init_gauss_project's loop,
+// scp_sim.c:2320-2372): b is in place and its block partial sums in h->part
+// (nb blocks).  chi is left in x, less the xbar held in h->cg[CG_XBAR].
+static int cg_solve(scp_gpu *h, int nb, double *b, double *x, double *r, double *p, double *Ap, int *iters) {
     const long long n3 = h->N3;
-    const int nb = red_blocks(n3);
-    GaussArgs a = gauss_args(h, X, S);
-    const double dV = h->p.dx * h->p.dx * h->p.dx;
-    int rc;
-    if (h->p.bc_type == 2) {
-        net_charge_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, dV, h->part);
-        fold_partials_kernel<2, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
-        CK(cudaGetLastError());
-        if ((rc = fold_to_host(h, 2))) return rc;
-        const double qn = fold_get(h, 0), qa = fold_get(h, 1);
-        if (fabs(qn) > 1e-6 * fmax(qa, 1.0)) return SCP_ENETCHARGE;
-    }
-    if (!h->p.gauss_project) return SCP_OK;
-    double *tmp = nullptr;
-    CK(cudaMallocAsync(&tmp, sizeof(double) * 5 * n3, h->stream));
-    double *b = tmp, *x = tmp + n3, *r = tmp + 2 * n3, *p = tmp + 3 * n3, *Ap = tmp + 4 * n3;
     const double n3d = (double)n3, idx2 = 1.0 / (h->p.dx * h->p.dx);
-    gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, b, h->part);
     fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
     cg_scalar_kernel<<<1, 1, 0, h->stream>>>(0, n3d, h->fold, h->cg);
     cg_start_kernel<<<nb, kRedThreads, 0, h->stream>>>(n3, b, r, p, x, h->cg, h->part);
@@ -363,10 +362,32 @@ static int gauss_startup(scp_gpu *h, const double *X, double *S) {
         CK(cudaStreamSynchronize(h->stream));
         if (h->h_small[CG_DONE] != 0.0) break;
     }
-    h->cg_iters = (int)h->h_small[CG_IT];
-    if (h->h_small[CG_RMAX] > h->h_small[CG_TOL]) {
+    *iters = (int)h->h_small[CG_IT];
+    return (h->h_small[CG_RMAX] > h->h_small[CG_TOL]) ? SCP_EGAUSS : SCP_OK;
+}
+
+static int gauss_startup(scp_gpu *h, const double *X, double *S) {
+    const long long n3 = h->N3;
+    const int nb = red_blocks(n3);
+    GaussArgs a = gauss_args(h, X, S);
+    const double dV = h->p.dx * h->p.dx * h->p.dx;
+    int rc;
+    if (h->p.bc_type == 2) {
+        net_charge_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, dV, h->part);
+        fold_partials_kernel<2, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+        CK(cudaGetLastError());
+        if ((rc = fold_to_host(h, 2))) return rc;
+        const double qn = fold_get(h, 0), qa = fold_get(h, 1);
+        if (fabs(qn) > 1e-6 * fmax(qa, 1.0)) return SCP_ENETCHARGE;
+    }
+    if (!h->p.gauss_project) return SCP_OK;
+    double *tmp = nullptr;
+    CK(cudaMallocAsync(&tmp, sizeof(double) * 5 * n3, h->stream));
+    double *b = tmp, *x = tmp + n3, *r = tmp + 2 * n3, *p = tmp + 3 * n3, *Ap = tmp + 4 * n3;
+    gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, b, h->part);
+    if ((rc = cg_solve(h, nb, b, x, r, p, Ap, &h->cg_iters))) {
         cudaFreeAsync(tmp, h->stream);
-        return SCP_EGAUSS;
+        return rc;
     }
     gauss_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, x, h->cg);
     gauss_sum_kernel<<<nb, kRedThreads, 0, h->stream>>>(a, h->part);
@@ -374,7 +395,27 @@ static int gauss_startup(scp_gpu *h, const double *X, double *S) {
     CK(cudaGetLastError());
     CK(cudaFreeAsync(tmp, h->stream));
     if ((rc = fold_to_host(h, 1))) return rc;
-    h->G_offset = fold_get(h, 0) / n3d;
+    h->G_offset = fold_get(h, 0) / (double)n3;
+    return SCP_OK;
+}
+
+// init_gauss2_project (scp_sim.c:2414-2458): the same solve for the second
+// gauge's residual, correction into E2, no frozen offset
+static int gauss2_startup(scp_gpu *h) {
+    const long long n3 = h->N3;
+    const int nb = red_blocks(n3);
+    double *tmp = nullptr;
+    CK(cudaMallocAsync(&tmp, sizeof(double) * 5 * n3, h->stream));
+    double *b = tmp, *x = tmp + n3, *r = tmp + 2 * n3, *p = tmp + 3 * n3, *Ap = tmp + 4 * n3;
+    gext_gauss2_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc, b, h->part);
+    int iters = 0, rc;
+    if ((rc = cg_solve(h, nb, b, x, r, p, Ap, &iters))) {
+        cudaFreeAsync(tmp, h->stream);
+        return rc;
+    }
+    gext_gauss2_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc, x, h->cg);
+    CK(cudaGetLastError());
+    CK(cudaFreeAsync(tmp, h->stream));
     return SCP_OK;
 }
 
@@ -581,9 +622,123 @@ static int real_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     return SCP_OK;
 }
 
+// ---------------------------------------------------------------- gauged extensions
+
+static bool gext_on(const scp_gpu_params *p) {
+    return p->complex_gauge && (p->higgs_v > 0 || p->g_gauge2 != 0);
+}
+
+// pass A (links), pass B (plaquettes), pass C (forces and field kicks)
+static void gext_forces(scp_gpu *h) {
+    const int nb = red_blocks(h->N3);
+    gext_links_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+    gext_plaq_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+    gext_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+}
+
+// one verlet_step (scp_sim.c:1583-1716): kick, drift, forces, kick, sponge
+static int gext_step(scp_gpu *h) {
+    const int nb = red_blocks(h->N3);
+    gext_kick_kernel<false><<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+    gext_drift_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+    gext_forces(h);
+    gext_kick_kernel<true><<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+    CK(cudaGetLastError());
+    return SCP_OK;
+}
+
+static int init_gext(scp_gpu *h, const double *const *cols, bool on_device) {
+    int rc;
+    if ((rc = alloc_common(h))) return rc;
+    const long long n3 = h->N3;
+    const scp_gpu_params &p = h->p;
+    h->g2 = p.g_gauge2 != 0 ? 1 : 0;
+    h->higgs = p.higgs_v > 0 ? 1 : 0;
+    // X S A (15 each), LC LS PS (3 each), then T2 E2 K2 PS2 (3 each), then H HV HA
+    const size_t narr = 54 + (h->g2 ? 12 : 0) + (h->higgs ? 3 : 0);
+    CK(cudaMallocAsync(&h->gbuf, sizeof(double) * narr * (size_t)n3, h->stream));
+    CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
+    h->dev_bytes += sizeof(double) * (narr + 1) * (size_t)n3;
+    CK(cudaMemsetAsync(h->gbuf, 0, sizeof(double) * narr * (size_t)n3, h->stream));
+    GextState &g = h->gs;
+    double *b = h->gbuf;
+    g.X = b; b += 15 * n3;
+    g.S = b; b += 15 * n3;
+    g.A = b; b += 15 * n3;
+    g.LC = b; b += 3 * n3;
+    g.LS = b; b += 3 * n3;
+    g.PS = b; b += 3 * n3;
+    if (h->g2) {
+        g.T2 = b; b += 3 * n3;
+        g.E2 = b; b += 3 * n3;
+        g.K2 = b; b += 3 * n3;
+        g.PS2 = b; b += 3 * n3;
+    }
+    if (h->higgs) {
+        g.H = b; b += n3;
+        g.HV = b; b += n3;
+        g.HA = b;
+    }
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int c = 0; c < 30; c++) {
+        int field, mom;
+        sfa_col_source(c, &field, &mom);
+        CK(cudaMemcpyAsync((mom ? g.S : g.X) + (size_t)field * n3, cols[c], sizeof(double) * n3, kind, h->stream));
+    }
+    GextConsts &k = h->gc;
+    k.N = p.N; k.N3 = n3; k.L = p.L; k.dx = p.dx; k.dV = p.dx * p.dx * p.dx;
+    k.idx1 = 1.0 / (2.0 * p.dx); k.idx2 = 1.0 / (p.dx * p.dx); k.inva = 1.0 / p.dx;
+    k.hdt = 0.5 * p.dt; k.dt = p.dt;
+    k.mu = p.mu; k.kappa = p.kappa; k.m2 = p.m2; k.mtheta2 = p.mtheta2; k.eta = p.eta;
+    k.g = p.g_gauge;
+    k.stp = 1.0 / (p.g_gauge * p.dx * p.dx * p.dx);
+    k.gad = -p.g_gauge * p.dx * p.dt;
+    k.g2on = h->g2;
+    k.g2 = p.g_gauge2;
+    k.stp2 = h->g2 ? 1.0 / (p.g_gauge2 * p.dx * p.dx * p.dx) : 0.0;
+    k.gad2 = -p.g_gauge2 * p.dx * p.dt;
+    for (int a = 0; a < 3; a++) k.q[a] = p.gauge2_q[a];
+    k.higgs = h->higgs;
+    k.hv = p.higgs_v; k.hlam = p.higgs_lam; k.hkap = p.higgs_kap;
+    k.damp = damping_on(h) ? 1 : 0;
+    k.damp_width = p.damp_width; k.damp_rate = p.damp_rate;
+    // the reference's start-up order (scp_sim.c:2802-2836): Higgs start value,
+    // net-charge check and Gauss projection, second Gauss projection, forces
+    if (h->higgs) gext_higgs_init_kernel<<<red_blocks(n3), kRedThreads, 0, h->stream>>>(g, k, p.higgs_rvoid);
+    CK(cudaGetLastError());
+    if ((rc = gauss_startup(h, g.X, g.S))) return rc;
+    if (h->g2 && p.gauss_project && (rc = gauss2_startup(h))) return rc;
+    gext_forces(h);
+    CK(cudaGetLastError());
+    // the generic diagnostics, snapshot and info code reads these
+    h->X[0] = h->X[1] = g.X;
+    h->S = g.S;
+    h->cur = 0;
+    h->shape = 1;
+    return SCP_OK;
+}
+
+// Higgs energy (summed into E_total by the reference, scp_sim.c:2034)
+static int gext_higgs_energy(scp_gpu *h, double *e) {
+    const int nb = red_blocks(h->N3);
+    gext_higgs_energy_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc, h->part);
+    fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    CK(cudaGetLastError());
+    int rc;
+    if ((rc = fold_to_host(h, 1))) return rc;
+    *e = fold_get(h, 0);
+    return SCP_OK;
+}
+
+// columns of a snapshot: th2 and E2 follow the 30 gauged ones with the second gauge
+static int snap_ncols(const scp_gpu *h) {
+    return h->links ? (h->g2 ? 36 : 30) : (h->real ? 12 : 24);
+}
+
 // source slot of host column c: the packed complex layout, or the 6-field one
 static void col_source(const scp_gpu *h, int c, int *field, int *mom) {
     if (h->rp) { *field = c % 6; *mom = c >= 6; return; }
+    if (c >= 30) { *field = (c - 30) % 3; *mom = c >= 33; return; }   // th2 / E2
     sfa_col_source(c, field, mom);
 }
 
@@ -613,7 +768,8 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
     h->prec = p->precision_mode;
     fill_consts(h);
     h->rp = real_optional(p) ? 1 : 0;
-    rc = h->rp ? init_real(h, cols, on_device) : init_body(h, cols, on_device);
+    h->gx = gext_on(p) ? 1 : 0;
+    rc = h->rp ? init_real(h, cols, on_device) : (h->gx ? init_gext(h, cols, on_device) : init_body(h, cols, on_device));
     if (rc == SCP_OK) {
         cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
@@ -644,9 +800,9 @@ int scp_gpu_step(scp_gpu *h, int nsteps) {
     if (nsteps == 0) return SCP_OK;
     CK(cudaSetDevice(h->device));
     int rc;
-    if (h->rp) {
+    if (h->rp || h->gx) {
         for (int n = 0; n < nsteps; n++)
-            if ((rc = real_step(h))) return rc;
+            if ((rc = h->rp ? real_step(h) : gext_step(h))) return rc;
         h->steps += nsteps;
         return SCP_OK;
     }
@@ -759,6 +915,15 @@ int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     if (!h || !out) return SCP_EINVAL;
     CK(cudaSetDevice(h->device));
     if (h->rp) return real_diag(h, out);
+    if (h->gx) {
+        ViewF64 V{h->gs.X, h->gs.S, h->N3};
+        int rc = diag_with(h, V, out);
+        if (rc || !h->higgs) return rc;
+        double eh = 0.0;
+        if ((rc = gext_higgs_energy(h, &eh))) return rc;
+        out->v[SCP_DIAG_E_TOTAL] += eh;
+        return isfinite(out->v[SCP_DIAG_E_TOTAL]) ? SCP_OK : SCP_ENONFINITE;
+    }
     if (h->prec == SCP_PREC_FP64) {
         ViewF64 V{h->X[h->cur ^ 1], h->S, h->N3};
         return diag_with(h, V, out);
@@ -784,7 +949,7 @@ __global__ void snap_col_kernel(View V, int field, int mom, long long n, int dty
 
 template <class View>
 static int snapshot_with(scp_gpu *h, const View &V, int dtype, void *const *host_cols) {
-    const int ncols = h->links ? 30 : (h->real ? 12 : 24);
+    const int ncols = snap_ncols(h);
     const long long n3 = h->N3;
     const int nb = red_blocks(n3);
     const size_t es = dtype == SCP_DTYPE_F64 ? 8 : (dtype == SCP_DTYPE_F32 ? 4 : 2);
@@ -792,7 +957,17 @@ static int snapshot_with(scp_gpu *h, const View &V, int dtype, void *const *host
         if (!host_cols[c]) return SCP_EINVAL;
         int field, mom;
         col_source(h, c, &field, &mom);
-        if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {   // straight copy of the FP64 column
+        if (c >= 30) {   // second gauge: th2 / E2 (FP64 state)
+            const double *src = (mom ? h->gs.E2 : h->gs.T2) + (size_t)field * n3;
+            if (dtype == SCP_DTYPE_F64) {
+                CK(cudaMemcpyAsync(host_cols[c], src, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
+            } else {
+                ViewF64 V2{h->gs.T2, h->gs.E2, n3};
+                snap_col_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V2, field, mom, n3, dtype, h->stage);
+                CK(cudaGetLastError());
+                CK(cudaMemcpyAsync(host_cols[c], h->stage, es * n3, cudaMemcpyDeviceToHost, h->stream));
+            }
+        } else if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {   // straight copy of the FP64 column
             const double *src = (mom ? h->S : h->X[h->cur ^ 1]) + (size_t)field * n3;
             CK(cudaMemcpyAsync(host_cols[c], src, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
         } else {
@@ -826,7 +1001,7 @@ int scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols) {
 // with them), then copy the staging to the host on the copy stream.
 template <class View>
 static int snapshot_async_with(scp_gpu *h, const View &V, int dtype, void *const *host_cols) {
-    const int ncols = h->links ? 30 : (h->real ? 12 : 24);
+    const int ncols = snap_ncols(h);
     const long long n3 = h->N3;
     const size_t es = dtype == SCP_DTYPE_F64 ? 8 : (dtype == SCP_DTYPE_F32 ? 4 : 2);
     const size_t col = es * (size_t)n3, need = col * ncols;
@@ -853,7 +1028,15 @@ static int snapshot_async_with(scp_gpu *h, const View &V, int dtype, void *const
     for (int c = 0; c < ncols; c++) {
         int field, mom;
         col_source(h, c, &field, &mom);
-        if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {
+        if (c >= 30) {   // second gauge: th2 / E2 (FP64 state)
+            const double *src = (mom ? h->gs.E2 : h->gs.T2) + (size_t)field * n3;
+            if (dtype == SCP_DTYPE_F64) {
+                CK(cudaMemcpyAsync(stage + c * col, src, col, cudaMemcpyDeviceToDevice, h->stream));
+            } else {
+                ViewF64 V2{h->gs.T2, h->gs.E2, n3};
+                snap_col_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V2, field, mom, n3, dtype, stage + c * col);
+            }
+        } else if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {
             const double *src = (mom ? h->S : h->X[h->cur ^ 1]) + (size_t)field * n3;
             CK(cudaMemcpyAsync(stage + c * col, src, col, cudaMemcpyDeviceToDevice, h->stream));
         } else {
@@ -922,6 +1105,8 @@ int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
     info->state_bytes_per_site = (h->prec == SCP_PREC_FP64)
                                      ? 2.0 * 8.0 * nfs
                                      : 4.0 * nfs + 12.0 * 2.0 + (h->gauged ? 3.0 * 4.0 : 0.0) + 4.0 * nfs;
+    // extensions: positions and momenta (30), th2 / E2 (6), H / Hdot (2), FP64
+    if (h->gx) info->state_bytes_per_site = 8.0 * (30.0 + 6.0 * h->g2 + 2.0 * h->higgs);
     info->step_bytes_per_site = 2.0 * info->state_bytes_per_site;
     info->tile_x = kShapes[h->shape].tx;
     info->tile_y = kShapes[h->shape].ty;
@@ -953,7 +1138,7 @@ void scp_gpu_free(scp_gpu *h) {
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->stream) {
         void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->count, h->stage,
-                        h->snap_dev, h->rbuf};
+                        h->snap_dev, h->rbuf, h->gbuf};
         for (void *b : bufs)
             if (b) cudaFreeAsync(b, h->stream);
         cudaStreamSynchronize(h->stream);
@@ -1090,6 +1275,7 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     if (rc) return rc;
     if (!dev_cols || !out) return SCP_EINVAL;
     if (pp->real_fields) return SCP_EUNSUPPORTED;   // takes the complex column set
+    if (gext_on(pp)) return SCP_EUNSUPPORTED;        // no Higgs energy term
     if (pp->N > SCP_DIAG_STATIC_MAX_N) {
         snprintf(g_cuda_err, sizeof g_cuda_err, "scp_gpu_diag_noalloc: N=%d exceeds SCP_DIAG_STATIC_MAX_N=%d",
                  pp->N, SCP_DIAG_STATIC_MAX_N);

@@ -17,9 +17,10 @@
  *   gpu_device     = <ordinal>       (default 0)
  *   gpu_async_snap = 1 | 0          (default 1: snapshots copied and written
  *                                     while the GPU keeps stepping)
- * It covers the complex (complex_phi=1), gauged (complex_gauge=1) and real
- * 6-field (complex_phi=0, with its optional terms) stepper
- * with bc_type 0 or 2; other modes are refused with a message.
+ * It covers the complex (complex_phi=1), gauged (complex_gauge=1, with the
+ * Higgs condensate and the second gauge) and real 6-field (complex_phi=0,
+ * with its optional terms) stepper with bc_type 0 or 2; other modes are
+ * refused with a message.
  *
  * Build: make -C scp_b200/host REF=<kardianos/scp checkout>
  */
@@ -76,22 +77,25 @@ static Grid *grid_new(const Config *c, double **cols, int ncols) {
     return g;
 }
 
-/* Column schema of the complex / gauged snapshot (sfa/sim/scp_sim.c:2862-2897). */
+/* Column schema of the complex / gauged snapshot (sfa/sim/scp_sim.c:2862-2907;
+ * th2 / E2 with the second gauge). */
 static void add_columns(SFA *sfa, uint8_t dt, int n) {
-    static const char *names[30] = {
+    static const char *names[36] = {
         "phi_x", "phi_y", "phi_z", "theta_x", "theta_y", "theta_z",
         "phi_vx", "phi_vy", "phi_vz", "theta_vx", "theta_vy", "theta_vz",
         "phiim_x", "phiim_y", "phiim_z", "thetaim_x", "thetaim_y", "thetaim_z",
         "phiim_vx", "phiim_vy", "phiim_vz", "thetaim_vx", "thetaim_vy", "thetaim_vz",
-        "th_x", "th_y", "th_z", "E_x", "E_y", "E_z"};
-    static const uint8_t sem[30] = {
+        "th_x", "th_y", "th_z", "E_x", "E_y", "E_z",
+        "th2_x", "th2_y", "th2_z", "E2_x", "E2_y", "E2_z"};
+    static const uint8_t sem[36] = {
         SFA_POSITION, SFA_POSITION, SFA_POSITION, SFA_ANGLE, SFA_ANGLE, SFA_ANGLE,
         SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY,
         SFA_POSITION, SFA_POSITION, SFA_POSITION, SFA_ANGLE, SFA_ANGLE, SFA_ANGLE,
         SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY,
+        SFA_ANGLE, SFA_ANGLE, SFA_ANGLE, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY,
         SFA_ANGLE, SFA_ANGLE, SFA_ANGLE, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY};
-    static const uint8_t comp[30] = {0, 1, 2, 0, 1, 2, 0, 1, 2, 3, 4, 5, 3, 4, 5, 3, 4, 5,
-                                     6, 7, 8, 9, 10, 11, 6, 7, 8, 12, 13, 14};
+    static const uint8_t comp[36] = {0, 1, 2, 0, 1, 2, 0, 1, 2, 3, 4, 5, 3, 4, 5, 3, 4, 5,
+                                     6, 7, 8, 9, 10, 11, 6, 7, 8, 12, 13, 14, 9, 10, 11, 15, 16, 17};
     for (int k = 0; k < n; k++) sfa_add_column(sfa, names[k], dt, sem[k], comp[k]);
 }
 
@@ -107,7 +111,7 @@ typedef struct {
     SFA *sfa;
     int ncols, dtype, async;
     size_t col_bytes;
-    void *cols[2][30];
+    void *cols[2][36];
     int pinned[2];
     double t[2];
     int busy[2];          /* set queued to or being written by the writer */
@@ -282,13 +286,22 @@ int main(int argc, char **argv) {
         return 1;
     }
     if (c.bc_type == 1) { fprintf(stderr, "ERROR: bc_type=1 is not supported by scp_sim_b200\n"); return 1; }
-    if (c.n_fabrics != 1 || c.higgs_v > 0 || c.g_gauge2 != 0 || c.n_locks > 0 || c.test_gauge_xform) {
-        fprintf(stderr, "ERROR: multi-fabric, Higgs, second gauge, locks and test_gauge_xform are not supported\n");
+    if (c.n_fabrics != 1 || c.n_locks > 0 || c.test_gauge_xform) {
+        fprintf(stderr, "ERROR: multi-fabric, locks and test_gauge_xform are not supported\n");
+        return 1;
+    }
+    /* Higgs and second gauge: ignored without complex_gauge, as the reference does
+     * (scp_sim.c:229-238); with g_gauge = 0 the reference's ungauged dispatch never
+     * evolves them, which this driver refuses */
+    const int gext = c.complex_gauge && (c.higgs_v > 0 || c.g_gauge2 != 0);
+    if (gext && c.g_gauge == 0.0) {
+        fprintf(stderr, "ERROR: higgs_v / g_gauge2 need g_gauge != 0\n");
         return 1;
     }
     if (c.bc_type == 2) { c.damp_width = 0.0; c.damp_rate = 0.0; }   /* as the CUDA reference (scp_sim.cu:5170-5172) */
     const int gauged = c.complex_gauge && c.g_gauge != 0.0;
     const int ncols = c.complex_gauge ? 30 : (c.complex_phi ? 24 : 12);
+    const int snap_cols = ncols + ((c.complex_gauge && c.g_gauge2 != 0) ? 6 : 0);   /* + th2, E2 */
     double *cols[30] = {0};
     Grid *g = grid_new(&c, cols, ncols);
     if (!g) { fprintf(stderr, "FATAL: host allocation\n"); return 1; }
@@ -308,6 +321,9 @@ int main(int argc, char **argv) {
     p.real_fields = c.complex_phi ? 0 : 1;
     p.mode = c.mode; p.inv_alpha = c.inv_alpha; p.inv_beta = c.inv_beta; p.kappa_gamma = c.kappa_gamma;
     p.alpha_cs = c.alpha_cs; p.beta_h = c.beta_h; p.kappa_h = c.kappa_h;
+    p.higgs_v = c.higgs_v; p.higgs_lam = c.higgs_lam; p.higgs_kap = c.higgs_kap; p.higgs_rvoid = c.higgs_rvoid;
+    p.g_gauge2 = c.g_gauge2;
+    p.gauge2_q[0] = c.gauge2_q0; p.gauge2_q[1] = c.gauge2_q1; p.gauge2_q[2] = c.gauge2_q2;
     scp_gpu *h = NULL;
     int rc = scp_gpu_init(&p, (const double *const *)cols, &h);
     if (rc) return fail("scp_gpu_init", rc);
@@ -324,10 +340,10 @@ int main(int argc, char **argv) {
     if (!sfa) { fprintf(stderr, "ERROR: cannot create output file '%s'\n", c.output); return 1; }
     sfa->flags = SFA_CODEC_COLZSTD | SFA_FLAG_STREAMING;
     sfa_embed_kvmd(sfa, &c);
-    add_columns(sfa, sdt, ncols);
+    add_columns(sfa, sdt, snap_cols);
     sfa_finalize_header(sfa);
     static Snap snap;
-    if (snap_open(&snap, h, sfa, ncols, c.precision, g->N3, gpu_async_snap)) {
+    if (snap_open(&snap, h, sfa, snap_cols, c.precision, g->N3, gpu_async_snap)) {
         fprintf(stderr, "FATAL: snapshot buffers\n");
         return 1;
     }

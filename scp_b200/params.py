@@ -49,6 +49,12 @@ class CParams(ctypes.Structure):
         ("alpha_cs", ctypes.c_double),
         ("beta_h", ctypes.c_double),
         ("kappa_h", ctypes.c_double),
+        ("higgs_v", ctypes.c_double),
+        ("higgs_lam", ctypes.c_double),
+        ("higgs_kap", ctypes.c_double),
+        ("higgs_rvoid", ctypes.c_double),
+        ("g_gauge2", ctypes.c_double),
+        ("gauge2_q", ctypes.c_double * 3),
     ]
 
 
@@ -89,6 +95,16 @@ class Params:
     alpha_cs: float = 0.0
     beta_h: float = 0.0
     kappa_h: float = 0.0
+    # extensions of the gauged stepper (scp_config.h defaults): Higgs condensate
+    # (higgs_v > 0) and second compact U(1) gauge (g_gauge2 != 0)
+    higgs_v: float = 0.0
+    higgs_lam: float = 1.0
+    higgs_kap: float = 2.0
+    higgs_rvoid: float = 0.0
+    g_gauge2: float = 0.0
+    gauge2_q0: float = 1.0
+    gauge2_q1: float = 1.0
+    gauge2_q2: float = -2.0
 
     @property
     def dx(self) -> float:
@@ -112,9 +128,19 @@ class Params:
 
     @property
     def ncols(self) -> int:
+        """Columns of an initial state (the second gauge starts at zero)."""
         if self.real_fields:
             return 12
         return 30 if self.complex_gauge else 24
+
+    @property
+    def gauge2(self) -> bool:
+        return bool(self.complex_gauge) and self.g_gauge2 != 0.0
+
+    @property
+    def snap_ncols(self) -> int:
+        """Columns of a snapshot: th2 and E2 follow when the second gauge is on."""
+        return self.ncols + (6 if self.gauge2 else 0)
 
     def steps_for(self, T: float) -> int:
         """Step count of a run of length T, as the reference rounds it."""
@@ -151,6 +177,14 @@ class Params:
         c.alpha_cs = self.alpha_cs
         c.beta_h = self.beta_h
         c.kappa_h = self.kappa_h
+        c.higgs_v = self.higgs_v
+        c.higgs_lam = self.higgs_lam
+        c.higgs_kap = self.higgs_kap
+        c.higgs_rvoid = self.higgs_rvoid
+        c.g_gauge2 = self.g_gauge2
+        c.gauge2_q[0] = self.gauge2_q0
+        c.gauge2_q[1] = self.gauge2_q1
+        c.gauge2_q[2] = self.gauge2_q2
         return c
 
     def to_cfg(self, **extra) -> str:
@@ -166,19 +200,23 @@ class Params:
             "mode": self.mode, "inv_alpha": repr(self.inv_alpha), "inv_beta": repr(self.inv_beta),
             "kappa_gamma": repr(self.kappa_gamma), "alpha_cs": repr(self.alpha_cs), "beta_h": repr(self.beta_h),
             "kappa_h": repr(self.kappa_h),
+            "higgs_v": repr(self.higgs_v), "higgs_lam": repr(self.higgs_lam), "higgs_kap": repr(self.higgs_kap),
+            "higgs_rvoid": repr(self.higgs_rvoid), "g_gauge2": repr(self.g_gauge2),
+            "gauge2_q0": repr(self.gauge2_q0), "gauge2_q1": repr(self.gauge2_q1), "gauge2_q2": repr(self.gauge2_q2),
         }
         kv.update(extra)
         return "".join(f"{k} = {v}\n" for k, v in kv.items())
 
 
 # Column names of the SFA snapshot schema in registration order
-# (sfa/sim/scp_sim.c:2862-2897).
+# (sfa/sim/scp_sim.c:2862-2902; th2/E2 only with the second gauge).
 COLUMN_NAMES = (
     "phi_x", "phi_y", "phi_z", "theta_x", "theta_y", "theta_z",
     "phi_vx", "phi_vy", "phi_vz", "theta_vx", "theta_vy", "theta_vz",
     "phiim_x", "phiim_y", "phiim_z", "thetaim_x", "thetaim_y", "thetaim_z",
     "phiim_vx", "phiim_vy", "phiim_vz", "thetaim_vx", "thetaim_vy", "thetaim_vz",
     "th_x", "th_y", "th_z", "E_x", "E_y", "E_z",
+    "th2_x", "th2_y", "th2_z", "E2_x", "E2_y", "E2_z",
 )
 
 # Diagnostic slot names: the reference diag TSV columns after "t"

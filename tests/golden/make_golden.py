@@ -8,6 +8,7 @@ grids) or a fixed sample of its sites (64^3), and its diag TSV rows.
 """
 from __future__ import annotations
 
+import json
 import os
 import sys
 
@@ -41,6 +42,20 @@ def small_case(name: str, N: int, gauged: bool, nsteps: int, diag_every: int, **
     print(name, "written", r["wall_ms_per_step"], "ms/step")
 
 
+def gext_case(name: str, N: int, nsteps: int, diag_every: int, **over):
+    """Gauged run with the Higgs condensate and / or the second gauge: the
+    36-column final frame (th2 and E2 appended) and the diag rows."""
+    st = seeds.small_state(N, True, **over)
+    p = st.params
+    r = oracle.run_reference(p, st.cols(), nsteps, diag_every=diag_every, threads=os.cpu_count())
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        N=N, nsteps=nsteps, diag_every=diag_every, over=json.dumps(over),
+        final=np.stack(r["cols"]), diag=r["diag"], diag_header=np.array(r["diag_header"]),
+        names=np.array(r["names"]))
+    print(name, "written", r["wall_ms_per_step"], "ms/step")
+
+
 def workload_case(name: str, wl: str, nsteps: int, diag_every: int):
     st = seeds.make_state(wl)
     p = st.params
@@ -61,3 +76,7 @@ if __name__ == "__main__":
     small_case("ref_gauged_n10_damped", 10, True, 40, 10, bc_type=0, damp_width=2.0, damp_rate=0.05)
     small_case("ref_complex_n13_damped", 13, False, 40, 10, bc_type=0, damp_width=2.0, damp_rate=0.05)
     workload_case("ref_c0_64_1000", "c0", 1000, 10)
+    gext_case("ref_higgs_gauge2_n12", 12, 60, 10, seed=41, higgs_v=1.0, higgs_rvoid=2.0, g_gauge2=0.2)
+    gext_case("ref_higgs_gauge2_n11_damped", 11, 40, 10, seed=43, higgs_v=0.8, higgs_lam=0.5, higgs_kap=1.5,
+              g_gauge2=-0.15, gauge2_q0=1.0, gauge2_q1=-1.0, gauge2_q2=0.5,
+              bc_type=0, damp_width=2.0, damp_rate=0.05)

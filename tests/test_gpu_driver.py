@@ -22,12 +22,14 @@ def _run(binary, cfg, cwd, extra=()):
     return r.stdout
 
 
-@pytest.mark.parametrize("gauged", [False, True, "g0", "sync", "real", "real_terms"])
+@pytest.mark.parametrize("gauged", [False, True, "g0", "sync", "real", "real_terms", "gext", "gext_sync"])
 def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
     """gauged="g0": complex_gauge=1 with g_gauge=0, the reference's ungauged
     dispatch with the link columns carried; "sync": gauged with the
     synchronous snapshot path (gpu_async_snap = 0) instead of the pipelined one;
-    "real": the real 6-field mode (complex_phi = 0); "real_terms": with optional terms."""
+    "real": the real 6-field mode (complex_phi = 0); "real_terms": with optional terms;
+    "gext": gauged with the Higgs condensate and the second gauge (36 SFA columns),
+    "gext_sync" the same through the synchronous snapshot path."""
     assert os.path.exists(DRIVER), "host driver not built (make -C scp_b200/host)"
     if gauged == "g0":
         st = seeds.small_state(16, True, seed=13, g_gauge=0.0)
@@ -35,6 +37,8 @@ def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
         st = seeds.real_state(16, seed=13)
     elif gauged == "real_terms":
         st = seeds.real_state(16, seed=13, mode=3, alpha_cs=0.2, kappa_h=0.1)
+    elif gauged in ("gext", "gext_sync"):
+        st = seeds.small_state(16, True, seed=13, higgs_v=1.0, higgs_rvoid=2.0, g_gauge2=0.2)
     else:
         st = seeds.small_state(16, bool(gauged), seed=13)
     p = st.params
@@ -49,18 +53,19 @@ def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
         cfg.write_text(p.to_cfg(init="sfa", init_sfa=seed, init_frame=0, T=repr(nsteps * p.dt), precision="f64",
                                 output=str(d / "out.sfa"), diag_file=str(d / "diag.tsv"),
                                 snap_dt=repr(nsteps // 2 * p.dt), diag_dt=repr(10 * p.dt)))
-        extra = ("-gpu_async_snap", "0") if (name == "b200" and gauged == "sync") else ()
+        extra = ("-gpu_async_snap", "0") if (name == "b200" and gauged in ("sync", "gext_sync")) else ()
         _run(binary, str(cfg), str(d), extra)
         hdr, rows = oracle.read_diag(str(d / "diag.tsv"))
         frames = [oracle.read_frame(str(d / "out.sfa"), f, p.N ** 3) for f in (0, 1, 2)]
         outs[name] = (hdr, rows, frames)
     (hr, rr, fr), (hb, rb, fb) = outs["ref"], outs["b200"]
+    tol = 1e-10 if str(gauged).startswith("gext") else 1e-11
     assert hr == hb and rr.shape == rb.shape
     for f in range(3):
         assert fr[f][0] == fb[f][0]                                   # column names and order
         for a, b in zip(fr[f][1], fb[f][1]):
             nb = np.linalg.norm(a)
-            assert np.linalg.norm(a - b) <= 1e-11 * max(nb, 1e-30) + 1e-300
+            assert np.linalg.norm(a - b) <= tol * max(nb, 1e-30) + 1e-300
     for ci, h in enumerate(hr):
         ref, got = rr[:, ci], rb[:, ci]
         scale = np.maximum(np.abs(ref), 1e-9)

@@ -48,3 +48,33 @@ def test_ball_is_phase_rotating():
     assert np.allclose(st["phiim_vy"], 0.8 * st["phi_y"])
     c = st.params.N // 2
     assert math.isclose(math.atan2(st["phiim_y"][c, c, c], st["phi_y"][c, c, c]), 2 * math.pi / 3, rel_tol=1e-12)
+
+
+def test_gauged_extension_params():
+    """Higgs / second-gauge keys: reference defaults, config text, snapshot width."""
+    p = seeds.params_for("c1")
+    assert (p.higgs_v, p.higgs_lam, p.higgs_kap, p.higgs_rvoid) == (0.0, 1.0, 2.0, 0.0)
+    assert (p.g_gauge2, p.gauge2_q0, p.gauge2_q1, p.gauge2_q2) == (0.0, 1.0, 1.0, -2.0)
+    assert p.snap_ncols == 30
+    q = seeds.params_for("c1", g_gauge2=0.1, higgs_v=1.0)
+    assert q.ncols == 30 and q.snap_ncols == 36
+    assert "g_gauge2 = 0.1\n" in q.to_cfg() and "higgs_v = 1.0\n" in q.to_cfg()
+    c = q.to_c()
+    assert c.g_gauge2 == 0.1 and list(c.gauge2_q) == [1.0, 1.0, -2.0]
+    assert seeds.params_for("c0", g_gauge2=0.1).snap_ncols == 24   # ignored without complex_gauge
+
+
+def test_gauged_extension_fixtures():
+    """The Higgs / second-gauge fixtures hold the reference's 36-column frame."""
+    import json
+    import os
+    from scp_b200.params import COLUMN_NAMES
+    gold = os.path.join(os.path.dirname(__file__), "golden")
+    for name in ("ref_higgs_gauge2_n12", "ref_higgs_gauge2_n11_damped"):
+        f = np.load(os.path.join(gold, name + ".npz"))
+        over = json.loads(str(f["over"]))
+        assert over["g_gauge2"] != 0 and over["higgs_v"] > 0
+        assert list(f["names"]) == list(COLUMN_NAMES)
+        assert f["final"].shape == (36, int(f["N"]) ** 3) and np.all(np.isfinite(f["final"]))
+        assert np.abs(f["final"][30:33]).max() > 0          # th2 moved off its zero start
+        assert len(f["diag"]) == int(f["nsteps"]) // int(f["diag_every"]) + 1
