@@ -25,6 +25,11 @@
  *   30-32 th2_x..z  33-35 E2_x..z     (snapshots only, when g_gauge2 != 0:
  *                                      the second gauge starts at zero, as the
  *                                      reference's SFA seed loader leaves it)
+ * Three fabrics (n_fabrics = 3): the 30 columns above are fabric C with the
+ * shared links; init takes 48 more, fabric Q (30-53) then fabric L (54-77),
+ * each in the 24-column complex order 0-23; snapshots carry C and then L
+ * (30-53: lphi_*, lth_*, lphi_v*, lth_v*, lphiim_*, lthim_*, lphiim_v*,
+ * lthim_v*), the reference's schema (scp_sim.c:2907-2932).
  * Each column is N^3 values, site index (i*N + j)*N + k, k fastest.
  *
  * Threading: one handle is driven by one host thread at a time.  Every handle
@@ -41,7 +46,7 @@ extern "C" {
 #endif
 
 #define SCP_GPU_ABI_VERSION 5
-#define SCP_GPU_MAX_COLS 36
+#define SCP_GPU_MAX_COLS 78
 
 /* status codes */
 #define SCP_OK              0
@@ -108,6 +113,15 @@ typedef struct {
     double  higgs_v, higgs_lam, higgs_kap, higgs_rvoid;
     double  g_gauge2;
     double  gauge2_q[3];
+    /* Three matter fabrics C, Q, L under the shared links (n_fabrics = 3; needs
+     * complex_gauge = 1 and g_gauge != 0, not with the Higgs or the second gauge;
+     * FP64).  Each fabric has its own bag and couples to the links with charge
+     * q_fab[f] (q_C, q_Q, q_L); the Gauss law uses sum_f q_f rho_f.  mf_lock_CQ = 1
+     * keeps Q equal to C at every step (the Q columns passed to init are then
+     * ignored); 0 evolves Q on its own (scp_config.h:135-149). */
+    int32_t n_fabrics;
+    int32_t mf_lock_CQ;
+    double  q_fab[3];
 } scp_gpu_params;
 
 /* Diagnostic slots: the reference diag TSV columns after "t"
@@ -121,6 +135,9 @@ enum {
     SCP_DIAG_THP2V, SCP_DIAG_GAUSS_MAX, SCP_DIAG_GAUSS_L2, SCP_DIAG_E_EM, SCP_DIAG_Q_FLUX,
     SCP_DIAG_Q_P0, SCP_DIAG_Q_P1, SCP_DIAG_Q_P2,
     SCP_DIAG_CENTROID_X, SCP_DIAG_CENTROID_Y, SCP_DIAG_CENTROID_Z,
+    /* three fabrics only (compute_mf_charges, scp_sim.c:2247-2261): integrated
+     * Noether charge of C, Q, L and the EM charge sum_f q_f Q_f */
+    SCP_DIAG_Q_C, SCP_DIAG_Q_Q, SCP_DIAG_Q_L, SCP_DIAG_Q_EM,
     SCP_DIAG_NSLOTS = 40
 };
 typedef struct { double v[SCP_DIAG_NSLOTS]; } scp_gpu_diag_out;
@@ -140,7 +157,8 @@ typedef struct {
 
 typedef struct scp_gpu scp_gpu;
 
-/* Allocate device state, upload the host columns (12 real, 24 complex or 30 gauged),
+/* Allocate device state, upload the host columns (12 real, 24 complex, 30 gauged,
+ * 78 with three fabrics),
  * and run the start-up sequence of the reference main (scp_sim.cu:5151-5245):
  * net-charge check (gauged, periodic), Gauss projection, first force. */
 int  scp_gpu_init(const scp_gpu_params *p, const double *const *host_cols, scp_gpu **out);

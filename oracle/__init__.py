@@ -193,12 +193,23 @@ def run_reference(params, cols: Sequence[np.ndarray], nsteps: int, diag_every: i
         raise RuntimeError("reference binary not built (oracle/_ref)")
     tmp = tempfile.mkdtemp(prefix="scpref_", dir=workdir)
     seed = os.path.join(tmp, "seed.sfa")
-    write_seed(seed, params, cols)
+    fabric_seeds = {}
+    if getattr(params, "n_fabrics", 1) == 3:
+        # fabric C with the links, then the L (and, unlocked, Q) seeds the
+        # reference loads by init_sfa_L / init_sfa_Q (24-column complex files)
+        write_seed(seed, params, cols[:30])
+        fabric_seeds["init_sfa_L"] = os.path.join(tmp, "seed_L.sfa")
+        write_seed(fabric_seeds["init_sfa_L"], params, cols[54:78])
+        if not params.mf_lock_CQ:
+            fabric_seeds["init_sfa_Q"] = os.path.join(tmp, "seed_Q.sfa")
+            write_seed(fabric_seeds["init_sfa_Q"], params, cols[30:54])
+    else:
+        write_seed(seed, params, cols)
     T = nsteps * params.dt
     de = diag_every if diag_every else nsteps
     kv = dict(init="sfa", init_sfa=seed, init_frame=0, T=repr(T), precision="f64",
               output=os.path.join(tmp, "out.sfa"), diag_file=os.path.join(tmp, "diag.tsv"),
-              snap_dt=repr(T if read_final else 1e9 * params.dt), diag_dt=repr(de * params.dt))
+              snap_dt=repr(T if read_final else 1e9 * params.dt), diag_dt=repr(de * params.dt), **fabric_seeds)
     if extra_cfg:
         kv.update(extra_cfg)
     cfg = os.path.join(tmp, "run.cfg")

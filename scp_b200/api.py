@@ -12,7 +12,7 @@ from typing import Sequence
 import numpy as np
 
 from . import native
-from .params import COLUMN_NAMES, DIAG_NAMES, Params
+from .params import DIAG_NAMES, Params
 
 DTYPE_F16, DTYPE_F32, DTYPE_F64 = 0, 1, 2
 _NP_DTYPE = {DTYPE_F16: np.uint16, DTYPE_F32: np.float32, DTYPE_F64: np.float64}
@@ -94,7 +94,7 @@ class Simulation:
         native.check(native.lib().scp_gpu_snapshot_wait(self._h), "scp_gpu_snapshot_wait")
 
     def snapshot_dict(self, dtype: int = DTYPE_F64) -> dict:
-        return dict(zip(COLUMN_NAMES, self.snapshot(dtype)))
+        return dict(zip(self.params.snap_names, self.snapshot(dtype)))
 
     def info(self) -> native.Info:
         inf = native.Info()

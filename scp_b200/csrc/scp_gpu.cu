@@ -24,6 +24,7 @@
 #include "launch.cuh"
 #include "real.cuh"
 #include "gext.cuh"
+#include "mf.cuh"
 
 #include <math.h>
 #include <stdio.h>
@@ -107,6 +108,11 @@ struct scp_gpu {
     double *gbuf = nullptr;
     GextState gs{};
     GextConsts gc{};
+    // three fabrics C, Q, L: separate per-site FP64 kernels (mf.cuh)
+    int mfab = 0;
+    double *mbuf = nullptr;
+    MfState ms{};
+    MfConsts mc{};
     int device;
     cudaStream_t stream = nullptr;
     // FP64 state
@@ -164,6 +170,13 @@ static int validate(const scp_gpu_params *p) {
         if (p->g_gauge == 0) return SCP_EUNSUPPORTED;   // the ungauged dispatch never evolves them
         if (p->precision_mode != SCP_PREC_FP64) return SCP_EUNSUPPORTED;
         if (!isfinite(p->g_gauge2) || !isfinite(p->higgs_v)) return SCP_EINVAL;
+    }
+    if (p->n_fabrics != 0 && p->n_fabrics != 1 && p->n_fabrics != 3) return SCP_EINVAL;
+    if (p->n_fabrics == 3) {   // cfg_validate's rules (scp_config.h:518-534)
+        if (!p->complex_gauge || p->real_fields) return SCP_EINVAL;
+        if (p->higgs_v > 0 || p->g_gauge2 != 0) return SCP_EUNSUPPORTED;
+        if (p->g_gauge == 0) return SCP_EUNSUPPORTED;   // the ungauged dispatch leaves Q and L unforced
+        if (p->precision_mode != SCP_PREC_FP64) return SCP_EUNSUPPORTED;
     }
     return SCP_OK;
 }
@@ -730,15 +743,182 @@ static int gext_higgs_energy(scp_gpu *h, double *e) {
     return SCP_OK;
 }
 
-// columns of a snapshot: th2 and E2 follow the 30 gauged ones with the second gauge
+// ---------------------------------------------------------------- three fabrics
+
+static DiagConsts diag_consts(const scp_gpu *h);
+template <class View>
+static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out);
+
+static void mf_forces(scp_gpu *h) {
+    const int nb = red_blocks(h->N3);
+    mf_plaq_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+    mf_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+}
+
+// verlet_step's multi-fabric branch (scp_sim.c:1583-1716)
+static int mf_step(scp_gpu *h) {
+    const int nb = red_blocks(h->N3);
+    mf_kick_kernel<false><<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+    mf_drift_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+    mf_forces(h);
+    mf_kick_kernel<true><<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+    CK(cudaGetLastError());
+    return SCP_OK;
+}
+
+// the start-up of main with three fabrics (scp_sim.c:2818-2836): fabrics in
+// place, net-charge check and Gauss projection with rho_em, first forces
+static int mf_gauss_startup(scp_gpu *h) {
+    const long long n3 = h->N3;
+    const int nb = red_blocks(n3);
+    int rc;
+    if (h->p.bc_type == 2) {
+        mf_net_charge_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc, h->part);
+        fold_partials_kernel<2, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+        CK(cudaGetLastError());
+        if ((rc = fold_to_host(h, 2))) return rc;
+        const double qn = fold_get(h, 0), qa = fold_get(h, 1);
+        if (fabs(qn) > 1e-6 * fmax(qa, 1.0)) return SCP_ENETCHARGE;
+    }
+    if (!h->p.gauss_project) return SCP_OK;
+    double *tmp = nullptr;
+    CK(cudaMallocAsync(&tmp, sizeof(double) * 5 * n3, h->stream));
+    double *b = tmp, *x = tmp + n3, *r = tmp + 2 * n3, *p = tmp + 3 * n3, *Ap = tmp + 4 * n3;
+    mf_gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc, b, h->part);
+    if ((rc = cg_solve(h, nb, b, x, r, p, Ap, &h->cg_iters))) {
+        cudaFreeAsync(tmp, h->stream);
+        return rc;
+    }
+    gauss_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(gauss_args(h, h->ms.XC, h->ms.SC), x, h->cg);
+    mf_gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc, nullptr, h->part);
+    fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    CK(cudaGetLastError());
+    CK(cudaFreeAsync(tmp, h->stream));
+    if ((rc = fold_to_host(h, 1))) return rc;
+    h->G_offset = fold_get(h, 0) / (double)n3;
+    h->mc.G_offset = h->G_offset;
+    return SCP_OK;
+}
+
+static int init_mf(scp_gpu *h, const double *const *cols, bool on_device) {
+    int rc;
+    if ((rc = alloc_common(h))) return rc;
+    const long long n3 = h->N3;
+    const scp_gpu_params &p = h->p;
+    const int lock = p.mf_lock_CQ ? 1 : 0;
+    // C: X S A (15 each); L: X S A (12 each); Q: X S A (12 each) unless locked; PS (3)
+    const size_t narr = 45 + 36 + (lock ? 0 : 36) + 3;
+    CK(cudaMallocAsync(&h->mbuf, sizeof(double) * narr * (size_t)n3, h->stream));
+    CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
+    h->dev_bytes += sizeof(double) * (narr + 1) * (size_t)n3;
+    CK(cudaMemsetAsync(h->mbuf, 0, sizeof(double) * narr * (size_t)n3, h->stream));
+    MfState &m = h->ms;
+    double *b = h->mbuf;
+    m.XC = b; b += 15 * n3;
+    m.SC = b; b += 15 * n3;
+    m.AC = b; b += 15 * n3;
+    m.XL = b; b += 12 * n3;
+    m.SL = b; b += 12 * n3;
+    m.AL = b; b += 12 * n3;
+    if (lock) {
+        m.XQ = m.XC; m.SQ = m.SC; m.AQ = m.AC;
+    } else {
+        m.XQ = b; b += 12 * n3;
+        m.SQ = b; b += 12 * n3;
+        m.AQ = b; b += 12 * n3;
+    }
+    m.PS = b;
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int c = 0; c < 78; c++) {
+        const int base = c < 30 ? 0 : (c < 54 ? 30 : 54);
+        if (base == 30 && lock) continue;   // Q is C
+        int field, mom;
+        sfa_col_source(c - base, &field, &mom);
+        double *X = base == 0 ? m.XC : (base == 30 ? m.XQ : m.XL);
+        double *S = base == 0 ? m.SC : (base == 30 ? m.SQ : m.SL);
+        CK(cudaMemcpyAsync((mom ? S : X) + (size_t)field * n3, cols[c], sizeof(double) * n3, kind, h->stream));
+    }
+    MfConsts &k = h->mc;
+    k.N = p.N; k.N3 = n3; k.L = p.L; k.dx = p.dx; k.dV = p.dx * p.dx * p.dx;
+    k.idx1 = 1.0 / (2.0 * p.dx); k.idx2 = 1.0 / (p.dx * p.dx); k.inva = 1.0 / p.dx;
+    k.hdt = 0.5 * p.dt; k.dt = p.dt;
+    k.mu = p.mu; k.kappa = p.kappa; k.m2 = p.m2; k.mtheta2 = p.mtheta2; k.eta = p.eta;
+    k.g = p.g_gauge;
+    k.stp = 1.0 / (p.g_gauge * p.dx * p.dx * p.dx);
+    k.gad = -p.g_gauge * p.dx * p.dt;
+    for (int f = 0; f < 3; f++) k.q[f] = p.q_fab[f];
+    k.lock = lock;
+    k.damp = damping_on(h) ? 1 : 0;
+    k.damp_width = p.damp_width; k.damp_rate = p.damp_rate;
+    const double Rint = (p.bc_type == 0) ? (p.L - p.damp_width - p.dx) : 1e300;
+    k.Rint2 = Rint * Rint;
+    k.G_offset = 0.0;
+    if ((rc = mf_gauss_startup(h))) return rc;
+    mf_forces(h);
+    CK(cudaGetLastError());
+    // the generic diagnostics, snapshot and info code reads these
+    h->X[0] = h->X[1] = m.XC;
+    h->S = m.SC;
+    h->cur = 0;
+    h->shape = 1;
+    return SCP_OK;
+}
+
+// fabric C's diagnostics, plus fabric L's energies (compute_energy_complex_gauge,
+// scp_sim.c:1977-2028), the Gauss norm with rho_em and the fabric charges
+static int mf_diag(scp_gpu *h, scp_gpu_diag_out *out) {
+    ViewF64 V{h->ms.XC, h->ms.SC, h->N3};
+    int rc = diag_with(h, V, out);
+    if (rc && rc != SCP_ENONFINITE) return rc;
+    const int nb = red_blocks(h->N3);
+    const DiagConsts c = diag_consts(h);
+    ViewFab VL{h->ms.XL, h->ms.SL, h->ms.XC, h->ms.SC, h->N3};
+    diag_pass1_kernel<ViewFab><<<nb, kRedThreads, 0, h->stream>>>(VL, c, h->part);
+    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    CK(cudaGetLastError());
+    if ((rc = fold_to_host(h, DS_EC + 1))) return rc;
+    double *o = out->v;
+    for (int q = 0; q <= DS_EC; q++) o[SCP_DIAG_E_PHI_KIN + q] += h->h_small[q];   // DS_EPK..DS_EC = slots 0..7
+    o[SCP_DIAG_E_TOTAL] = o[SCP_DIAG_E_PHI_KIN] + o[SCP_DIAG_E_THETA_KIN] + o[SCP_DIAG_E_GRAD] + o[SCP_DIAG_E_MASS] +
+                          o[SCP_DIAG_E_POT] + o[SCP_DIAG_E_TGRAD] + o[SCP_DIAG_E_TMASS] + o[SCP_DIAG_E_COUPLING] +
+                          o[SCP_DIAG_E_EM];
+    mf_diag_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc, h->part);
+    fold_partials_kernel<MS_NSUM, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    CK(cudaGetLastError());
+    if ((rc = fold_to_host(h, MS_NSUM + 1))) return rc;
+    const double *f = h->h_small, dV = c.dV;
+    o[SCP_DIAG_GAUSS_MAX] = f[MS_NSUM];
+    o[SCP_DIAG_GAUSS_L2] = f[MS_NOM] > 0 ? sqrt(f[MS_GL2] / f[MS_NOM]) : 0.0;
+    o[SCP_DIAG_Q_C] = f[MS_QC] * dV;
+    o[SCP_DIAG_Q_Q] = f[MS_QQ] * dV;
+    o[SCP_DIAG_Q_L] = f[MS_QL] * dV;
+    o[SCP_DIAG_Q_EM] = f[MS_QEM] * dV;
+    return isfinite(o[SCP_DIAG_E_TOTAL]) ? SCP_OK : SCP_ENONFINITE;
+}
+
+// columns of a snapshot: th2 and E2 follow the 30 gauged ones with the second
+// gauge; fabric L's 24 with three fabrics
 static int snap_ncols(const scp_gpu *h) {
+    if (h->mfab) return 54;
     return h->links ? (h->g2 ? 36 : 30) : (h->real ? 12 : 24);
 }
 
-// source slot of host column c: the packed complex layout, or the 6-field one
-static void col_source(const scp_gpu *h, int c, int *field, int *mom) {
-    if (h->rp) { *field = c % 6; *mom = c >= 6; return; }
-    if (c >= 30) { *field = (c - 30) % 3; *mom = c >= 33; return; }   // th2 / E2
+// source of host column c: the packed arrays it lives in (positions, momenta)
+// and its slot there
+static void col_source(const scp_gpu *h, int c, const double **X, const double **S, int *field, int *mom) {
+    *X = h->X[h->cur ^ 1];
+    *S = h->S;
+    if (h->rp) { *field = c % 6; *mom = c >= 6; return; }   // the 6-field layout
+    if (c >= 30 && h->g2) {                                 // th2 / E2
+        *X = h->gs.T2; *S = h->gs.E2;
+        *field = (c - 30) % 3; *mom = c >= 33;
+        return;
+    }
+    if (c >= 30 && h->mfab) {                               // fabric L
+        *X = h->ms.XL; *S = h->ms.SL;
+        sfa_col_source(c - 30, field, mom);
+        return;
+    }
     sfa_col_source(c, field, mom);
 }
 
@@ -748,9 +928,9 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
     int rc = validate(p);
     if (rc) return rc;
     if (!cols) return SCP_EINVAL;
-    const int ncols = p->complex_gauge ? 30 : (p->real_fields ? 12 : 24);
+    const int ncols = p->n_fabrics == 3 ? 78 : (p->complex_gauge ? 30 : (p->real_fields ? 12 : 24));
     for (int c = 0; c < ncols; c++)
-        if (!cols[c]) return SCP_EINVAL;
+        if (!cols[c] && !(c >= 30 && c < 54 && p->n_fabrics == 3 && p->mf_lock_CQ)) return SCP_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p->device || p->device < 0) return SCP_ENODEV;
     CK(cudaSetDevice(p->device));
@@ -769,7 +949,11 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
     fill_consts(h);
     h->rp = real_optional(p) ? 1 : 0;
     h->gx = gext_on(p) ? 1 : 0;
-    rc = h->rp ? init_real(h, cols, on_device) : (h->gx ? init_gext(h, cols, on_device) : init_body(h, cols, on_device));
+    h->mfab = p->n_fabrics == 3 ? 1 : 0;
+    if (h->rp) rc = init_real(h, cols, on_device);
+    else if (h->gx) rc = init_gext(h, cols, on_device);
+    else if (h->mfab) rc = init_mf(h, cols, on_device);
+    else rc = init_body(h, cols, on_device);
     if (rc == SCP_OK) {
         cudaError_t e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
@@ -800,9 +984,9 @@ int scp_gpu_step(scp_gpu *h, int nsteps) {
     if (nsteps == 0) return SCP_OK;
     CK(cudaSetDevice(h->device));
     int rc;
-    if (h->rp || h->gx) {
+    if (h->rp || h->gx || h->mfab) {
         for (int n = 0; n < nsteps; n++)
-            if ((rc = h->rp ? real_step(h) : gext_step(h))) return rc;
+            if ((rc = h->rp ? real_step(h) : (h->gx ? gext_step(h) : mf_step(h)))) return rc;
         h->steps += nsteps;
         return SCP_OK;
     }
@@ -877,8 +1061,7 @@ static void diag_assemble(const double *f1, const double *f2, const double *pt, 
     }
 }
 
-template <class View>
-static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
+static DiagConsts diag_consts(const scp_gpu *h) {
     const scp_gpu_params &p = h->p;
     DiagConsts c;
     c.N = h->N; c.N3 = h->N3; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx; c.idx1 = 1.0 / (2.0 * p.dx);
@@ -893,6 +1076,13 @@ static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
     const double Rint = (p.bc_type == 0) ? (p.L - p.damp_width - p.dx) : 1e300;
     c.Rint2 = Rint * Rint;
     c.G_offset = h->G_offset;
+    return c;
+}
+
+template <class View>
+static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
+    const scp_gpu_params &p = h->p;
+    const DiagConsts c = diag_consts(h);
     const int nb = red_blocks(h->N3);
     diag_pass1_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->part);
     fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
@@ -915,6 +1105,7 @@ int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     if (!h || !out) return SCP_EINVAL;
     CK(cudaSetDevice(h->device));
     if (h->rp) return real_diag(h, out);
+    if (h->mfab) return mf_diag(h, out);
     if (h->gx) {
         ViewF64 V{h->gs.X, h->gs.S, h->N3};
         int rc = diag_with(h, V, out);
@@ -955,23 +1146,19 @@ static int snapshot_with(scp_gpu *h, const View &V, int dtype, void *const *host
     const size_t es = dtype == SCP_DTYPE_F64 ? 8 : (dtype == SCP_DTYPE_F32 ? 4 : 2);
     for (int c = 0; c < ncols; c++) {
         if (!host_cols[c]) return SCP_EINVAL;
+        const double *Xs, *Ss;
         int field, mom;
-        col_source(h, c, &field, &mom);
-        if (c >= 30) {   // second gauge: th2 / E2 (FP64 state)
-            const double *src = (mom ? h->gs.E2 : h->gs.T2) + (size_t)field * n3;
-            if (dtype == SCP_DTYPE_F64) {
-                CK(cudaMemcpyAsync(host_cols[c], src, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
-            } else {
-                ViewF64 V2{h->gs.T2, h->gs.E2, n3};
-                snap_col_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V2, field, mom, n3, dtype, h->stage);
-                CK(cudaGetLastError());
-                CK(cudaMemcpyAsync(host_cols[c], h->stage, es * n3, cudaMemcpyDeviceToHost, h->stream));
-            }
-        } else if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {   // straight copy of the FP64 column
-            const double *src = (mom ? h->S : h->X[h->cur ^ 1]) + (size_t)field * n3;
+        col_source(h, c, &Xs, &Ss, &field, &mom);
+        if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {   // straight copy of the FP64 column
+            const double *src = (mom ? Ss : Xs) + (size_t)field * n3;
             CK(cudaMemcpyAsync(host_cols[c], src, sizeof(double) * n3, cudaMemcpyDeviceToHost, h->stream));
         } else {
-            snap_col_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, field, mom, n3, dtype, h->stage);
+            if (h->prec == SCP_PREC_FP64) {
+                ViewF64 V2{Xs, Ss, n3};
+                snap_col_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V2, field, mom, n3, dtype, h->stage);
+            } else {
+                snap_col_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, field, mom, n3, dtype, h->stage);
+            }
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(host_cols[c], h->stage, es * n3, cudaMemcpyDeviceToHost, h->stream));
         }
@@ -1026,19 +1213,15 @@ static int snapshot_async_with(scp_gpu *h, const View &V, int dtype, void *const
     char *stage = (char *)h->snap_dev;
     const int nb = red_blocks(n3);
     for (int c = 0; c < ncols; c++) {
+        const double *Xs, *Ss;
         int field, mom;
-        col_source(h, c, &field, &mom);
-        if (c >= 30) {   // second gauge: th2 / E2 (FP64 state)
-            const double *src = (mom ? h->gs.E2 : h->gs.T2) + (size_t)field * n3;
-            if (dtype == SCP_DTYPE_F64) {
-                CK(cudaMemcpyAsync(stage + c * col, src, col, cudaMemcpyDeviceToDevice, h->stream));
-            } else {
-                ViewF64 V2{h->gs.T2, h->gs.E2, n3};
-                snap_col_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V2, field, mom, n3, dtype, stage + c * col);
-            }
-        } else if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {
-            const double *src = (mom ? h->S : h->X[h->cur ^ 1]) + (size_t)field * n3;
+        col_source(h, c, &Xs, &Ss, &field, &mom);
+        if (h->prec == SCP_PREC_FP64 && dtype == SCP_DTYPE_F64) {
+            const double *src = (mom ? Ss : Xs) + (size_t)field * n3;
             CK(cudaMemcpyAsync(stage + c * col, src, col, cudaMemcpyDeviceToDevice, h->stream));
+        } else if (h->prec == SCP_PREC_FP64) {
+            ViewF64 V2{Xs, Ss, n3};
+            snap_col_kernel<ViewF64><<<nb, kRedThreads, 0, h->stream>>>(V2, field, mom, n3, dtype, stage + c * col);
         } else {
             snap_col_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, field, mom, n3, dtype, stage + c * col);
         }
@@ -1107,6 +1290,8 @@ int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
                                      : 4.0 * nfs + 12.0 * 2.0 + (h->gauged ? 3.0 * 4.0 : 0.0) + 4.0 * nfs;
     // extensions: positions and momenta (30), th2 / E2 (6), H / Hdot (2), FP64
     if (h->gx) info->state_bytes_per_site = 8.0 * (30.0 + 6.0 * h->g2 + 2.0 * h->higgs);
+    // three fabrics: C with the links (30), L (24), Q (24) unless it is C
+    if (h->mfab) info->state_bytes_per_site = 8.0 * (30.0 + 24.0 + (h->mc.lock ? 0.0 : 24.0));
     info->step_bytes_per_site = 2.0 * info->state_bytes_per_site;
     info->tile_x = kShapes[h->shape].tx;
     info->tile_y = kShapes[h->shape].ty;
@@ -1138,7 +1323,7 @@ void scp_gpu_free(scp_gpu *h) {
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->stream) {
         void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->count, h->stage,
-                        h->snap_dev, h->rbuf, h->gbuf};
+                        h->snap_dev, h->rbuf, h->gbuf, h->mbuf};
         for (void *b : bufs)
             if (b) cudaFreeAsync(b, h->stream);
         cudaStreamSynchronize(h->stream);
@@ -1276,6 +1461,7 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     if (!dev_cols || !out) return SCP_EINVAL;
     if (pp->real_fields) return SCP_EUNSUPPORTED;   // takes the complex column set
     if (gext_on(pp)) return SCP_EUNSUPPORTED;        // no Higgs energy term
+    if (pp->n_fabrics == 3) return SCP_EUNSUPPORTED;  // one fabric
     if (pp->N > SCP_DIAG_STATIC_MAX_N) {
         snprintf(g_cuda_err, sizeof g_cuda_err, "scp_gpu_diag_noalloc: N=%d exceeds SCP_DIAG_STATIC_MAX_N=%d",
                  pp->N, SCP_DIAG_STATIC_MAX_N);

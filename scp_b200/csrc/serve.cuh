@@ -510,6 +510,7 @@ static int srv_submit(scp_srv *s, const scp_gpu_params *p, const double *const *
     if (p->device != s->cfg.device) return SCP_EINVAL;
     if (p->real_fields) return SCP_EUNSUPPORTED;   // the server takes complex and gauged requests
     if (p->complex_gauge && (p->higgs_v > 0 || p->g_gauge2 != 0)) return SCP_EUNSUPPORTED;   // fused kernels only
+    if (p->n_fabrics == 3) return SCP_EUNSUPPORTED;
     auto q = std::make_unique<SrvReq>();
     q->p = *p;
     q->nsteps = nsteps;

@@ -18,9 +18,9 @@
  *   gpu_async_snap = 1 | 0          (default 1: snapshots copied and written
  *                                     while the GPU keeps stepping)
  * It covers the complex (complex_phi=1), gauged (complex_gauge=1, with the
- * Higgs condensate and the second gauge) and real 6-field (complex_phi=0,
- * with its optional terms) stepper with bc_type 0 or 2; other modes are
- * refused with a message.
+ * Higgs condensate, the second gauge or three matter fabrics) and real
+ * 6-field (complex_phi=0, with its optional terms) stepper with bc_type 0 or
+ * 2; other modes are refused with a message.
  *
  * Build: make -C scp_b200/host REF=<kardianos/scp checkout>
  */
@@ -54,7 +54,8 @@ static double wall_now(void) {
     return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
-/* Host arrays in SFA column order (24 or 30 columns of N^3 doubles). */
+/* Host arrays in SFA column order (24 or 30 columns of N^3 doubles; 78 with
+ * three fabrics: C, Q, L). */
 static Grid *grid_new(const Config *c, double **cols, int ncols) {
     Grid *g = calloc(1, sizeof(Grid));
     if (!g) return NULL;
@@ -71,15 +72,23 @@ static Grid *grid_new(const Config *c, double **cols, int ncols) {
         g->phi_vel[a] = cols[6 + a];  g->theta_vel[a] = cols[9 + a];
         g->phi_im[a] = cols[12 + a];  g->theta_im[a] = cols[15 + a];
         g->phi_im_vel[a] = cols[18 + a]; g->theta_im_vel[a] = cols[21 + a];
-        g->th[a] = ncols == 30 ? cols[24 + a] : NULL;
-        g->Efield[a] = ncols == 30 ? cols[27 + a] : NULL;
+        g->th[a] = ncols >= 30 ? cols[24 + a] : NULL;
+        g->Efield[a] = ncols >= 30 ? cols[27 + a] : NULL;
     }
     return g;
 }
 
-/* Column schema of the complex / gauged snapshot (sfa/sim/scp_sim.c:2862-2907;
- * th2 / E2 with the second gauge). */
-static void add_columns(SFA *sfa, uint8_t dt, int n) {
+/* Fabric L's snapshot columns (scp_sim.c:2907-2932): names, and semantic /
+ * component as fabric C's complex columns 0-23. */
+static const char *l_names[24] = {
+    "lphi_x", "lphi_y", "lphi_z", "lth_x", "lth_y", "lth_z",
+    "lphi_vx", "lphi_vy", "lphi_vz", "lth_vx", "lth_vy", "lth_vz",
+    "lphiim_x", "lphiim_y", "lphiim_z", "lthim_x", "lthim_y", "lthim_z",
+    "lphiim_vx", "lphiim_vy", "lphiim_vz", "lthim_vx", "lthim_vy", "lthim_vz"};
+
+/* Column schema of the complex / gauged snapshot (sfa/sim/scp_sim.c:2862-2932;
+ * th2 / E2 with the second gauge; fabric L after C with three fabrics). */
+static void add_columns(SFA *sfa, uint8_t dt, int n, int fabrics) {
     static const char *names[36] = {
         "phi_x", "phi_y", "phi_z", "theta_x", "theta_y", "theta_z",
         "phi_vx", "phi_vy", "phi_vz", "theta_vx", "theta_vy", "theta_vz",
@@ -96,7 +105,64 @@ static void add_columns(SFA *sfa, uint8_t dt, int n) {
         SFA_ANGLE, SFA_ANGLE, SFA_ANGLE, SFA_VELOCITY, SFA_VELOCITY, SFA_VELOCITY};
     static const uint8_t comp[36] = {0, 1, 2, 0, 1, 2, 0, 1, 2, 3, 4, 5, 3, 4, 5, 3, 4, 5,
                                      6, 7, 8, 9, 10, 11, 6, 7, 8, 12, 13, 14, 9, 10, 11, 15, 16, 17};
+    if (fabrics == 3) {
+        for (int k = 0; k < 30; k++) sfa_add_column(sfa, names[k], dt, sem[k], comp[k]);
+        for (int k = 0; k < 24; k++) sfa_add_column(sfa, l_names[k], dt, sem[k], comp[k]);
+        return;
+    }
     for (int k = 0; k < n; k++) sfa_add_column(sfa, names[k], dt, sem[k], comp[k]);
+}
+
+/* One fabric from an SFA frame into 24 complex columns, each source column
+ * placed by its semantic and component as load_sfa_into_fabric does
+ * (scp_sim.c:426-479; gauge columns are not loaded). */
+static int load_fabric(const char *path, int frame, int N, double **cols24) {
+    SFA *sfa = sfa_open(path);
+    if (!sfa) { fprintf(stderr, "FATAL: cannot open SFA '%s'\n", path); return 1; }
+    if ((int)sfa->Nx != N || (int)sfa->Ny != N || (int)sfa->Nz != N) {
+        fprintf(stderr, "FATAL: SFA grid %ux%ux%u != sim %d^3\n", sfa->Nx, sfa->Ny, sfa->Nz, N);
+        sfa_close(sfa);
+        return 1;
+    }
+    if (frame < 0) frame = (int)sfa->total_frames + frame;
+    if (frame < 0 || frame >= (int)sfa->total_frames) {
+        fprintf(stderr, "FATAL: frame %d out of range [0,%u)\n", frame, sfa->total_frames);
+        sfa_close(sfa);
+        return 1;
+    }
+    uint8_t *buf = malloc(sfa->frame_bytes);
+    if (!buf) { sfa_close(sfa); return 1; }
+    sfa_read_frame(sfa, frame, buf);
+    const long n3 = (long)N * N * N;
+    uint64_t off = 0;
+    int nload = 0;
+    for (uint32_t col = 0; col < sfa->n_columns; col++) {
+        const int dtype = sfa->columns[col].dtype, sem = sfa->columns[col].semantic;
+        const int comp = sfa->columns[col].component;
+        const uint8_t *src = buf + off;
+        int slot = -1;   /* index into the complex 24-column order */
+        if (sem == SFA_POSITION && comp < 3) slot = comp;
+        else if (sem == SFA_ANGLE && comp < 3) slot = 3 + comp;
+        else if (sem == SFA_VELOCITY && comp < 3) slot = 6 + comp;
+        else if (sem == SFA_VELOCITY && comp < 6) slot = 9 + comp - 3;
+        else if (sem == SFA_POSITION && comp < 6) slot = 12 + comp - 3;
+        else if (sem == SFA_ANGLE && comp < 6) slot = 15 + comp - 3;
+        else if (sem == SFA_VELOCITY && comp < 9) slot = 18 + comp - 6;
+        else if (sem == SFA_VELOCITY && comp < 12) slot = 21 + comp - 9;
+        if (slot >= 0) {
+            double *dst = cols24[slot];
+            for (long i = 0; i < n3; i++)
+                dst[i] = dtype == SFA_F64 ? ((const double *)src)[i]
+                       : dtype == SFA_F32 ? (double)((const float *)src)[i]
+                                          : f16_to_f64(((const uint16_t *)src)[i]);
+            nload++;
+        }
+        off += (uint64_t)n3 * sfa_dtype_size[dtype];
+    }
+    printf("  Loaded %d columns into fabric from %s\n", nload, path);
+    free(buf);
+    sfa_close(sfa);
+    return 0;
 }
 
 /* Snapshot pipeline: two host buffer sets (page-locked when available).
@@ -111,7 +177,7 @@ typedef struct {
     SFA *sfa;
     int ncols, dtype, async;
     size_t col_bytes;
-    void *cols[2][36];
+    void *cols[2][54];
     int pinned[2];
     double t[2];
     int busy[2];          /* set queued to or being written by the writer */
@@ -215,7 +281,7 @@ static int snap_close(Snap *s) {
 
 /* One diag TSV row in the reference's column set and formats
  * (sfa/sim/scp_sim.c:2993-3003, :3045-3066). */
-static void diag_row(FILE *fp, double t, const scp_gpu_diag_out *d, int gauged, int complex) {
+static void diag_row(FILE *fp, double t, const scp_gpu_diag_out *d, int gauged, int complex, int mf) {
     const double *v = d->v;
     fprintf(fp, "%.2f\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e\t%.6e", t,
             v[SCP_DIAG_E_PHI_KIN], v[SCP_DIAG_E_THETA_KIN], v[SCP_DIAG_E_GRAD], v[SCP_DIAG_E_MASS],
@@ -232,6 +298,9 @@ static void diag_row(FILE *fp, double t, const scp_gpu_diag_out *d, int gauged, 
     if (gauged)
         fprintf(fp, "\t%.6e\t%.6e\t%.12e\t%.12e", v[SCP_DIAG_GAUSS_MAX], v[SCP_DIAG_GAUSS_L2], v[SCP_DIAG_E_EM],
                 v[SCP_DIAG_Q_FLUX]);
+    if (mf)
+        fprintf(fp, "\t%.12e\t%.12e\t%.12e\t%.12e", v[SCP_DIAG_Q_C], v[SCP_DIAG_Q_Q], v[SCP_DIAG_Q_L],
+                v[SCP_DIAG_Q_EM]);
     fprintf(fp, "\t%.12e\t%.12e\t%.12e\n", v[SCP_DIAG_Q_P0], v[SCP_DIAG_Q_P1], v[SCP_DIAG_Q_P2]);
 }
 
@@ -286,8 +355,13 @@ int main(int argc, char **argv) {
         return 1;
     }
     if (c.bc_type == 1) { fprintf(stderr, "ERROR: bc_type=1 is not supported by scp_sim_b200\n"); return 1; }
-    if (c.n_fabrics != 1 || c.n_locks > 0 || c.test_gauge_xform) {
-        fprintf(stderr, "ERROR: multi-fabric, locks and test_gauge_xform are not supported\n");
+    if (c.n_locks > 0 || c.test_gauge_xform) {
+        fprintf(stderr, "ERROR: locks and test_gauge_xform are not supported\n");
+        return 1;
+    }
+    const int mf = c.n_fabrics == 3;
+    if (mf && c.g_gauge == 0.0) {
+        fprintf(stderr, "ERROR: n_fabrics=3 needs g_gauge != 0\n");
         return 1;
     }
     /* Higgs and second gauge: ignored without complex_gauge, as the reference does
@@ -301,13 +375,27 @@ int main(int argc, char **argv) {
     if (c.bc_type == 2) { c.damp_width = 0.0; c.damp_rate = 0.0; }   /* as the CUDA reference (scp_sim.cu:5170-5172) */
     const int gauged = c.complex_gauge && c.g_gauge != 0.0;
     const int ncols = c.complex_gauge ? 30 : (c.complex_phi ? 24 : 12);
-    const int snap_cols = ncols + ((c.complex_gauge && c.g_gauge2 != 0) ? 6 : 0);   /* + th2, E2 */
-    double *cols[30] = {0};
-    Grid *g = grid_new(&c, cols, ncols);
+    const int snap_cols = mf ? 54 : ncols + ((c.complex_gauge && c.g_gauge2 != 0) ? 6 : 0);   /* + L or th2, E2 */
+    double *cols[78] = {0};
+    Grid *g = grid_new(&c, cols, mf ? 78 : ncols);   /* three fabrics: C, then Q and L (24 each) */
     if (!g) { fprintf(stderr, "FATAL: host allocation\n"); return 1; }
     printf("dx=%.4f dt=%.6f device=%d precision=%s\n\n", g->dx, g->dt, gpu_dev,
            gpu_prec == SCP_PREC_FP32C ? "fp32c" : "fp64");
     do_init(g, &c);
+    if (mf) {   /* mf_post_init (scp_sim.c:485-509): L seed, then Q by lock / seed / copy / zero */
+        if (c.init_sfa_L[0]) {
+            if (load_fabric(c.init_sfa_L, c.init_frame, c.N, cols + 54)) return 1;
+        } else {
+            printf("WARNING: n_fabrics=3 but init_sfa_L empty — L fabric is zero\n");
+        }
+        if (c.mf_lock_CQ) {
+            printf("Multi-fab: Q ← C lock (Q is C on the device)\n");
+        } else if (c.init_sfa_Q[0]) {
+            if (load_fabric(c.init_sfa_Q, c.init_frame, c.N, cols + 30)) return 1;
+        } else if (c.mf_seed_Q) {
+            for (int k = 0; k < 24; k++) memcpy(cols[30 + k], cols[k], sizeof(double) * g->N3);
+        }
+    }
 
     scp_gpu_params p;
     memset(&p, 0, sizeof p);
@@ -324,6 +412,8 @@ int main(int argc, char **argv) {
     p.higgs_v = c.higgs_v; p.higgs_lam = c.higgs_lam; p.higgs_kap = c.higgs_kap; p.higgs_rvoid = c.higgs_rvoid;
     p.g_gauge2 = c.g_gauge2;
     p.gauge2_q[0] = c.gauge2_q0; p.gauge2_q[1] = c.gauge2_q1; p.gauge2_q[2] = c.gauge2_q2;
+    p.n_fabrics = c.n_fabrics; p.mf_lock_CQ = c.mf_lock_CQ;
+    p.q_fab[0] = c.q_C; p.q_fab[1] = c.q_Q; p.q_fab[2] = c.q_L;
     scp_gpu *h = NULL;
     int rc = scp_gpu_init(&p, (const double *const *)cols, &h);
     if (rc) return fail("scp_gpu_init", rc);
@@ -340,7 +430,7 @@ int main(int argc, char **argv) {
     if (!sfa) { fprintf(stderr, "ERROR: cannot create output file '%s'\n", c.output); return 1; }
     sfa->flags = SFA_CODEC_COLZSTD | SFA_FLAG_STREAMING;
     sfa_embed_kvmd(sfa, &c);
-    add_columns(sfa, sdt, snap_cols);
+    add_columns(sfa, sdt, snap_cols, c.n_fabrics);
     sfa_finalize_header(sfa);
     static Snap snap;
     if (snap_open(&snap, h, sfa, snap_cols, c.precision, g->N3, gpu_async_snap)) {
@@ -356,6 +446,7 @@ int main(int argc, char **argv) {
     if (c.complex_phi)
         fprintf(fp, "\tQ_phi\tQ_theta\tQ_total\ts_max\tr_core\tomega_core\tQ_core\tthp1u\tthp1v\tthp2u\tthp2v");
     if (c.complex_gauge) fprintf(fp, "\tgauss_max\tgauss_l2\tE_em\tQ_flux");
+    if (mf) fprintf(fp, "\tQ_C\tQ_Q\tQ_L\tQ_em");
     if (c.complex_phi) fprintf(fp, "\tQ_p0\tQ_p1\tQ_p2");
     fprintf(fp, "\n");
 
@@ -367,7 +458,7 @@ int main(int argc, char **argv) {
     const double E0 = d.v[SCP_DIAG_E_TOTAL];
     printf("INIT: E_total=%.4e E_pot=%.4f phi_max=%.4f P_int=%.4e theta_rms=%.3e\n\n", E0, d.v[SCP_DIAG_E_POT],
            d.v[SCP_DIAG_PHI_MAX], d.v[SCP_DIAG_P_INT], d.v[SCP_DIAG_THETA_RMS]);
-    diag_row(fp, 0.0, &d, c.complex_gauge, c.complex_phi);
+    diag_row(fp, 0.0, &d, c.complex_gauge, c.complex_phi, mf);
 
     int major = diag_every * 25;
     if (major > n_steps / 10) { major = (n_steps / 10 / diag_every) * diag_every; if (major < diag_every) major = diag_every; }
@@ -386,7 +477,7 @@ int main(int argc, char **argv) {
         if (step % snap_every == 0 && (rc = snap_start(&snap, t))) return fail("snapshot", rc);
         if (step % diag_every == 0) {
             if ((rc = scp_gpu_diag(h, &d))) return fail("diag", rc);
-            diag_row(fp, t, &d, c.complex_gauge, c.complex_phi);
+            diag_row(fp, t, &d, c.complex_gauge, c.complex_phi, mf);
             fflush(fp);
             if (step % major == 0) {
                 const double wall = wall_now() - wall0;

@@ -55,6 +55,9 @@ class CParams(ctypes.Structure):
         ("higgs_rvoid", ctypes.c_double),
         ("g_gauge2", ctypes.c_double),
         ("gauge2_q", ctypes.c_double * 3),
+        ("n_fabrics", ctypes.c_int32),
+        ("mf_lock_CQ", ctypes.c_int32),
+        ("q_fab", ctypes.c_double * 3),
     ]
 
 
@@ -105,6 +108,12 @@ class Params:
     gauge2_q0: float = 1.0
     gauge2_q1: float = 1.0
     gauge2_q2: float = -2.0
+    # three matter fabrics C, Q, L under the shared links (scp_config.h defaults)
+    n_fabrics: int = 1
+    mf_lock_CQ: int = 1
+    q_C: float = 0.0
+    q_Q: float = 1.0
+    q_L: float = -1.0
 
     @property
     def dx(self) -> float:
@@ -128,10 +137,25 @@ class Params:
 
     @property
     def ncols(self) -> int:
-        """Columns of an initial state (the second gauge starts at zero)."""
+        """Columns of an initial state (the second gauge starts at zero; three
+        fabrics add Q and L, 24 each)."""
         if self.real_fields:
             return 12
+        if self.n_fabrics == 3:
+            return 78
         return 30 if self.complex_gauge else 24
+
+    @property
+    def input_names(self) -> tuple:
+        if self.n_fabrics == 3:
+            return COLUMN_NAMES[:30] + Q_COLUMN_NAMES + L_COLUMN_NAMES
+        return COLUMN_NAMES[: self.ncols]
+
+    @property
+    def snap_names(self) -> tuple:
+        if self.n_fabrics == 3:
+            return COLUMN_NAMES[:30] + L_COLUMN_NAMES
+        return COLUMN_NAMES[: self.snap_ncols]
 
     @property
     def gauge2(self) -> bool:
@@ -139,7 +163,10 @@ class Params:
 
     @property
     def snap_ncols(self) -> int:
-        """Columns of a snapshot: th2 and E2 follow when the second gauge is on."""
+        """Columns of a snapshot: th2 and E2 follow when the second gauge is on;
+        fabric L follows C with three fabrics."""
+        if self.n_fabrics == 3:
+            return 54
         return self.ncols + (6 if self.gauge2 else 0)
 
     def steps_for(self, T: float) -> int:
@@ -185,6 +212,11 @@ class Params:
         c.gauge2_q[0] = self.gauge2_q0
         c.gauge2_q[1] = self.gauge2_q1
         c.gauge2_q[2] = self.gauge2_q2
+        c.n_fabrics = self.n_fabrics
+        c.mf_lock_CQ = self.mf_lock_CQ
+        c.q_fab[0] = self.q_C
+        c.q_fab[1] = self.q_Q
+        c.q_fab[2] = self.q_L
         return c
 
     def to_cfg(self, **extra) -> str:
@@ -203,6 +235,8 @@ class Params:
             "higgs_v": repr(self.higgs_v), "higgs_lam": repr(self.higgs_lam), "higgs_kap": repr(self.higgs_kap),
             "higgs_rvoid": repr(self.higgs_rvoid), "g_gauge2": repr(self.g_gauge2),
             "gauge2_q0": repr(self.gauge2_q0), "gauge2_q1": repr(self.gauge2_q1), "gauge2_q2": repr(self.gauge2_q2),
+            "n_fabrics": self.n_fabrics, "mf_lock_CQ": self.mf_lock_CQ,
+            "q_C": repr(self.q_C), "q_Q": repr(self.q_Q), "q_L": repr(self.q_L),
         }
         kv.update(extra)
         return "".join(f"{k} = {v}\n" for k, v in kv.items())
@@ -219,6 +253,16 @@ COLUMN_NAMES = (
     "th2_x", "th2_y", "th2_z", "E2_x", "E2_y", "E2_z",
 )
 
+# Fabric L's snapshot columns (scp_sim.c:2907-2932), in the complex order
+L_COLUMN_NAMES = (
+    "lphi_x", "lphi_y", "lphi_z", "lth_x", "lth_y", "lth_z",
+    "lphi_vx", "lphi_vy", "lphi_vz", "lth_vx", "lth_vy", "lth_vz",
+    "lphiim_x", "lphiim_y", "lphiim_z", "lthim_x", "lthim_y", "lthim_z",
+    "lphiim_vx", "lphiim_vy", "lphiim_vz", "lthim_vx", "lthim_vy", "lthim_vz",
+)
+# Fabric Q's initial columns (init only; the reference writes no Q columns)
+Q_COLUMN_NAMES = tuple("q" + n[1:] for n in L_COLUMN_NAMES)
+
 # Diagnostic slot names: the reference diag TSV columns after "t"
 # (scp_sim.c:2993-3003), then centroid extras.
 DIAG_NAMES = (
@@ -227,4 +271,5 @@ DIAG_NAMES = (
     "Q_phi", "Q_theta", "Q_total", "s_max", "r_core", "omega_core", "Q_core",
     "thp1u", "thp1v", "thp2u", "thp2v", "gauss_max", "gauss_l2", "E_em", "Q_flux",
     "Q_p0", "Q_p1", "Q_p2", "centroid_x", "centroid_y", "centroid_z",
+    "Q_C", "Q_Q", "Q_L", "Q_em",
 )

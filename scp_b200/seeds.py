@@ -87,13 +87,11 @@ class State(dict):
         super().__init__()
         self.params = params
         n = params.N
-        from .params import COLUMN_NAMES
-        for name in COLUMN_NAMES[: params.ncols]:
+        for name in params.input_names:
             self[name] = np.zeros((n, n, n))
 
     def cols(self) -> list[np.ndarray]:
-        from .params import COLUMN_NAMES
-        return [np.ascontiguousarray(self[n]) for n in COLUMN_NAMES[: self.params.ncols]]
+        return [np.ascontiguousarray(self[n]) for n in self.params.input_names]
 
 
 def coords(p: Params) -> np.ndarray:
@@ -242,4 +240,31 @@ def small_state(N: int, gauged: bool, seed: int = 7, L: float | None = None, **o
     if gauged:
         add_noise(st, ("th_x", "th_y", "th_z"), 0.05, seed=seed + 200)
     neutralise(st)
+    return st
+
+
+def mf_state(N: int, seed: int = 7, L: float | None = None, shift: float = 0.0, l_charge: float = 0.0,
+             **over) -> State:
+    """A three-fabric test state (n_fabrics = 3): fabric C and the links are
+    small_state(N, gauged) with `seed`; fabrics Q and L are two more complex
+    small states (seeds seed+1, seed+2; L's balls moved by `shift` along y).
+    Each fabric is net-neutral by itself, so every choice of charges is,
+    unless `l_charge` != 0 adds l_charge |Phi_L|^2 to L's charge density (for
+    runs with the sponge, which have no net-charge check)."""
+    over = dict(over, n_fabrics=3)
+    st = small_state(N, True, seed=seed, L=L, **over)
+    p = st.params
+    from .params import COLUMN_NAMES, L_COLUMN_NAMES, Q_COLUMN_NAMES
+    for names, sd in ((Q_COLUMN_NAMES, seed + 1), (L_COLUMN_NAMES, seed + 2)):
+        f = small_state(N, False, seed=sd, L=p.L)
+        if names is L_COLUMN_NAMES and shift:
+            for k in list(f):
+                f[k] = np.roll(f[k], int(round(shift / p.dx)), axis=1)
+        for dst, src in zip(names, COLUMN_NAMES[:24]):
+            st[dst] = f[src].copy()
+    if l_charge:
+        for ax in "xyz":
+            u, v = st["lphi_" + ax].copy(), st["lphiim_" + ax].copy()
+            st["lphi_v" + ax] -= l_charge * v
+            st["lphiim_v" + ax] += l_charge * u
     return st

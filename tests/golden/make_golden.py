@@ -56,6 +56,20 @@ def gext_case(name: str, N: int, nsteps: int, diag_every: int, **over):
     print(name, "written", r["wall_ms_per_step"], "ms/step")
 
 
+def mf_case(name: str, N: int, nsteps: int, diag_every: int, **kw):
+    """Three matter fabrics (n_fabrics = 3) from seeds.mf_state: the 54-column
+    final frame (C with the links, then L) and the diag rows."""
+    st = seeds.mf_state(N, **kw)
+    p = st.params
+    r = oracle.run_reference(p, st.cols(), nsteps, diag_every=diag_every, threads=os.cpu_count())
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        N=N, nsteps=nsteps, diag_every=diag_every, kw=json.dumps(kw),
+        final=np.stack(r["cols"]), diag=r["diag"], diag_header=np.array(r["diag_header"]),
+        names=np.array(r["names"]))
+    print(name, "written", r["wall_ms_per_step"], "ms/step")
+
+
 def workload_case(name: str, wl: str, nsteps: int, diag_every: int):
     st = seeds.make_state(wl)
     p = st.params
@@ -80,3 +94,6 @@ if __name__ == "__main__":
     gext_case("ref_higgs_gauge2_n11_damped", 11, 40, 10, seed=43, higgs_v=0.8, higgs_lam=0.5, higgs_kap=1.5,
               g_gauge2=-0.15, gauge2_q0=1.0, gauge2_q1=-1.0, gauge2_q2=0.5,
               bc_type=0, damp_width=2.0, damp_rate=0.05)
+    mf_case("ref_mf_lock_n12", 12, 40, 10, seed=81, shift=1.5)
+    mf_case("ref_mf_free_n11_damped", 11, 40, 10, seed=83, shift=-1.0, l_charge=0.05, mf_lock_CQ=0,
+            q_C=0.5, q_Q=1.0, q_L=-1.5, bc_type=0, damp_width=2.0, damp_rate=0.05)

@@ -78,3 +78,33 @@ def test_gauged_extension_fixtures():
         assert f["final"].shape == (36, int(f["N"]) ** 3) and np.all(np.isfinite(f["final"]))
         assert np.abs(f["final"][30:33]).max() > 0          # th2 moved off its zero start
         assert len(f["diag"]) == int(f["nsteps"]) // int(f["diag_every"]) + 1
+
+
+def test_three_fabric_params_and_fixtures():
+    """n_fabrics = 3: 78 initial columns (C, Q, L), 54 snapshot columns (C, L),
+    config keys; the committed fixtures hold the reference's 54-column frames."""
+    import json
+    import os
+    st = seeds.mf_state(8, seed=3, mf_lock_CQ=0, q_L=-2.0)
+    p = st.params
+    assert p.ncols == 78 and p.snap_ncols == 54 and len(st.cols()) == 78
+    assert p.input_names[30] == "qphi_x" and p.input_names[54] == "lphi_x" and p.snap_names[30] == "lphi_x"
+    cfg = p.to_cfg()
+    assert "n_fabrics = 3\n" in cfg and "mf_lock_CQ = 0\n" in cfg and "q_L = -2.0\n" in cfg
+    c = p.to_c()
+    assert c.n_fabrics == 3 and c.mf_lock_CQ == 0 and list(c.q_fab) == [0.0, 1.0, -2.0]
+    from scp_b200.params import COLUMN_NAMES, L_COLUMN_NAMES, Q_COLUMN_NAMES
+    for names in (COLUMN_NAMES[:24], Q_COLUMN_NAMES, L_COLUMN_NAMES):   # every fabric net-neutral
+        v = [st[n] for n in names]   # complex order: phi theta phi_v theta_v, then the imaginary parts
+        rho = sum(v[a] * v[18 + a] - v[12 + a] * v[6 + a] + v[3 + a] * v[21 + a] - v[15 + a] * v[9 + a]
+                  for a in range(3))
+        assert abs(rho.sum()) < 1e-12 * np.abs(rho).sum()
+    gold = os.path.join(os.path.dirname(__file__), "golden")
+    for name in ("ref_mf_lock_n12", "ref_mf_free_n11_damped"):
+        f = np.load(os.path.join(gold, name + ".npz"))
+        kw = json.loads(str(f["kw"]))
+        q = seeds.mf_state(int(f["N"]), **kw).params
+        assert list(f["names"]) == list(q.snap_names)
+        assert f["final"].shape == (54, int(f["N"]) ** 3) and np.all(np.isfinite(f["final"]))
+        assert np.abs(f["final"][30:54]).max() > 0               # fabric L evolved
+        assert list(f["diag_header"][-7:-3]) == ["Q_C", "Q_Q", "Q_L", "Q_em"]
