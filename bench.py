@@ -54,8 +54,21 @@ WORKLOADS = {
     "c1x": ("c1", 0, "gauged FP64 128^3 two balls + Higgs condensate (v=1, lambda=1, kappa_H=2, cavity r=4) "
                      "+ second U(1) gauge (g2=0.1, charges 1,1,-2): per-site FP64 kernels"),
 }
+WORKLOADS["c1m"] = ("c1", 0, "gauged FP64 128^3, three fabrics: C = the two balls, Q locked to C, L = C's "
+                            "matter moved 8 sites along y; charges 0, 1, -1: per-site FP64 kernels")
 # parameters a workload adds to its seed's
-WORKLOAD_OVER = {"c1x": dict(higgs_v=1.0, higgs_rvoid=4.0, g_gauge2=0.1)}
+WORKLOAD_OVER = {"c1x": dict(higgs_v=1.0, higgs_rvoid=4.0, g_gauge2=0.1), "c1m": dict(n_fabrics=3)}
+
+
+def workload_state(name: str, params):
+    """Initial state of a bench workload: its seed's, with fabric L filled for c1m."""
+    from scp_b200 import seeds
+    from scp_b200.params import COLUMN_NAMES, L_COLUMN_NAMES
+    st = seeds.make_state(WORKLOADS[name][0], params)
+    if name == "c1m":
+        for dst, src in zip(L_COLUMN_NAMES, COLUMN_NAMES[:24]):
+            st[dst] = np.roll(st[src], 8, axis=1)
+    return st
 METRIC = "site-updates/s"
 
 
@@ -195,7 +208,7 @@ def run_reference_arm(args, rank, world):
            "parallelism": "cpu-openmp"}
     if rank != 0:
         return None
-    st = seeds.make_state(seed, params)
+    st = workload_state(args.workload, params)
     cb = cpu_baseline(params, st.cols(), args.warmup + args.steps)
     val = cb["value"]
     line = {"metric": METRIC, "value": val, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -505,9 +518,10 @@ def main():
     over = dict(N=args.n, L=(args.n - 1) / 4.0) if args.n else {}
     params = seeds.params_for(seed, precision=prec, device=local, tile_variant=args.tile, **over,
                               **WORKLOAD_OVER.get(args.workload, {}))
-    # kernels per step: one fused launch, or the six per-site passes of the extensions
-    launches_per_step = 6 if (params.complex_gauge and (params.higgs_v > 0 or params.g_gauge2 != 0)) else 1
-    st = seeds.make_state(seed, params)
+    # kernels per step: one fused launch, or the four per-site sweeps of the extensions
+    ext = params.complex_gauge and (params.higgs_v > 0 or params.g_gauge2 != 0 or params.n_fabrics == 3)
+    launches_per_step = 4 if ext else 1
+    st = workload_state(args.workload, params)
     cols = st.cols()
     n3 = params.N ** 3
 

@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "gauss.cuh"
 #include "reduce.cuh"
+#include "trig.cuh"
 
 namespace scp {
 
@@ -51,35 +52,35 @@ __device__ __forceinline__ void gext_nb(long long idx, int N, long long np[3], l
     nm[2] = (long long)i * NN + (long long)j * N + wrapi(k - 1, N);
 }
 
-// pass A (:1072-1079): gauge-1 link cos/sin; pass B (:1090-1109): plaquette
-// sines of planes (0,1) (1,2) (2,0) for both gauges
-__global__ void __launch_bounds__(kRedThreads) gext_links_kernel(GextState s, GextConsts c) {
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < c.N3;
-         idx += (long long)gridDim.x * blockDim.x) {
-        for (int d = 0; d < 3; d++) {
-            const double t = s.X[(FTH + d) * c.N3 + idx];
-            s.LC[d * c.N3 + idx] = cos(t);
-            s.LS[d * c.N3 + idx] = sin(t);
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kRedThreads) gext_plaq_kernel(GextState s, GextConsts c) {
+// pass A (:1072-1079, gauge-1 link cos/sin) and pass B (:1090-1109,
+// plaquette sines of planes (0,1) (1,2) (2,0) for both gauges) in one sweep
+__global__ void __launch_bounds__(kRedThreads) gext_links_plaq_kernel(GextState s, GextConsts c) {
     const long long N3 = c.N3;
     const double *th = s.X + FTH * N3;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            double sn, cs;
+            sincos_any(th[d * N3 + idx], &sn, &cs);
+            s.LC[d * N3 + idx] = cs;
+            s.LS[d * N3 + idx] = sn;
+        }
         long long np[3], nm[3];
         gext_nb(idx, c.N, np, nm);
         const int pa[3] = {0, 1, 2}, pb[3] = {1, 2, 0};
+#pragma unroll
         for (int p = 0; p < 3; p++) {
             const int a = pa[p], b = pb[p];
+            double sn, cs;
             const double ang = th[a * N3 + idx] + th[b * N3 + np[a]] - th[a * N3 + np[b]] - th[b * N3 + idx];
-            s.PS[p * N3 + idx] = sin(ang);
+            sincos_any(ang, &sn, &cs);
+            s.PS[p * N3 + idx] = sn;
             if (c.g2on) {
                 const double *t2 = s.T2;
                 const double ang2 = t2[a * N3 + idx] + t2[b * N3 + np[a]] - t2[a * N3 + np[b]] - t2[b * N3 + idx];
-                s.PS2[p * N3 + idx] = sin(ang2);
+                sincos_any(ang2, &sn, &cs);
+                s.PS2[p * N3 + idx] = sn;
             }
         }
     }
@@ -95,19 +96,23 @@ __global__ void __launch_bounds__(kRedThreads) gext_force_kernel(GextState s, Ge
         long long np[3], nm[3];
         gext_nb(idx, c.N, np, nm);
         double fu[6], fv[6];
+        #pragma unroll
         for (int a = 0; a < 3; a++) {
             fu[a] = Q(FU + a, idx); fv[a] = Q(FV + a, idx);
             fu[3 + a] = Q(FTU + a, idx); fv[3 + a] = Q(FTV + a, idx);
         }
         double TRp[3][6], TIp[3][6], TRm[3][6], TIm[3][6];
         double tup[3][3], tvp[3][3];
+        #pragma unroll
         for (int d = 0; d < 3; d++) {
+            #pragma unroll
             for (int a = 0; a < 3; a++) {
                 double cP, sP, cM, sM;
                 if (c.g2on) {   // combined link th + q_a th2 for component a
                     const double php = Q(FTH + d, idx) + c.q[a] * s.T2[d * N3 + idx];
                     const double phm = Q(FTH + d, nm[d]) + c.q[a] * s.T2[d * N3 + nm[d]];
-                    cP = cos(php); sP = sin(php); cM = cos(phm); sM = sin(phm);
+                    sincos_any(php, &sP, &cP);
+                    sincos_any(phm, &sM, &cM);
                 } else {
                     cP = s.LC[d * N3 + idx]; sP = s.LS[d * N3 + idx];
                     cM = s.LC[d * N3 + nm[d]]; sM = s.LS[d * N3 + nm[d]];
@@ -132,12 +137,15 @@ __global__ void __launch_bounds__(kRedThreads) gext_force_kernel(GextState s, Ge
         const double prod_rest[3] = {s2_1 * s2_2, s2_0 * s2_2, s2_0 * s2_1};
         const double hh = c.higgs ? s.H[idx] * s.H[idx] : 0.0;
         double DcU[3][6], DcV[3][6];
+        #pragma unroll
         for (int d = 0; d < 3; d++)
+            #pragma unroll
             for (int f = 0; f < 6; f++) {
                 DcU[d][f] = (TRp[d][f] - TRm[d][f]) * c.idx1;
                 DcV[d][f] = (TIp[d][f] - TIm[d][f]) * c.idx1;
             }
         const int ci1[3] = {1, 2, 0}, ci2[3] = {2, 0, 1};
+        #pragma unroll
         for (int a = 0; a < 3; a++) {
             const int d1 = ci1[a], d2 = ci2[a];
             const double reDxT = DcU[d1][3 + ci2[a]] - DcU[d2][3 + ci1[a]];
@@ -175,9 +183,11 @@ __global__ void __launch_bounds__(kRedThreads) gext_force_kernel(GextState s, Ge
             st2[1] = -(P2[0 * N3 + idx] - P2[0 * N3 + nm[0]]) + (P2[1 * N3 + idx] - P2[1 * N3 + nm[2]]);
             st2[2] = (P2[2 * N3 + idx] - P2[2 * N3 + nm[0]]) - (P2[1 * N3 + idx] - P2[1 * N3 + nm[1]]);
         }
+        #pragma unroll
         for (int d = 0; d < 3; d++) {
             const double cP = s.LC[d * N3 + idx], sP = s.LS[d * N3 + idx];
             double Jg = 0.0;
+            #pragma unroll
             for (int a = 0; a < 3; a++) {
                 Jg += fu[a] * TIp[d][a] - fv[a] * TRp[d][a];
                 Jg += fu[3 + a] * TIp[d][3 + a] - fv[3 + a] * TRp[d][3 + a];
@@ -191,6 +201,7 @@ __global__ void __launch_bounds__(kRedThreads) gext_force_kernel(GextState s, Ge
             s.A[(FTH + d) * N3 + idx] = c.stp * st[d] + c.g * Jlat;
             if (c.g2on) {
                 double Jg2 = 0.0;
+                #pragma unroll
                 for (int a = 0; a < 3; a++) {
                     Jg2 += c.q[a] * (fu[a] * TIp[d][a] - fv[a] * TRp[d][a]);
                     Jg2 += c.q[a] * (fu[3 + a] * TIp[d][3 + a] - fv[3 + a] * TRp[d][3 + a]);
@@ -201,19 +212,20 @@ __global__ void __launch_bounds__(kRedThreads) gext_force_kernel(GextState s, Ge
     }
 }
 
-// stage 1 / stage 4 kicks: momenta, E, E2, Hdot += dt/2 * accelerations; with
-// SPONGE (stage 5, apply_damping :1440-1473) the matter momenta and E are
-// then damped (not E2, not Hdot)
-template <bool SPONGE>
-__global__ void gext_kick_kernel(GextState s, GextConsts c) {
+// stage 4 kick: momenta, E, E2, Hdot += dt/2 * accelerations; then stage 5
+// (apply_damping, :1440-1473): the matter momenta and E are damped in the
+// sponge (not E2, not Hdot)
+__global__ void __launch_bounds__(kRedThreads) gext_kick_damp_kernel(GextState s, GextConsts c) {
     const long long N3 = c.N3;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
         for (int f = 0; f < 15; f++) s.S[f * N3 + idx] += c.hdt * s.A[f * N3 + idx];
         if (c.g2on)
+#pragma unroll
             for (int d = 0; d < 3; d++) s.E2[d * N3 + idx] += c.hdt * s.K2[d * N3 + idx];
         if (c.higgs) s.HV[idx] += c.hdt * s.HA[idx];
-        if (SPONGE && c.damp) {
+        if (c.damp) {
             const long long NN = (long long)c.N * c.N;
             const int i = (int)(idx / NN), j = (int)((idx / c.N) % c.N), k = (int)(idx % c.N);
             const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
@@ -223,29 +235,48 @@ __global__ void gext_kick_kernel(GextState s, GextConsts c) {
                 double sc = (r - Rd) / c.damp_width;
                 if (sc > 1) sc = 1;
                 const double dmp = 1.0 - c.damp_rate * sc * sc;
+#pragma unroll
                 for (int f = 0; f < 15; f++) s.S[f * N3 + idx] *= dmp;
             }
         }
     }
 }
 
-// stage 2: drift of the matter, the wrapped links of both gauges, and H
-__global__ void gext_drift_kernel(GextState s, GextConsts c) {
+// stage 1 kick and stage 2 drift of the matter, the wrapped links of both
+// gauges, and H, in one sweep (each site's drift needs only its own kicked
+// momenta, kept in registers)
+__global__ void __launch_bounds__(kRedThreads) gext_kick_drift_kernel(GextState s, GextConsts c) {
     const long long N3 = c.N3;
     const double twopi = 2.0 * 3.14159265358979323846;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
-        for (int f = 0; f < 12; f++) s.X[f * N3 + idx] += c.dt * s.S[f * N3 + idx];
-        for (int d = 0; d < 3; d++) {
-            const double v = s.X[(FTH + d) * N3 + idx] + c.gad * s.S[(FTH + d) * N3 + idx];
-            s.X[(FTH + d) * N3 + idx] = v - twopi * rint(v / twopi);
+        double v[15];
+#pragma unroll
+        for (int f = 0; f < 15; f++) {
+            v[f] = s.S[f * N3 + idx] + c.hdt * s.A[f * N3 + idx];
+            s.S[f * N3 + idx] = v[f];
         }
-        if (c.g2on)
+#pragma unroll
+        for (int f = 0; f < 12; f++) s.X[f * N3 + idx] += c.dt * v[f];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double w = s.X[(FTH + d) * N3 + idx] + c.gad * v[FTH + d];
+            s.X[(FTH + d) * N3 + idx] = w - twopi * rint(w / twopi);
+        }
+        if (c.g2on) {
+#pragma unroll
             for (int d = 0; d < 3; d++) {
-                const double v = s.T2[d * N3 + idx] + c.gad2 * s.E2[d * N3 + idx];
-                s.T2[d * N3 + idx] = v - twopi * rint(v / twopi);
+                const double e2 = s.E2[d * N3 + idx] + c.hdt * s.K2[d * N3 + idx];
+                s.E2[d * N3 + idx] = e2;
+                const double w = s.T2[d * N3 + idx] + c.gad2 * e2;
+                s.T2[d * N3 + idx] = w - twopi * rint(w / twopi);
             }
-        if (c.higgs) s.H[idx] += c.dt * s.HV[idx];
+        }
+        if (c.higgs) {
+            const double hv = s.HV[idx] + c.hdt * s.HA[idx];
+            s.HV[idx] = hv;
+            s.H[idx] += c.dt * hv;
+        }
     }
 }
 

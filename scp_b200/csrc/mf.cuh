@@ -19,6 +19,7 @@
 #include "gauss.cuh"
 #include "reduce.cuh"
 #include "gext.cuh"
+#include "trig.cuh"
 
 namespace scp {
 
@@ -75,21 +76,25 @@ __device__ __forceinline__ double mf_gauss_at(const MfState &s, const MfConsts &
 // One fabric's matter accelerations (written to A when A is not null) and
 // its lattice current J_lat per direction, with charge-q links
 // (force_fabric_gauged_accum's site body, scp_sim.c:1292-1381).
-__device__ __noinline__ void mf_fabric_site(const double *Xf, double *A, const double *th, double q, long long idx,
+__device__ __forceinline__ void mf_fabric_site(const double *Xf, double *A, const double *th, double q, long long idx,
                                             const long long np[3], const long long nm[3], const MfConsts &c,
                                             double Jlat[3]) {
     const long long N3 = c.N3;
     double fu[6], fv[6];
+    #pragma unroll
     for (int a = 0; a < 3; a++) {
         fu[a] = Xf[(FU + a) * N3 + idx]; fv[a] = Xf[(FV + a) * N3 + idx];
         fu[3 + a] = Xf[(FTU + a) * N3 + idx]; fv[3 + a] = Xf[(FTV + a) * N3 + idx];
     }
     double TRp[3][6], TIp[3][6], TRm[3][6], TIm[3][6];
     double tup[3][3], tvp[3][3], cPd[3], sPd[3];
+    #pragma unroll
     for (int d = 0; d < 3; d++) {
-        const double cP = cos(q * th[d * N3 + idx]), sP = sin(q * th[d * N3 + idx]);
-        const double cM = cos(q * th[d * N3 + nm[d]]), sM = sin(q * th[d * N3 + nm[d]]);
+        double cP, sP, cM, sM;
+        sincos_any(q * th[d * N3 + idx], &sP, &cP);
+        sincos_any(q * th[d * N3 + nm[d]], &sM, &cM);
         cPd[d] = cP; sPd[d] = sP;
+        #pragma unroll
         for (int a = 0; a < 3; a++) {
             const double upn = Xf[(FU + a) * N3 + np[d]], vpn = Xf[(FV + a) * N3 + np[d]];
             const double umn = Xf[(FU + a) * N3 + nm[d]], vmn = Xf[(FV + a) * N3 + nm[d]];
@@ -112,11 +117,14 @@ __device__ __noinline__ void mf_fabric_site(const double *Xf, double *A, const d
         const double Vp = 0.5 * c.mu / (den * den);
         const double prod_rest[3] = {s2_1 * s2_2, s2_0 * s2_2, s2_0 * s2_1};
         double DcU[3][6], DcV[3][6];
+        #pragma unroll
         for (int d = 0; d < 3; d++)
+            #pragma unroll
             for (int f = 0; f < 6; f++) {
                 DcU[d][f] = (TRp[d][f] - TRm[d][f]) * c.idx1;
                 DcV[d][f] = (TIp[d][f] - TIm[d][f]) * c.idx1;
             }
+        #pragma unroll
         for (int a = 0; a < 3; a++) {
             const int d1 = ci1[a], d2 = ci2[a];
             const double reDxT = DcU[d1][3 + ci2[a]] - DcU[d2][3 + ci1[a]];
@@ -135,9 +143,11 @@ __device__ __noinline__ void mf_fabric_site(const double *Xf, double *A, const d
             A[(FTV + a) * N3 + idx] = lapV_T - c.mtheta2 * fv[3 + a] + c.eta * imDxP;
         }
     }
+    #pragma unroll
     for (int d = 0; d < 3; d++) {
         const double cP = cPd[d], sP = sPd[d];
         double Jg = 0.0;
+        #pragma unroll
         for (int a = 0; a < 3; a++) {
             Jg += fu[a] * TIp[d][a] - fv[a] * TRp[d][a];
             Jg += fu[3 + a] * TIp[d][3 + a] - fv[3 + a] * TRp[d][3 + a];
@@ -160,10 +170,13 @@ __global__ void __launch_bounds__(kRedThreads) mf_plaq_kernel(MfState s, MfConst
         long long np[3], nm[3];
         gext_nb(idx, c.N, np, nm);
         const int pa[3] = {0, 1, 2}, pb[3] = {1, 2, 0};
+        #pragma unroll
         for (int p = 0; p < 3; p++) {
             const int a = pa[p], b = pb[p];
             const double ang = th[a * N3 + idx] + th[b * N3 + np[a]] - th[a * N3 + np[b]] - th[b * N3 + idx];
-            s.PS[p * N3 + idx] = sin(ang);
+            double sn, cs;
+            sincos_any(ang, &sn, &cs);
+            s.PS[p * N3 + idx] = sn;
         }
     }
 }
@@ -196,18 +209,20 @@ __global__ void __launch_bounds__(kRedThreads) mf_force_kernel(MfState s, MfCons
     }
 }
 
-// stage 1 / 4 kicks of every fabric and E (Q skipped when locked); with
-// SPONGE the stage-5 damping of all matter momenta and E (:1440-1473)
-template <bool SPONGE>
-__global__ void __launch_bounds__(kRedThreads) mf_kick_kernel(MfState s, MfConsts c) {
+// stage 4 kick of every fabric and E (Q skipped when locked), then the
+// stage-5 damping of all matter momenta and E in the sponge (:1440-1473)
+__global__ void __launch_bounds__(kRedThreads) mf_kick_damp_kernel(MfState s, MfConsts c) {
     const long long N3 = c.N3;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
         for (int f = 0; f < 15; f++) s.SC[f * N3 + idx] += c.hdt * s.AC[f * N3 + idx];
         if (!c.lock)
+#pragma unroll
             for (int f = 0; f < 12; f++) s.SQ[f * N3 + idx] += c.hdt * s.AQ[f * N3 + idx];
+#pragma unroll
         for (int f = 0; f < 12; f++) s.SL[f * N3 + idx] += c.hdt * s.AL[f * N3 + idx];
-        if (SPONGE && c.damp) {
+        if (c.damp) {
             const long long NN = (long long)c.N * c.N;
             const int i = (int)(idx / NN), j = (int)((idx / c.N) % c.N), k = (int)(idx % c.N);
             const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
@@ -217,28 +232,45 @@ __global__ void __launch_bounds__(kRedThreads) mf_kick_kernel(MfState s, MfConst
                 double sc = (r - Rd) / c.damp_width;
                 if (sc > 1) sc = 1;
                 const double dmp = 1.0 - c.damp_rate * sc * sc;
+#pragma unroll
                 for (int f = 0; f < 15; f++) s.SC[f * N3 + idx] *= dmp;
                 if (!c.lock)
+#pragma unroll
                     for (int f = 0; f < 12; f++) s.SQ[f * N3 + idx] *= dmp;
+#pragma unroll
                 for (int f = 0; f < 12; f++) s.SL[f * N3 + idx] *= dmp;
             }
         }
     }
 }
 
-// stage 2: drift of every fabric (Q skipped when locked) and of the wrapped links
-__global__ void __launch_bounds__(kRedThreads) mf_drift_kernel(MfState s, MfConsts c) {
+// one fabric's stage 1 kick and stage 2 drift at one site
+__device__ __forceinline__ void mf_kick_drift_fabric(double *X, double *S, const double *A, long long N3, long long idx,
+                                                     double hdt, double dt) {
+#pragma unroll
+    for (int f = 0; f < 12; f++) {
+        const double v = S[f * N3 + idx] + hdt * A[f * N3 + idx];
+        S[f * N3 + idx] = v;
+        X[f * N3 + idx] += dt * v;
+    }
+}
+
+// stage 1 kick and stage 2 drift of every fabric (Q skipped when locked),
+// E and the wrapped links, in one sweep
+__global__ void __launch_bounds__(kRedThreads) mf_kick_drift_kernel(MfState s, MfConsts c) {
     const long long N3 = c.N3;
     const double twopi = 2.0 * 3.14159265358979323846;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
-        for (int f = 0; f < 12; f++) s.XC[f * N3 + idx] += c.dt * s.SC[f * N3 + idx];
-        if (!c.lock)
-            for (int f = 0; f < 12; f++) s.XQ[f * N3 + idx] += c.dt * s.SQ[f * N3 + idx];
-        for (int f = 0; f < 12; f++) s.XL[f * N3 + idx] += c.dt * s.SL[f * N3 + idx];
+        mf_kick_drift_fabric(s.XC, s.SC, s.AC, N3, idx, c.hdt, c.dt);
+        if (!c.lock) mf_kick_drift_fabric(s.XQ, s.SQ, s.AQ, N3, idx, c.hdt, c.dt);
+        mf_kick_drift_fabric(s.XL, s.SL, s.AL, N3, idx, c.hdt, c.dt);
+#pragma unroll
         for (int d = 0; d < 3; d++) {
-            const double v = s.XC[(FTH + d) * N3 + idx] + c.gad * s.SC[(FTH + d) * N3 + idx];
-            s.XC[(FTH + d) * N3 + idx] = v - twopi * rint(v / twopi);
+            const double e = s.SC[(FTH + d) * N3 + idx] + c.hdt * s.AC[(FTH + d) * N3 + idx];
+            s.SC[(FTH + d) * N3 + idx] = e;
+            const double w = s.XC[(FTH + d) * N3 + idx] + c.gad * e;
+            s.XC[(FTH + d) * N3 + idx] = w - twopi * rint(w / twopi);
         }
     }
 }

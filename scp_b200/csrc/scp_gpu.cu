@@ -644,18 +644,17 @@ static bool gext_on(const scp_gpu_params *p) {
 // pass A (links), pass B (plaquettes), pass C (forces and field kicks)
 static void gext_forces(scp_gpu *h) {
     const int nb = red_blocks(h->N3);
-    gext_links_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
-    gext_plaq_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+    gext_links_plaq_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
     gext_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
 }
 
-// one verlet_step (scp_sim.c:1583-1716): kick, drift, forces, kick, sponge
+// one verlet_step (scp_sim.c:1583-1716) in four sweeps: kick + drift, links
+// and plaquettes, forces, kick + sponge
 static int gext_step(scp_gpu *h) {
     const int nb = red_blocks(h->N3);
-    gext_kick_kernel<false><<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
-    gext_drift_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+    gext_kick_drift_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
     gext_forces(h);
-    gext_kick_kernel<true><<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+    gext_kick_damp_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
     CK(cudaGetLastError());
     return SCP_OK;
 }
@@ -755,13 +754,13 @@ static void mf_forces(scp_gpu *h) {
     mf_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
 }
 
-// verlet_step's multi-fabric branch (scp_sim.c:1583-1716)
+// verlet_step's multi-fabric branch (scp_sim.c:1583-1716) in four sweeps:
+// kick + drift, plaquettes, forces, kick + sponge
 static int mf_step(scp_gpu *h) {
     const int nb = red_blocks(h->N3);
-    mf_kick_kernel<false><<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
-    mf_drift_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+    mf_kick_drift_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
     mf_forces(h);
-    mf_kick_kernel<true><<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+    mf_kick_damp_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
     CK(cudaGetLastError());
     return SCP_OK;
 }

@@ -94,6 +94,17 @@ __device__ __forceinline__ void sincos_bounded(T x, T *sn, T *cs) {
     *cs = (q & 2) ? -c1 : c1;
 }
 
+// sin and cos of any x: the bounded routine below 2^19, CUDA's sin / cos
+// beyond (angles scaled by a user charge can be large)
+__device__ __forceinline__ void sincos_any(double x, double *sn, double *cs) {
+    if (fabs(x) < 0x1p19) {
+        sincos_bounded(x, sn, cs);
+    } else {
+        *sn = sin(x);
+        *cs = cos(x);
+    }
+}
+
 template <class T>
 __device__ __forceinline__ T sin_bounded(T x) {
     T s, c;
