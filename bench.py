@@ -518,9 +518,10 @@ def main():
     over = dict(N=args.n, L=(args.n - 1) / 4.0) if args.n else {}
     params = seeds.params_for(seed, precision=prec, device=local, tile_variant=args.tile, **over,
                               **WORKLOAD_OVER.get(args.workload, {}))
-    # kernels per step: one fused launch, or the four per-site sweeps of the extensions
+    # kernels per step: one fused launch, or the three per-site sweeps of the
+    # extensions (and their closing kick after the last step)
     ext = params.complex_gauge and (params.higgs_v > 0 or params.g_gauge2 != 0 or params.n_fabrics == 3)
-    launches_per_step = 4 if ext else 1
+    launches_per_step = 3 if ext else 1
     st = workload_state(args.workload, params)
     cols = st.cols()
     n3 = params.N ** 3
@@ -597,7 +598,7 @@ def main():
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "bytes_per_site": bytes_site,
                      "traffic": (lambda t: t * n3 if t else None)(profiled_traffic(args.workload))},
-        "gpu_launches": args.steps * launches_per_step,
+        "gpu_launches": args.steps * launches_per_step + (1 if ext else 0),
         "clocks": clocks,
         "e2e": e2e,
     }

@@ -212,6 +212,19 @@ __global__ void __launch_bounds__(kRedThreads) gext_force_kernel(GextState s, Ge
     }
 }
 
+// sponge factor of apply_damping at a site (1 outside the sponge)
+__device__ __forceinline__ double sponge_factor(int N, double L, double dx, double width, double rate, long long idx) {
+    const long long NN = (long long)N * N;
+    const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+    const double x = -L + i * dx, y = -L + j * dx, z = -L + k * dx;
+    const double r = sqrt(x * x + y * y + z * z);
+    const double Rd = L - width;
+    if (!(r > Rd)) return 1.0;
+    double sc = (r - Rd) / width;
+    if (sc > 1) sc = 1;
+    return 1.0 - rate * sc * sc;
+}
+
 // stage 4 kick: momenta, E, E2, Hdot += dt/2 * accelerations; then stage 5
 // (apply_damping, :1440-1473): the matter momenta and E are damped in the
 // sponge (not E2, not Hdot)
@@ -226,34 +239,36 @@ __global__ void __launch_bounds__(kRedThreads) gext_kick_damp_kernel(GextState s
             for (int d = 0; d < 3; d++) s.E2[d * N3 + idx] += c.hdt * s.K2[d * N3 + idx];
         if (c.higgs) s.HV[idx] += c.hdt * s.HA[idx];
         if (c.damp) {
-            const long long NN = (long long)c.N * c.N;
-            const int i = (int)(idx / NN), j = (int)((idx / c.N) % c.N), k = (int)(idx % c.N);
-            const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
-            const double r = sqrt(x * x + y * y + z * z);
-            const double Rd = c.L - c.damp_width;
-            if (r > Rd) {
-                double sc = (r - Rd) / c.damp_width;
-                if (sc > 1) sc = 1;
-                const double dmp = 1.0 - c.damp_rate * sc * sc;
+            const double dmp = sponge_factor(c.N, c.L, c.dx, c.damp_width, c.damp_rate, idx);
+            if (dmp != 1.0)
 #pragma unroll
                 for (int f = 0; f < 15; f++) s.S[f * N3 + idx] *= dmp;
-            }
         }
     }
 }
 
 // stage 1 kick and stage 2 drift of the matter, the wrapped links of both
 // gauges, and H, in one sweep (each site's drift needs only its own kicked
-// momenta, kept in registers)
+// momenta, kept in registers).  PREV: the previous step's stage 4 kick and
+// stage 5 sponge come first, with the same accelerations, in the same
+// operation order as two separate sweeps.
+template <bool PREV>
 __global__ void __launch_bounds__(kRedThreads) gext_kick_drift_kernel(GextState s, GextConsts c) {
     const long long N3 = c.N3;
     const double twopi = 2.0 * 3.14159265358979323846;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
         double v[15];
+        const double dmp = (PREV && c.damp) ? sponge_factor(c.N, c.L, c.dx, c.damp_width, c.damp_rate, idx) : 1.0;
 #pragma unroll
         for (int f = 0; f < 15; f++) {
-            v[f] = s.S[f * N3 + idx] + c.hdt * s.A[f * N3 + idx];
+            const double a = s.A[f * N3 + idx];
+            double w = s.S[f * N3 + idx];
+            if (PREV) {
+                w = w + c.hdt * a;
+                if (dmp != 1.0) w *= dmp;
+            }
+            v[f] = w + c.hdt * a;
             s.S[f * N3 + idx] = v[f];
         }
 #pragma unroll
@@ -266,14 +281,20 @@ __global__ void __launch_bounds__(kRedThreads) gext_kick_drift_kernel(GextState 
         if (c.g2on) {
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-                const double e2 = s.E2[d * N3 + idx] + c.hdt * s.K2[d * N3 + idx];
+                const double k2 = s.K2[d * N3 + idx];
+                double e2 = s.E2[d * N3 + idx];
+                if (PREV) e2 = e2 + c.hdt * k2;
+                e2 = e2 + c.hdt * k2;
                 s.E2[d * N3 + idx] = e2;
                 const double w = s.T2[d * N3 + idx] + c.gad2 * e2;
                 s.T2[d * N3 + idx] = w - twopi * rint(w / twopi);
             }
         }
         if (c.higgs) {
-            const double hv = s.HV[idx] + c.hdt * s.HA[idx];
+            const double ha = s.HA[idx];
+            double hv = s.HV[idx];
+            if (PREV) hv = hv + c.hdt * ha;
+            hv = hv + c.hdt * ha;
             s.HV[idx] = hv;
             s.H[idx] += c.dt * hv;
         }

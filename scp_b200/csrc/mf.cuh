@@ -223,15 +223,8 @@ __global__ void __launch_bounds__(kRedThreads) mf_kick_damp_kernel(MfState s, Mf
 #pragma unroll
         for (int f = 0; f < 12; f++) s.SL[f * N3 + idx] += c.hdt * s.AL[f * N3 + idx];
         if (c.damp) {
-            const long long NN = (long long)c.N * c.N;
-            const int i = (int)(idx / NN), j = (int)((idx / c.N) % c.N), k = (int)(idx % c.N);
-            const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
-            const double r = sqrt(x * x + y * y + z * z);
-            const double Rd = c.L - c.damp_width;
-            if (r > Rd) {
-                double sc = (r - Rd) / c.damp_width;
-                if (sc > 1) sc = 1;
-                const double dmp = 1.0 - c.damp_rate * sc * sc;
+            const double dmp = sponge_factor(c.N, c.L, c.dx, c.damp_width, c.damp_rate, idx);
+            if (dmp != 1.0) {
 #pragma unroll
                 for (int f = 0; f < 15; f++) s.SC[f * N3 + idx] *= dmp;
                 if (!c.lock)
@@ -244,30 +237,47 @@ __global__ void __launch_bounds__(kRedThreads) mf_kick_damp_kernel(MfState s, Mf
     }
 }
 
-// one fabric's stage 1 kick and stage 2 drift at one site
+// one fabric's stage 1 kick and stage 2 drift at one site; PREV: the
+// previous step's stage 4 kick and sponge factor dmp first
+template <bool PREV>
 __device__ __forceinline__ void mf_kick_drift_fabric(double *X, double *S, const double *A, long long N3, long long idx,
-                                                     double hdt, double dt) {
+                                                     double hdt, double dt, double dmp) {
 #pragma unroll
     for (int f = 0; f < 12; f++) {
-        const double v = S[f * N3 + idx] + hdt * A[f * N3 + idx];
+        const double a = A[f * N3 + idx];
+        double w = S[f * N3 + idx];
+        if (PREV) {
+            w = w + hdt * a;
+            if (dmp != 1.0) w *= dmp;
+        }
+        const double v = w + hdt * a;
         S[f * N3 + idx] = v;
         X[f * N3 + idx] += dt * v;
     }
 }
 
 // stage 1 kick and stage 2 drift of every fabric (Q skipped when locked),
-// E and the wrapped links, in one sweep
+// E and the wrapped links, in one sweep; PREV: the previous step's stage 4
+// kick and stage 5 sponge first, in the operation order of separate sweeps
+template <bool PREV>
 __global__ void __launch_bounds__(kRedThreads) mf_kick_drift_kernel(MfState s, MfConsts c) {
     const long long N3 = c.N3;
     const double twopi = 2.0 * 3.14159265358979323846;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
-        mf_kick_drift_fabric(s.XC, s.SC, s.AC, N3, idx, c.hdt, c.dt);
-        if (!c.lock) mf_kick_drift_fabric(s.XQ, s.SQ, s.AQ, N3, idx, c.hdt, c.dt);
-        mf_kick_drift_fabric(s.XL, s.SL, s.AL, N3, idx, c.hdt, c.dt);
+        const double dmp = (PREV && c.damp) ? sponge_factor(c.N, c.L, c.dx, c.damp_width, c.damp_rate, idx) : 1.0;
+        mf_kick_drift_fabric<PREV>(s.XC, s.SC, s.AC, N3, idx, c.hdt, c.dt, dmp);
+        if (!c.lock) mf_kick_drift_fabric<PREV>(s.XQ, s.SQ, s.AQ, N3, idx, c.hdt, c.dt, dmp);
+        mf_kick_drift_fabric<PREV>(s.XL, s.SL, s.AL, N3, idx, c.hdt, c.dt, dmp);
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const double e = s.SC[(FTH + d) * N3 + idx] + c.hdt * s.AC[(FTH + d) * N3 + idx];
+            const double ea = s.AC[(FTH + d) * N3 + idx];
+            double e = s.SC[(FTH + d) * N3 + idx];
+            if (PREV) {
+                e = e + c.hdt * ea;
+                if (dmp != 1.0) e *= dmp;
+            }
+            e = e + c.hdt * ea;
             s.SC[(FTH + d) * N3 + idx] = e;
             const double w = s.XC[(FTH + d) * N3 + idx] + c.gad * e;
             s.XC[(FTH + d) * N3 + idx] = w - twopi * rint(w / twopi);

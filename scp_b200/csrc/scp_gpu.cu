@@ -648,12 +648,17 @@ static void gext_forces(scp_gpu *h) {
     gext_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
 }
 
-// one verlet_step (scp_sim.c:1583-1716) in four sweeps: kick + drift, links
-// and plaquettes, forces, kick + sponge
-static int gext_step(scp_gpu *h) {
+// nsteps verlet_steps (scp_sim.c:1583-1716): kick + drift, links and
+// plaquettes, forces per step; each step's closing kick + sponge runs inside
+// the next step's first sweep, and as its own sweep after the last step, so
+// the state is synchronous between calls
+static int gext_steps(scp_gpu *h, int nsteps) {
     const int nb = red_blocks(h->N3);
-    gext_kick_drift_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
-    gext_forces(h);
+    for (int n = 0; n < nsteps; n++) {
+        if (n == 0) gext_kick_drift_kernel<false><<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+        else gext_kick_drift_kernel<true><<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+        gext_forces(h);
+    }
     gext_kick_damp_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
     CK(cudaGetLastError());
     return SCP_OK;
@@ -754,12 +759,16 @@ static void mf_forces(scp_gpu *h) {
     mf_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
 }
 
-// verlet_step's multi-fabric branch (scp_sim.c:1583-1716) in four sweeps:
-// kick + drift, plaquettes, forces, kick + sponge
-static int mf_step(scp_gpu *h) {
+// nsteps of verlet_step's multi-fabric branch (scp_sim.c:1583-1716): kick +
+// drift, plaquettes, forces per step; the closing kick + sponge of each step
+// runs inside the next step's first sweep, and on its own after the last
+static int mf_steps(scp_gpu *h, int nsteps) {
     const int nb = red_blocks(h->N3);
-    mf_kick_drift_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
-    mf_forces(h);
+    for (int n = 0; n < nsteps; n++) {
+        if (n == 0) mf_kick_drift_kernel<false><<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+        else mf_kick_drift_kernel<true><<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+        mf_forces(h);
+    }
     mf_kick_damp_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
     CK(cudaGetLastError());
     return SCP_OK;
@@ -983,9 +992,14 @@ int scp_gpu_step(scp_gpu *h, int nsteps) {
     if (nsteps == 0) return SCP_OK;
     CK(cudaSetDevice(h->device));
     int rc;
-    if (h->rp || h->gx || h->mfab) {
+    if (h->gx || h->mfab) {
+        if ((rc = h->gx ? gext_steps(h, nsteps) : mf_steps(h, nsteps))) return rc;
+        h->steps += nsteps;
+        return SCP_OK;
+    }
+    if (h->rp) {
         for (int n = 0; n < nsteps; n++)
-            if ((rc = h->rp ? real_step(h) : (h->gx ? gext_step(h) : mf_step(h)))) return rc;
+            if ((rc = real_step(h))) return rc;
         h->steps += nsteps;
         return SCP_OK;
     }
