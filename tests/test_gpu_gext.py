@@ -159,3 +159,15 @@ def test_gext_snapshots(gpu):
     for c in range(36):
         assert np.array_equal(s32[c], s64[c].astype(np.float32)), c
         assert np.array_equal(bufs[c], s64[c]), c
+
+
+def test_gext_matches_reference_binary_48(gpu):
+    """Both extensions at 48^3 for 100 steps against the reference CPU binary."""
+    st = seeds.small_state(48, True, seed=77, higgs_v=1.0, higgs_rvoid=4.0, g_gauge2=0.15)
+    p = st.params
+    ref = oracle.run_reference(p, st.cols(), 100, diag_every=25)
+    rows, got = run_rows(p, st.cols(), 100, 25)
+    assert len(got) == 36
+    for c in range(36):
+        assert rel_l2(got[c], ref["cols"][c]) < TOL_FRAME, COLUMN_NAMES[c]
+    check_diag(rows, ref["diag"], ref["diag_header"])

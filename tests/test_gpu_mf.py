@@ -153,3 +153,16 @@ def test_mf_snapshots(gpu):
     for c in range(54):
         assert np.array_equal(s32[c], s64[c].astype(np.float32)), c
         assert np.array_equal(bufs[c], s64[c]), c
+
+
+@pytest.mark.parametrize("lock", [1, 0])
+def test_mf_matches_reference_binary_48(gpu, lock):
+    """Three fabrics at 48^3 for 100 steps against the reference CPU binary."""
+    st = seeds.mf_state(48, seed=78, shift=4.0, mf_lock_CQ=lock)
+    p = st.params
+    ref = oracle.run_reference(p, st.cols(), 100, diag_every=25)
+    rows, got = run_rows(p, st.cols(), 100, 25)
+    assert len(got) == 54
+    for c in range(54):
+        assert rel_l2(got[c], ref["cols"][c]) < TOL_FRAME, p.snap_names[c]
+    check_diag(rows, ref["diag"], ref["diag_header"])
