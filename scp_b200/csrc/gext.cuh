@@ -6,12 +6,13 @@
 // sfa/sim/scp_sim.c:1053-1263; verlet_step, :1583-1716; Higgs energy,
 // :1970-1975; second Gauss projection, :2400-2458.
 //
-// These runs use plain per-site kernels over global memory in the
-// reference's three-pass form (link cos/sin, plaquette sines, forces) and
-// its arithmetic order, with the state in the packed layout of the fused
-// kernels (X: u v tu tv th, S: du dv dtu dtv E, synchronous after every step)
-// so that the diagnostics and snapshots are shared.  Gauged runs without
-// these extensions take the fused kernels.
+// These runs use per-site kernels over global memory in the reference's
+// arithmetic order, three sweeps per step (kick + drift, link cos/sin and
+// plaquette sines, forces) and a closing kick after the last step of a call,
+// with the state in the packed layout of the fused kernels (X: u v tu tv th,
+// S: du dv dtu dtv E, synchronous between calls) so that the diagnostics and
+// snapshots are shared.  Gauged runs without these extensions take the fused
+// kernels.
 #pragma once
 #include "common.cuh"
 #include "gauss.cuh"
