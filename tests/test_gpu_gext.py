@@ -171,3 +171,18 @@ def test_gext_matches_reference_binary_48(gpu):
     for c in range(36):
         assert rel_l2(got[c], ref["cols"][c]) < TOL_FRAME, COLUMN_NAMES[c]
     check_diag(rows, ref["diag"], ref["diag_header"])
+
+
+def test_gext_chunking_is_bitwise(gpu):
+    """A step's closing kick and sponge run inside the next step's first sweep
+    within one call and on their own at the end of a call, in the same
+    operation order: 1 + 3 + 36 steps equal 40 steps in one call, bit for bit."""
+    st = seeds.small_state(15, True, seed=79, higgs_v=1.0, higgs_rvoid=2.0, g_gauge2=0.2,
+                           bc_type=0, damp_width=2.5, damp_rate=0.03)
+    p = st.params
+    with Simulation(p, st.cols()) as a, Simulation(p, st.cols()) as b:
+        a.step(40)
+        for k in (1, 3, 36):
+            b.step(k)
+        A, B = a.snapshot(), b.snapshot()
+    assert all(np.array_equal(x, y) for x, y in zip(A, B))
