@@ -566,6 +566,7 @@ def main():
         nd = 0
         t0 = time.perf_counter()
         sim2 = Simulation(params, pin_in)
+        t_init = time.perf_counter()
         done = 0
         while done < args.steps:
             k = min(10, args.steps - done)
@@ -573,8 +574,10 @@ def main():
             done += k
             sim2.diag_vector()
             nd += 1
+        t_steps = time.perf_counter()
         sim2.snapshot(out=snap)
         t1 = time.perf_counter()
+        cg_iters = sim2.info().cg_iterations
         sim2.close()
         wall = max_over_ranks(t1 - t0, dist, f"cuda:{local}")
         h2d = sum(c.nbytes for c in cols)
@@ -583,7 +586,9 @@ def main():
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "wall_s": wall, "includes": "init upload from page-locked host columns, Gauss projection, "
                                            "steps, diag every 10 steps, final f64 snapshot into page-locked "
-                                           "host columns"}
+                                           "host columns",
+               "split_s": {"init": t_init - t0, "steps_and_diag": t_steps - t_init, "snapshot": t1 - t_steps},
+               "cg_iterations": cg_iters}
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,

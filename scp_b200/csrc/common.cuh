@@ -54,4 +54,21 @@ __device__ __forceinline__ double wrap_angle(double v) {
 
 __device__ __forceinline__ int wrapi(int x, int N) { return x < 0 ? x + N : (x >= N ? x - N : x); }
 
+// (i, j, k) of site idx = (i*N + j)*N + k: 32-bit divisions while the index
+// fits (N <= 1625), 64-bit beyond
+__device__ __forceinline__ void site_ijk(long long idx, int N, int *i, int *j, int *k) {
+    if (idx <= 0xFFFFFFFFll) {
+        const unsigned u = (unsigned)idx, n = (unsigned)N, nn = n * n;
+        const unsigned ii = u / nn, r = u - ii * nn, jj = r / n;
+        *i = (int)ii;
+        *j = (int)jj;
+        *k = (int)(r - jj * n);
+    } else {
+        const long long NN = (long long)N * N;
+        *i = (int)(idx / NN);
+        *j = (int)((idx / N) % N);
+        *k = (int)(idx % N);
+    }
+}
+
 }  // namespace scp

@@ -6,6 +6,7 @@
 // order; sums are folded deterministically (reduce.cuh).
 #pragma once
 #include "reduce.cuh"
+#include "trig.cuh"
 
 namespace scp {
 
@@ -47,14 +48,17 @@ template <class View>
 __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagConsts c, double *part) {
     __shared__ double scratch[kDiag1Q * 32];
     double S[DS_NSUM], M[DM_NMAX];
+    #pragma unroll
     for (int q = 0; q < DS_NSUM; q++) S[q] = 0.0;
+    #pragma unroll
     for (int q = 0; q < DM_NMAX; q++) M[q] = 0.0;
     const int N = c.N;
     const long long NN = (long long)N * N;
     const double dV = c.dV, idx1 = c.idx1;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < c.N3;
          idx += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        int i, j, k;
+        site_ijk(idx, N, &i, &j, &k);
         const long long np[3] = {(long long)wrapi(i + 1, N) * NN + (long long)j * N + k,
                                  (long long)i * NN + (long long)wrapi(j + 1, N) * N + k,
                                  (long long)i * NN + (long long)j * N + wrapi(k + 1, N)};
@@ -62,18 +66,21 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagCon
                                  (long long)i * NN + (long long)wrapi(j - 1, N) * N + k,
                                  (long long)i * NN + (long long)j * N + wrapi(k - 1, N)};
         double fu[6], fv[6];
+        #pragma unroll
         for (int a = 0; a < 3; a++) {
             fu[a] = V.q(FU + a, idx);  fv[a] = V.q(FV + a, idx);
             fu[3 + a] = V.q(FTU + a, idx); fv[3 + a] = V.q(FTV + a, idx);
         }
         // ---- energies
         double DcU[3][6], DcV[3][6];
+        #pragma unroll
         for (int d = 0; d < 3; d++) {
             double cP = 1.0, sP = 0.0, cM = 1.0, sM = 0.0;
             if (c.gauged) {
-                sincos(V.q(FTH + d, idx), &sP, &cP);
-                sincos(V.q(FTH + d, nm[d]), &sM, &cM);
+                sincos_any(V.q(FTH + d, idx), &sP, &cP);
+                sincos_any(V.q(FTH + d, nm[d]), &sM, &cM);
             }
+            #pragma unroll
             for (int q = 0; q < 6; q++) {
                 const int fre = q < 3 ? FU + q : FTU + q - 3, fim = q < 3 ? FV + q : FTV + q - 3;
                 const double upn = V.q(fre, np[d]), vpn = V.q(fim, np[d]);
@@ -88,6 +95,7 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagCon
             }
         }
         double s2[3];
+        #pragma unroll
         for (int a = 0; a < 3; a++) {
             s2[a] = fu[a] * fu[a] + fv[a] * fv[a];
             const double pu = V.p(FU + a, idx), pv = V.p(FV + a, idx);
@@ -118,10 +126,12 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagCon
         S[DS_EP] += (c.mu / 2.0) * s / (1.0 + c.kappa * s) * dV;
         M[DM_PMAX] = fmax(M[DM_PMAX], sqrt(s));
         S[DS_PINT] += sqrt(s) * dV;
+        #pragma unroll
         for (int a = 0; a < 3; a++) S[DS_TRS] += fu[3 + a] * fu[3 + a] + fv[3 + a] * fv[3 + a];
         // ---- charges
         const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
         double rho2 = 0.0, qpv = 0.0, qtv = 0.0, sprod = 1.0;
+        #pragma unroll
         for (int a = 0; a < 3; a++) {
             const double u = fu[a], v = fv[a];
             const double ud = V.p(FU + a, idx), vd = V.p(FV + a, idx);
@@ -148,6 +158,7 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagCon
             const double divE = (E0 - V.p(FTH + 0, nm[0]) + E1 - V.p(FTH + 1, nm[1])
                                  + E2 - V.p(FTH + 2, nm[2])) / c.dx;
             double rho = 0.0;
+            #pragma unroll
             for (int a = 0; a < 3; a++)
                 rho += fu[a] * V.p(FV + a, idx) - fv[a] * V.p(FU + a, idx)
                      + fu[3 + a] * V.p(FTV + a, idx) - fv[3 + a] * V.p(FTU + a, idx);
@@ -160,10 +171,13 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagCon
             double ee = 0.5 * (E0 * E0 + E1 * E1 + E2 * E2);
             if (c.gauged) {
                 const double th0 = V.q(FTH + 0, idx), th1 = V.q(FTH + 1, idx), th2 = V.q(FTH + 2, idx);
-                double bb = 0.0;
-                bb += 1.0 - cos(th0 + V.q(FTH + 1, np[0]) - V.q(FTH + 0, np[1]) - th1);
-                bb += 1.0 - cos(th1 + V.q(FTH + 2, np[1]) - V.q(FTH + 1, np[2]) - th2);
-                bb += 1.0 - cos(th2 + V.q(FTH + 0, np[2]) - V.q(FTH + 2, np[0]) - th0);
+                double bb = 0.0, sn, cs;
+                sincos_any(th0 + V.q(FTH + 1, np[0]) - V.q(FTH + 0, np[1]) - th1, &sn, &cs);
+                bb += 1.0 - cs;
+                sincos_any(th1 + V.q(FTH + 2, np[1]) - V.q(FTH + 1, np[2]) - th2, &sn, &cs);
+                bb += 1.0 - cs;
+                sincos_any(th2 + V.q(FTH + 0, np[2]) - V.q(FTH + 2, np[0]) - th0, &sn, &cs);
+                bb += 1.0 - cs;
                 ee += c.bpre * bb;
             }
             S[DS_EEM] += ee * dV;
@@ -189,11 +203,11 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass2_kernel(View V, DiagCon
     const double cz = M0 < 1e-30 ? 0.0 : fin1[DS_CZ] * c.dV / M0;
     const double sthr = fin1[DS_NSUM + DM_SMAX] * (1.0 - 1e-12);
     const int N = c.N;
-    const long long NN = (long long)N * N;
     double S[1] = {0.0}, M[1] = {-INFINITY};   // M holds -(lowest qualifying index)
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < c.N3;
          idx += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        int i, j, k;
+        site_ijk(idx, N, &i, &j, &k);
         const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
         double rho2 = 0.0, sp = 1.0;
         for (int a = 0; a < 3; a++) {

@@ -32,7 +32,8 @@ __device__ __forceinline__ double rho_site(const GaussArgs &a, long long idx) {
 __device__ __forceinline__ double gauss_site(const GaussArgs &a, long long idx) {
     const int N = a.N;
     const long long NN = (long long)N * N;
-    const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+    int i, j, k;
+    site_ijk(idx, N, &i, &j, &k);
     const double *E0 = a.S + (FTH + 0) * a.N3, *E1 = a.S + (FTH + 1) * a.N3, *E2 = a.S + (FTH + 2) * a.N3;
     const long long im = (long long)wrapi(i - 1, N) * NN + (long long)j * N + k;
     const long long jm = (long long)i * NN + (long long)wrapi(j - 1, N) * N + k;
@@ -114,7 +115,8 @@ __global__ void __launch_bounds__(kRedThreads) cg_dirapply_kernel(int N, long lo
     auto P = [&](long long y) { return fma(beta, pold[y], r[y]); };
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
          idx += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        int i, j, k;
+        site_ijk(idx, N, &i, &j, &k);
         const double pc = P(idx);
         const double lap = (P((long long)wrapi(i + 1, N) * NN + (long long)j * N + k)
                             + P((long long)wrapi(i - 1, N) * NN + (long long)j * N + k)
@@ -198,7 +200,8 @@ __global__ void gauss_correct_kernel(GaussArgs a, const double *x, const double 
     const double xbar = cg[CG_XBAR];
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < a.N3;
          idx += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+        int i, j, k;
+        site_ijk(idx, N, &i, &j, &k);
         const double c0 = x[idx] - xbar;
         a.S[(FTH + 0) * a.N3 + idx] += ((x[(long long)wrapi(i + 1, N) * NN + (long long)j * N + k] - xbar) - c0) / a.dx;
         a.S[(FTH + 1) * a.N3 + idx] += ((x[(long long)i * NN + (long long)wrapi(j + 1, N) * N + k] - xbar) - c0) / a.dx;

@@ -44,7 +44,8 @@ struct GextState {
 
 __device__ __forceinline__ void gext_nb(long long idx, int N, long long np[3], long long nm[3]) {
     const long long NN = (long long)N * N;
-    const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+    int i, j, k;
+    site_ijk(idx, N, &i, &j, &k);
     np[0] = (long long)wrapi(i + 1, N) * NN + (long long)j * N + k;
     nm[0] = (long long)wrapi(i - 1, N) * NN + (long long)j * N + k;
     np[1] = (long long)i * NN + (long long)wrapi(j + 1, N) * N + k;
@@ -215,8 +216,8 @@ __global__ void __launch_bounds__(kRedThreads) gext_force_kernel(GextState s, Ge
 
 // sponge factor of apply_damping at a site (1 outside the sponge)
 __device__ __forceinline__ double sponge_factor(int N, double L, double dx, double width, double rate, long long idx) {
-    const long long NN = (long long)N * N;
-    const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+    int i, j, k;
+    site_ijk(idx, N, &i, &j, &k);
     const double x = -L + i * dx, y = -L + j * dx, z = -L + k * dx;
     const double r = sqrt(x * x + y * y + z * z);
     const double Rd = L - width;
@@ -330,12 +331,13 @@ __global__ void __launch_bounds__(256) gext_higgs_energy_kernel(GextState s, Gex
 // Higgs start value (the reference's main, scp_sim.c:2802-2817): the VEV, or
 // a central cavity of radius rvoid with a tanh wall of width 0.6
 __global__ void gext_higgs_init_kernel(GextState s, GextConsts c, double rvoid) {
-    const long long N3 = c.N3, NN = (long long)c.N * c.N;
+    const long long N3 = c.N3;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
         double h = c.hv;
         if (rvoid > 0.0) {
-            const int i = (int)(idx / NN), j = (int)((idx / c.N) % c.N), k = (int)(idx % c.N);
+            int i, j, k;
+            site_ijk(idx, c.N, &i, &j, &k);
             const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
             const double r = sqrt(x * x + y * y + z * z);
             h = c.hv * 0.5 * (1.0 + tanh((r - rvoid) / 0.6));

@@ -322,12 +322,13 @@ __global__ void __launch_bounds__(kRedThreads) mf_diag_kernel(MfState s, MfConst
     __shared__ double scratch[(MS_NSUM + 1) * 32];
     double S[MS_NSUM], M[1] = {0.0};
     for (int q = 0; q < MS_NSUM; q++) S[q] = 0.0;
-    const long long N3 = c.N3, NN = (long long)c.N * c.N;
+    const long long N3 = c.N3;
     for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < N3;
          idx += (long long)gridDim.x * blockDim.x) {
         long long np[3], nm[3];
         gext_nb(idx, c.N, np, nm);
-        const int i = (int)(idx / NN), j = (int)((idx / c.N) % c.N), k = (int)(idx % c.N);
+        int i, j, k;
+        site_ijk(idx, c.N, &i, &j, &k);
         const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
         const double rc = mf_rho(s.XC, s.SC, N3, idx), rq = mf_rho(s.XQ, s.SQ, N3, idx);
         const double rl = mf_rho(s.XL, s.SL, N3, idx);

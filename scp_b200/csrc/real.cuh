@@ -37,7 +37,8 @@ struct RealNb {
 
 __device__ __forceinline__ RealNb real_nb(long long idx, int N, int *i_, int *j_, int *k_) {
     const long long NN = (long long)N * N;
-    const int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+    int i, j, k;
+    site_ijk(idx, N, &i, &j, &k);
     RealNb n;
     n.ip = (long long)wrapi(i + 1, N) * NN + (long long)j * N + k;
     n.im = (long long)wrapi(i - 1, N) * NN + (long long)j * N + k;
@@ -170,8 +171,8 @@ __global__ void real_kick_damp_kernel(double *v, const double *acc, RealConsts c
          idx += (long long)gridDim.x * blockDim.x) {
         double d = 1.0;
         if (c.damp) {
-            const long long NN = (long long)c.N * c.N;
-            const int i = (int)(idx / NN), j = (int)((idx / c.N) % c.N), k = (int)(idx % c.N);
+            int i, j, k;
+            site_ijk(idx, c.N, &i, &j, &k);
             const double xx = -c.L + i * c.dx, yy = -c.L + j * c.dx, zz = -c.L + k * c.dx;
             const double r = sqrt(xx * xx + yy * yy + zz * zz);
             const double Rd = c.L - c.damp_width;
