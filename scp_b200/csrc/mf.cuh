@@ -199,8 +199,17 @@ __global__ void __launch_bounds__(kRedThreads) mf_force_kernel(MfState s, MfCons
         st[1] = -(PS[0 * N3 + idx] - PS[0 * N3 + nm[0]]) + (PS[1 * N3 + idx] - PS[1 * N3 + nm[2]]);
         st[2] = (PS[2 * N3 + idx] - PS[2 * N3 + nm[0]]) - (PS[1 * N3 + idx] - PS[1 * N3 + nm[1]]);
         double E[3], J[3];
-        mf_fabric_site(s.XC, c.lock ? nullptr : s.AC, th, c.q[0], idx, np, nm, c, J);
-        for (int d = 0; d < 3; d++) E[d] = c.stp * st[d] + c.g * c.q[0] * J[d];
+        if (c.lock && c.q[0] == 0.0) {
+            // locked with q_C = 0 (the reference's default): the C pass stores
+            // nothing (the q_Q pass overwrites C's accelerations) and adds
+            // g*0*J_C, so for finite fields it leaves E = staples alone
+#pragma unroll
+            for (int d = 0; d < 3; d++) E[d] = c.stp * st[d];
+        } else {
+            mf_fabric_site(s.XC, c.lock ? nullptr : s.AC, th, c.q[0], idx, np, nm, c, J);
+#pragma unroll
+            for (int d = 0; d < 3; d++) E[d] = c.stp * st[d] + c.g * c.q[0] * J[d];
+        }
         mf_fabric_site(s.XQ, s.AQ, th, c.q[1], idx, np, nm, c, J);
         for (int d = 0; d < 3; d++) E[d] += c.g * c.q[1] * J[d];
         mf_fabric_site(s.XL, s.AL, th, c.q[2], idx, np, nm, c, J);
