@@ -40,3 +40,13 @@ def gpu():
     from scp_b200 import native
     native.lib()
     return True
+
+
+@pytest.fixture(scope="session")
+def reference():
+    """The reference's own CPU binary (oracle/_ref, built from the reference
+    tree by `make -C oracle ref`); tests that run it skip without it."""
+    import oracle
+    if not oracle.reference_available():
+        pytest.skip("reference binary not built (make -C oracle ref needs the reference tree)")
+    return True

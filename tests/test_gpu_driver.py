@@ -24,7 +24,7 @@ def _run(binary, cfg, cwd, extra=()):
 
 @pytest.mark.parametrize("gauged", [False, True, "g0", "sync", "real", "real_terms", "gext", "gext_sync", "mf",
                                     "mf_free"])
-def test_driver_matches_reference_binary(gpu, tmp_path, gauged):
+def test_driver_matches_reference_binary(gpu, reference, tmp_path, gauged):
     """gauged="g0": complex_gauge=1 with g_gauge=0, the reference's ungauged
     dispatch with the link columns carried; "sync": gauged with the
     synchronous snapshot path (gpu_async_snap = 0) instead of the pipelined one;

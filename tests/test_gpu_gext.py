@@ -73,7 +73,7 @@ GEXT = [dict(higgs_v=1.0),
 
 @pytest.mark.parametrize("over", GEXT, ids=lambda t: "-".join(f"{k}{v}" for k, v in t.items()))
 @pytest.mark.parametrize("N", [16, 17])
-def test_gext_matches_reference_binary(gpu, N, over):
+def test_gext_matches_reference_binary(gpu, reference, N, over):
     """Each extension alone and together, even and odd N, periodic and with
     the sponge, against the reference CPU binary on the same seed."""
     st = seeds.small_state(N, True, seed=50 + N, **over)
@@ -161,7 +161,7 @@ def test_gext_snapshots(gpu):
         assert np.array_equal(bufs[c], s64[c]), c
 
 
-def test_gext_matches_reference_binary_48(gpu):
+def test_gext_matches_reference_binary_48(gpu, reference):
     """Both extensions at 48^3 for 100 steps against the reference CPU binary."""
     st = seeds.small_state(48, True, seed=77, higgs_v=1.0, higgs_rvoid=4.0, g_gauge2=0.15)
     p = st.params

@@ -78,7 +78,7 @@ MF = [dict(),
 
 @pytest.mark.parametrize("kw", MF, ids=lambda t: "-".join(f"{k}{v}" for k, v in t.items()) or "lock")
 @pytest.mark.parametrize("N", [16, 15])
-def test_mf_matches_reference_binary(gpu, N, kw):
+def test_mf_matches_reference_binary(gpu, reference, N, kw):
     """Locked and free Q (free Q seeded from its own state or as a copy of C),
     custom charges with eta = 0, a charged L fabric under the sponge; even and
     odd N; against the reference CPU binary on the same seeds."""
@@ -157,7 +157,7 @@ def test_mf_snapshots(gpu):
 
 
 @pytest.mark.parametrize("lock", [1, 0])
-def test_mf_matches_reference_binary_48(gpu, lock):
+def test_mf_matches_reference_binary_48(gpu, reference, lock):
     """Three fabrics at 48^3 for 100 steps against the reference CPU binary."""
     st = seeds.mf_state(48, seed=78, shift=4.0, mf_lock_CQ=lock)
     p = st.params

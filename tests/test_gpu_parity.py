@@ -128,7 +128,7 @@ def test_snapshot_async_matches_sync_while_stepping(gpu, prec, dtype):
 
 
 @pytest.mark.parametrize("N,nsteps,damped", [(16, 40, False), (33, 60, True), (64, 200, False)])
-def test_real_mode_matches_reference_binary(gpu, N, nsteps, damped):
+def test_real_mode_matches_reference_binary(gpu, reference, N, nsteps, damped):
     """The reference's real 6-field mode (complex_phi = 0, compute_forces with
     its default terms) run by the reference CPU binary and by this library on
     the same seed: final frame per column and every diag TSV column; odd N and
@@ -157,7 +157,7 @@ REAL_TERMS = [dict(mode=1), dict(mode=3), dict(alpha_cs=0.3), dict(beta_h=0.5), 
 
 
 @pytest.mark.parametrize("terms", REAL_TERMS, ids=lambda t: "-".join(f"{k}{v}" for k, v in t.items()))
-def test_real_mode_optional_terms_match_reference_binary(gpu, terms):
+def test_real_mode_optional_terms_match_reference_binary(gpu, reference, terms):
     """The real mode's optional terms (mass modes 1 and 3, Cosserat strain,
     curl-squared hardening, chiral helicity; compute_forces, scp_sim.c:743-929)
     on the separate real-mode kernels, against the reference CPU binary: final
