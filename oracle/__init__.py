@@ -36,6 +36,9 @@ class OrcParams(ctypes.Structure):
         ("g", ctypes.c_double), ("bc_type", ctypes.c_int), ("damp_width", ctypes.c_double),
         ("damp_rate", ctypes.c_double), ("qdiag_radius", ctypes.c_double),
         ("qdiag_probe1", ctypes.c_double), ("qdiag_probe2", ctypes.c_double),
+        ("higgs_v", ctypes.c_double), ("higgs_lam", ctypes.c_double), ("higgs_kap", ctypes.c_double),
+        ("higgs_rvoid", ctypes.c_double), ("g2", ctypes.c_double), ("q2", ctypes.c_double * 3),
+        ("n_fabrics", ctypes.c_int), ("mf_lock", ctypes.c_int), ("q_fab", ctypes.c_double * 3),
     ]
 
 
@@ -82,6 +85,14 @@ def _orc_params(p) -> OrcParams:
     o.g = p.g_gauge
     o.bc_type, o.damp_width, o.damp_rate = p.bc_type, p.damp_width, p.damp_rate
     o.qdiag_radius, o.qdiag_probe1, o.qdiag_probe2 = p.qdiag_radius, p.qdiag_probe1, p.qdiag_probe2
+    o.higgs_v, o.higgs_lam = getattr(p, "higgs_v", 0.0), getattr(p, "higgs_lam", 1.0)
+    o.higgs_kap, o.higgs_rvoid = getattr(p, "higgs_kap", 2.0), getattr(p, "higgs_rvoid", 0.0)
+    o.g2 = getattr(p, "g_gauge2", 0.0)
+    for a, k in enumerate(("gauge2_q0", "gauge2_q1", "gauge2_q2")):
+        o.q2[a] = getattr(p, k, (1.0, 1.0, -2.0)[a])
+    o.n_fabrics, o.mf_lock = getattr(p, "n_fabrics", 1), getattr(p, "mf_lock_CQ", 1)
+    for a, k in enumerate(("q_C", "q_Q", "q_L")):
+        o.q_fab[a] = getattr(p, k, (0.0, 1.0, -1.0)[a])
     return o
 
 
@@ -103,16 +114,21 @@ class Oracle:
         lib().orc_step(self._h, int(n))
 
     def cols(self) -> list[np.ndarray]:
+        """Current state in snapshot column order (th2 / E2 or fabric L
+        appended when those extensions are on)."""
         n3 = self.params.N ** 3
-        out = [np.empty(n3) for _ in range(self.ncols)]
-        arr = (ctypes.c_void_p * self.ncols)(*[c.ctypes.data for c in out])
+        nc = getattr(self.params, "snap_ncols", self.ncols)
+        out = [np.empty(n3) for _ in range(nc)]
+        arr = (ctypes.c_void_p * nc)(*[c.ctypes.data for c in out])
         lib().orc_get(self._h, arr)
         return out
 
     def diag(self) -> np.ndarray:
-        buf = (ctypes.c_double * NDIAG)()
-        lib().orc_diag(self._h, buf)
-        return np.array(buf[:])
+        """The reference diag TSV columns after t (31), and Q_C, Q_Q, Q_L, Q_em
+        with three fabrics."""
+        buf = (ctypes.c_double * 40)()
+        n = lib().orc_diag(self._h, buf)
+        return np.array(buf[:n])
 
     def accelerations(self) -> list[np.ndarray]:
         n3 = self.params.N ** 3

@@ -1,8 +1,9 @@
 /* scp_oracle.c -- TEST INFRASTRUCTURE ONLY.
  *
  * CPU restatement of the reference's complex (v66) and gauged (v69) lattice
- * leapfrog stepper, kardianos/scp sfa/sim/scp_sim.c, single fabric, no Higgs,
- * no second gauge, bc_type 0 (absorbing sphere) or 2 (periodic).  It is the
+ * leapfrog stepper, kardianos/scp sfa/sim/scp_sim.c, with the gauged
+ * extensions (v71 Higgs condensate and second U(1) gauge, v75 three matter
+ * fabrics), bc_type 0 (absorbing sphere) or 2 (periodic).  It is the
  * checker for the CUDA library's parity tests and is never part of the
  * product.  Parity of this restatement is pinned against the reference
  * binary itself (oracle/_ref/scp_sim, built from the reference sources by
@@ -33,9 +34,13 @@ enum { U0 = 0, V0 = 3, TU0 = 6, TV0 = 9 };
 struct orc_state {
     orc_params P;
     long N3;
-    double *q[12], *p[12], *a[12];   /* positions, velocities, accelerations */
+    double *q[12], *p[12], *a[12];   /* positions, velocities, accelerations (fabric C) */
     double *th[3], *E[3], *K[3];     /* links, electric field, E-kick */
     double *lc[3], *ls[3], *ps[3];   /* scratch: link cos/sin, plaquette sines */
+    int higgs, g2on, mf;             /* extensions present */
+    double *th2[3], *E2[3], *K2[3], *ps2[3];   /* second gauge */
+    double *H, *HV, *HA;                       /* Higgs field, velocity, acceleration */
+    double *fq[2][12], *fp[2][12], *fa[2][12]; /* fabrics Q (0) and L (1) */
     double G_offset;
     int cg_iters;
     double *mem;
@@ -126,7 +131,9 @@ static inline double plaq_angle(double *const th[3], int a, int b, long idx, con
     return th[a][idx] + th[b][np[a]] - th[a][np[b]] - th[b][idx];
 }
 
-/* compute_forces_complex_gauge, scp_sim.c:1053-1263 (G2 = HIG = 0) */
+/* compute_forces_complex_gauge, scp_sim.c:1053-1263, with its v71 terms:
+ * Higgs back-reaction and H_acc (HIG), second gauge (G2: matter transported
+ * by th + q_a th2, staples and current of th2 into K2) */
 static void forces_gauge(orc_state *s) {
     const orc_params *P = &s->P;
     const int N = P->N;
@@ -134,6 +141,9 @@ static void forces_gauge(orc_state *s) {
     const double dx = P->dx, idx2 = 1.0 / (dx * dx), idx1 = 1.0 / (2.0 * dx), inva = 1.0 / dx;
     const double MU = P->mu, KAPPA = P->kappa, MASS2 = P->m2, MTHETA2 = P->mtheta2, ETA = P->eta;
     const double GG = P->g, STP = 1.0 / (GG * dx * dx * dx);
+    const int HIG = s->higgs, G2 = s->g2on;
+    const double HV = P->higgs_v, HLAM = P->higgs_lam, HKAP = P->higgs_kap;
+    const double GG2 = P->g2, STP2 = G2 ? 1.0 / (GG2 * dx * dx * dx) : 0.0;
     static const int pa[3] = {0, 1, 2}, pb[3] = {1, 2, 0};
     static const int ci1[3] = {1, 2, 0}, ci2[3] = {2, 0, 1};
 
@@ -145,6 +155,8 @@ static void forces_gauge(orc_state *s) {
         nbr_t n = nbrs(N, idx);
         long np[3] = {n.ip, n.jp, n.kp};
         for (int p = 0; p < 3; p++) s->ps[p][idx] = sin(plaq_angle(s->th, pa[p], pb[p], idx, np));
+        if (G2)
+            for (int p = 0; p < 3; p++) s->ps2[p][idx] = sin(plaq_angle(s->th2, pa[p], pb[p], idx, np));
     }
     /* pass C: matter accelerations and E-kick */
 #pragma omp parallel for schedule(static)
@@ -158,9 +170,16 @@ static void forces_gauge(orc_state *s) {
         }
         double TRp[3][6], TIp[3][6], TRm[3][6], TIm[3][6], tup[3][3], tvp[3][3];
         for (int d = 0; d < 3; d++) {
-            double cP = s->lc[d][idx], sP = s->ls[d][idx];
-            double cM = s->lc[d][nm[d]], sM = s->ls[d][nm[d]];
             for (int a = 0; a < 3; a++) {
+                double cP, sP, cM, sM;
+                if (G2) {   /* combined link th + q_a th2 of component a */
+                    double php = s->th[d][idx] + P->q2[a] * s->th2[d][idx];
+                    double phm = s->th[d][nm[d]] + P->q2[a] * s->th2[d][nm[d]];
+                    cP = cos(php); sP = sin(php); cM = cos(phm); sM = sin(phm);
+                } else {
+                    cP = s->lc[d][idx]; sP = s->ls[d][idx];
+                    cM = s->lc[d][nm[d]]; sM = s->ls[d][nm[d]];
+                }
                 double upn = s->q[U0 + a][np[d]], vpn = s->q[V0 + a][np[d]];
                 double umn = s->q[U0 + a][nm[d]], vmn = s->q[V0 + a][nm[d]];
                 double tpn = s->q[TU0 + a][np[d]], wpn = s->q[TV0 + a][np[d]];
@@ -179,6 +198,7 @@ static void forces_gauge(orc_state *s) {
         double den = 1.0 + KAPPA * sp;
         double Vp = 0.5 * MU / (den * den);
         double rest[3] = {s1 * s2, s0 * s2, s0 * s1};
+        double hh = HIG ? s->H[idx] * s->H[idx] : 0.0;
         double DcU[3][6], DcV[3][6];
         for (int d = 0; d < 3; d++)
             for (int f = 0; f < 6; f++) {
@@ -199,10 +219,29 @@ static void forces_gauge(orc_state *s) {
                             + TRp[2][3 + a] + TRm[2][3 + a] - 6.0 * fu[3 + a]) * idx2;
             double lapVT = (TIp[0][3 + a] + TIm[0][3 + a] + TIp[1][3 + a] + TIm[1][3 + a]
                             + TIp[2][3 + a] + TIm[2][3 + a] - 6.0 * fv[3 + a]) * idx2;
-            s->a[U0 + a][idx] = lapUP - MASS2 * fu[a] - 2.0 * Vp * fu[a] * rest[a] + ETA * reDxT;
-            s->a[V0 + a][idx] = lapVP - MASS2 * fv[a] - 2.0 * Vp * fv[a] * rest[a] + ETA * imDxT;
+            double au = lapUP - MASS2 * fu[a] - 2.0 * Vp * fu[a] * rest[a] + ETA * reDxT;
+            double av = lapVP - MASS2 * fv[a] - 2.0 * Vp * fv[a] * rest[a] + ETA * imDxT;
+            if (HIG) {   /* - HKAP hh f prod_rest (scp_sim.c:1196-1200) */
+                au = au - HKAP * hh * fu[a] * rest[a];
+                av = av - HKAP * hh * fv[a] * rest[a];
+            }
+            s->a[U0 + a][idx] = au;
+            s->a[V0 + a][idx] = av;
             s->a[TU0 + a][idx] = lapUT - MTHETA2 * fu[3 + a] + ETA * reDxP;
             s->a[TV0 + a][idx] = lapVT - MTHETA2 * fv[3 + a] + ETA * imDxP;
+        }
+        if (HIG) {   /* Hddot = lapH - lam H (H^2 - v^2) - kap s H (:1206-1211) */
+            double *H = s->H;
+            double lapH = (H[n.ip] + H[n.im] + H[n.jp] + H[n.jm] + H[n.kp] + H[n.km] - 6.0 * H[idx]) * idx2;
+            double h = H[idx];
+            s->HA[idx] = lapH - HLAM * h * (h * h - HV * HV) - HKAP * sp * h;
+        }
+        double st2[3] = {0, 0, 0};
+        if (G2) {
+            double *const *q2 = s->ps2;
+            st2[0] = (q2[0][idx] - q2[0][nm[1]]) - (q2[2][idx] - q2[2][nm[2]]);
+            st2[1] = -(q2[0][idx] - q2[0][nm[0]]) + (q2[1][idx] - q2[1][nm[2]]);
+            st2[2] = (q2[2][idx] - q2[2][nm[0]]) - (q2[1][idx] - q2[1][nm[1]]);
         }
         double *const *ps = s->ps;
         double st[3];
@@ -225,12 +264,149 @@ static void forces_gauge(orc_state *s) {
                        + (tup[d][d2] * WpI2 - tvp[d][d2] * WpR2);
             double Jlat = inva * Jg - 0.5 * ETA * (T12 - T21);
             s->K[d][idx] = STP * st[d] + GG * Jlat;
+            if (G2) {   /* relative current of the second gauge (:1251-1259) */
+                double Jg2 = 0.0;
+                for (int a = 0; a < 3; a++) {
+                    Jg2 += P->q2[a] * (fu[a] * TIp[d][a] - fv[a] * TRp[d][a]);
+                    Jg2 += P->q2[a] * (fu[3 + a] * TIp[d][3 + a] - fv[3 + a] * TRp[d][3 + a]);
+                }
+                s->K2[d][idx] = STP2 * st2[d] + GG2 * inva * Jg2;
+            }
         }
     }
 }
 
+/* Matter accelerations of one fabric (view X positions, A accelerations; A
+ * = NULL stores none) with charge-q_em links, and the current it adds to the
+ * E kick: mode 0 sets K = staples + g q_em J, mode 1 adds g q_em J
+ * (force_fabric_gauged_accum, scp_sim.c:1274-1382) */
+static void fabric_accum(orc_state *s, double *const *X, double *const *A, double q_em, int mode) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long N3 = s->N3;
+    const double dx = P->dx, idx2 = 1.0 / (dx * dx), idx1 = 1.0 / (2.0 * dx), inva = 1.0 / dx;
+    const double MU = P->mu, KAPPA = P->kappa, MASS2 = P->m2, MTHETA2 = P->mtheta2, ETA = P->eta;
+    const double GG = P->g, STP = 1.0 / (GG * dx * dx * dx);
+    static const int ci1[3] = {1, 2, 0}, ci2[3] = {2, 0, 1};
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        long np[3] = {n.ip, n.jp, n.kp}, nm[3] = {n.im, n.jm, n.km};
+        double fu[6], fv[6];
+        for (int a = 0; a < 3; a++) {
+            fu[a] = X[U0 + a][idx];      fv[a] = X[V0 + a][idx];
+            fu[3 + a] = X[TU0 + a][idx]; fv[3 + a] = X[TV0 + a][idx];
+        }
+        double TRp[3][6], TIp[3][6], TRm[3][6], TIm[3][6], tup[3][3], tvp[3][3];
+        for (int d = 0; d < 3; d++) {
+            double cP = cos(q_em * s->th[d][idx]), sP = sin(q_em * s->th[d][idx]);
+            double cM = cos(q_em * s->th[d][nm[d]]), sM = sin(q_em * s->th[d][nm[d]]);
+            for (int a = 0; a < 3; a++) {
+                double upn = X[U0 + a][np[d]], vpn = X[V0 + a][np[d]];
+                double umn = X[U0 + a][nm[d]], vmn = X[V0 + a][nm[d]];
+                double tpn = X[TU0 + a][np[d]], wpn = X[TV0 + a][np[d]];
+                double tmn = X[TU0 + a][nm[d]], wmn = X[TV0 + a][nm[d]];
+                TRp[d][a] = cP * upn - sP * vpn;       TIp[d][a] = cP * vpn + sP * upn;
+                TRm[d][a] = cM * umn + sM * vmn;       TIm[d][a] = cM * vmn - sM * umn;
+                TRp[d][3 + a] = cP * tpn - sP * wpn;   TIp[d][3 + a] = cP * wpn + sP * tpn;
+                TRm[d][3 + a] = cM * tmn + sM * wmn;   TIm[d][3 + a] = cM * wmn - sM * tmn;
+                tup[d][a] = tpn; tvp[d][a] = wpn;
+            }
+        }
+        double s0 = fu[0] * fu[0] + fv[0] * fv[0];
+        double s1 = fu[1] * fu[1] + fv[1] * fv[1];
+        double s2 = fu[2] * fu[2] + fv[2] * fv[2];
+        double sp = s0 * s1 * s2;
+        double den = 1.0 + KAPPA * sp;
+        double Vp = 0.5 * MU / (den * den);
+        double rest[3] = {s1 * s2, s0 * s2, s0 * s1};
+        double DcU[3][6], DcV[3][6];
+        for (int d = 0; d < 3; d++)
+            for (int f = 0; f < 6; f++) {
+                DcU[d][f] = (TRp[d][f] - TRm[d][f]) * idx1;
+                DcV[d][f] = (TIp[d][f] - TIm[d][f]) * idx1;
+            }
+        if (A)
+            for (int a = 0; a < 3; a++) {
+                int d1 = ci1[a], d2 = ci2[a];
+                double reDxT = DcU[d1][3 + d2] - DcU[d2][3 + d1];
+                double imDxT = DcV[d1][3 + d2] - DcV[d2][3 + d1];
+                double reDxP = DcU[d1][d2] - DcU[d2][d1];
+                double imDxP = DcV[d1][d2] - DcV[d2][d1];
+                double lapUP = (TRp[0][a] + TRm[0][a] + TRp[1][a] + TRm[1][a] + TRp[2][a] + TRm[2][a]
+                                - 6.0 * fu[a]) * idx2;
+                double lapVP = (TIp[0][a] + TIm[0][a] + TIp[1][a] + TIm[1][a] + TIp[2][a] + TIm[2][a]
+                                - 6.0 * fv[a]) * idx2;
+                double lapUT = (TRp[0][3 + a] + TRm[0][3 + a] + TRp[1][3 + a] + TRm[1][3 + a]
+                                + TRp[2][3 + a] + TRm[2][3 + a] - 6.0 * fu[3 + a]) * idx2;
+                double lapVT = (TIp[0][3 + a] + TIm[0][3 + a] + TIp[1][3 + a] + TIm[1][3 + a]
+                                + TIp[2][3 + a] + TIm[2][3 + a] - 6.0 * fv[3 + a]) * idx2;
+                A[U0 + a][idx] = lapUP - MASS2 * fu[a] - 2.0 * Vp * fu[a] * rest[a] + ETA * reDxT;
+                A[V0 + a][idx] = lapVP - MASS2 * fv[a] - 2.0 * Vp * fv[a] * rest[a] + ETA * imDxT;
+                A[TU0 + a][idx] = lapUT - MTHETA2 * fu[3 + a] + ETA * reDxP;
+                A[TV0 + a][idx] = lapVT - MTHETA2 * fv[3 + a] + ETA * imDxP;
+            }
+        double *const *ps = s->ps;
+        double st[3];
+        st[0] = (ps[0][idx] - ps[0][nm[1]]) - (ps[2][idx] - ps[2][nm[2]]);
+        st[1] = -(ps[0][idx] - ps[0][nm[0]]) + (ps[1][idx] - ps[1][nm[2]]);
+        st[2] = (ps[2][idx] - ps[2][nm[0]]) - (ps[1][idx] - ps[1][nm[1]]);
+        for (int d = 0; d < 3; d++) {
+            double cP = cos(q_em * s->th[d][idx]), sP = sin(q_em * s->th[d][idx]);
+            double Jg = 0.0;
+            for (int a = 0; a < 3; a++) {
+                Jg += fu[a] * TIp[d][a] - fv[a] * TRp[d][a];
+                Jg += fu[3 + a] * TIp[d][3 + a] - fv[3 + a] * TRp[d][3 + a];
+            }
+            int d1 = ci1[d], d2 = ci2[d];
+            double WpR1 = cP * fu[d2] + sP * fv[d2], WpI1 = cP * fv[d2] - sP * fu[d2];
+            double WpR2 = cP * fu[d1] + sP * fv[d1], WpI2 = cP * fv[d1] - sP * fu[d1];
+            double T12 = (fu[3 + d1] * TIp[d][d2] - fv[3 + d1] * TRp[d][d2])
+                       + (tup[d][d1] * WpI1 - tvp[d][d1] * WpR1);
+            double T21 = (fu[3 + d2] * TIp[d][d1] - fv[3 + d2] * TRp[d][d1])
+                       + (tup[d][d2] * WpI2 - tvp[d][d2] * WpR2);
+            double Jlat = inva * Jg - 0.5 * ETA * (T12 - T21);
+            double jterm = GG * q_em * Jlat;
+            if (mode == 0) s->K[d][idx] = STP * st[d] + jterm;
+            else s->K[d][idx] += jterm;
+        }
+    }
+}
+
+/* mf_lock_copy_CQ, scp_sim.c:150-172: Q <- C, fields, velocities, accelerations */
+static void lock_copy(orc_state *s) {
+    size_t bytes = s->N3 * sizeof(double);
+    for (int f = 0; f < 12; f++) {
+        memcpy(s->fq[0][f], s->q[f], bytes);
+        memcpy(s->fp[0][f], s->p[f], bytes);
+        memcpy(s->fa[0][f], s->a[f], bytes);
+    }
+}
+
+/* compute_forces_complex_gauge_mf, scp_sim.c:1390-1433 */
+static void forces_mf(orc_state *s) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long N3 = s->N3;
+    static const int pa[3] = {0, 1, 2}, pb[3] = {1, 2, 0};
+    link_trig(s);
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        long np[3] = {n.ip, n.jp, n.kp};
+        for (int p = 0; p < 3; p++) s->ps[p][idx] = sin(plaq_angle(s->th, pa[p], pb[p], idx, np));
+    }
+    fabric_accum(s, s->q, s->a, P->q_fab[0], 0);
+    if (P->mf_lock) fabric_accum(s, s->q, s->a, P->q_fab[1], 1);
+    else fabric_accum(s, s->fq[0], s->fa[0], P->q_fab[1], 1);
+    fabric_accum(s, s->fq[1], s->fa[1], P->q_fab[2], 1);
+    if (P->mf_lock) lock_copy(s);
+}
+
 static void forces(orc_state *s) {
-    if (s->P.gauge) forces_gauge(s); else forces_complex(s);
+    if (s->mf) forces_mf(s);
+    else if (s->P.gauge) forces_gauge(s);
+    else forces_complex(s);
 }
 
 /* ---------------------------------------------------------------- stepping */
@@ -254,33 +430,46 @@ static void damping(orc_state *s) {
             double d = 1.0 - DR * sc * sc;
             for (int f = 0; f < 12; f++) s->p[f][idx] *= d;
             if (P->gauge) for (int c = 0; c < 3; c++) s->E[c][idx] *= d;
+            if (s->mf)   /* Q and L velocities too (not E2, not the Higgs) */
+                for (int fb = 0; fb < 2; fb++)
+                    for (int f = 0; f < 12; f++) s->fp[fb][f][idx] *= d;
         }
     }
 }
 
-static void half_kick(orc_state *s, double hdt) {
-    for (int f = 0; f < 12; f++) {
-        double *v = s->p[f], *a = s->a[f];
+static void axpy(double *v, const double *a, double h, long n) {
 #pragma omp parallel for schedule(static)
-        for (long i = 0; i < s->N3; i++) v[i] += hdt * a[i];
+    for (long i = 0; i < n; i++) v[i] += h * a[i];
+}
+
+/* stage 1 / stage 4 kicks of verlet_step (scp_sim.c:1590-1620, :1670-1705):
+ * matter of C (and Q unless locked, and L), E, E2, Hdot; with three fabrics
+ * and the lock, stage 4 copies C into Q before the E kick */
+static void half_kick(orc_state *s, double hdt, int stage4) {
+    for (int f = 0; f < 12; f++) axpy(s->p[f], s->a[f], hdt, s->N3);
+    if (s->mf) {
+        if (!s->P.mf_lock)
+            for (int f = 0; f < 12; f++) axpy(s->fp[0][f], s->fa[0][f], hdt, s->N3);
+        for (int f = 0; f < 12; f++) axpy(s->fp[1][f], s->fa[1][f], hdt, s->N3);
+        if (stage4 && s->P.mf_lock) lock_copy(s);
     }
     if (s->P.gauge)
-        for (int c = 0; c < 3; c++) {
-            double *E = s->E[c], *K = s->K[c];
-#pragma omp parallel for schedule(static)
-            for (long i = 0; i < s->N3; i++) E[i] += hdt * K[i];
-        }
+        for (int c = 0; c < 3; c++) axpy(s->E[c], s->K[c], hdt, s->N3);
+    if (s->g2on)
+        for (int c = 0; c < 3; c++) axpy(s->E2[c], s->K2[c], hdt, s->N3);
+    if (s->higgs) axpy(s->HV, s->HA, hdt, s->N3);
 }
 
 /* verlet_step, scp_sim.c:1583-1716: kick, drift (+ link drift and wrap),
  * forces, kick, boundary */
 static void verlet(orc_state *s) {
     const double dt = s->P.dt, hdt = 0.5 * dt;
-    half_kick(s, hdt);
-    for (int f = 0; f < 12; f++) {
-        double *x = s->q[f], *v = s->p[f];
-#pragma omp parallel for schedule(static)
-        for (long i = 0; i < s->N3; i++) x[i] += dt * v[i];
+    half_kick(s, hdt, 0);
+    for (int f = 0; f < 12; f++) axpy(s->q[f], s->p[f], dt, s->N3);
+    if (s->mf) {
+        if (!s->P.mf_lock)
+            for (int f = 0; f < 12; f++) axpy(s->fq[0][f], s->fp[0][f], dt, s->N3);
+        for (int f = 0; f < 12; f++) axpy(s->fq[1][f], s->fp[1][f], dt, s->N3);
     }
     if (s->P.gauge) {
         const double gad = -s->P.g * s->P.dx * dt;
@@ -290,8 +479,17 @@ static void verlet(orc_state *s) {
             for (long i = 0; i < s->N3; i++) th[i] = wrap_angle(th[i] + gad * E[i]);
         }
     }
+    if (s->g2on) {
+        const double gad2 = -s->P.g2 * s->P.dx * dt;
+        for (int c = 0; c < 3; c++) {
+            double *th = s->th2[c], *E = s->E2[c];
+#pragma omp parallel for schedule(static)
+            for (long i = 0; i < s->N3; i++) th[i] = wrap_angle(th[i] + gad2 * E[i]);
+        }
+    }
+    if (s->higgs) axpy(s->H, s->HV, dt, s->N3);
     forces(s);
-    half_kick(s, hdt);
+    half_kick(s, hdt, 1);
     if (s->P.bc_type == 0) damping(s);
 }
 
@@ -309,11 +507,27 @@ static inline double rho_at(const orc_state *s, long idx) {
     return r;
 }
 
+/* Noether density of fabric f (0 = Q, 1 = L) (fabric_rho_at, scp_sim.c:174-180) */
+static inline double fabric_rho(const orc_state *s, int f, long idx) {
+    double r = 0;
+    for (int a = 0; a < 3; a++)
+        r += s->fq[f][U0 + a][idx] * s->fp[f][V0 + a][idx] - s->fq[f][V0 + a][idx] * s->fp[f][U0 + a][idx]
+           + s->fq[f][TU0 + a][idx] * s->fp[f][TV0 + a][idx] - s->fq[f][TV0 + a][idx] * s->fp[f][TU0 + a][idx];
+    return r;
+}
+
+/* EM charge density: rho of fabric C, or sum_f q_f rho_f with three fabrics
+ * (em_rho_at, scp_sim.c:184-197) */
+static inline double em_rho_at(const orc_state *s, long idx) {
+    if (!s->mf) return rho_at(s, idx);
+    return s->P.q_fab[0] * rho_at(s, idx) + s->P.q_fab[1] * fabric_rho(s, 0, idx) + s->P.q_fab[2] * fabric_rho(s, 1, idx);
+}
+
 /* gauss_residual_at, scp_sim.c:2176-2181 */
 static inline double gauss_at(const orc_state *s, long idx, const nbr_t *n) {
     double divE = (s->E[0][idx] - s->E[0][n->im] + s->E[1][idx] - s->E[1][n->jm]
                    + s->E[2][idx] - s->E[2][n->km]) / s->P.dx;
-    return divE - s->P.g * rho_at(s, idx);
+    return divE - s->P.g * em_rho_at(s, idx);
 }
 
 /* net_charge_check, scp_sim.c:2264-2279: 0 when neutral */
@@ -322,30 +536,27 @@ static int net_charge_ok(const orc_state *s) {
     double qn = 0, qa = 0;
 #pragma omp parallel for reduction(+ : qn, qa) schedule(static)
     for (long idx = 0; idx < s->N3; idx++) {
-        double r = rho_at(s, idx);
+        double r = em_rho_at(s, idx);
         qn += r * dV;
         qa += fabs(r) * dV;
     }
     return !(fabs(qn) > 1e-6 * fmax(qa, 1.0));
 }
 
-/* init_gauss_project, scp_sim.c:2284-2400: CG on -lap chi = G - mean(G),
- * E += forward gradient of chi, freeze G_offset = mean(G) */
-static int gauss_project(orc_state *s) {
+/* The CG of init_gauss_project (scp_sim.c:2314-2366), also used by
+ * init_gauss2_project (:2430-2447): b -= mean(b); solve -lap chi = b on the
+ * periodic 7-point Laplacian to 1e-13 max(1, max|b|), chi kept zero-mean.
+ * Returns 0 with chi in xv, or -3 when 20000 iterations do not converge. */
+static int cg_poisson(const orc_state *s, double *b, double *xv, int *iters) {
     const int N = s->P.N;
     const long N3 = s->N3;
     const double dx = s->P.dx, idx2 = 1.0 / (dx * dx);
-    double *b = malloc(N3 * sizeof(double)), *xv = calloc(N3, sizeof(double));
     double *r = malloc(N3 * sizeof(double)), *pp = malloc(N3 * sizeof(double));
     double *Ap = malloc(N3 * sizeof(double));
-    if (!b || !xv || !r || !pp || !Ap) return -4;
+    if (!r || !pp || !Ap) { free(r); free(pp); free(Ap); return -4; }
     double gsum = 0, gmax0 = 0;
 #pragma omp parallel for reduction(+ : gsum) schedule(static)
-    for (long idx = 0; idx < N3; idx++) {
-        nbr_t n = nbrs(N, idx);
-        b[idx] = gauss_at(s, idx, &n);
-        gsum += b[idx];
-    }
+    for (long idx = 0; idx < N3; idx++) gsum += b[idx];
     double gbar = gsum / (double)N3;
 #pragma omp parallel for reduction(max : gmax0) schedule(static)
     for (long idx = 0; idx < N3; idx++) {
@@ -356,6 +567,7 @@ static int gauss_project(orc_state *s) {
     const double tol = 1e-13 * fmax(1.0, gmax0);
     memcpy(r, b, N3 * sizeof(double));
     memcpy(pp, b, N3 * sizeof(double));
+    memset(xv, 0, N3 * sizeof(double));
     double rz = 0;
 #pragma omp parallel for reduction(+ : rz) schedule(static)
     for (long idx = 0; idx < N3; idx++) rz += r[idx] * r[idx];
@@ -390,8 +602,26 @@ static int gauss_project(orc_state *s) {
         rmax = rm;
         it++;
     }
-    int ok = !(rmax > tol);
-    if (ok) {
+    *iters = it;
+    free(r); free(pp); free(Ap);
+    return (rmax > tol) ? -3 : 0;
+}
+
+/* init_gauss_project, scp_sim.c:2284-2400: CG on -lap chi = G - mean(G),
+ * E += forward gradient of chi, freeze G_offset = mean(G) */
+static int gauss_project(orc_state *s) {
+    const int N = s->P.N;
+    const long N3 = s->N3;
+    const double dx = s->P.dx;
+    double *b = malloc(N3 * sizeof(double)), *xv = malloc(N3 * sizeof(double));
+    if (!b || !xv) { free(b); free(xv); return -4; }
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        b[idx] = gauss_at(s, idx, &n);
+    }
+    int rc = cg_poisson(s, b, xv, &s->cg_iters);
+    if (rc == 0) {
 #pragma omp parallel for schedule(static)
         for (long idx = 0; idx < N3; idx++) {
             nbr_t n = nbrs(N, idx);
@@ -407,9 +637,44 @@ static int gauss_project(orc_state *s) {
         }
         s->G_offset = osum / (double)N3;
     }
-    s->cg_iters = it;
-    free(b); free(xv); free(r); free(pp); free(Ap);
-    return ok ? 0 : -3;
+    free(b); free(xv);
+    return rc;
+}
+
+/* gauss2_residual_at, scp_sim.c:2402-2412: div E2 - g2 sum_a q_a rho_a */
+static inline double gauss2_at(const orc_state *s, long idx, const nbr_t *n) {
+    double divE = (s->E2[0][idx] - s->E2[0][n->im] + s->E2[1][idx] - s->E2[1][n->jm]
+                   + s->E2[2][idx] - s->E2[2][n->km]) / s->P.dx;
+    double rho = 0;
+    for (int a = 0; a < 3; a++)
+        rho += s->P.q2[a] * (s->q[U0 + a][idx] * s->p[V0 + a][idx] - s->q[V0 + a][idx] * s->p[U0 + a][idx]
+                             + s->q[TU0 + a][idx] * s->p[TV0 + a][idx] - s->q[TV0 + a][idx] * s->p[TU0 + a][idx]);
+    return divE - s->P.g2 * rho;
+}
+
+/* init_gauss2_project, scp_sim.c:2414-2458: the same solve, correction into E2 */
+static int gauss2_project(orc_state *s) {
+    const int N = s->P.N;
+    const long N3 = s->N3;
+    const double dx = s->P.dx;
+    double *b = malloc(N3 * sizeof(double)), *xv = malloc(N3 * sizeof(double));
+    if (!b || !xv) { free(b); free(xv); return -4; }
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        b[idx] = gauss2_at(s, idx, &n);
+    }
+    int it = 0, rc = cg_poisson(s, b, xv, &it);
+    if (rc == 0)
+#pragma omp parallel for schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            nbr_t n = nbrs(N, idx);
+            s->E2[0][idx] += (xv[n.ip] - xv[idx]) / dx;
+            s->E2[1][idx] += (xv[n.jp] - xv[idx]) / dx;
+            s->E2[2][idx] += (xv[n.kp] - xv[idx]) / dx;
+        }
+    free(b); free(xv);
+    return rc;
 }
 
 /* ---------------------------------------------------------------- diagnostics */
@@ -505,6 +770,74 @@ static void diag_energy(orc_state *s, double *out) {
         double Pmod = sqrt(sp);
         if (Pmod > Pm) Pm = Pmod;
     }
+    /* v71 Higgs energy density (scp_sim.c:1970-1975): 1/2 Hdot^2 + 1/2 |grad H|^2
+     * + (lam/4)(H^2 - v^2)^2 + (kap/2) s H^2; joins E_total only */
+    double ehg = 0;
+    if (s->higgs) {
+        const double HV = P->higgs_v, HLAM = P->higgs_lam, HKAP = P->higgs_kap;
+#pragma omp parallel for reduction(+ : ehg) schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            nbr_t n = nbrs(N, idx);
+            double sp = 1.0;
+            for (int a = 0; a < 3; a++) sp *= U[a][idx] * U[a][idx] + Vv[a][idx] * Vv[a][idx];
+            double h = s->H[idx], hv = s->HV[idx];
+            double gx = (s->H[n.ip] - s->H[n.im]) * idx1, gy = (s->H[n.jp] - s->H[n.jm]) * idx1;
+            double gz = (s->H[n.kp] - s->H[n.km]) * idx1;
+            double hd = h * h - HV * HV;
+            ehg += (0.5 * hv * hv + 0.5 * (gx * gx + gy * gy + gz * gz) + 0.25 * HLAM * hd * hd
+                    + 0.5 * HKAP * sp * h * h) * dV;
+        }
+    }
+    /* v75 fabric L's matter energy with the unit-charge links (:1977-2028) */
+    if (s->mf) {
+        double *const *X = s->fq[1], *const *Pv = s->fp[1];
+        double l_epk = 0, l_eg = 0, l_em = 0, l_ep = 0, l_etk = 0, l_etg = 0, l_etm = 0, l_ec = 0;
+#pragma omp parallel for reduction(+ : l_epk, l_eg, l_em, l_ep, l_etk, l_etg, l_etm, l_ec) schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            nbr_t n = nbrs(N, idx);
+            long np[3] = {n.ip, n.jp, n.kp}, nm[3] = {n.im, n.jm, n.km};
+            double fu[6], fv[6];
+            for (int a = 0; a < 3; a++) {
+                fu[a] = X[U0 + a][idx]; fv[a] = X[V0 + a][idx];
+                fu[3 + a] = X[TU0 + a][idx]; fv[3 + a] = X[TV0 + a][idx];
+            }
+            double DcU[3][6], DcV[3][6];
+            for (int d = 0; d < 3; d++) {
+                double cP = s->lc[d][idx], sP = s->ls[d][idx];
+                double cM = s->lc[d][nm[d]], sM = s->ls[d][nm[d]];
+                for (int a = 0; a < 3; a++) {
+                    double upn = X[U0 + a][np[d]], vpn = X[V0 + a][np[d]];
+                    double umn = X[U0 + a][nm[d]], vmn = X[V0 + a][nm[d]];
+                    double tpn = X[TU0 + a][np[d]], wpn = X[TV0 + a][np[d]];
+                    double tmn = X[TU0 + a][nm[d]], wmn = X[TV0 + a][nm[d]];
+                    DcU[d][a] = ((cP * upn - sP * vpn) - (cM * umn + sM * vmn)) * idx1;
+                    DcV[d][a] = ((cP * vpn + sP * upn) - (cM * vmn - sM * umn)) * idx1;
+                    DcU[d][3 + a] = ((cP * tpn - sP * wpn) - (cM * tmn + sM * wmn)) * idx1;
+                    DcV[d][3 + a] = ((cP * wpn + sP * tpn) - (cM * wmn - sM * tmn)) * idx1;
+                }
+            }
+            double s2[3];
+            for (int a = 0; a < 3; a++) {
+                s2[a] = fu[a] * fu[a] + fv[a] * fv[a];
+                l_epk += 0.5 * (Pv[U0 + a][idx] * Pv[U0 + a][idx] + Pv[V0 + a][idx] * Pv[V0 + a][idx]) * dV;
+                l_etk += 0.5 * (Pv[TU0 + a][idx] * Pv[TU0 + a][idx] + Pv[TV0 + a][idx] * Pv[TV0 + a][idx]) * dV;
+                l_eg += 0.5 * (DcU[0][a] * DcU[0][a] + DcU[1][a] * DcU[1][a] + DcU[2][a] * DcU[2][a]
+                               + DcV[0][a] * DcV[0][a] + DcV[1][a] * DcV[1][a] + DcV[2][a] * DcV[2][a]) * dV;
+                l_em += 0.5 * MASS2 * s2[a] * dV;
+                l_etg += 0.5 * (DcU[0][3 + a] * DcU[0][3 + a] + DcU[1][3 + a] * DcU[1][3 + a]
+                                + DcU[2][3 + a] * DcU[2][3 + a] + DcV[0][3 + a] * DcV[0][3 + a]
+                                + DcV[1][3 + a] * DcV[1][3 + a] + DcV[2][3 + a] * DcV[2][3 + a]) * dV;
+                l_etm += 0.5 * MTHETA2 * (fu[3 + a] * fu[3 + a] + fv[3 + a] * fv[3 + a]) * dV;
+                double reDxT = DcU[ci1[a]][3 + ci2[a]] - DcU[ci2[a]][3 + ci1[a]];
+                double imDxT = DcV[ci1[a]][3 + ci2[a]] - DcV[ci2[a]][3 + ci1[a]];
+                l_ec -= ETA * (fu[a] * reDxT + fv[a] * imDxT) * dV;
+            }
+            double sp = s2[0] * s2[1] * s2[2];
+            l_ep += (MU / 2.0) * sp / (1.0 + KAPPA * sp) * dV;
+        }
+        epk += l_epk; etk += l_etk; eg += l_eg; em += l_em; ep += l_ep;
+        etg += l_etg; etm += l_etm; ec += l_ec;
+    }
     double trs = 0, pint = 0;
 #pragma omp parallel for reduction(+ : trs, pint) schedule(static)
     for (long i = 0; i < N3; i++) {
@@ -516,7 +849,7 @@ static void diag_energy(orc_state *s, double *out) {
     }
     out[0] = epk; out[1] = etk; out[2] = eg; out[3] = em; out[4] = ep;
     out[5] = etg; out[6] = etm; out[7] = ec;
-    out[8] = epk + etk + eg + em + ep + etg + etm + ec + eem;
+    out[8] = epk + etk + eg + em + ep + etg + etm + ec + eem + ehg;
     out[9] = pm; out[10] = Pm; out[11] = pint; out[12] = sqrt(trs / (6.0 * N3));
 }
 
@@ -641,24 +974,53 @@ static void diag_gauss(orc_state *s, double *out) {
     out[27] = (GG != 0) ? (fsum - OFF * (double)nC * dV) / GG : 0.0;
 }
 
+/* compute_mf_charges, scp_sim.c:2247-2261, into out[31..34] */
+static void diag_mf_charges(orc_state *s, double *out) {
+    const double dV = s->P.dx * s->P.dx * s->P.dx;
+    double sc = 0, sq = 0, sl = 0, se = 0;
+#pragma omp parallel for reduction(+ : sc, sq, sl, se) schedule(static)
+    for (long idx = 0; idx < s->N3; idx++) {
+        double rc = rho_at(s, idx), rq = fabric_rho(s, 0, idx), rl = fabric_rho(s, 1, idx);
+        sc += rc; sq += rq; sl += rl;
+        se += s->P.q_fab[0] * rc + s->P.q_fab[1] * rq + s->P.q_fab[2] * rl;
+    }
+    out[31] = sc * dV; out[32] = sq * dV; out[33] = sl * dV; out[34] = se * dV;
+}
+
 int orc_diag(orc_state *s, double *out) {
-    for (int i = 0; i < 31; i++) out[i] = 0.0;
+    const int n = s->mf ? 35 : 31;
+    for (int i = 0; i < n; i++) out[i] = 0.0;
     diag_energy(s, out);
     diag_charges(s, out);
     if (s->P.gauge) diag_gauss(s, out);
-    return 31;
+    if (s->mf) diag_mf_charges(s, out);
+    return n;
 }
 
 /* ---------------------------------------------------------------- lifecycle */
 
+/* fabric f (0 = Q, 1 = L) from 24 columns in the complex column order */
+static void fabric_in(orc_state *s, int f, const double *const *cols) {
+    size_t bytes = s->N3 * sizeof(double);
+    for (int a = 0; a < 3; a++) {
+        memcpy(s->fq[f][U0 + a], cols[0 + a], bytes);  memcpy(s->fq[f][TU0 + a], cols[3 + a], bytes);
+        memcpy(s->fp[f][U0 + a], cols[6 + a], bytes);  memcpy(s->fp[f][TU0 + a], cols[9 + a], bytes);
+        memcpy(s->fq[f][V0 + a], cols[12 + a], bytes); memcpy(s->fq[f][TV0 + a], cols[15 + a], bytes);
+        memcpy(s->fp[f][V0 + a], cols[18 + a], bytes); memcpy(s->fp[f][TV0 + a], cols[21 + a], bytes);
+    }
+}
+
 orc_state *orc_create(const orc_params *p, const double *const *cols, int project, int *status) {
     *status = 0;
     if (!p || p->N < 3 || p->dx <= 0 || p->dt <= 0 || (p->gauge && p->g == 0.0)) { *status = -1; return NULL; }
+    const int higgs = p->gauge && p->higgs_v > 0, g2on = p->gauge && p->g2 != 0, mf = p->gauge && p->n_fabrics == 3;
+    if (mf && (higgs || g2on)) { *status = -1; return NULL; }   /* cfg_validate, scp_config.h:522-534 */
     orc_state *s = calloc(1, sizeof(orc_state));
     if (!s) { *status = -4; return NULL; }
     s->P = *p;
     s->N3 = (long)p->N * p->N * p->N;
-    int nblk = 36 + (p->gauge ? 18 : 0);
+    s->higgs = higgs; s->g2on = g2on; s->mf = mf;
+    int nblk = 36 + (p->gauge ? 18 : 0) + (g2on ? 12 : 0) + (higgs ? 3 : 0) + (mf ? 72 : 0);
     s->mem = calloc((size_t)nblk * s->N3, sizeof(double));
     if (!s->mem) { free(s); *status = -4; return NULL; }
     double *m = s->mem;
@@ -670,6 +1032,17 @@ orc_state *orc_create(const orc_params *p, const double *const *cols, int projec
             s->th[c] = m; m += s->N3; s->E[c] = m; m += s->N3; s->K[c] = m; m += s->N3;
             s->lc[c] = m; m += s->N3; s->ls[c] = m; m += s->N3; s->ps[c] = m; m += s->N3;
         }
+    if (g2on)   /* th2 and E2 start at zero: the reference's SFA loader leaves them */
+        for (int c = 0; c < 3; c++) {
+            s->th2[c] = m; m += s->N3; s->E2[c] = m; m += s->N3;
+            s->K2[c] = m; m += s->N3; s->ps2[c] = m; m += s->N3;
+        }
+    if (higgs) { s->H = m; m += s->N3; s->HV = m; m += s->N3; s->HA = m; m += s->N3; }
+    if (mf)
+        for (int fb = 0; fb < 2; fb++)
+            for (int f = 0; f < 12; f++) {
+                s->fq[fb][f] = m; m += s->N3; s->fp[fb][f] = m; m += s->N3; s->fa[fb][f] = m; m += s->N3;
+            }
     /* column order -> packed slots */
     size_t bytes = s->N3 * sizeof(double);
     for (int a = 0; a < 3; a++) {
@@ -679,10 +1052,33 @@ orc_state *orc_create(const orc_params *p, const double *const *cols, int projec
         memcpy(s->p[V0 + a], cols[18 + a], bytes); memcpy(s->p[TV0 + a], cols[21 + a], bytes);
         if (p->gauge) { memcpy(s->th[a], cols[24 + a], bytes); memcpy(s->E[a], cols[27 + a], bytes); }
     }
+    /* the start-up of main (scp_sim.c:2802-2836): Higgs start value, fabrics
+     * (mf_post_init: Q is C under the lock), net charge, Gauss projections */
+    if (higgs) {
+        const int N = p->N;
+        const long NN = (long)N * N;
+        for (long idx = 0; idx < s->N3; idx++) {
+            double h = p->higgs_v;
+            if (p->higgs_rvoid > 0.0) {
+                int i = (int)(idx / NN), j = (int)((idx / N) % N), k = (int)(idx % N);
+                double x = -p->L + i * p->dx, y = -p->L + j * p->dx, z = -p->L + k * p->dx;
+                double r = sqrt(x * x + y * y + z * z);
+                h = p->higgs_v * 0.5 * (1.0 + tanh((r - p->higgs_rvoid) / 0.6));
+            }
+            s->H[idx] = h;
+            s->HV[idx] = 0.0;
+        }
+    }
+    if (mf) {
+        fabric_in(s, 1, cols + 54);
+        if (p->mf_lock) lock_copy(s);
+        else fabric_in(s, 0, cols + 30);
+    }
     if (p->gauge) {
         if (p->bc_type == 2 && !net_charge_ok(s)) { orc_free(s); *status = -2; return NULL; }
         if (project) {
             int rc = gauss_project(s);
+            if (!rc && g2on) rc = gauss2_project(s);
             if (rc) { orc_free(s); *status = rc; return NULL; }
         }
     }
@@ -704,6 +1100,14 @@ void orc_get(const orc_state *s, double *const *cols) {
         memcpy(cols[12 + a], s->q[V0 + a], bytes); memcpy(cols[15 + a], s->q[TV0 + a], bytes);
         memcpy(cols[18 + a], s->p[V0 + a], bytes); memcpy(cols[21 + a], s->p[TV0 + a], bytes);
         if (s->P.gauge) { memcpy(cols[24 + a], s->th[a], bytes); memcpy(cols[27 + a], s->E[a], bytes); }
+        if (s->g2on) { memcpy(cols[30 + a], s->th2[a], bytes); memcpy(cols[33 + a], s->E2[a], bytes); }
+        if (s->mf) {   /* fabric L after C, the complex column order */
+            double *const *L = cols + 30;
+            memcpy(L[0 + a], s->fq[1][U0 + a], bytes);  memcpy(L[3 + a], s->fq[1][TU0 + a], bytes);
+            memcpy(L[6 + a], s->fp[1][U0 + a], bytes);  memcpy(L[9 + a], s->fp[1][TU0 + a], bytes);
+            memcpy(L[12 + a], s->fq[1][V0 + a], bytes); memcpy(L[15 + a], s->fq[1][TV0 + a], bytes);
+            memcpy(L[18 + a], s->fp[1][V0 + a], bytes); memcpy(L[21 + a], s->fp[1][TV0 + a], bytes);
+        }
     }
 }
 

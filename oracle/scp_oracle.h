@@ -15,6 +15,9 @@
  *   21-23 thetaim_v{x,y,z}
  *   24-26 th_{x,y,z}       (link angles, gauged only)
  *   27-29 E_{x,y,z}        (link electric field, gauged only)
+ *   30-35 th2_*, E2_*      (orc_get only, second gauge on)
+ * Three fabrics: orc_create takes 30 + 24 (Q) + 24 (L) columns, orc_get
+ * returns the 30 of C and the 24 of L (the reference's archive schema).
  *
  * Diagnostic slots (orc_diag) follow the reference diag TSV column order
  * (sfa/sim/scp_sim.c:2993-3003) without the leading time column; see
@@ -35,6 +38,15 @@ typedef struct {
     int bc_type;        /* 0 absorbing sphere, 2 periodic */
     double damp_width, damp_rate;
     double qdiag_radius, qdiag_probe1, qdiag_probe2;
+    /* gauged extensions (gauge = 1 only; all zero = off): Higgs condensate
+     * (higgs_v > 0) and second compact U(1) gauge (g2 != 0, charges q2[]);
+     * three matter fabrics (n_fabrics = 3, EM charges q_fab[] = q_C, q_Q, q_L,
+     * mf_lock = 1 keeps Q a copy of C as the reference does) */
+    double higgs_v, higgs_lam, higgs_kap, higgs_rvoid;
+    double g2;
+    double q2[3];
+    int n_fabrics, mf_lock;
+    double q_fab[3];
 } orc_params;
 
 typedef struct orc_state orc_state;
@@ -48,7 +60,8 @@ orc_state *orc_create(const orc_params *p, const double *const *cols, int projec
 void orc_free(orc_state *s);
 void orc_step(orc_state *s, int nsteps);
 void orc_get(const orc_state *s, double *const *cols);
-/* 31 diagnostics in TSV order (see header comment); returns slot count */
+/* 31 diagnostics in TSV order (see header comment), then Q_C, Q_Q, Q_L,
+ * Q_em with three fabrics (35); returns the slot count */
 int orc_diag(orc_state *s, double *out);
 double orc_g_offset(const orc_state *s);
 int orc_cg_iterations(const orc_state *s);

@@ -89,3 +89,35 @@ def test_three_fabric_covariance(gpu, lock, q):
         assert close(A[c], B[c], 1e-11), c
     for key in ("Q_C", "Q_Q", "Q_L", "Q_em", "gauss_max", "E_em"):
         assert abs(da[key] - db[key]) <= 1e-10 * max(abs(da[key]), 1.0), key
+
+
+EXT_CASES = [("gext", 9), ("gext", 20), ("mf_lock", 9), ("mf_free", 20)]
+
+
+@pytest.mark.parametrize("kind,N", EXT_CASES)
+def test_extensions_match_oracle_in_chunks(gpu, kind, N):
+    """The extension steppers against the C restatement (oracle/scp_oracle.c,
+    itself pinned to the reference binary) after 1, 5 and 12 steps, grids the
+    reference comparisons do not use."""
+    import oracle
+    if kind == "gext":
+        st = seeds.small_state(N, True, seed=N, higgs_v=1.0, higgs_rvoid=1.5, g_gauge2=0.2, gauge2_q0=1.0,
+                               gauge2_q1=-1.0, gauge2_q2=0.0)
+    elif kind == "mf_lock":
+        st = seeds.mf_state(N, seed=N, q_C=0.5)
+    else:
+        st = seeds.mf_state(N, seed=N, shift=1.0, mf_lock_CQ=0, l_charge=0.02, bc_type=0, damp_width=3.0,
+                            damp_rate=0.05)
+    p = st.params
+    o = oracle.Oracle(p, st.cols())
+    with Simulation(p, st.cols()) as sim:
+        for chunk in (1, 4, 7):
+            sim.step(chunk)
+            o.step(chunk)
+            got, want = sim.snapshot(), o.cols()
+            assert len(got) == len(want) == p.snap_ncols
+            for c in range(len(got)):
+                a, b = got[c], want[c]
+                nb = np.linalg.norm(b)
+                err = np.linalg.norm(a - b) / nb if nb > 0 else np.linalg.norm(a - b)
+                assert err < 1e-10, (chunk, c)

@@ -96,3 +96,82 @@ def test_gauge_xform_kat_oracle():
     o = oracle.Oracle(st.params, st.cols())
     worst, rel = o.gauge_xform_test()
     assert worst <= 1e-12, rel
+
+
+# ------------------------------------------------------------ gauged extensions
+
+EXT = ["ref_higgs_gauge2_n12", "ref_higgs_gauge2_n11_damped", "ref_mf_lock_n12", "ref_mf_free_n11_damped"]
+ROUNDOFF = ("gauss_max", "gauss_l2", "Q_flux", "Q_phi", "Q_theta", "Q_total", "Q_core", "Q_p0", "Q_p1", "Q_p2",
+            "E_coupling", "Q_C", "Q_Q", "Q_L", "Q_em")
+ORC_NAMES = ("E_phi_kin", "E_theta_kin", "E_grad", "E_mass", "E_pot", "E_tgrad", "E_tmass", "E_coupling",
+             "E_total", "phi_max", "P_max", "P_int", "theta_rms", "Q_phi", "Q_theta", "Q_total", "s_max",
+             "r_core", "omega_core", "Q_core", "thp1u", "thp1v", "thp2u", "thp2v", "gauss_max", "gauss_l2",
+             "E_em", "Q_flux", "Q_p0", "Q_p1", "Q_p2", "Q_C", "Q_Q", "Q_L", "Q_em")
+
+
+def ext_state(f):
+    import json
+    if "kw" in f.files:
+        return seeds.mf_state(int(f["N"]), **json.loads(str(f["kw"])))
+    return seeds.small_state(int(f["N"]), True, **json.loads(str(f["over"])))
+
+
+def check_series(rows, want_rows, header):
+    """Oracle diag vectors against the reference TSV rows, matched by name."""
+    want = np.asarray(want_rows)
+    have = np.array(rows)
+    for ci, h in enumerate(header):
+        if h == "t":
+            continue
+        ref, got = want[:, ci], have[:, ORC_NAMES.index(h)]
+        scale = np.maximum(np.abs(ref), 1e-9)
+        tol = np.maximum(1e-5 * scale, 1e-11) if h in ROUNDOFF else 2e-6 * scale
+        assert np.all(np.abs(got - ref) <= tol), h
+
+
+@pytest.mark.parametrize("name", EXT)
+def test_oracle_matches_reference_extensions(name):
+    """Higgs condensate + second gauge, and three fabrics (locked and free Q):
+    the restatement against the reference's frames (36 / 54 columns) and every
+    diag TSV column."""
+    f = load(name)
+    st = ext_state(f)
+    o = oracle.Oracle(st.params, st.cols())
+    rows = [o.diag()]
+    every = int(f["diag_every"])
+    for _ in range(int(f["nsteps"]) // every):
+        o.step(every)
+        rows.append(o.diag())
+    got = o.cols()
+    assert len(got) == f["final"].shape[0] == st.params.snap_ncols
+    for c in range(len(got)):
+        assert rel_l2(got[c], f["final"][c]) < 1e-12, (name, str(f["names"][c]))
+    check_series(rows, f["diag"], [str(h) for h in f["diag_header"]])
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference binary not built (make -C oracle ref)")
+@pytest.mark.parametrize("kind", ["higgs", "gauge2", "mf_lock", "mf_free"])
+def test_oracle_matches_reference_binary_extensions(kind):
+    """Each extension on its own at another size, seed and set of couplings,
+    the restatement against the reference binary run here."""
+    if kind == "higgs":
+        st = seeds.small_state(14, True, seed=5, higgs_v=0.9, higgs_rvoid=2.0, higgs_lam=1.3, higgs_kap=2.5)
+    elif kind == "gauge2":
+        st = seeds.small_state(13, True, seed=6, g_gauge2=-0.25, gauge2_q0=0.5, gauge2_q1=2.0, gauge2_q2=-1.0)
+    elif kind == "mf_lock":
+        st = seeds.mf_state(13, seed=7, shift=1.0, q_C=0.4, q_Q=1.0, q_L=-2.0)
+    else:
+        st = seeds.mf_state(14, seed=8, shift=-1.5, mf_lock_CQ=0, l_charge=0.03, bc_type=0, damp_width=2.0,
+                            damp_rate=0.04)
+    p = st.params
+    ref = oracle.run_reference(p, st.cols(), 30, diag_every=10)
+    o = oracle.Oracle(p, st.cols())
+    rows = [o.diag()]
+    for _ in range(3):
+        o.step(10)
+        rows.append(o.diag())
+    got = o.cols()
+    assert len(got) == len(ref["cols"])
+    for c in range(len(got)):
+        assert rel_l2(got[c], ref["cols"][c]) < 1e-12, (kind, ref["names"][c])
+    check_series(rows, ref["diag"], ref["diag_header"])
