@@ -70,6 +70,20 @@ def mf_case(name: str, N: int, nsteps: int, diag_every: int, **kw):
     print(name, "written", r["wall_ms_per_step"], "ms/step")
 
 
+def real_case(name: str, N: int, nsteps: int, diag_every: int, **over):
+    """The real 6-field mode (complex_phi = 0), with optional terms when given:
+    the 12-column final frame and the diag rows."""
+    st = seeds.real_state(N, **over)
+    p = st.params
+    r = oracle.run_reference(p, st.cols(), nsteps, diag_every=diag_every, threads=os.cpu_count())
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        N=N, nsteps=nsteps, diag_every=diag_every, over=json.dumps(over),
+        final=np.stack(r["cols"]), diag=r["diag"], diag_header=np.array(r["diag_header"]),
+        names=np.array(r["names"]))
+    print(name, "written", r["wall_ms_per_step"], "ms/step")
+
+
 def workload_case(name: str, wl: str, nsteps: int, diag_every: int):
     st = seeds.make_state(wl)
     p = st.params
@@ -93,6 +107,9 @@ if __name__ == "__main__":
     gext_case("ref_higgs_gauge2_n12", 12, 60, 10, seed=41, higgs_v=1.0, higgs_rvoid=2.0, g_gauge2=0.2)
     gext_case("ref_higgs_gauge2_n11_damped", 11, 40, 10, seed=43, higgs_v=0.8, higgs_lam=0.5, higgs_kap=1.5,
               g_gauge2=-0.15, gauge2_q0=1.0, gauge2_q1=-1.0, gauge2_q2=0.5,
+              bc_type=0, damp_width=2.0, damp_rate=0.05)
+    real_case("ref_real_n12", 12, 60, 10, seed=91)
+    real_case("ref_real_terms_n11_damped", 11, 40, 10, seed=92, mode=3, alpha_cs=0.2, beta_h=0.3, kappa_h=0.1,
               bc_type=0, damp_width=2.0, damp_rate=0.05)
     mf_case("ref_mf_lock_n12", 12, 40, 10, seed=81, shift=1.5)
     mf_case("ref_mf_free_n11_damped", 11, 40, 10, seed=83, shift=-1.0, l_charge=0.05, mf_lock_CQ=0,

@@ -179,6 +179,30 @@ def test_real_mode_optional_terms_match_reference_binary(gpu, reference, terms):
     assert np.all(np.abs(have - want) <= 2e-6 * np.abs(want) + 1e-12)
 
 
+@pytest.mark.parametrize("name", ["ref_real_n12", "ref_real_terms_n11_damped"])
+def test_real_mode_matches_golden(gpu, name):
+    """The real 6-field mode, plain and with every optional term under the
+    sponge, against frames and diag rows the reference binary recorded
+    (tests/golden/make_golden.py)."""
+    import json
+    f = np.load(os.path.join(GOLD, name + ".npz"))
+    st = seeds.real_state(int(f["N"]), **json.loads(str(f["over"])))
+    p = st.params
+    every = int(f["diag_every"])
+    rows = []
+    with Simulation(p, st.cols()) as sim:
+        rows.append(sim.diag_vector())
+        for _ in range(int(f["nsteps"]) // every):
+            sim.step(every)
+            rows.append(sim.diag_vector())
+        got = sim.snapshot()
+    assert len(got) == 12 == f["final"].shape[0]
+    assert worst_rel(got, f["final"]) < 1e-11
+    want = np.asarray(f["diag"])[:, 1:]
+    have = np.array(rows)[:, :want.shape[1]]
+    assert np.all(np.abs(have - want) <= 2e-6 * np.abs(want) + 1e-12)
+
+
 def test_real_mode_fp32c_tracks_fp64(gpu):
     """FP32-compensated real mode against the FP64 real mode after 100 steps."""
     from scp_b200 import PREC_FP32C

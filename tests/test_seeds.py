@@ -108,3 +108,17 @@ def test_three_fabric_params_and_fixtures():
         assert f["final"].shape == (54, int(f["N"]) ** 3) and np.all(np.isfinite(f["final"]))
         assert np.abs(f["final"][30:54]).max() > 0               # fabric L evolved
         assert list(f["diag_header"][-7:-3]) == ["Q_C", "Q_Q", "Q_L", "Q_em"]
+
+
+def test_real_mode_fixtures():
+    """The real-mode fixtures hold the reference's 12-column frames and its
+    real-mode diag TSV (energies and amplitudes only)."""
+    import json
+    import os
+    gold = os.path.join(os.path.dirname(__file__), "golden")
+    for name in ("ref_real_n12", "ref_real_terms_n11_damped"):
+        f = np.load(os.path.join(gold, name + ".npz"))
+        st = seeds.real_state(int(f["N"]), **json.loads(str(f["over"])))
+        assert f["final"].shape == (12, int(f["N"]) ** 3) and np.all(np.isfinite(f["final"]))
+        assert list(f["names"])[:3] == ["phi_x", "phi_y", "phi_z"] and len(f["diag_header"]) == 14
+        assert st.params.real_fields == 1 and len(st.cols()) == 12
