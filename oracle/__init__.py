@@ -39,6 +39,9 @@ class OrcParams(ctypes.Structure):
         ("higgs_v", ctypes.c_double), ("higgs_lam", ctypes.c_double), ("higgs_kap", ctypes.c_double),
         ("higgs_rvoid", ctypes.c_double), ("g2", ctypes.c_double), ("q2", ctypes.c_double * 3),
         ("n_fabrics", ctypes.c_int), ("mf_lock", ctypes.c_int), ("q_fab", ctypes.c_double * 3),
+        ("real_fields", ctypes.c_int), ("mode", ctypes.c_int), ("inv_alpha", ctypes.c_double),
+        ("inv_beta", ctypes.c_double), ("kappa_gamma", ctypes.c_double), ("alpha_cs", ctypes.c_double),
+        ("beta_h", ctypes.c_double), ("kappa_h", ctypes.c_double),
     ]
 
 
@@ -93,6 +96,10 @@ def _orc_params(p) -> OrcParams:
     o.n_fabrics, o.mf_lock = getattr(p, "n_fabrics", 1), getattr(p, "mf_lock_CQ", 1)
     for a, k in enumerate(("q_C", "q_Q", "q_L")):
         o.q_fab[a] = getattr(p, k, (0.0, 1.0, -1.0)[a])
+    o.real_fields, o.mode = getattr(p, "real_fields", 0), getattr(p, "mode", 0)
+    for k, d in (("inv_alpha", 2.25), ("inv_beta", 5.0), ("kappa_gamma", 2.0), ("alpha_cs", 0.0),
+                 ("beta_h", 0.0), ("kappa_h", 0.0)):
+        setattr(o, k, getattr(p, k, d))
     return o
 
 

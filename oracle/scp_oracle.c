@@ -3,7 +3,8 @@
  * CPU restatement of the reference's complex (v66) and gauged (v69) lattice
  * leapfrog stepper, kardianos/scp sfa/sim/scp_sim.c, with the gauged
  * extensions (v71 Higgs condensate and second U(1) gauge, v75 three matter
- * fabrics), bc_type 0 (absorbing sphere) or 2 (periodic).  It is the
+ * fabrics) and the real 6-field mode with its optional terms, bc_type 0
+ * (absorbing sphere) or 2 (periodic).  It is the
  * checker for the CUDA library's parity tests and is never part of the
  * product.  Parity of this restatement is pinned against the reference
  * binary itself (oracle/_ref/scp_sim, built from the reference sources by
@@ -37,7 +38,8 @@ struct orc_state {
     double *q[12], *p[12], *a[12];   /* positions, velocities, accelerations (fabric C) */
     double *th[3], *E[3], *K[3];     /* links, electric field, E-kick */
     double *lc[3], *ls[3], *ps[3];   /* scratch: link cos/sin, plaquette sines */
-    int higgs, g2on, mf;             /* extensions present */
+    int higgs, g2on, mf, real;       /* extensions present; real 6-field mode */
+    double *mis[3], *hq[3];          /* real mode scratch: Cosserat mismatch, hardening vector */
     double *th2[3], *E2[3], *K2[3], *ps2[3];   /* second gauge */
     double *H, *HV, *HA;                       /* Higgs field, velocity, acceleration */
     double *fq[2][12], *fp[2][12], *fa[2][12]; /* fabrics Q (0) and L (1) */
@@ -403,8 +405,104 @@ static void forces_mf(orc_state *s) {
     if (P->mf_lock) lock_copy(s);
 }
 
+/* compute_forces, scp_sim.c:743-929: the real 6-field mode (phi = u, theta =
+ * tu; v = tv = 0), its mass modes 1 and 3, chiral helicity kappa_h, Cosserat
+ * strain alpha_cs and curl-squared hardening beta_h (two passes over the
+ * mismatch M and hardening vector Q) */
+static void forces_real(orc_state *s) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long N3 = s->N3;
+    const double idx2 = 1.0 / (P->dx * P->dx), idx1 = 1.0 / (2.0 * P->dx);
+    const double MU = P->mu, KAPPA = P->kappa, MASS2 = P->m2, MTHETA2 = P->mtheta2, ETA = P->eta;
+    const double KH = P->kappa_h, ACS = P->alpha_cs, BH = P->beta_h;
+    const int MODE = P->mode;
+    const double KG = P->kappa_gamma, IA = P->inv_alpha, IB = P->inv_beta;
+    double *const *phi = s->q + U0, *const *th = s->q + TU0;
+    if (ACS != 0 || BH != 0) {
+#pragma omp parallel for schedule(static)
+        for (long idx = 0; idx < N3; idx++) {
+            nbr_t n = nbrs(N, idx);
+            double cp0 = curl_a(phi, 0, &n, idx1), cp1 = curl_a(phi, 1, &n, idx1), cp2 = curl_a(phi, 2, &n, idx1);
+            if (ACS != 0) {
+                s->mis[0][idx] = cp0 * 0.5 - th[0][idx];
+                s->mis[1][idx] = cp1 * 0.5 - th[1][idx];
+                s->mis[2][idx] = cp2 * 0.5 - th[2][idx];
+            }
+            if (BH != 0) {
+                double t0 = th[0][idx], t1 = th[1][idx], t2 = th[2][idx];
+                double T2 = t0 * t0 + t1 * t1 + t2 * t2;
+                double coeff = 0.5 * BH * T2;
+                s->hq[0][idx] = coeff * cp0;
+                s->hq[1][idx] = coeff * cp1;
+                s->hq[2][idx] = coeff * cp2;
+            }
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        double p0 = phi[0][idx], p1 = phi[1][idx], p2 = phi[2][idx];
+        double sig = p0 * p0 + p1 * p1 + p2 * p2;
+        double me2 = (MODE == 1) ? IA / (1.0 + IB * sig) : MASS2;
+        double keff = (MODE == 3) ? KAPPA / (1.0 + KG * sig) : KAPPA;
+        double Pp = p0 * p1 * p2, P2 = Pp * Pp;
+        double den = 1.0 + keff * P2;
+        double dVdP = MU * Pp / (den * den);
+        double t2c = 0;
+        if (MODE == 3 && KG > 0) {
+            double D = 1.0 + KG * sig + KAPPA * P2;
+            t2c = MU * KG * KAPPA * P2 * P2 / (D * D);
+        }
+        double curl_phi[3] = {curl_a(phi, 0, &n, idx1), curl_a(phi, 1, &n, idx1), curl_a(phi, 2, &n, idx1)};
+        double h = p0 * curl_phi[0] + p1 * curl_phi[1] + p2 * curl_phi[2];
+        double dP2dx = 0, dP2dy = 0, dP2dz = 0;
+        if (KH != 0) {
+            double Pip = phi[0][n.ip] * phi[1][n.ip] * phi[2][n.ip], Pim = phi[0][n.im] * phi[1][n.im] * phi[2][n.im];
+            double Pjp = phi[0][n.jp] * phi[1][n.jp] * phi[2][n.jp], Pjm = phi[0][n.jm] * phi[1][n.jm] * phi[2][n.jm];
+            double Pkp = phi[0][n.kp] * phi[1][n.kp] * phi[2][n.kp], Pkm = phi[0][n.km] * phi[1][n.km] * phi[2][n.km];
+            dP2dx = (Pip * Pip - Pim * Pim) * idx1;
+            dP2dy = (Pjp * Pjp - Pjm * Pjm) * idx1;
+            dP2dz = (Pkp * Pkp - Pkm * Pkm) * idx1;
+        }
+        double curl_M[3] = {0, 0, 0}, curl_Q[3] = {0, 0, 0};
+        if (ACS != 0)
+            for (int a = 0; a < 3; a++) curl_M[a] = curl_a(s->mis, a, &n, idx1);
+        if (BH != 0)
+            for (int a = 0; a < 3; a++) curl_Q[a] = curl_a(s->hq, a, &n, idx1);
+        double curl_sq = curl_phi[0] * curl_phi[0] + curl_phi[1] * curl_phi[1] + curl_phi[2] * curl_phi[2];
+        for (int a = 0; a < 3; a++) {
+            double lap = (phi[a][n.ip] + phi[a][n.im] + phi[a][n.jp] + phi[a][n.jm] + phi[a][n.kp] + phi[a][n.km]
+                          - 6.0 * phi[a][idx]) * idx2;
+            double dPda = (a == 0) ? p1 * p2 : (a == 1) ? p0 * p2 : p0 * p1;
+            double ct = curl_a(th, a, &n, idx1);
+            double chiral = 0;
+            if (KH != 0) {
+                double t1 = 2.0 * Pp * dPda * h, t2 = 2.0 * P2 * curl_phi[a], t3;
+                if (a == 0) t3 = -(dP2dz * p1 - dP2dy * p2);
+                else if (a == 1) t3 = -(dP2dx * p2 - dP2dz * p0);
+                else t3 = -(dP2dy * p0 - dP2dx * p1);
+                chiral = KH * (t1 + t2 + t3);
+            }
+            double cosserat_phi = -ACS * curl_M[a];
+            double harden_phi = -2.0 * curl_Q[a];
+            s->a[U0 + a][idx] = lap - me2 * phi[a][idx] - dVdP * dPda - t2c * phi[a][idx] + ETA * ct + chiral
+                              + cosserat_phi + harden_phi;
+        }
+        for (int a = 0; a < 3; a++) {
+            double lapt = (th[a][n.ip] + th[a][n.im] + th[a][n.jp] + th[a][n.jm] + th[a][n.kp] + th[a][n.km]
+                           - 6.0 * th[a][idx]) * idx2;
+            double cp = curl_a(phi, a, &n, idx1);
+            double cosserat_theta = (ACS != 0) ? 2.0 * ACS * s->mis[a][idx] : 0.0;
+            double harden_theta = -BH * curl_sq * th[a][idx];
+            s->a[TU0 + a][idx] = lapt - MTHETA2 * th[a][idx] + ETA * cp + cosserat_theta + harden_theta;
+        }
+    }
+}
+
 static void forces(orc_state *s) {
-    if (s->mf) forces_mf(s);
+    if (s->real) forces_real(s);
+    else if (s->mf) forces_mf(s);
     else if (s->P.gauge) forces_gauge(s);
     else forces_complex(s);
 }
@@ -974,6 +1072,76 @@ static void diag_gauss(orc_state *s, double *out) {
     out[27] = (GG != 0) ? (fsum - OFF * (double)nC * dV) / GG : 0.0;
 }
 
+/* compute_energy, theta_rms and P_integrated of the real mode
+ * (scp_sim.c:1722-1816) into out[0..12] */
+static void diag_energy_real(orc_state *s, double *out) {
+    const orc_params *P = &s->P;
+    const int N = P->N;
+    const long N3 = s->N3;
+    const double dx = P->dx, dV = dx * dx * dx, idx1 = 1.0 / (2.0 * dx);
+    const double MU = P->mu, KAPPA = P->kappa, MASS2 = P->m2, MTHETA2 = P->mtheta2, ETA = P->eta;
+    const int MODE = P->mode;
+    const double KG = P->kappa_gamma;
+    double *const *phi = s->q + U0, *const *th = s->q + TU0, *const *pv = s->p + U0, *const *tv = s->p + TU0;
+    double epk = 0, etk = 0, eg = 0, em = 0, ep = 0, etg = 0, etm = 0, ec = 0, pm = 0, Pm = 0;
+#pragma omp parallel for reduction(+ : epk, etk, eg, em, ep, etg, etm, ec) reduction(max : pm, Pm) schedule(static)
+    for (long idx = 0; idx < N3; idx++) {
+        nbr_t n = nbrs(N, idx);
+        double p0 = phi[0][idx], p1 = phi[1][idx], p2 = phi[2][idx];
+        double sig = p0 * p0 + p1 * p1 + p2 * p2;
+        double me2 = (MODE == 1) ? P->inv_alpha / (1.0 + P->inv_beta * sig) : MASS2;
+        double keff = (MODE == 3) ? KAPPA / (1.0 + KG * sig) : KAPPA;
+        for (int a = 0; a < 3; a++) {
+            epk += 0.5 * pv[a][idx] * pv[a][idx] * dV;
+            etk += 0.5 * tv[a][idx] * tv[a][idx] * dV;
+            double gx = (phi[a][n.ip] - phi[a][n.im]) * idx1, gy = (phi[a][n.jp] - phi[a][n.jm]) * idx1;
+            double gz = (phi[a][n.kp] - phi[a][n.km]) * idx1;
+            eg += 0.5 * (gx * gx + gy * gy + gz * gz) * dV;
+            em += 0.5 * me2 * phi[a][idx] * phi[a][idx] * dV;
+            double tgx = (th[a][n.ip] - th[a][n.im]) * idx1, tgy = (th[a][n.jp] - th[a][n.jm]) * idx1;
+            double tgz = (th[a][n.kp] - th[a][n.km]) * idx1;
+            etg += 0.5 * (tgx * tgx + tgy * tgy + tgz * tgz) * dV;
+            etm += 0.5 * MTHETA2 * th[a][idx] * th[a][idx] * dV;
+            double ap = fabs(phi[a][idx]);
+            if (ap > pm) pm = ap;
+        }
+        double Pp = p0 * p1 * p2, P2 = Pp * Pp;
+        if (MODE == 3) {
+            double D = 1.0 + KG * sig + KAPPA * P2;
+            ep += (MU / 2.0) * P2 * (1.0 + KG * sig) / D * dV;
+        } else {
+            ep += (MU / 2.0) * P2 / (1.0 + keff * P2) * dV;
+        }
+        double Pa = fabs(Pp);
+        if (Pa > Pm) Pm = Pa;
+        double cx0 = curl_a(phi, 0, &n, idx1), cx1 = curl_a(phi, 1, &n, idx1), cx2 = curl_a(phi, 2, &n, idx1);
+        if (P->alpha_cs != 0) {   /* alpha |curl(phi)/2 - theta|^2 */
+            double m0 = cx0 * 0.5 - th[0][idx], m1 = cx1 * 0.5 - th[1][idx], m2c = cx2 * 0.5 - th[2][idx];
+            ep += P->alpha_cs * (m0 * m0 + m1 * m1 + m2c * m2c) * dV;
+        }
+        if (P->beta_h != 0) {     /* (beta/2) |theta|^2 |curl phi|^2 */
+            double csq = cx0 * cx0 + cx1 * cx1 + cx2 * cx2;
+            double T2 = th[0][idx] * th[0][idx] + th[1][idx] * th[1][idx] + th[2][idx] * th[2][idx];
+            ep += 0.5 * P->beta_h * T2 * csq * dV;
+        }
+        if (P->kappa_h != 0) {    /* kappa_h P^2 phi . curl phi */
+            double hel = p0 * cx0 + p1 * cx1 + p2 * cx2;
+            ep += P->kappa_h * P2 * hel * dV;
+        }
+        for (int a = 0; a < 3; a++) ec -= ETA * phi[a][idx] * curl_a(th, a, &n, idx1) * dV;
+    }
+    double trs = 0, pint = 0;
+#pragma omp parallel for reduction(+ : trs, pint) schedule(static)
+    for (long i = 0; i < N3; i++) {
+        for (int a = 0; a < 3; a++) trs += th[a][i] * th[a][i];
+        pint += fabs(phi[0][i] * phi[1][i] * phi[2][i]) * dV;
+    }
+    out[0] = epk; out[1] = etk; out[2] = eg; out[3] = em; out[4] = ep;
+    out[5] = etg; out[6] = etm; out[7] = ec;
+    out[8] = epk + etk + eg + em + ep + etg + etm + ec;
+    out[9] = pm; out[10] = Pm; out[11] = pint; out[12] = sqrt(trs / (3.0 * N3));
+}
+
 /* compute_mf_charges, scp_sim.c:2247-2261, into out[31..34] */
 static void diag_mf_charges(orc_state *s, double *out) {
     const double dV = s->P.dx * s->P.dx * s->P.dx;
@@ -988,6 +1156,11 @@ static void diag_mf_charges(orc_state *s, double *out) {
 }
 
 int orc_diag(orc_state *s, double *out) {
+    if (s->real) {
+        for (int i = 0; i < 13; i++) out[i] = 0.0;
+        diag_energy_real(s, out);
+        return 13;
+    }
     const int n = s->mf ? 35 : 31;
     for (int i = 0; i < n; i++) out[i] = 0.0;
     diag_energy(s, out);
@@ -1014,13 +1187,15 @@ orc_state *orc_create(const orc_params *p, const double *const *cols, int projec
     *status = 0;
     if (!p || p->N < 3 || p->dx <= 0 || p->dt <= 0 || (p->gauge && p->g == 0.0)) { *status = -1; return NULL; }
     const int higgs = p->gauge && p->higgs_v > 0, g2on = p->gauge && p->g2 != 0, mf = p->gauge && p->n_fabrics == 3;
+    const int real = p->real_fields != 0;
     if (mf && (higgs || g2on)) { *status = -1; return NULL; }   /* cfg_validate, scp_config.h:522-534 */
+    if (real && p->gauge) { *status = -1; return NULL; }
     orc_state *s = calloc(1, sizeof(orc_state));
     if (!s) { *status = -4; return NULL; }
     s->P = *p;
     s->N3 = (long)p->N * p->N * p->N;
-    s->higgs = higgs; s->g2on = g2on; s->mf = mf;
-    int nblk = 36 + (p->gauge ? 18 : 0) + (g2on ? 12 : 0) + (higgs ? 3 : 0) + (mf ? 72 : 0);
+    s->higgs = higgs; s->g2on = g2on; s->mf = mf; s->real = real;
+    int nblk = 36 + (p->gauge ? 18 : 0) + (g2on ? 12 : 0) + (higgs ? 3 : 0) + (mf ? 72 : 0) + (real ? 6 : 0);
     s->mem = calloc((size_t)nblk * s->N3, sizeof(double));
     if (!s->mem) { free(s); *status = -4; return NULL; }
     double *m = s->mem;
@@ -1043,8 +1218,18 @@ orc_state *orc_create(const orc_params *p, const double *const *cols, int projec
             for (int f = 0; f < 12; f++) {
                 s->fq[fb][f] = m; m += s->N3; s->fp[fb][f] = m; m += s->N3; s->fa[fb][f] = m; m += s->N3;
             }
-    /* column order -> packed slots */
+    if (real)
+        for (int c = 0; c < 3; c++) { s->mis[c] = m; m += s->N3; s->hq[c] = m; m += s->N3; }
+    /* column order -> packed slots (the real mode: 12 columns, imaginary parts zero) */
     size_t bytes = s->N3 * sizeof(double);
+    if (real) {
+        for (int a = 0; a < 3; a++) {
+            memcpy(s->q[U0 + a], cols[0 + a], bytes);  memcpy(s->q[TU0 + a], cols[3 + a], bytes);
+            memcpy(s->p[U0 + a], cols[6 + a], bytes);  memcpy(s->p[TU0 + a], cols[9 + a], bytes);
+        }
+        forces(s);
+        return s;
+    }
     for (int a = 0; a < 3; a++) {
         memcpy(s->q[U0 + a], cols[0 + a], bytes);  memcpy(s->q[TU0 + a], cols[3 + a], bytes);
         memcpy(s->p[U0 + a], cols[6 + a], bytes);  memcpy(s->p[TU0 + a], cols[9 + a], bytes);
@@ -1094,6 +1279,13 @@ void orc_free(orc_state *s) {
 
 void orc_get(const orc_state *s, double *const *cols) {
     size_t bytes = s->N3 * sizeof(double);
+    if (s->real) {
+        for (int a = 0; a < 3; a++) {
+            memcpy(cols[0 + a], s->q[U0 + a], bytes);  memcpy(cols[3 + a], s->q[TU0 + a], bytes);
+            memcpy(cols[6 + a], s->p[U0 + a], bytes);  memcpy(cols[9 + a], s->p[TU0 + a], bytes);
+        }
+        return;
+    }
     for (int a = 0; a < 3; a++) {
         memcpy(cols[0 + a], s->q[U0 + a], bytes);  memcpy(cols[3 + a], s->q[TU0 + a], bytes);
         memcpy(cols[6 + a], s->p[U0 + a], bytes);  memcpy(cols[9 + a], s->p[TU0 + a], bytes);

@@ -47,6 +47,10 @@ typedef struct {
     double q2[3];
     int n_fabrics, mf_lock;
     double q_fab[3];
+    /* real 6-field mode (complex_phi = 0, gauge = 0): 12 columns (0-11 of the
+     * order above); its optional terms as the reference's Config names them */
+    int real_fields, mode;
+    double inv_alpha, inv_beta, kappa_gamma, alpha_cs, beta_h, kappa_h;
 } orc_params;
 
 typedef struct orc_state orc_state;
@@ -61,7 +65,8 @@ void orc_free(orc_state *s);
 void orc_step(orc_state *s, int nsteps);
 void orc_get(const orc_state *s, double *const *cols);
 /* 31 diagnostics in TSV order (see header comment), then Q_C, Q_Q, Q_L,
- * Q_em with three fabrics (35); returns the slot count */
+ * Q_em with three fabrics (35); the real mode's 13 (energies, amplitudes,
+ * theta_rms); returns the slot count */
 int orc_diag(orc_state *s, double *out);
 double orc_g_offset(const orc_state *s);
 int orc_cg_iterations(const orc_state *s);

@@ -175,3 +175,40 @@ def test_oracle_matches_reference_binary_extensions(kind):
     for c in range(len(got)):
         assert rel_l2(got[c], ref["cols"][c]) < 1e-12, (kind, ref["names"][c])
     check_series(rows, ref["diag"], ref["diag_header"])
+
+
+# ------------------------------------------------------------ real 6-field mode
+
+@pytest.mark.parametrize("name", ["ref_real_n12", "ref_real_terms_n11_damped"])
+def test_oracle_matches_reference_real_mode(name):
+    """The real mode (compute_forces / compute_energy), plain and with every
+    optional term under the sponge: frames and the 13 diag TSV columns."""
+    import json
+    f = load(name)
+    st = seeds.real_state(int(f["N"]), **json.loads(str(f["over"])))
+    o = oracle.Oracle(st.params, st.cols())
+    rows = [o.diag()]
+    every = int(f["diag_every"])
+    for _ in range(int(f["nsteps"]) // every):
+        o.step(every)
+        rows.append(o.diag())
+    got = o.cols()
+    assert len(got) == 12 == f["final"].shape[0]
+    for c in range(12):
+        assert rel_l2(got[c], f["final"][c]) < 1e-12, (name, str(f["names"][c]))
+    want = np.asarray(f["diag"])[:, 1:]
+    have = np.array(rows)
+    assert have.shape == want.shape
+    assert np.all(np.abs(have - want) <= 1e-6 * np.abs(want) + 1e-12)
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="reference binary not built (make -C oracle ref)")
+@pytest.mark.parametrize("terms", [dict(mode=1), dict(mode=3), dict(alpha_cs=0.3), dict(beta_h=0.5),
+                                   dict(kappa_h=0.2)], ids=lambda t: "-".join(f"{k}{v}" for k, v in t.items()))
+def test_oracle_real_terms_match_reference_binary(terms):
+    st = seeds.real_state(13, seed=21, **terms)
+    ref = oracle.run_reference(st.params, st.cols(), 30, diag_every=10)
+    o = oracle.Oracle(st.params, st.cols())
+    o.step(30)
+    for c, (g, r) in enumerate(zip(o.cols(), ref["cols"])):
+        assert rel_l2(g, r) < 1e-12, (terms, c)
