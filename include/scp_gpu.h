@@ -209,14 +209,16 @@ int  scp_gpu_check_trig(int n, const double *x, double *err);
 /* Diagnostics for callers that must not allocate device memory.
  *
  * No counterpart in the reference.  Some hosts of this library cannot call
- * cudaMalloc while they run a simulation: a caller that replays captured
- * work, a process whose device memory is carved up and owned by another
- * framework, or a real-time loop that treats any allocation as a failure.
- * This entry point computes the same diagnostics as scp_gpu_diag for a state
- * that the caller already holds on the device, without a handle and without
- * allocating: its reduction scratch is a fixed array that lives in the
- * library (SCP_DIAG_STATIC_SCRATCH_BYTES, about 300 KB, held by every GPU
- * that loads the library until the process exits).
+ * cudaMalloc while they run a simulation: a process whose device memory is
+ * carved up and owned by another framework (its allocator holds the whole
+ * pool, so a cudaMalloc outside it fails or fragments that pool), or a
+ * real-time loop that treats any allocation, with its implicit device
+ * synchronisation, as a failure.  This entry point computes the same
+ * diagnostics as scp_gpu_diag for a state that the caller already holds on
+ * the device, without a handle and without allocating: its reduction scratch
+ * is a fixed array that lives in the library (SCP_DIAG_STATIC_SCRATCH_BYTES,
+ * about 300 KB, held by every GPU that loads the library until the process
+ * exits).
  *
  *   p          grid and physics parameters (as for scp_gpu_init)
  *   dev_cols   24 or 30 device pointers, FP64 columns in the SFA order above
@@ -225,11 +227,15 @@ int  scp_gpu_check_trig(int n, const double *x, double *err);
  *   out        host result, slot order as scp_gpu_diag
  *
  * Grids larger than SCP_DIAG_STATIC_MAX_N per edge are rejected with
- * SCP_EINVAL.  The first call on a device looks up the scratch array's
- * device address (once per device); make that first call before any stream
- * capture.  All calls share the one scratch array, so calls whose work
- * overlaps on the GPU (two host threads, or two streams) race: serialise
- * them.  The call synchronises on `stream` before it returns. */
+ * SCP_EINVAL (scp_gpu_last_cuda_error names the limit).  The first call on
+ * a device (and the first after that device's context changed, e.g. after
+ * cudaDeviceReset) looks up the scratch array's device address; the call
+ * waits on `stream` and reads its results into host memory, so it must be
+ * made outside stream capture: on a capturing stream it returns
+ * SCP_EUNSUPPORTED before enqueuing anything.  All calls share the one
+ * scratch array, so calls whose work overlaps on the GPU (two host threads,
+ * or two streams) race: serialise them.  The call synchronises on `stream`
+ * before it returns. */
 #define SCP_DIAG_STATIC_MAX_N 2048
 #define SCP_DIAG_STATIC_SCRATCH_BYTES (8 * (1184 * 32 + 64 + 8))
 int  scp_gpu_diag_noalloc(const scp_gpu_params *p, const double *const *dev_cols, double G_offset,

@@ -48,11 +48,13 @@ class OrcParams(ctypes.Structure):
 _lib = None
 
 
-def build() -> None:
-    """Compile liboracle.so (and, with the reference tree present, _ref/)."""
+def build(ref: str | None = None) -> None:
+    """Compile liboracle.so and, given the path of a kardianos/scp checkout
+    (argument, else the SCP_REFERENCE environment variable), the reference
+    binaries under _ref/.  Without a checkout only liboracle.so is built."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    ref = os.environ.get("SCP_REFERENCE", "/root/reference")
-    if os.path.isdir(os.path.join(ref, "sfa", "sim")):
+    ref = ref or os.environ.get("SCP_REFERENCE")
+    if ref and os.path.isdir(os.path.join(ref, "sfa", "sim")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 

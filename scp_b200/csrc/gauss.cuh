@@ -175,6 +175,35 @@ __global__ void __launch_bounds__(kRedThreads) cg_update_kernel(long long n3, do
     }
 }
 
+// Warm start from a given chi (the spectral solve, spectral.cuh): r = b - A chi
+// = b + lap(chi) computed explicitly, p = r; partial sums r^2 and chi, max |r|.
+// The CG then goes on from chi with the unchanged stopping rule.
+__global__ void __launch_bounds__(kRedThreads) cg_warm_kernel(int N, long long n3, double idx2, const double *b,
+                                                              const double *x, double *r, double *p, double *part) {
+    __shared__ double scratch[3 * 32];
+    double S[2] = {0.0, 0.0}, M[1] = {0.0};
+    const long long NN = (long long)N * N;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        site_ijk(idx, N, &i, &j, &k);
+        const double xc = x[idx];
+        const double lap = (x[(long long)wrapi(i + 1, N) * NN + (long long)j * N + k]
+                            + x[(long long)wrapi(i - 1, N) * NN + (long long)j * N + k]
+                            + x[(long long)i * NN + (long long)wrapi(j + 1, N) * N + k]
+                            + x[(long long)i * NN + (long long)wrapi(j - 1, N) * N + k]
+                            + x[(long long)i * NN + (long long)j * N + wrapi(k + 1, N)]
+                            + x[(long long)i * NN + (long long)j * N + wrapi(k - 1, N)] - 6.0 * xc) * idx2;
+        const double rv = b[idx] + lap;
+        r[idx] = rv;
+        p[idx] = rv;
+        S[0] += rv * rv;
+        S[1] += xc;
+        M[0] = fmax(M[0], fabs(rv));
+    }
+    block_fold<2, 1>(S, M, scratch, part);
+}
+
 // single-thread scalar bookkeeping of the start-up
 __global__ void cg_scalar_kernel(int stage, double n3d, const double *fold, double *cg) {
     if (threadIdx.x | blockIdx.x) return;
@@ -187,6 +216,14 @@ __global__ void cg_scalar_kernel(int stage, double n3d, const double *fold, doub
             cg[CG_BETA] = 0.0;     // first direction p = r
             cg[CG_XBAR] = 0.0;
             cg[CG_DONE] = (fold[1] > cg[CG_TOL]) ? 0.0 : 1.0;
+            break;
+        case 2:   // after cg_warm_kernel: the residual of the starting chi decides
+            cg[CG_RZ] = fold[0];
+            cg[CG_XBAR] = fold[1] / n3d;
+            cg[CG_RMAX] = fold[2];
+            cg[CG_BETA] = 0.0;
+            cg[CG_IT] = 0.0;
+            cg[CG_DONE] = (fold[2] > cg[CG_TOL]) ? 0.0 : 1.0;
             break;
     }
 }

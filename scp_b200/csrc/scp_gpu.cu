@@ -21,11 +21,13 @@
 #include "gauss.cuh"
 #include "reduce.cuh"
 #include "snapshot.cuh"
+#include "spectral.cuh"
 #include "launch.cuh"
 #include "real.cuh"
 #include "gext.cuh"
 #include "mf.cuh"
 
+#include <cuda.h>   // driver API types only (entry points come through the runtime)
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -359,6 +361,40 @@ static int cg_solve(scp_gpu *h, int nb, double *b, double *x, double *r, double 
     fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
     cg_scalar_kernel<<<1, 1, 0, h->stream>>>(1, n3d, h->fold, h->cg);
     CK(cudaGetLastError());
+    if (spectral_supported(h->N)) {
+        // start from the direct spectral solution of the same periodic 7-point
+        // problem (spectral.cuh): r and p are its complex work arrays, then the
+        // explicit residual of that chi restarts the iteration
+        const int N = h->N, nc = spectral_ctas(N);
+        const size_t sm = spectral_smem_bytes(N);
+        CK(cudaFuncSetAttribute(is_pow2(N) ? (const void *)spectral_pass_kernel<true>
+                                           : (const void *)spectral_pass_kernel<false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        const double *in_re[5] = {b, r, r, r, r};
+        const double *in_im[5] = {nullptr, p, p, p, p};
+        double *out_re[5] = {r, r, r, r, x};
+        double *out_im[5] = {p, p, p, p, nullptr};
+        for (int pass = 0; pass < 5; pass++) {
+            if (is_pow2(N))
+                spectral_pass_kernel<true><<<nc, kFftThreads, sm, h->stream>>>(pass, N, idx2, in_re[pass],
+                                                                               in_im[pass], out_re[pass],
+                                                                               out_im[pass]);
+            else
+                spectral_pass_kernel<false><<<nc, kFftThreads, sm, h->stream>>>(pass, N, idx2, in_re[pass],
+                                                                                in_im[pass], out_re[pass],
+                                                                                out_im[pass]);
+        }
+        cg_warm_kernel<<<nb, kRedThreads, 0, h->stream>>>(N, n3, idx2, b, x, r, p, h->part);
+        fold_partials_kernel<2, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+        cg_scalar_kernel<<<1, 1, 0, h->stream>>>(2, n3d, h->fold, h->cg);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(h->h_small, h->cg, sizeof(double) * CG_N, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->h_small[CG_DONE] != 0.0) {   // converged at the start: no iterations
+            *iters = 0;
+            return (h->h_small[CG_RMAX] > h->h_small[CG_TOL]) ? SCP_EGAUSS : SCP_OK;
+        }
+    }
     // the right-hand side is not needed any more: b is the second direction buffer
     double *dirs[2] = {p, b};
     // iterations in device-checked batches (see gauss.cuh); two launches each
@@ -1074,22 +1110,28 @@ static void diag_assemble(const double *f1, const double *f2, const double *pt, 
     }
 }
 
-static DiagConsts diag_consts(const scp_gpu *h) {
-    const scp_gpu_params &p = h->p;
+// Reduction constants of a state on grid p: the one place DiagConsts is
+// filled, for the handle diagnostics and for scp_gpu_diag_noalloc alike.
+static DiagConsts diag_consts_for(const scp_gpu_params &p, int gauged, int links, int real, double G_offset) {
     DiagConsts c;
-    c.N = h->N; c.N3 = h->N3; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx; c.idx1 = 1.0 / (2.0 * p.dx);
+    c.N = p.N; c.N3 = (long long)p.N * p.N * p.N; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx;
+    c.idx1 = 1.0 / (2.0 * p.dx);
     c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
-    c.gauged = h->gauged;
-    c.links = h->links;
-    c.real = h->real;
-    c.g = h->gauged ? p.g_gauge : 0.0;
-    c.bpre = h->gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
+    c.gauged = gauged;
+    c.links = links;
+    c.real = real;
+    c.g = gauged ? p.g_gauge : 0.0;
+    c.bpre = gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
     c.R2 = p.qdiag_radius * p.qdiag_radius;
     c.Rcube = p.qdiag_radius;
     const double Rint = (p.bc_type == 0) ? (p.L - p.damp_width - p.dx) : 1e300;
     c.Rint2 = Rint * Rint;
-    c.G_offset = h->G_offset;
+    c.G_offset = G_offset;
     return c;
+}
+
+static DiagConsts diag_consts(const scp_gpu *h) {
+    return diag_consts_for(h->p, h->gauged, h->links, h->real, h->G_offset);
 }
 
 template <class View>
@@ -1414,44 +1456,68 @@ extern "C" int scp_gpu_check_trig(int n, const double *x, double *err) {
     return SCP_OK;
 }
 
-extern "C" {
-
-}  // extern "C"
-
 // ---------------------------------------------------------------- allocation-free diagnostics
 //
 // For callers that cannot allocate device memory (see scp_gpu_diag_noalloc
 // in include/scp_gpu.h).  The reduction scratch is this file-scope device
 // array: partial rows of the two reduction passes, the folded values and
 // the point reads.  Its name in host code is only a stand-in for the symbol,
-// so the device address is looked up with cudaGetSymbolAddress, once per
-// device with that device current, and passed to the kernels.
+// so the device address is looked up with cudaGetSymbolAddress, with the
+// device current, and passed to the kernels.
 
 namespace {
 
 constexpr int kStaticPartRows = kRedMaxBlocks;      // one row of 32 doubles per CTA
 constexpr size_t kStaticDoubles = (size_t)kStaticPartRows * 32 + 64 + 8;
 static_assert(kStaticDoubles * 8 == SCP_DIAG_STATIC_SCRATCH_BYTES, "scratch size in the header");
+// red_blocks() never launches more CTAs than kRedMaxBlocks, so one partial row
+// per CTA fits for every grid up to SCP_DIAG_STATIC_MAX_N per edge
+static_assert(kStaticPartRows >= kRedMaxBlocks, "one partial row per reduction CTA");
+static_assert(SCP_DIAG_STATIC_MAX_N <= 2048, "the static scratch limit is within the library's grid limit");
 
 __device__ __align__(256) double g_diag_scratch[kStaticDoubles];
+
+// Driver context current on this thread (cuCtxGetCurrent through the runtime's
+// driver entry point, so the library needs no link against libcuda).
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+CUcontext current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (CtxGetCurrentFn)f;
+    }();
+    CUcontext c = nullptr;
+    if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return c;
+}
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 double *g_scratch_addr[kMaxDevices] = {};
+CUcontext g_scratch_ctx[kMaxDevices] = {};
 
-// Device address of g_diag_scratch on the current device (looked up once).
+// Device address of g_diag_scratch for the device current on this thread.
+// The lookup is made once per device and repeated only when the device's
+// context has changed since (a cudaDeviceReset, or a caller that made a
+// different context current), so a stale address is never handed out.
 int static_scratch(int dev, double **out) {
     if (dev < 0 || dev >= kMaxDevices) return SCP_ENODEV;
+    const CUcontext ctx = current_context();
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    if (!g_scratch_addr[dev] || !ctx || ctx != g_scratch_ctx[dev]) {
         void *ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_diag_scratch);
         if (e != cudaSuccess || !ptr) {
             snprintf(g_cuda_err, sizeof g_cuda_err, "cudaGetSymbolAddress(g_diag_scratch): %s",
                      cudaGetErrorString(e));
+            g_scratch_addr[dev] = nullptr;
             return SCP_ECUDA;
         }
         g_scratch_addr[dev] = (double *)ptr;
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch_addr[dev];
     return SCP_OK;
@@ -1469,16 +1535,28 @@ struct ViewCols {
 
 extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *const *dev_cols, double G_offset,
                                     void *stream_ptr, scp_gpu_diag_out *out) {
-    int rc = validate(pp);
-    if (rc) return rc;
-    if (!dev_cols || !out) return SCP_EINVAL;
-    if (pp->real_fields) return SCP_EUNSUPPORTED;   // takes the complex column set
-    if (gext_on(pp)) return SCP_EUNSUPPORTED;        // no Higgs energy term
-    if (pp->n_fabrics == 3) return SCP_EUNSUPPORTED;  // one fabric
+    if (!pp || !dev_cols || !out) return SCP_EINVAL;
+    // the size limit of the static scratch comes first, so its own message
+    // reaches the caller for every grid it does not cover
     if (pp->N > SCP_DIAG_STATIC_MAX_N) {
         snprintf(g_cuda_err, sizeof g_cuda_err, "scp_gpu_diag_noalloc: N=%d exceeds SCP_DIAG_STATIC_MAX_N=%d",
                  pp->N, SCP_DIAG_STATIC_MAX_N);
         return SCP_EINVAL;
+    }
+    int rc = validate(pp);
+    if (rc) return rc;
+    if (pp->real_fields) return SCP_EUNSUPPORTED;   // takes the complex column set
+    if (gext_on(pp)) return SCP_EUNSUPPORTED;        // no Higgs energy term
+    if (pp->n_fabrics == 3) return SCP_EUNSUPPORTED;  // one fabric
+    cudaStream_t st = (cudaStream_t)stream_ptr;
+    // The call waits for its own results and copies them into a host array on
+    // this stack frame, which cannot be part of a captured graph: refuse a
+    // capturing stream before anything is enqueued on it.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        snprintf(g_cuda_err, sizeof g_cuda_err, "scp_gpu_diag_noalloc: the stream is capturing a graph");
+        return SCP_EUNSUPPORTED;
     }
     const scp_gpu_params &p = *pp;
     const int links = p.complex_gauge ? 1 : 0;
@@ -1499,23 +1577,9 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     double *scratch = nullptr;
     if ((rc = static_scratch(dev, &scratch))) return rc;
     double *part = scratch, *fold = scratch + (size_t)kStaticPartRows * 32, *point = fold + 64;
-    cudaStream_t st = (cudaStream_t)stream_ptr;
     const long long n3 = (long long)p.N * p.N * p.N;
     const int nb = red_blocks(n3);
-    if (nb > kStaticPartRows) return SCP_EINVAL;
-    DiagConsts c;
-    c.N = p.N; c.N3 = n3; c.L = p.L; c.dx = p.dx; c.dV = p.dx * p.dx * p.dx; c.idx1 = 1.0 / (2.0 * p.dx);
-    c.m2 = p.m2; c.mtheta2 = p.mtheta2; c.eta = p.eta; c.mu = p.mu; c.kappa = p.kappa;
-    c.gauged = gauged;
-    c.links = links;
-    c.real = 0;
-    c.g = gauged ? p.g_gauge : 0.0;
-    c.bpre = gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
-    c.R2 = p.qdiag_radius * p.qdiag_radius;
-    c.Rcube = p.qdiag_radius;
-    const double Rint = (p.bc_type == 0) ? (p.L - p.damp_width - p.dx) : 1e300;
-    c.Rint2 = Rint * Rint;
-    c.G_offset = G_offset;
+    const DiagConsts c = diag_consts_for(p, gauged, links, 0, G_offset);
     // every scratch word read below is written first in the same call (each
     // CTA writes its whole partial row, the folds write their outputs), so
     // no clearing is needed; the fold area is zeroed only so a failed launch

@@ -27,6 +27,19 @@ EXPORTS = (
 
 DIAG_NSLOTS = 40
 
+# status codes (include/scp_gpu.h)
+SCP_OK = 0
+SCP_EINVAL = -1
+SCP_ENOMEM = -2
+SCP_ECUDA = -3
+SCP_ENETCHARGE = -4
+SCP_EGAUSS = -5
+SCP_ENONFINITE = -6
+SCP_EUNSUPPORTED = -7
+SCP_ENODEV = -8
+SCP_EBUSY = -9
+SCP_ETIMEOUT = -10
+
 
 class DiagOut(ctypes.Structure):
     _fields_ = [("v", ctypes.c_double * DIAG_NSLOTS)]

@@ -21,7 +21,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("SCP_REFERENCE", "/root/reference")
+REF = os.environ.get("SCP_REFERENCE", "")   # path of the kardianos/scp checkout (required)
 SOLVER = os.path.join(ROOT, "oracle", "_ref", "radial_qball")
 PROFILE = os.path.join(HERE, "profile_omega1.3900.txt")
 SERIES = os.path.join(HERE, "ref_qcons_v66.npz")
@@ -40,8 +40,10 @@ def read_series(path: str) -> np.ndarray:
 
 
 if __name__ == "__main__":
+    if not REF or not os.path.isdir(os.path.join(REF, "v66")):
+        sys.exit("set SCP_REFERENCE to the path of the kardianos/scp checkout")
     if not os.path.exists(SOLVER):
-        sys.exit("build the reference tools first: make -C oracle ref")
+        sys.exit("build the reference tools first: make -C oracle ref REF=$SCP_REFERENCE")
     write_profile(PROFILE)
     series = read_series(os.path.join(REF, "v66", "results", "qcons_harness2.out"))
     assert series.shape[1] == len(COLUMNS)

@@ -240,6 +240,28 @@ def test_gpu_gauss_projection_matches_oracle(gpu):
     assert d["gauss_max"] < 1e-11
 
 
+@pytest.mark.parametrize("N", [32, 48, 13])
+def test_gpu_gauss_spectral_start_matches_oracle(gpu, N):
+    """The start-up projection begins from the direct spectral solve of the
+    periodic 7-point problem (radix-2 for N = 32, the direct transform for
+    48 and 13) and finishes with the reference's CG stopping rule: E, the
+    frozen offset and the Gauss residual agree with the CPU checker, whose CG
+    starts from zero and takes many more iterations."""
+    L = (N - 1) / 4.0
+    st = seeds.make_state("c1", seeds.params_for("c1", N=N, L=L))
+    o = oracle.Oracle(st.params, st.cols())
+    with Simulation(st.params, st.cols()) as sim:
+        inf = sim.info()
+        got = sim.snapshot()
+        d = sim.diag()
+    ref = o.cols()
+    for c in range(27, 30):
+        assert rel_l2(got[c], ref[c]) < 1e-10, c
+    assert abs(inf.G_offset - o.g_offset) < 1e-12
+    assert d["gauss_max"] < 1e-11
+    assert inf.cg_iterations <= max(60, o.cg_iterations // 4), (inf.cg_iterations, o.cg_iterations)
+
+
 def test_gpu_c0_64_1000_parity(gpu):
     """Config-0 workload: 1000 FP64 steps within 1e-10 relative L2 per field of
     the CPU checker, energy series identical to the printed precision, and
