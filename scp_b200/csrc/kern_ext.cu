@@ -1,0 +1,167 @@
+// kern_ext.cu -- instantiations and launchers of the extension steppers'
+// ring kernels (Higgs condensate / second gauge, three fabrics).
+#include "ext_launch.cuh"
+#include "fabrics.cuh"
+#include "higgs_u1.cuh"
+#include "real6.cuh"
+
+namespace scp {
+
+namespace {
+
+constexpr int kExtTX = 32, kExtTY = 8;
+
+template <class M>
+int ring_plan(int N, int nsm, ExtPlan *p) {
+    using S = RingShape<M::NR, kExtTX, kExtTY>;
+    auto fn = ring_kernel<M, kExtTX, kExtTY>;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_bytes) != cudaSuccess)
+        return -1;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kExtTX * kExtTY, S::smem_bytes) != cudaSuccess ||
+        occ < 1)
+        return -1;
+    plan_ring_tiles(N, kExtTX, kExtTY, nsm * occ, p);
+    p->smem = S::smem_bytes;
+    return 0;
+}
+
+template <bool H, bool G>
+cudaError_t hu_launch(const ExtPlan &p, const HuConsts &c, const HuIO &io, cudaStream_t st) {
+    using M = HiggsU1<H, G>;
+    typename M::Args a;
+    const long long n3 = c.N3;
+    for (int f = 0; f < M::NR; f++) a.src.f[f] = io.x + f * n3;
+    a.N = c.N;
+    a.c = c;
+    a.win = io.win;
+    a.wout = io.wout;
+    a.xout = io.xout;
+    a.sout = io.sout;
+    a.flag = io.flag;
+    a.first = io.first;
+    a.sync = io.sync;
+    a.damp = io.damp;
+    ring_kernel<M, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+int hu_plan(bool higgs, bool g2, int N, int nsm, ExtPlan *plan) {
+    if (higgs && g2) return ring_plan<HiggsU1<true, true>>(N, nsm, plan);
+    if (higgs) return ring_plan<HiggsU1<true, false>>(N, nsm, plan);
+    return ring_plan<HiggsU1<false, true>>(N, nsm, plan);
+}
+
+cudaError_t hu_step(bool higgs, bool g2, const ExtPlan &plan, const HuConsts &c, const HuIO &io, cudaStream_t st) {
+    if (higgs && g2) return hu_launch<true, true>(plan, c, io, st);
+    if (higgs) return hu_launch<true, false>(plan, c, io, st);
+    return hu_launch<false, true>(plan, c, io, st);
+}
+
+int fabric_plan(int N, int nsm, ExtPlan *fabric, ExtPlan *second, ExtPlan *link) {
+    if (ring_plan<FabricPass<false>>(N, nsm, fabric)) return -1;
+    if (ring_plan<FabricPass<true>>(N, nsm, second)) return -1;
+    return ring_plan<LinkPass>(N, nsm, link);
+}
+
+namespace {
+template <bool SECOND>
+cudaError_t fabric_launch(const ExtPlan &p, const FabConsts &c, const FabIO &io, cudaStream_t st) {
+    using M = FabricPass<SECOND>;
+    typename M::Args a;
+    const long long n3 = c.N3;
+    for (int f = 0; f < 12; f++) a.src.f[f] = io.x + f * n3;
+    for (int d = 0; d < 3; d++) a.src.f[M::TH + d] = io.th + d * n3;
+    a.N = c.N;
+    a.c = c;
+    a.qf = io.qf;
+    a.gqf = io.gqf;
+    a.qx = io.qx;
+    a.gqx = io.gqx;
+    a.win = io.win;
+    a.wout = io.wout;
+    a.xout = io.xout;
+    a.sout = io.sout;
+    a.kacc = io.kacc;
+    a.flag = io.flag;
+    a.first = io.first;
+    a.sync = io.sync;
+    a.damp = io.damp;
+    a.accumulate = io.accumulate;
+    ring_kernel<M, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t fabric_step(const ExtPlan &plan, const FabConsts &c, const FabIO &io, cudaStream_t st) {
+    return io.second ? fabric_launch<true>(plan, c, io, st) : fabric_launch<false>(plan, c, io, st);
+}
+
+cudaError_t link_step(const ExtPlan &p, const FabConsts &c, const LinkIO &io, cudaStream_t st) {
+    LinkPass::Args a;
+    const long long n3 = c.N3;
+    for (int d = 0; d < 3; d++) a.src.f[d] = io.th + d * n3;
+    a.N = c.N;
+    a.c = c;
+    a.kacc = io.kacc;
+    a.win = io.win;
+    a.wout = io.wout;
+    a.xout = io.thout;
+    a.sout = io.sout;
+    a.flag = io.flag;
+    a.first = io.first;
+    a.sync = io.sync;
+    a.damp = io.damp;
+    ring_kernel<LinkPass, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg);
+    return cudaGetLastError();
+}
+
+int r6_plan(bool aux, int N, int nsm, ExtPlan *aux_plan, ExtPlan *step_plan) {
+    if (aux) {
+        if (ring_plan<R6Aux>(N, nsm, aux_plan)) return -1;
+        return ring_plan<R6Step<true>>(N, nsm, step_plan);
+    }
+    return ring_plan<R6Step<false>>(N, nsm, step_plan);
+}
+
+namespace {
+template <bool AUX>
+cudaError_t r6_launch(const ExtPlan &p, const R6Consts &c, const R6IO &io, cudaStream_t st) {
+    using M = R6Step<AUX>;
+    typename M::Args a;
+    const long long n3 = c.N3;
+    for (int f = 0; f < 6; f++) a.src.f[f] = io.x + f * n3;
+    if (AUX)
+        for (int f = 0; f < 6; f++) a.src.f[6 + f] = io.aux + f * n3;
+    a.N = c.N;
+    a.c = c;
+    a.win = io.win;
+    a.wout = io.wout;
+    a.xout = io.xout;
+    a.sout = io.sout;
+    a.flag = io.flag;
+    a.first = io.first;
+    a.sync = io.sync;
+    a.damp = io.damp;
+    ring_kernel<M, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t r6_step(const ExtPlan &aux_plan, const ExtPlan &step_plan, const R6Consts &c, const R6IO &io,
+                    cudaStream_t st) {
+    if (!io.aux) return r6_launch<false>(step_plan, c, io, st);
+    R6Aux::Args a;
+    for (int f = 0; f < 6; f++) a.src.f[f] = io.x + f * c.N3;
+    a.N = c.N;
+    a.c = c;
+    a.aux = io.aux;
+    ring_kernel<R6Aux, kExtTX, kExtTY><<<aux_plan.grid, kExtTX * kExtTY, aux_plan.smem, st>>>(a, aux_plan.tg);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return r6_launch<true>(step_plan, c, io, st);
+}
+
+}  // namespace scp

@@ -23,9 +23,8 @@
 #include "snapshot.cuh"
 #include "spectral.cuh"
 #include "launch.cuh"
-#include "real.cuh"
-#include "gext.cuh"
-#include "mf.cuh"
+#include "ext_launch.cuh"
+#include "ext_startup.cuh"
 
 #include <cuda.h>   // driver API types only (entry points come through the runtime)
 #include <math.h>
@@ -100,21 +99,23 @@ struct scp_gpu {
     int gauged, nf, prec;
     int links;                   // th / E columns carried (complex_gauge; with g = 0 they stay constant)
     int real;                    // real 6-field mode: 12 host columns, imaginary sector held at zero
-    // real 6-field mode with optional terms: separate per-site kernels (real.cuh)
+    // real 6-field mode with optional terms: ring kernels of real6.cuh; X[0..1],
+    // W and S hold 6 arrays, raux the auxiliary C and B (strain, hardening)
     int rp = 0;
-    double *rbuf = nullptr, *rx = nullptr, *rv = nullptr, *ra = nullptr, *rmq = nullptr;
-    RealConsts rc{};
-    // gauged stepper with the Higgs condensate and/or the second gauge: separate
-    // per-site FP64 kernels (gext.cuh)
+    double *raux = nullptr;
+    R6Consts r6{};
+    // gauged stepper with the Higgs condensate and/or the second gauge: one
+    // fused ring kernel per step (higgs_u1.cuh); X[0..1], W and S hold nx arrays
     int gx = 0, g2 = 0, higgs = 0;
-    double *gbuf = nullptr;
-    GextState gs{};
-    GextConsts gc{};
-    // three fabrics C, Q, L: separate per-site FP64 kernels (mf.cuh)
-    int mfab = 0;
-    double *mbuf = nullptr;
-    MfState ms{};
-    MfConsts mc{};
+    HuConsts hc{};
+    // three fabrics C, Q, L: one ring kernel per fabric and one for the links
+    // per step (fabrics.cuh); X[0..1], W and S hold C (15), L (12), Q (12, free)
+    int mfab = 0, fab_lock = 0;
+    double qfab[3] = {0.0, 0.0, 0.0};
+    FabConsts fc{};
+    double *kacc = nullptr;      // accumulated currents (3 arrays)
+    ExtPlan xplan{}, xplan2{}, lplan{};
+    int nx = 0;                  // position arrays per buffer of the extension layouts
     int device;
     cudaStream_t stream = nullptr;
     // FP64 state
@@ -456,13 +457,14 @@ static int gauss2_startup(scp_gpu *h) {
     double *tmp = nullptr;
     CK(cudaMallocAsync(&tmp, sizeof(double) * 5 * n3, h->stream));
     double *b = tmp, *x = tmp + n3, *r = tmp + 2 * n3, *p = tmp + 3 * n3, *Ap = tmp + 4 * n3;
-    gext_gauss2_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc, b, h->part);
+    double *E2 = h->S + (size_t)HiggsU1<false, true>::TH2 * n3;
+    hu_gauss2_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->X[0], h->S, E2, h->hc, b, h->part);
     int iters = 0, rc;
     if ((rc = cg_solve(h, nb, b, x, r, p, Ap, &iters))) {
         cudaFreeAsync(tmp, h->stream);
         return rc;
     }
-    gext_gauss2_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc, x, h->cg);
+    hu_gauss2_apply_kernel<<<nb, kRedThreads, 0, h->stream>>>(E2, x, h->cg, h->hc);
     CK(cudaGetLastError());
     CK(cudaFreeAsync(tmp, h->stream));
     return SCP_OK;
@@ -592,19 +594,23 @@ static bool real_optional(const scp_gpu_params *p) {
     return p->real_fields && (p->mode != 0 || p->alpha_cs != 0 || p->beta_h != 0 || p->kappa_h != 0);
 }
 
-static void real_forces(scp_gpu *h) {
-    const int nb = red_blocks(h->N3);
-    if (h->rc.acs != 0 || h->rc.bh != 0) real_pass1_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->rx, h->rmq, h->rc);
-    real_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->rx, h->rmq, h->ra, h->rc);
-}
+static int ext_slab(scp_gpu *h, int nx);
 
-// one verlet_step (scp_sim.c:1583-1716): kick, drift, forces, kick, sponge
-static int real_step(scp_gpu *h) {
-    const int nb = red_blocks(h->N3);
-    real_kick_drift_kernel<<<red_blocks(6 * h->N3), kRedThreads, 0, h->stream>>>(h->rx, h->rv, h->ra, h->rc);
-    real_forces(h);
-    real_kick_damp_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->rv, h->ra, h->rc);
-    CK(cudaGetLastError());
+// one step of the real mode: [auxiliary fields,] forces and fused leapfrog
+static int r6_launch_step(scp_gpu *h, bool first, bool sync) {
+    R6IO io;
+    io.x = h->X[h->cur];
+    io.xout = h->X[h->cur ^ 1];
+    io.win = first ? h->S : h->W;
+    io.wout = h->W;
+    io.sout = h->S;
+    io.aux = h->raux;
+    io.flag = h->flag;
+    io.first = first;
+    io.sync = sync;
+    io.damp = damping_on(h);
+    CK(r6_step(h->xplan2, h->xplan, h->r6, io, h->stream));
+    h->cur ^= 1;
     return SCP_OK;
 }
 
@@ -612,61 +618,56 @@ static int init_real(scp_gpu *h, const double *const *cols, bool on_device) {
     int rc;
     if ((rc = alloc_common(h))) return rc;
     const long long n3 = h->N3;
-    CK(cudaMallocAsync(&h->rbuf, sizeof(double) * 24 * (size_t)n3, h->stream));
-    CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
-    h->dev_bytes += sizeof(double) * 25 * (size_t)n3;
-    h->rx = h->rbuf;
-    h->rv = h->rbuf + 6 * n3;
-    h->ra = h->rbuf + 12 * n3;
-    h->rmq = h->rbuf + 18 * n3;
-    CK(cudaMemsetAsync(h->rmq, 0, sizeof(double) * 6 * (size_t)n3, h->stream));
-    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    for (int c = 0; c < 12; c++)
-        CK(cudaMemcpyAsync((c < 6 ? h->rx + c * n3 : h->rv + (c - 6) * n3), cols[c], sizeof(double) * n3, kind,
-                           h->stream));
     const scp_gpu_params &p = h->p;
-    RealConsts &r = h->rc;
+    if ((rc = ext_slab(h, 6))) return rc;
+    const bool aux = p.alpha_cs != 0 || p.beta_h != 0;
+    if (aux) {
+        CK(cudaMallocAsync(&h->raux, sizeof(double) * 6 * (size_t)n3, h->stream));
+        CK(cudaMemsetAsync(h->raux, 0, sizeof(double) * 6 * (size_t)n3, h->stream));
+        h->dev_bytes += sizeof(double) * 6 * n3;
+    }
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int c = 0; c < 12; c++)   // phi, theta, then their velocities
+        CK(cudaMemcpyAsync((c < 6 ? h->X[0] + c * n3 : h->S + (c - 6) * n3), cols[c], sizeof(double) * n3, kind,
+                           h->stream));
+    R6Consts &r = h->r6;
     r.N = p.N; r.N3 = n3; r.L = p.L; r.dx = p.dx; r.dV = p.dx * p.dx * p.dx;
     r.idx1 = 1.0 / (2.0 * p.dx); r.idx2 = 1.0 / (p.dx * p.dx); r.hdt = 0.5 * p.dt; r.dt = p.dt;
     r.mu = p.mu; r.kappa = p.kappa; r.m2 = p.m2; r.mtheta2 = p.mtheta2; r.eta = p.eta;
-    r.kh = p.kappa_h; r.acs = p.alpha_cs; r.bh = p.beta_h; r.kg = p.kappa_gamma; r.ia = p.inv_alpha; r.ib = p.inv_beta;
+    r.kh = p.kappa_h; r.alpha = p.alpha_cs; r.beta = p.beta_h; r.kg = p.kappa_gamma;
+    r.ia = p.inv_alpha; r.ib = p.inv_beta;
     r.mode = p.mode;
-    r.damp = damping_on(h) ? 1 : 0;
     r.damp_width = p.damp_width; r.damp_rate = p.damp_rate;
-    real_forces(h);                                  // the reference computes forces before its loop
-    CK(cudaGetLastError());
-    // the generic snapshot and info code reads these
-    h->X[0] = h->X[1] = h->rx;
-    h->S = h->rv;
-    h->cur = 0;
-    h->shape = 1;
-    return SCP_OK;
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    if (r6_plan(aux, h->N, nsm, &h->xplan2, &h->xplan)) return SCP_EUNSUPPORTED;
+    return r6_launch_step(h, true, false);
 }
 
 static int real_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     const int nb = red_blocks(h->N3);
-    real_energy_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->rx, h->rv, h->rc, h->part);
-    fold_partials_kernel<RS_NSUM, RM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    r6_energy_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->X[h->cur ^ 1], h->S, h->r6, h->part);
+    fold_partials_kernel<R6_NSUM, R6_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * (RS_NSUM + RM_NMAX), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * (R6_NSUM + R6_NMAX), cudaMemcpyDeviceToHost,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
     const double *f = h->h_small;
     double *o = out->v;
     for (int q = 0; q < SCP_DIAG_NSLOTS; q++) o[q] = 0.0;
-    o[SCP_DIAG_E_PHI_KIN] = f[RS_EPK];
-    o[SCP_DIAG_E_THETA_KIN] = f[RS_ETK];
-    o[SCP_DIAG_E_GRAD] = f[RS_EG];
-    o[SCP_DIAG_E_MASS] = f[RS_EM];
-    o[SCP_DIAG_E_POT] = f[RS_EP];
-    o[SCP_DIAG_E_TGRAD] = f[RS_ETG];
-    o[SCP_DIAG_E_TMASS] = f[RS_ETM];
-    o[SCP_DIAG_E_COUPLING] = f[RS_EC];
-    o[SCP_DIAG_E_TOTAL] = f[RS_EPK] + f[RS_ETK] + f[RS_EG] + f[RS_EM] + f[RS_EP] + f[RS_ETG] + f[RS_ETM] + f[RS_EC];
-    o[SCP_DIAG_PHI_MAX] = f[RS_NSUM + RM_PM];
-    o[SCP_DIAG_P_MAX] = f[RS_NSUM + RM_PMAX];
-    o[SCP_DIAG_P_INT] = f[RS_PINT];
-    o[SCP_DIAG_THETA_RMS] = sqrt(f[RS_TH2] / (3.0 * (double)h->N3));
+    const int slot[8] = {SCP_DIAG_E_PHI_KIN, SCP_DIAG_E_THETA_KIN, SCP_DIAG_E_GRAD, SCP_DIAG_E_MASS,
+                         SCP_DIAG_E_POT, SCP_DIAG_E_TGRAD, SCP_DIAG_E_TMASS, SCP_DIAG_E_COUPLING};
+    const int term[8] = {R6_EPK, R6_ETK, R6_EG, R6_EM, R6_EP, R6_ETG, R6_ETM, R6_EC};
+    double total = 0.0;
+    for (int q = 0; q < 8; q++) {
+        o[slot[q]] = f[term[q]];
+        total += f[term[q]];
+    }
+    o[SCP_DIAG_E_TOTAL] = total;
+    o[SCP_DIAG_PHI_MAX] = f[R6_NSUM + R6_PHIMAX];
+    o[SCP_DIAG_P_MAX] = f[R6_NSUM + R6_PMAX];
+    o[SCP_DIAG_P_INT] = f[R6_PINT];
+    o[SCP_DIAG_THETA_RMS] = sqrt(f[R6_TH2] / (3.0 * (double)h->N3));
     if (!isfinite(o[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
     return SCP_OK;
 }
@@ -677,26 +678,38 @@ static bool gext_on(const scp_gpu_params *p) {
     return p->complex_gauge && (p->higgs_v > 0 || p->g_gauge2 != 0);
 }
 
-// pass A (links), pass B (plaquettes), pass C (forces and field kicks)
-static void gext_forces(scp_gpu *h) {
-    const int nb = red_blocks(h->N3);
-    gext_links_plaq_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
-    gext_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
+// FP64 slab of the extension layouts: positions X[0], X[1], momenta W and
+// the synchronous momenta S, nx arrays each
+static int ext_slab(scp_gpu *h, int nx) {
+    const size_t nel = (size_t)nx * h->N3;
+    h->nx = nx;
+    CK(cudaMallocAsync(&h->slab, sizeof(double) * 4 * nel, h->stream));
+    CK(cudaMallocAsync(&h->stage, sizeof(double) * h->N3, h->stream));
+    h->dev_bytes += sizeof(double) * (4 * nel + h->N3);
+    CK(cudaMemsetAsync(h->slab, 0, sizeof(double) * 4 * nel, h->stream));
+    h->X[0] = h->slab;
+    h->X[1] = h->slab + nel;
+    h->W = h->slab + 2 * nel;
+    h->S = h->slab + 3 * nel;
+    h->cur = 0;
+    h->shape = 1;
+    return SCP_OK;
 }
 
-// nsteps verlet_steps (scp_sim.c:1583-1716): kick + drift, links and
-// plaquettes, forces per step; each step's closing kick + sponge runs inside
-// the next step's first sweep, and as its own sweep after the last step, so
-// the state is synchronous between calls
-static int gext_steps(scp_gpu *h, int nsteps) {
-    const int nb = red_blocks(h->N3);
-    for (int n = 0; n < nsteps; n++) {
-        if (n == 0) gext_kick_drift_kernel<false><<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
-        else gext_kick_drift_kernel<true><<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
-        gext_forces(h);
-    }
-    gext_kick_damp_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc);
-    CK(cudaGetLastError());
+// one step of the Higgs / second-gauge stepper: x_{n+1} in X[cur] -> X[cur^1]
+static int hu_launch_step(scp_gpu *h, bool first, bool sync) {
+    HuIO io;
+    io.x = h->X[h->cur];
+    io.xout = h->X[h->cur ^ 1];
+    io.win = first ? h->S : h->W;
+    io.wout = h->W;
+    io.sout = h->S;
+    io.flag = h->flag;
+    io.first = first;
+    io.sync = sync;
+    io.damp = damping_on(h);
+    CK(hu_step(h->higgs, h->g2, h->xplan, h->hc, io, h->stream));
+    h->cur ^= 1;
     return SCP_OK;
 }
 
@@ -707,38 +720,15 @@ static int init_gext(scp_gpu *h, const double *const *cols, bool on_device) {
     const scp_gpu_params &p = h->p;
     h->g2 = p.g_gauge2 != 0 ? 1 : 0;
     h->higgs = p.higgs_v > 0 ? 1 : 0;
-    // X S A (15 each), LC LS PS (3 each), then T2 E2 K2 PS2 (3 each), then H HV HA
-    const size_t narr = 54 + (h->g2 ? 12 : 0) + (h->higgs ? 3 : 0);
-    CK(cudaMallocAsync(&h->gbuf, sizeof(double) * narr * (size_t)n3, h->stream));
-    CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
-    h->dev_bytes += sizeof(double) * (narr + 1) * (size_t)n3;
-    CK(cudaMemsetAsync(h->gbuf, 0, sizeof(double) * narr * (size_t)n3, h->stream));
-    GextState &g = h->gs;
-    double *b = h->gbuf;
-    g.X = b; b += 15 * n3;
-    g.S = b; b += 15 * n3;
-    g.A = b; b += 15 * n3;
-    g.LC = b; b += 3 * n3;
-    g.LS = b; b += 3 * n3;
-    g.PS = b; b += 3 * n3;
-    if (h->g2) {
-        g.T2 = b; b += 3 * n3;
-        g.E2 = b; b += 3 * n3;
-        g.K2 = b; b += 3 * n3;
-        g.PS2 = b; b += 3 * n3;
-    }
-    if (h->higgs) {
-        g.H = b; b += n3;
-        g.HV = b; b += n3;
-        g.HA = b;
-    }
+    if ((rc = ext_slab(h, 15 + 3 * h->g2 + h->higgs))) return rc;
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    for (int c = 0; c < 30; c++) {
+    for (int c = 0; c < 30; c++) {   // th2, E2 start at zero
         int field, mom;
         sfa_col_source(c, &field, &mom);
-        CK(cudaMemcpyAsync((mom ? g.S : g.X) + (size_t)field * n3, cols[c], sizeof(double) * n3, kind, h->stream));
+        CK(cudaMemcpyAsync((mom ? h->S : h->X[0]) + (size_t)field * n3, cols[c], sizeof(double) * n3, kind,
+                           h->stream));
     }
-    GextConsts &k = h->gc;
+    HuConsts &k = h->hc;
     k.N = p.N; k.N3 = n3; k.L = p.L; k.dx = p.dx; k.dV = p.dx * p.dx * p.dx;
     k.idx1 = 1.0 / (2.0 * p.dx); k.idx2 = 1.0 / (p.dx * p.dx); k.inva = 1.0 / p.dx;
     k.hdt = 0.5 * p.dt; k.dt = p.dt;
@@ -746,35 +736,34 @@ static int init_gext(scp_gpu *h, const double *const *cols, bool on_device) {
     k.g = p.g_gauge;
     k.stp = 1.0 / (p.g_gauge * p.dx * p.dx * p.dx);
     k.gad = -p.g_gauge * p.dx * p.dt;
-    k.g2on = h->g2;
     k.g2 = p.g_gauge2;
     k.stp2 = h->g2 ? 1.0 / (p.g_gauge2 * p.dx * p.dx * p.dx) : 0.0;
     k.gad2 = -p.g_gauge2 * p.dx * p.dt;
     for (int a = 0; a < 3; a++) k.q[a] = p.gauge2_q[a];
-    k.higgs = h->higgs;
     k.hv = p.higgs_v; k.hlam = p.higgs_lam; k.hkap = p.higgs_kap;
-    k.damp = damping_on(h) ? 1 : 0;
     k.damp_width = p.damp_width; k.damp_rate = p.damp_rate;
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    if (hu_plan(h->higgs, h->g2, h->N, nsm, &h->xplan)) return SCP_EUNSUPPORTED;
     // the reference's start-up order (scp_sim.c:2802-2836): Higgs start value,
-    // net-charge check and Gauss projection, second Gauss projection, forces
-    if (h->higgs) gext_higgs_init_kernel<<<red_blocks(n3), kRedThreads, 0, h->stream>>>(g, k, p.higgs_rvoid);
+    // net-charge check and Gauss projection, second Gauss projection, first force
+    const int hf = 15 + 3 * h->g2;
+    if (h->higgs)
+        hu_higgs_start_kernel<<<red_blocks(n3), kRedThreads, 0, h->stream>>>(h->X[0] + (size_t)hf * n3,
+                                                                              h->S + (size_t)hf * n3, k,
+                                                                              p.higgs_rvoid);
     CK(cudaGetLastError());
-    if ((rc = gauss_startup(h, g.X, g.S))) return rc;
+    if ((rc = gauss_startup(h, h->X[0], h->S))) return rc;
     if (h->g2 && p.gauss_project && (rc = gauss2_startup(h))) return rc;
-    gext_forces(h);
-    CK(cudaGetLastError());
-    // the generic diagnostics, snapshot and info code reads these
-    h->X[0] = h->X[1] = g.X;
-    h->S = g.S;
-    h->cur = 0;
-    h->shape = 1;
-    return SCP_OK;
+    return hu_launch_step(h, true, false);
 }
 
-// Higgs energy (summed into E_total by the reference, scp_sim.c:2034)
+// Higgs energy of the current state (the reference adds it to E_total, scp_sim.c:2034)
 static int gext_higgs_energy(scp_gpu *h, double *e) {
     const int nb = red_blocks(h->N3);
-    gext_higgs_energy_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->gs, h->gc, h->part);
+    const size_t hf = (size_t)(15 + 3 * h->g2) * h->N3;
+    const double *X = h->X[h->cur ^ 1];
+    hu_higgs_energy_kernel<<<nb, kRedThreads, 0, h->stream>>>(X, X + hf, h->S + hf, h->hc, h->part);
     fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
     CK(cudaGetLastError());
     int rc;
@@ -789,58 +778,110 @@ static DiagConsts diag_consts(const scp_gpu *h);
 template <class View>
 static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out);
 
-static void mf_forces(scp_gpu *h) {
-    const int nb = red_blocks(h->N3);
-    mf_plaq_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
-    mf_force_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
+// slots of the three-fabric layout
+constexpr int kFabL = 15, kFabQ = 27;
+
+// the fabrics at the time of buffers (X, P)
+static FabView fab_view(const scp_gpu *h, const double *X, const double *P) {
+    const size_t n3 = h->N3;
+    FabView f;
+    f.XC = X; f.PC = P;
+    f.XL = X + kFabL * n3; f.PL = P + kFabL * n3;
+    f.XQ = h->fab_lock ? X : X + kFabQ * n3;
+    f.PQ = h->fab_lock ? P : P + kFabQ * n3;
+    f.N3 = h->N3;
+    for (int q = 0; q < 3; q++) f.q[q] = h->qfab[q];
+    return f;
 }
 
-// nsteps of verlet_step's multi-fabric branch (scp_sim.c:1583-1716): kick +
-// drift, plaquettes, forces per step; the closing kick + sponge of each step
-// runs inside the next step's first sweep, and on its own after the last
-static int mf_steps(scp_gpu *h, int nsteps) {
-    const int nb = red_blocks(h->N3);
-    for (int n = 0; n < nsteps; n++) {
-        if (n == 0) mf_kick_drift_kernel<false><<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
-        else mf_kick_drift_kernel<true><<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
-        mf_forces(h);
+// one step of the three-fabric stepper: C (with the locked Q's force and
+// currents), Q when free, L, then the links
+static int fab_launch_step(scp_gpu *h, bool first, bool sync) {
+    const size_t n3 = h->N3;
+    const double *X = h->X[h->cur];
+    double *Xo = h->X[h->cur ^ 1];
+    const double *Win = first ? h->S : h->W;
+    const double g = h->p.g_gauge;
+    auto fabric = [&](size_t slot, double qf, bool second, double qx, bool acc) -> int {
+        FabIO io;
+        io.x = X + slot * n3;
+        io.th = X + (size_t)FTH * n3;
+        io.xout = Xo + slot * n3;
+        io.win = Win + slot * n3;
+        io.wout = h->W + slot * n3;
+        io.sout = h->S + slot * n3;
+        io.kacc = h->kacc;
+        io.flag = h->flag;
+        io.qf = qf;
+        io.gqf = g * qf;
+        io.qx = qx;
+        io.gqx = g * qx;
+        io.first = first;
+        io.sync = sync;
+        io.damp = damping_on(h);
+        io.accumulate = acc;
+        io.second = second;
+        CK(fabric_step(second ? h->xplan2 : h->xplan, h->fc, io, h->stream));
+        return SCP_OK;
+    };
+    int rc;
+    const double qC = h->qfab[0], qQ = h->qfab[1], qL = h->qfab[2];
+    if (h->fab_lock) {
+        // C moves under the q_Q force; its q_C current precedes the q_Q one (none when q_C = 0)
+        if ((rc = fabric(0, qQ, qC != 0.0, qC, false))) return rc;
+    } else {
+        if ((rc = fabric(0, qC, false, 0.0, false))) return rc;
+        if ((rc = fabric(kFabQ, qQ, false, 0.0, true))) return rc;
     }
-    mf_kick_damp_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc);
-    CK(cudaGetLastError());
+    if ((rc = fabric(kFabL, qL, false, 0.0, true))) return rc;
+    LinkIO io;
+    io.th = X + (size_t)FTH * n3;
+    io.thout = Xo + (size_t)FTH * n3;
+    io.kacc = h->kacc;
+    io.win = Win + (size_t)FTH * n3;
+    io.wout = h->W + (size_t)FTH * n3;
+    io.sout = h->S + (size_t)FTH * n3;
+    io.flag = h->flag;
+    io.first = first;
+    io.sync = sync;
+    io.damp = damping_on(h);
+    CK(link_step(h->lplan, h->fc, io, h->stream));
+    h->cur ^= 1;
     return SCP_OK;
 }
 
-// the start-up of main with three fabrics (scp_sim.c:2818-2836): fabrics in
-// place, net-charge check and Gauss projection with rho_em, first forces
+// the start-up of main with three fabrics (scp_sim.c:2818-2836): net-charge
+// check and Gauss projection with rho_em, frozen offset
 static int mf_gauss_startup(scp_gpu *h) {
     const long long n3 = h->N3;
     const int nb = red_blocks(n3);
+    const FabView f = fab_view(h, h->X[0], h->S);
+    const scp_gpu_params &p = h->p;
     int rc;
-    if (h->p.bc_type == 2) {
-        mf_net_charge_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc, h->part);
+    if (p.bc_type == 2) {
+        fabric_net_charge_kernel<<<nb, kRedThreads, 0, h->stream>>>(f, p.dx * p.dx * p.dx, h->part);
         fold_partials_kernel<2, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
         CK(cudaGetLastError());
         if ((rc = fold_to_host(h, 2))) return rc;
         const double qn = fold_get(h, 0), qa = fold_get(h, 1);
         if (fabs(qn) > 1e-6 * fmax(qa, 1.0)) return SCP_ENETCHARGE;
     }
-    if (!h->p.gauss_project) return SCP_OK;
+    if (!p.gauss_project) return SCP_OK;
     double *tmp = nullptr;
     CK(cudaMallocAsync(&tmp, sizeof(double) * 5 * n3, h->stream));
-    double *b = tmp, *x = tmp + n3, *r = tmp + 2 * n3, *p = tmp + 3 * n3, *Ap = tmp + 4 * n3;
-    mf_gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc, b, h->part);
-    if ((rc = cg_solve(h, nb, b, x, r, p, Ap, &h->cg_iters))) {
+    double *b = tmp, *x = tmp + n3, *r = tmp + 2 * n3, *pp = tmp + 3 * n3, *Ap = tmp + 4 * n3;
+    fabric_gauss_kernel<<<nb, kRedThreads, 0, h->stream>>>(f, h->N, p.dx, p.g_gauge, b, h->part);
+    if ((rc = cg_solve(h, nb, b, x, r, pp, Ap, &h->cg_iters))) {
         cudaFreeAsync(tmp, h->stream);
         return rc;
     }
-    gauss_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(gauss_args(h, h->ms.XC, h->ms.SC), x, h->cg);
-    mf_gauss_rhs_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc, nullptr, h->part);
+    gauss_correct_kernel<<<nb, kRedThreads, 0, h->stream>>>(gauss_args(h, h->X[0], h->S), x, h->cg);
+    fabric_gauss_kernel<<<nb, kRedThreads, 0, h->stream>>>(f, h->N, p.dx, p.g_gauge, nullptr, h->part);
     fold_partials_kernel<1, 0><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
     CK(cudaGetLastError());
     CK(cudaFreeAsync(tmp, h->stream));
     if ((rc = fold_to_host(h, 1))) return rc;
     h->G_offset = fold_get(h, 0) / (double)n3;
-    h->mc.G_offset = h->G_offset;
     return SCP_OK;
 }
 
@@ -849,40 +890,23 @@ static int init_mf(scp_gpu *h, const double *const *cols, bool on_device) {
     if ((rc = alloc_common(h))) return rc;
     const long long n3 = h->N3;
     const scp_gpu_params &p = h->p;
-    const int lock = p.mf_lock_CQ ? 1 : 0;
-    // C: X S A (15 each); L: X S A (12 each); Q: X S A (12 each) unless locked; PS (3)
-    const size_t narr = 45 + 36 + (lock ? 0 : 36) + 3;
-    CK(cudaMallocAsync(&h->mbuf, sizeof(double) * narr * (size_t)n3, h->stream));
-    CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
-    h->dev_bytes += sizeof(double) * (narr + 1) * (size_t)n3;
-    CK(cudaMemsetAsync(h->mbuf, 0, sizeof(double) * narr * (size_t)n3, h->stream));
-    MfState &m = h->ms;
-    double *b = h->mbuf;
-    m.XC = b; b += 15 * n3;
-    m.SC = b; b += 15 * n3;
-    m.AC = b; b += 15 * n3;
-    m.XL = b; b += 12 * n3;
-    m.SL = b; b += 12 * n3;
-    m.AL = b; b += 12 * n3;
-    if (lock) {
-        m.XQ = m.XC; m.SQ = m.SC; m.AQ = m.AC;
-    } else {
-        m.XQ = b; b += 12 * n3;
-        m.SQ = b; b += 12 * n3;
-        m.AQ = b; b += 12 * n3;
-    }
-    m.PS = b;
+    h->fab_lock = p.mf_lock_CQ ? 1 : 0;
+    for (int q = 0; q < 3; q++) h->qfab[q] = p.q_fab[q];
+    if ((rc = ext_slab(h, h->fab_lock ? 27 : 39))) return rc;
+    CK(cudaMallocAsync(&h->kacc, sizeof(double) * 3 * (size_t)n3, h->stream));
+    h->dev_bytes += sizeof(double) * 3 * n3;
+    // columns: C with the links (0-29), Q (30-53, skipped when locked), L (54-77)
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     for (int c = 0; c < 78; c++) {
+        if (c >= 30 && c < 54 && h->fab_lock) continue;
         const int base = c < 30 ? 0 : (c < 54 ? 30 : 54);
-        if (base == 30 && lock) continue;   // Q is C
+        const size_t slot = base == 0 ? 0 : (base == 30 ? kFabQ : kFabL);
         int field, mom;
         sfa_col_source(c - base, &field, &mom);
-        double *X = base == 0 ? m.XC : (base == 30 ? m.XQ : m.XL);
-        double *S = base == 0 ? m.SC : (base == 30 ? m.SQ : m.SL);
-        CK(cudaMemcpyAsync((mom ? S : X) + (size_t)field * n3, cols[c], sizeof(double) * n3, kind, h->stream));
+        CK(cudaMemcpyAsync((mom ? h->S : h->X[0]) + (slot + field) * n3, cols[c], sizeof(double) * n3, kind,
+                           h->stream));
     }
-    MfConsts &k = h->mc;
+    FabConsts &k = h->fc;
     k.N = p.N; k.N3 = n3; k.L = p.L; k.dx = p.dx; k.dV = p.dx * p.dx * p.dx;
     k.idx1 = 1.0 / (2.0 * p.dx); k.idx2 = 1.0 / (p.dx * p.dx); k.inva = 1.0 / p.dx;
     k.hdt = 0.5 * p.dt; k.dt = p.dt;
@@ -890,34 +914,26 @@ static int init_mf(scp_gpu *h, const double *const *cols, bool on_device) {
     k.g = p.g_gauge;
     k.stp = 1.0 / (p.g_gauge * p.dx * p.dx * p.dx);
     k.gad = -p.g_gauge * p.dx * p.dt;
-    for (int f = 0; f < 3; f++) k.q[f] = p.q_fab[f];
-    k.lock = lock;
-    k.damp = damping_on(h) ? 1 : 0;
     k.damp_width = p.damp_width; k.damp_rate = p.damp_rate;
-    const double Rint = (p.bc_type == 0) ? (p.L - p.damp_width - p.dx) : 1e300;
-    k.Rint2 = Rint * Rint;
-    k.G_offset = 0.0;
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    if (fabric_plan(h->N, nsm, &h->xplan, &h->xplan2, &h->lplan)) return SCP_EUNSUPPORTED;
     if ((rc = mf_gauss_startup(h))) return rc;
-    mf_forces(h);
-    CK(cudaGetLastError());
-    // the generic diagnostics, snapshot and info code reads these
-    h->X[0] = h->X[1] = m.XC;
-    h->S = m.SC;
-    h->cur = 0;
-    h->shape = 1;
-    return SCP_OK;
+    return fab_launch_step(h, true, false);
 }
 
 // fabric C's diagnostics, plus fabric L's energies (compute_energy_complex_gauge,
 // scp_sim.c:1977-2028), the Gauss norm with rho_em and the fabric charges
 static int mf_diag(scp_gpu *h, scp_gpu_diag_out *out) {
-    ViewF64 V{h->ms.XC, h->ms.SC, h->N3};
+    const double *X = h->X[h->cur ^ 1], *P = h->S;
+    const size_t n3 = h->N3;
+    ViewF64 V{X, P, h->N3};
     int rc = diag_with(h, V, out);
     if (rc && rc != SCP_ENONFINITE) return rc;
     const int nb = red_blocks(h->N3);
     const DiagConsts c = diag_consts(h);
-    ViewFab VL{h->ms.XL, h->ms.SL, h->ms.XC, h->ms.SC, h->N3};
-    diag_pass1_kernel<ViewFab><<<nb, kRedThreads, 0, h->stream>>>(VL, c, h->part);
+    ViewFabric VL{X + kFabL * n3, P + kFabL * n3, X, P, h->N3};
+    diag_pass1_kernel<ViewFabric><<<nb, kRedThreads, 0, h->stream>>>(VL, c, h->part);
     fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
     CK(cudaGetLastError());
     if ((rc = fold_to_host(h, DS_EC + 1))) return rc;
@@ -926,17 +942,19 @@ static int mf_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     o[SCP_DIAG_E_TOTAL] = o[SCP_DIAG_E_PHI_KIN] + o[SCP_DIAG_E_THETA_KIN] + o[SCP_DIAG_E_GRAD] + o[SCP_DIAG_E_MASS] +
                           o[SCP_DIAG_E_POT] + o[SCP_DIAG_E_TGRAD] + o[SCP_DIAG_E_TMASS] + o[SCP_DIAG_E_COUPLING] +
                           o[SCP_DIAG_E_EM];
-    mf_diag_kernel<<<nb, kRedThreads, 0, h->stream>>>(h->ms, h->mc, h->part);
-    fold_partials_kernel<MS_NSUM, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    const scp_gpu_params &p = h->p;
+    fabric_diag_kernel<<<nb, kRedThreads, 0, h->stream>>>(fab_view(h, X, P), h->N, p.L, p.dx, p.g_gauge, c.Rint2,
+                                                          h->G_offset, h->part);
+    fold_partials_kernel<FS_NSUM, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
     CK(cudaGetLastError());
-    if ((rc = fold_to_host(h, MS_NSUM + 1))) return rc;
+    if ((rc = fold_to_host(h, FS_NSUM + 1))) return rc;
     const double *f = h->h_small, dV = c.dV;
-    o[SCP_DIAG_GAUSS_MAX] = f[MS_NSUM];
-    o[SCP_DIAG_GAUSS_L2] = f[MS_NOM] > 0 ? sqrt(f[MS_GL2] / f[MS_NOM]) : 0.0;
-    o[SCP_DIAG_Q_C] = f[MS_QC] * dV;
-    o[SCP_DIAG_Q_Q] = f[MS_QQ] * dV;
-    o[SCP_DIAG_Q_L] = f[MS_QL] * dV;
-    o[SCP_DIAG_Q_EM] = f[MS_QEM] * dV;
+    o[SCP_DIAG_GAUSS_MAX] = f[FS_NSUM];
+    o[SCP_DIAG_GAUSS_L2] = f[FS_NIN] > 0 ? sqrt(f[FS_GL2] / f[FS_NIN]) : 0.0;
+    o[SCP_DIAG_Q_C] = f[FS_QC] * dV;
+    o[SCP_DIAG_Q_Q] = f[FS_QQ] * dV;
+    o[SCP_DIAG_Q_L] = f[FS_QL] * dV;
+    o[SCP_DIAG_Q_EM] = f[FS_QEM] * dV;
     return isfinite(o[SCP_DIAG_E_TOTAL]) ? SCP_OK : SCP_ENONFINITE;
 }
 
@@ -953,14 +971,13 @@ static void col_source(const scp_gpu *h, int c, const double **X, const double *
     *X = h->X[h->cur ^ 1];
     *S = h->S;
     if (h->rp) { *field = c % 6; *mom = c >= 6; return; }   // the 6-field layout
-    if (c >= 30 && h->g2) {                                 // th2 / E2
-        *X = h->gs.T2; *S = h->gs.E2;
-        *field = (c - 30) % 3; *mom = c >= 33;
+    if (c >= 30 && h->g2) {                                 // th2 / E2 after the 15-field block
+        *field = 15 + (c - 30) % 3; *mom = c >= 33;
         return;
     }
-    if (c >= 30 && h->mfab) {                               // fabric L
-        *X = h->ms.XL; *S = h->ms.SL;
+    if (c >= 30 && h->mfab) {                               // fabric L after C
         sfa_col_source(c - 30, field, mom);
+        *field += kFabL;
         return;
     }
     sfa_col_source(c, field, mom);
@@ -1029,13 +1046,16 @@ int scp_gpu_step(scp_gpu *h, int nsteps) {
     CK(cudaSetDevice(h->device));
     int rc;
     if (h->gx || h->mfab) {
-        if ((rc = h->gx ? gext_steps(h, nsteps) : mf_steps(h, nsteps))) return rc;
+        for (int n = 0; n < nsteps; n++) {
+            const bool last = (n == nsteps - 1);
+            if ((rc = h->gx ? hu_launch_step(h, false, last) : fab_launch_step(h, false, last))) return rc;
+        }
         h->steps += nsteps;
         return SCP_OK;
     }
     if (h->rp) {
         for (int n = 0; n < nsteps; n++)
-            if ((rc = real_step(h))) return rc;
+            if ((rc = r6_launch_step(h, false, n == nsteps - 1))) return rc;
         h->steps += nsteps;
         return SCP_OK;
     }
@@ -1162,7 +1182,7 @@ int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     if (h->rp) return real_diag(h, out);
     if (h->mfab) return mf_diag(h, out);
     if (h->gx) {
-        ViewF64 V{h->gs.X, h->gs.S, h->N3};
+        ViewF64 V{h->X[h->cur ^ 1], h->S, h->N3};
         int rc = diag_with(h, V, out);
         if (rc || !h->higgs) return rc;
         double eh = 0.0;
@@ -1346,7 +1366,7 @@ int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
     // extensions: positions and momenta (30), th2 / E2 (6), H / Hdot (2), FP64
     if (h->gx) info->state_bytes_per_site = 8.0 * (30.0 + 6.0 * h->g2 + 2.0 * h->higgs);
     // three fabrics: C with the links (30), L (24), Q (24) unless it is C
-    if (h->mfab) info->state_bytes_per_site = 8.0 * (30.0 + 24.0 + (h->mc.lock ? 0.0 : 24.0));
+    if (h->mfab) info->state_bytes_per_site = 8.0 * (30.0 + 24.0 + (h->fab_lock ? 0.0 : 24.0));
     info->step_bytes_per_site = 2.0 * info->state_bytes_per_site;
     info->tile_x = kShapes[h->shape].tx;
     info->tile_y = kShapes[h->shape].ty;
@@ -1378,7 +1398,7 @@ void scp_gpu_free(scp_gpu *h) {
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->stream) {
         void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->count, h->stage,
-                        h->snap_dev, h->rbuf, h->gbuf, h->mbuf};
+                        h->snap_dev, h->raux, h->kacc};
         for (void *b : bufs)
             if (b) cudaFreeAsync(b, h->stream);
         cudaStreamSynchronize(h->stream);
