@@ -45,7 +45,7 @@
 extern "C" {
 #endif
 
-#define SCP_GPU_ABI_VERSION 5
+#define SCP_GPU_ABI_VERSION 6
 #define SCP_GPU_MAX_COLS 78
 
 /* status codes */
@@ -153,6 +153,9 @@ typedef struct {
     double  step_bytes_per_site;    /* algorithmic bytes moved per site-update */
     int32_t tile_x, tile_y, seg_len; /* tile shape in use */
     int32_t sites_per_thread; /* 2: two-site packed FP32C kernel (even N), else 1 */
+    int32_t tma_staging;      /* 1: the FP64 step stages its planes with TMA tile loads
+                                 (full tiles of the default shapes; SCP_STAGING=cp in the
+                                 environment selects the cp.async ring instead), else 0 */
 } scp_gpu_info;
 
 typedef struct scp_gpu scp_gpu;

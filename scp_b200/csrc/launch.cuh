@@ -32,6 +32,11 @@ MultiFn<F32C> multi_fn_f32c(int shape, bool g, bool d, size_t *smem);
 StepFnT<F32C> step2_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
 MultiFn<F32C> multi2_fn(int shape, bool g, bool d, size_t *smem);
 
+// FP64 kernels with TMA plane staging (tma.cuh; shapes 1 and 2, full tiles only)
+struct TmaMaps;
+using TmaStepFn = void (*)(StepIO<F64>, StepConsts, TileGrid, const TmaMaps);
+TmaStepFn step_tma_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
+
 template <class P>
 StepFnT<P> step_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
 template <>

@@ -23,12 +23,14 @@
 #include "snapshot.cuh"
 #include "spectral.cuh"
 #include "launch.cuh"
+#include "tma.cuh"
 #include "ext_launch.cuh"
 #include "ext_startup.cuh"
 
 #include <cuda.h>   // driver API types only (entry points come through the runtime)
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -142,6 +144,10 @@ struct scp_gpu {
     size_t snap_dev_bytes = 0;
     cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
     int snap_pending = 0;
+    // TMA plane staging of the FP64 fused step (tma.cuh): the tensor maps of
+    // X[0] and X[1]
+    int tma = 0;
+    TmaMaps tmaps[2];
     // launch geometry
     int shape;
     int pairs = 0;               // 1: two-site packed FP32C kernel
@@ -266,6 +272,71 @@ static int occupancy2_of(scp_gpu *h, int shape, int *occ) {
 
 // FP32C grids of even N run the two-site packed kernel; the default tile is
 // 32 x 4 (one site per thread) and 32 x 8 (site pairs: 128 threads)
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link libcuda)
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (EncodeTiledFn)f;
+    }();
+    return fn;
+}
+
+// The tensor maps of one FP64 position buffer (nf fields of N^3): a 4-D view
+// (k, j, i, field) with boxes of TX x {TY+2, TY+1, 1} rows.  The buffer is the
+// handle's own allocation on this device.
+static bool encode_maps(const double *X, int N, int nf, int tx, int ty, TmaMaps *m) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t n = (cuuint64_t)N;
+    const cuuint64_t dims[4] = {n, n, n, (cuuint64_t)nf};
+    const cuuint64_t strides[3] = {n * 8, n * n * 8, n * n * n * 8};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUtensorMap *dst[3] = {&m->full, &m->part, &m->row};
+    const cuuint32_t rows[3] = {(cuuint32_t)ty + 2, (cuuint32_t)ty + 1, 1};
+    for (int q = 0; q < 3; q++) {
+        const cuuint32_t box[4] = {(cuuint32_t)tx, rows[q], 1, 1};
+        if (enc(dst[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)X, dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
+
+// TMA staging applies to FP64 grids cut into full tiles, with a 16-byte row
+// pitch and at least two tile rows along j; SCP_STAGING=cp in the environment
+// keeps the cp.async ring (for side-by-side measurements).
+static bool tma_eligible(const scp_gpu *h, int shape) {
+    if (h->prec != SCP_PREC_FP64 || (shape != 1 && shape != 2)) return false;
+    const char *e = getenv("SCP_STAGING");
+    if (e && strcmp(e, "cp") == 0) return false;
+    const TileShape ts = kShapes[shape];
+    const int N = h->N;
+    return N % 2 == 0 && N % ts.tx == 0 && N % ts.ty == 0 && N >= 2 * ts.ty && N >= ts.tx;
+}
+
+static int setup_tma(scp_gpu *h, int *occ) {
+    const TileShape ts = kShapes[h->shape];
+    size_t smem = 0;
+    for (int v = 0; v < 8; v++) {
+        TmaStepFn fn = step_tma_fn(h->shape, h->gauged, v & 1, (v >> 1) & 1, (v >> 2) & 1, &smem);
+        CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    TmaStepFn fn = step_tma_fn(h->shape, h->gauged, false, false, false, &smem);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, (const void *)fn, ts.tx * ts.ty, smem));
+    for (int b = 0; b < 2; b++)
+        if (!encode_maps(h->X[b], h->N, h->nf, ts.tx, ts.ty, &h->tmaps[b])) return SCP_EUNSUPPORTED;
+    return SCP_OK;
+}
+
 static int setup_launch(scp_gpu *h) {
     const bool pairs = h->prec == SCP_PREC_FP32C && h->N % 2 == 0;
     int shape = h->p.tile_variant;
@@ -277,7 +348,9 @@ static int setup_launch(scp_gpu *h) {
     const TileShape ts = kShapes[shape];
     h->threads = ts.tx * ts.ty / (pairs ? 2 : 1);
     int occ = 0, rc;
-    if (pairs) rc = occupancy2_of(h, shape, &occ);
+    h->tma = tma_eligible(h, shape) ? 1 : 0;
+    if (h->tma) rc = setup_tma(h, &occ);
+    else if (pairs) rc = occupancy2_of(h, shape, &occ);
     else if (h->prec == SCP_PREC_FP64) rc = occupancy_of<F64>(h, shape, &occ);
     else rc = occupancy_of<F32C>(h, shape, &occ);
     if (rc) return rc;
@@ -290,7 +363,6 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
     size_t smem = 0;
     const TileShape ts = kShapes[h->shape];
     if (h->prec == SCP_PREC_FP64) {
-        StepFnT<F64> fn = step_fn<F64>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
         StepIO<F64> io;
         io.xin = h->X[h->cur];
         io.xout = h->X[h->cur ^ 1];
@@ -302,7 +374,13 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         io.wout = h->W;
         io.sout = h->S;
         io.flag = h->flag;
-        fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+        if (h->tma) {
+            TmaStepFn fn = step_tma_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
+            fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg, h->tmaps[h->cur]);
+        } else {
+            StepFnT<F64> fn = step_fn<F64>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
+            fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+        }
     } else {
         StepIO<F32C> io;
         io.xin = h->X32[h->cur];
@@ -1074,6 +1152,7 @@ int scp_gpu_sync(scp_gpu *h) {
     CK(cudaStreamSynchronize(h->stream));
     int f = 0;
     memcpy(&f, h->h_small, sizeof(int));
+    if (f & kFlagTimeout) return SCP_ETIMEOUT;
     return f ? SCP_ENONFINITE : SCP_OK;
 }
 
@@ -1372,6 +1451,7 @@ int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
     info->tile_y = kShapes[h->shape].ty;
     info->seg_len = h->tg.seg;
     info->sites_per_thread = h->pairs ? 2 : 1;
+    info->tma_staging = h->tma;
     return SCP_OK;
 }
 

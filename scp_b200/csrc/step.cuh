@@ -113,20 +113,99 @@ __device__ __forceinline__ double link_wrap(double v) {
     return wrap_angle(v);
 }
 
-// One work item (a TX x TY column over one segment of planes) of one grid.
-// sync and damp are uniform per call; the single-grid kernel passes them as
-// constants, the multi-request kernel per request.
-template <class P, int TX, int TY, bool GAUGED, bool FIRST>
-__device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts &c, const TileGrid &tg, int item,
-                                          const bool SYNC, const bool DAMP, unsigned char *smem_raw) {
+// Plane staging of the classic ring: every thread copies its own site with
+// cp.async, and the halo rows and columns (periodic wrap, two corners for
+// the gauged plaquettes) are spread over the CTA's threads.  Slot layout
+// [NR][PY][PX] of StepLayout; any grid size.
+template <class P, int TX, int TY, bool GAUGED>
+struct CpStage {
     using T = typename P::T;
     using LY = StepLayout<P, TX, TY, GAUGED>;
-    constexpr int NF = LY::NF, PX = LY::PX, PY = LY::PY, NT = LY::NT;
-    T *xs = reinterpret_cast<T *>(smem_raw);     // [3][NR][PY][PX]
-    constexpr int NR = LY::NR;
-    auto XS = [&](int slot, int f, int r, int col) -> T & {
+    static constexpr int NF = LY::NF, NR = LY::NR, PX = LY::PX, PY = LY::PY, NT = LY::NT;
+    T *xs;
+    int N;
+    long long N3;
+    bool act;
+    int oc, c_s;
+    int h_s[LY::HPT], h_g[LY::HPT], h_nf[LY::HPT];
+
+    __device__ __forceinline__ explicit CpStage(unsigned char *smem) : xs(reinterpret_cast<T *>(smem)) {}
+
+    // per-item set-up: this thread's own site and its halo copies
+    __device__ __forceinline__ void begin(const StepConsts &c, int k0, int j0, int nk, int nj) {
+        N = c.N;
+        N3 = c.N3;
+        const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+        act = (tx < nk) && (ty < nj);
+        oc = (j0 + ty) * N + k0 + tx;
+        c_s = (ty + 1) * PX + tx + 1;
+        const int jlo = wrapi(j0 - 1, N), jhi = wrapi(j0 + nj, N);
+        const int klo = wrapi(k0 - 1, N), khi = wrapi(k0 + nk, N);
+#pragma unroll
+        for (int q = 0; q < LY::HPT; q++) {
+            const int h = tid + q * NT;
+            int r = 0, col = 0, gj = 0, gk = 0, nf = 0;
+            if (h < nk) { r = 0; col = h + 1; gj = jlo; gk = k0 + h; nf = NF; }
+            else if (h < 2 * nk) { r = nj + 1; col = h - nk + 1; gj = jhi; gk = k0 + h - nk; nf = NF; }
+            else if (h < 2 * nk + nj) { r = h - 2 * nk + 1; col = 0; gj = j0 + h - 2 * nk; gk = klo; nf = NF; }
+            else if (h < 2 * nk + 2 * nj) { r = h - 2 * nk - nj + 1; col = nk + 1; gj = j0 + h - 2 * nk - nj; gk = khi; nf = NF; }
+            else if (GAUGED && h == 2 * nk + 2 * nj) { r = nj + 1; col = 0; gj = jhi; gk = klo; nf = 3; }
+            else if (GAUGED && h == 2 * nk + 2 * nj + 1) { r = 0; col = nk + 1; gj = jlo; gk = khi; nf = 3; }
+            h_s[q] = r * PX + col;
+            h_g[q] = gj * N + gk;
+            h_nf[q] = nf;
+        }
+    }
+
+    __device__ __forceinline__ void issue(const StepIO<P> &io, int p, int slot) {
+        const long long pb = (long long)wrapi(p, N) * N * N;
+        T *sbase = xs + slot * LY::PLANE;
+        const T *gbase = io.xin + pb;
+        if (act) {
+#pragma unroll
+            for (int f = 0; f < NF; f++)
+                cp_async_elem(sbase + f * PY * PX + c_s, gbase + f * N3 + oc);
+            if constexpr (NR > NF) {
+#pragma unroll
+                for (int f = NF; f < NR; f++)
+                    cp_async_elem(sbase + f * PY * PX + c_s, io.tloin + pb + (f - NF) * N3 + oc);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < LY::HPT; q++) {
+            const int nf = h_nf[q];
+            if (nf == 0) continue;
+            const int f0 = (nf == NF) ? 0 : FTH;   // corners carry only the link angles
+#pragma unroll
+            for (int f = 0; f < NF; f++)
+                if (f >= f0) cp_async_elem(sbase + f * PY * PX + h_s[q], gbase + f * N3 + h_g[q]);
+            if constexpr (NR > NF) {
+#pragma unroll
+                for (int f = NF; f < NR; f++)
+                    cp_async_elem(sbase + f * PY * PX + h_s[q], io.tloin + pb + (f - NF) * N3 + h_g[q]);
+            }
+        }
+    }
+    __device__ __forceinline__ void commit() { cp_async_commit(); }
+    // everything issued so far has landed (for this thread; a barrier follows)
+    __device__ __forceinline__ void wait(int) { cp_async_wait<0>(); }
+    __device__ __forceinline__ bool failed() const { return false; }
+    __device__ __forceinline__ T at(int slot, int f, int r, int col) const {
         return xs[((slot * NR + f) * PY + r) * PX + col];
-    };
+    }
+};
+
+// One work item (a TX x TY column over one segment of planes) of one grid.
+// sync and damp are uniform per call; the single-grid kernel passes them as
+// constants, the multi-request kernel per request.  Stage stages the planes.
+template <class P, int TX, int TY, bool GAUGED, bool FIRST, class Stage>
+__device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts &c, const TileGrid &tg, int item,
+                                          const bool SYNC, const bool DAMP, Stage &stg) {
+    using T = typename P::T;
+    using LY = StepLayout<P, TX, TY, GAUGED>;
+    constexpr int NF = LY::NF;
+    constexpr int NR = LY::NR;
+    auto XS = [&](int slot, int f, int r, int col) -> T { return stg.at(slot, f, r, col); };
     const int N = c.N;
     const long long N3 = c.N3;
     const int tid = threadIdx.x;
@@ -145,56 +224,8 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
         const int nk = min(k0 + TX, N) - k0, nj = min(j0 + TY, N) - j0;   // valid extent of the tile
         const bool act = (tx < nk) && (ty < nj);
         const int oc = j * N + k;                                          // in-plane offset (act only)
-        const int jlo = wrapi(j0 - 1, N), jhi = wrapi(j0 + nj, N);
-        const int klo = wrapi(k0 - 1, N), khi = wrapi(k0 + nk, N);
-
-        // halo copies of this thread: smem (row, col) and in-plane global offset
-        int h_s[LY::HPT], h_g[LY::HPT], h_nf[LY::HPT];
-#pragma unroll
-        for (int q = 0; q < LY::HPT; q++) {
-            const int h = tid + q * NT;
-            int r = 0, col = 0, gj = 0, gk = 0, nf = 0;
-            if (h < nk) { r = 0; col = h + 1; gj = jlo; gk = k0 + h; nf = NF; }
-            else if (h < 2 * nk) { r = nj + 1; col = h - nk + 1; gj = jhi; gk = k0 + h - nk; nf = NF; }
-            else if (h < 2 * nk + nj) { r = h - 2 * nk + 1; col = 0; gj = j0 + h - 2 * nk; gk = klo; nf = NF; }
-            else if (h < 2 * nk + 2 * nj) { r = h - 2 * nk - nj + 1; col = nk + 1; gj = j0 + h - 2 * nk - nj; gk = khi; nf = NF; }
-            else if (GAUGED && h == 2 * nk + 2 * nj) { r = nj + 1; col = 0; gj = jhi; gk = klo; nf = 3; }
-            else if (GAUGED && h == 2 * nk + 2 * nj + 1) { r = 0; col = nk + 1; gj = jlo; gk = khi; nf = 3; }
-            h_s[q] = r * PX + col;
-            h_g[q] = gj * N + gk;
-            h_nf[q] = nf;
-        }
-        const int c_s = (ty + 1) * PX + tx + 1;
-
-        auto issue_plane = [&](int p, int slot) {
-            const long long pb = (long long)wrapi(p, N) * N * N;
-            T *sbase = xs + slot * LY::PLANE;
-            const T *gbase = io.xin + pb;
-            if (act) {
-#pragma unroll
-                for (int f = 0; f < NF; f++)
-                    cp_async_elem(sbase + f * PY * PX + c_s, gbase + f * N3 + oc);
-                if constexpr (NR > NF) {
-#pragma unroll
-                    for (int f = NF; f < NR; f++)
-                        cp_async_elem(sbase + f * PY * PX + c_s, io.tloin + pb + (f - NF) * N3 + oc);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < LY::HPT; q++) {
-                const int nf = h_nf[q];
-                if (nf == 0) continue;
-                const int f0 = (nf == NF) ? 0 : FTH;   // corners carry only the link angles
-#pragma unroll
-                for (int f = 0; f < NF; f++)
-                    if (f >= f0) cp_async_elem(sbase + f * PY * PX + h_s[q], gbase + f * N3 + h_g[q]);
-                if constexpr (NR > NF) {
-#pragma unroll
-                    for (int f = NF; f < NR; f++)
-                        cp_async_elem(sbase + f * PY * PX + h_s[q], io.tloin + pb + (f - NF) * N3 + h_g[q]);
-                }
-            }
-        };
+        stg.begin(c, k0, j0, nk, nj);
+        auto issue_plane = [&](int p, int slot) { stg.issue(io, p, slot); };
 
         // sine of the plaquette angle th_a(y) + th_b(y+a) - th_a(y+b) - th_b(y) of plane
         // (a,b) = (0,1) (1,2) (2,0) [q = 0, 1, 2] at ring position (r, col) of slot sc,
@@ -219,8 +250,9 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
         __syncthreads();   // previous item finished reading the ring
         issue_plane(i0 - 1, 0);
         issue_plane(i0, 1);
-        cp_async_commit();
-        cp_async_wait<0>();
+        stg.commit();
+        stg.wait(0);
+        stg.wait(1);
         __syncthreads();
         T xm[12];          // x(i-1) at this thread's site, matter fields
 #pragma unroll
@@ -233,14 +265,14 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             P2m = plaq_sin(2, 0, 1, ty + 1, tx + 1);
         }
         issue_plane(i0 + 1, 2);
-        cp_async_commit();
+        stg.commit();
 
         for (int i = i0; i < i1; i++) {
             const int sc = (i - i0 + 1) % 3, sp = (i - i0 + 2) % 3, sn = (i - i0) % 3;
-            cp_async_wait<0>();
+            stg.wait(sp);
             __syncthreads();
             if (i + 2 <= i1) issue_plane(i + 2, sn);
-            cp_async_commit();
+            stg.commit();
             const long long site = (long long)i * N * N + oc;
             T w[NF];
             uint16_t lo[P::COMP ? 12 : 1];
@@ -522,8 +554,9 @@ template <class P, int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP
 __global__ void __launch_bounds__(TX * TY, (MinBlocks<P, TX, TY, GAUGED>::value))
 step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    CpStage<P, TX, TY, GAUGED> stg(smem_raw);
     for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x)
-        step_item<P, TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, smem_raw);
+        step_item<P, TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, stg);
 }
 
 // ---------------------------------------------------------------- many grids per launch
@@ -583,7 +616,8 @@ step_multi_kernel(const ReqTable<P> *tab, int k) {
         const StepIO<P> io = q.io[(int)((s - q.s0) & 1)];
         const StepConsts c = q.c;
         const TileGrid tg = q.tg;
-        step_item<P, TX, TY, GAUGED, false>(io, c, tg, item - q.item0, false, DAMP, smem_raw);
+        CpStage<P, TX, TY, GAUGED> stg(smem_raw);
+        step_item<P, TX, TY, GAUGED, false>(io, c, tg, item - q.item0, false, DAMP, stg);
     }
 }
 

@@ -59,6 +59,7 @@ class Info(ctypes.Structure):
         ("tile_y", ctypes.c_int32),
         ("seg_len", ctypes.c_int32),
         ("sites_per_thread", ctypes.c_int32),
+        ("tma_staging", ctypes.c_int32),
     ]
 
 

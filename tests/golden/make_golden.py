@@ -84,26 +84,36 @@ def real_case(name: str, N: int, nsteps: int, diag_every: int, **over):
     print(name, "written", r["wall_ms_per_step"], "ms/step")
 
 
-def workload_case(name: str, wl: str, nsteps: int, diag_every: int):
-    st = seeds.make_state(wl)
+def workload_case(name: str, wl: str, nsteps: int, diag_every: int, **over):
+    st = seeds.make_state(wl, seeds.params_for(wl, **over) if over else None)
     p = st.params
     r = oracle.run_reference(p, st.cols(), nsteps, diag_every=diag_every, threads=os.cpu_count())
     idx = sample_sites(p.N ** 3)
     fin = np.stack(r["cols"])
     np.savez_compressed(
         os.path.join(HERE, f"{name}.npz"),
-        workload=wl, nsteps=nsteps, diag_every=diag_every, sites=idx,
+        workload=wl, over=json.dumps(over), nsteps=nsteps, diag_every=diag_every, sites=idx,
         sample=fin[:, idx], col_l2=np.linalg.norm(fin, axis=1), col_sum=fin.sum(axis=1),
         diag=r["diag"], diag_header=np.array(r["diag_header"]), names=np.array(r["names"]))
     print(name, "written", r["wall_ms_per_step"], "ms/step")
 
 
+CASES = {
+    "ref_c1_64_1000": lambda: workload_case("ref_c1_64_1000", "c1", 1000, 10, N=64, L=15.75),
+}
+
 if __name__ == "__main__":
+    only = sys.argv[1:]
+    if only:   # regenerate the named fixtures only
+        for name in only:
+            CASES[name]()
+        sys.exit(0)
     small_case("ref_complex_n12", 12, False, 60, 10)
     small_case("ref_gauged_n12", 12, True, 60, 10)
     small_case("ref_gauged_n10_damped", 10, True, 40, 10, bc_type=0, damp_width=2.0, damp_rate=0.05)
     small_case("ref_complex_n13_damped", 13, False, 40, 10, bc_type=0, damp_width=2.0, damp_rate=0.05)
     workload_case("ref_c0_64_1000", "c0", 1000, 10)
+    CASES["ref_c1_64_1000"]()
     gext_case("ref_higgs_gauge2_n12", 12, 60, 10, seed=41, higgs_v=1.0, higgs_rvoid=2.0, g_gauge2=0.2)
     gext_case("ref_higgs_gauge2_n11_damped", 11, 40, 10, seed=43, higgs_v=0.8, higgs_lam=0.5, higgs_kap=1.5,
               g_gauge2=-0.15, gauge2_q0=1.0, gauge2_q1=-1.0, gauge2_q2=0.5,

@@ -57,7 +57,7 @@ def test_struct_layouts_match_c(tmp_path):
 
 def test_errstr_and_version_without_gpu():
     lib = native.lib()
-    assert lib.scp_gpu_abi_version() == 5
+    assert lib.scp_gpu_abi_version() == 6
     assert lib.scp_gpu_errstr(-4).decode().startswith("gauged periodic")
     assert lib.scp_gpu_errstr(0).decode() == "ok"
 

@@ -1,0 +1,116 @@
+"""Parity at the benchmarked configurations.
+
+* Gauged 64^3 (two opposite balls, e = 0.1), 1000 steps, against the
+  reference binary's own run committed as a fixture (sampled sites, per-column
+  norms and sums, every diag TSV row).
+* The bench workload itself, gauged 128^3 (two balls 20 sites apart, e =
+  0.1), 1000 steps with diagnostics every 10 steps, against the reference CPU
+  binary run on the same seed: 1e-10 relative L2 per field, every TSV column,
+  Gauss residual at roundoff throughout.
+* The precision workload, 256^3 gauged with thermal noise, 2000 steps in
+  FP32-compensated mode against FP64: field relative L2 <= 1e-5 and relative
+  total-energy difference <= 1e-6.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from scp_b200 import DIAG_NAMES, PREC_FP32C, Params, seeds
+from scp_b200.api import Simulation
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+# sums that cancel to roundoff are compared with an absolute floor
+ROUNDOFF = ("gauss_max", "gauss_l2", "Q_flux", "Q_phi", "Q_theta", "Q_total", "Q_core", "Q_p0", "Q_p1", "Q_p2",
+            "E_coupling")
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a).reshape(-1), np.asarray(b).reshape(-1)
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / nb if nb > 0 else np.linalg.norm(a - b)
+
+
+def check_tsv(have_rows, want_rows, header):
+    """have: diag vectors in slot order; want: the reference's TSV rows (t
+    first; printed with 7 significant digits for most columns)."""
+    want, have = np.asarray(want_rows), np.array(have_rows)
+    assert want.shape[0] == have.shape[0]
+    for ci, h in enumerate(header):
+        if h == "t":
+            continue
+        ref, got = want[:, ci], have[:, DIAG_NAMES.index(h)]
+        scale = np.maximum(np.abs(ref), 1e-9)
+        tol = np.maximum(1e-5 * scale, 1e-11) if h in ROUNDOFF else 2e-6 * scale
+        bad = np.abs(got - ref) > tol
+        assert not bad.any(), (h, int(np.argmax(bad)), got[bad][:3], ref[bad][:3])
+
+
+def run_with_diag(p, cols, nsteps, every):
+    rows = []
+    with Simulation(p, cols) as sim:
+        rows.append(sim.diag_vector())
+        for _ in range(nsteps // every):
+            sim.step(every)
+            rows.append(sim.diag_vector())
+        got = sim.snapshot()
+    return rows, got
+
+
+def test_gpu_gauged_64_1000_golden(gpu):
+    """The gauged 64^3 x 1000 run of the reference binary (tests/golden/
+    ref_c1_64_1000.npz, made by tests/golden/make_golden.py)."""
+    f = np.load(os.path.join(GOLD, "ref_c1_64_1000.npz"))
+    st = seeds.make_state("c1", seeds.params_for("c1", N=64, L=15.75))
+    rows, got = run_with_diag(st.params, st.cols(), int(f["nsteps"]), int(f["diag_every"]))
+    idx = f["sites"]
+    for c in range(30):
+        assert rel_l2(got[c][idx], f["sample"][c]) < 1e-10, c
+        assert abs(np.linalg.norm(got[c]) - f["col_l2"][c]) <= 1e-10 * max(f["col_l2"][c], 1e-300), c
+    check_tsv(rows, f["diag"], [str(h) for h in f["diag_header"]])
+    assert max(r[DIAG_NAMES.index("gauss_max")] for r in rows) < 1e-10
+
+
+def test_gpu_bench_workload_128_1000_vs_reference(gpu, reference):
+    """The bench workload (gauged 128^3, two balls, e = 0.1) for 1000 steps
+    with diagnostics every 10 steps, against the reference CPU binary run on
+    the same seed."""
+    st = seeds.make_state("c1")
+    p = st.params
+    cols = st.cols()
+    r = oracle.run_reference(p, cols, 1000, diag_every=10)
+    rows, got = run_with_diag(p, cols, 1000, 10)
+    assert len(r["cols"]) == 30
+    for c in range(30):
+        assert rel_l2(got[c], r["cols"][c]) < 1e-10, (c, r["names"][c])
+    check_tsv(rows, r["diag"], r["diag_header"])
+    assert max(row[DIAG_NAMES.index("gauss_max")] for row in rows) < 1e-10
+
+
+def test_gpu_precision_workload_256_2000(gpu):
+    """The precision workload (gauged 256^3 + N(0, 0.01) thermal noise):
+    2000 FP32-compensated steps against 2000 FP64 steps from the same seed."""
+    st = seeds.make_state("c2")
+    p64 = st.params
+    p32 = Params(**{**p64.__dict__, "precision": PREC_FP32C})
+    cols = st.cols()
+    del st
+    ie = DIAG_NAMES.index("E_total")
+    with Simulation(p64, cols) as a, Simulation(p32, cols) as b:
+        e0 = a.diag_vector()[ie]
+        for _ in range(4):
+            a.step(500)
+            b.step(500)
+        ea, eb = a.diag_vector()[ie], b.diag_vector()[ie]
+        A = a.snapshot()
+        B = b.snapshot()
+    assert abs(eb - ea) / abs(e0) <= 1e-6, (ea, eb, e0)
+    n = len(A[0])
+    worst = 0.0
+    for c in range(30):
+        if np.linalg.norm(A[c]) > 1e-3 * np.sqrt(n):
+            worst = max(worst, rel_l2(B[c], A[c]))
+    assert worst <= 1e-5, worst
