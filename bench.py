@@ -227,6 +227,36 @@ def reference_gpu(params, cols, n_short: int = 50, n_long: int = 250) -> dict:
                     "difference of a 250-step and a 50-step run"}
 
 
+def short_rate(workload: str, steps: int = 20, warmup: int = 5) -> dict:
+    """Device-timed site-updates/s and HBM roofline fraction of one workload,
+    a short run (the 256^3 target configurations of the FP64 and FP32C modes)."""
+    from scp_b200 import seeds
+    from scp_b200.api import Simulation
+    seed, prec, desc = WORKLOADS[workload]
+    params = seeds.params_for(seed, precision=prec)
+    st = workload_state(workload, params)
+    cols = st.cols()
+    del st
+    n3 = params.N ** 3
+    with Simulation(params, cols) as sim:
+        del cols
+        sim.step(warmup)
+        sim.sync()
+        clk = Clocks(params.device)
+        clk.start()
+        ms = sim.time_steps(steps)
+        sim.sync()
+        clocks = clk.stop()
+        info = sim.info()
+    peaks = measured_peaks()
+    achieved = info.step_bytes_per_site * n3 / (ms / steps * 1e-3) / 1e9
+    return {"workload": desc, "N": params.N, "value": n3 * steps / (ms * 1e-3), "unit": METRIC,
+            "ms_per_step": ms / steps, "steps": steps, "bytes_per_site": info.step_bytes_per_site,
+            "roofline_frac": achieved / peaks["hbm_gbs"], "achieved_gbs": achieved,
+            "tma_staging": int(info.tma_staging), "sites_per_thread": int(info.sites_per_thread),
+            "clocks": {"sm_mhz": clocks.get("sm_mhz"), "reasons": clocks.get("reasons")}}
+
+
 def run_reference_arm(args, rank, world):
     from scp_b200 import seeds
     seed, prec, desc = WORKLOADS[args.workload]
@@ -255,15 +285,22 @@ def step_bytes(params) -> float:
     return 2.0 * (4.0 * nf + 24.0 + (12.0 if params.complex_gauge else 0.0) + 4.0 * nf)
 
 
-def run_served_mix(args) -> dict:
-    """Served mixed queue (c3): aggregate site-updates/s of the server over
-    the whole makespan (submission of the first request to completion of the
-    last), per-request latency percentiles, and the same requests one after
-    another in FP64 through scp_gpu handles."""
+def request_lines(reqs, ids, srv) -> list[dict]:
+    """One record per served request: grid, steps, sites, and its times on the
+    server's clock (submission, admission, completion)."""
+    out = []
+    for r, i in zip(reqs, ids):
+        s = srv.status(i)
+        out.append({"id": int(i), "N": r.params.N, "steps": r.nsteps, "sites": r.params.N ** 3,
+                    "site_updates": r.site_updates, "gauged": int(r.params.complex_gauge),
+                    "e": r.params.g_gauge if r.params.complex_gauge else 0.0,
+                    "latency_s": s.t_done - s.t_submit, "queue_s": s.t_admit - s.t_submit,
+                    "service_s": s.t_done - s.t_admit, "state": int(s.state)})
+    return out
+
+
+def served_once(reqs, args, rate_label: float, log_path: str | None):
     from scp_b200 import serve
-    reqs = serve.served_mix(n=args.requests, seed=2, rate=args.rate)
-    total = sum(r.site_updates for r in reqs)
-    algo = sum(step_bytes(r.params) * r.site_updates for r in reqs)
     with serve.Server(device=0, max_active=args.max_active, chunk_steps=25) as srv:
         clk = Clocks(0)
         clk.start()
@@ -271,16 +308,52 @@ def run_served_mix(args) -> dict:
         clocks = clk.stop()
         st = srv.stats()
         bad = [i for i in ids if srv.status(i).state != serve.DONE]
+        recs = request_lines(reqs, ids, srv)
     if bad:
         raise RuntimeError(f"{len(bad)} served requests failed")
+    if log_path:
+        with open(log_path, "a") as f:
+            for rec in recs:
+                f.write(json.dumps({"rate_per_s": rate_label, **rec}) + "\n")
+    return ids, makespan, lat, clocks, st, recs
+
+
+def run_served_mix(args) -> dict:
+    """Served mixed queue (c3): aggregate site-updates/s of the server over
+    the whole makespan (submission of the first request to completion of the
+    last), per-request latency percentiles, and the same requests one after
+    another through scp_gpu handles in FP64 and in FP32C (so the batching gain
+    and the precision gain are reported apart).  A second served run at
+    --load (default 0.75) of the capacity the first run measured gives the
+    latency below saturation."""
+    from scp_b200 import serve, PREC_FP32C
+    reqs = serve.served_mix(n=args.requests, seed=2, rate=args.rate)
+    total = sum(r.site_updates for r in reqs)
+    algo = sum(step_bytes(r.params) * r.site_updates for r in reqs)
+    log_path = args.request_log or None
+    if log_path and os.path.exists(log_path):
+        os.remove(log_path)
+    ids, makespan, lat, clocks, st, recs = served_once(reqs, args, args.rate, log_path)
     value = total / makespan
-    seq = None
+    # service capacity in requests per second of device time
+    capacity = len(reqs) / max(st.t_gpu, 1e-9)
+    below = None
+    if args.load > 0:
+        rate2 = args.load * capacity
+        reqs2 = serve.served_mix(n=args.requests, seed=2, rate=rate2)
+        _, makespan2, lat2, _, _, _ = served_once(reqs2, args, rate2, log_path)
+        below = {"rate_per_s": rate2, "load": args.load, "makespan_s": makespan2,
+                 "latency_s": {"p50": float(np.percentile(lat2, 50)), "p99": float(np.percentile(lat2, 99)),
+                               "max": float(lat2.max())},
+                 "value": sum(r.site_updates for r in reqs2) / makespan2}
+    seq = {}
     if not args.no_sequential:
         nseq = len(reqs) if args.seq_sample <= 0 else min(args.seq_sample, len(reqs))
         sub = reqs[:nseq]
-        t = serve.run_sequential(sub)
-        seq = {"value": sum(r.site_updates for r in sub) / t, "unit": METRIC, "requests": nseq,
-               "precision": "fp64", "wall_s": t}
+        for name, prec in (("fp64", 0), ("fp32c", PREC_FP32C)):
+            t = serve.run_sequential(sub, precision=prec)
+            seq[name] = {"value": sum(r.site_updates for r in sub) / t, "unit": METRIC, "requests": nseq,
+                         "precision": name, "wall_s": t}
     peaks = measured_peaks()
     achieved = algo / makespan / 1e9
     sizes = {}
@@ -295,12 +368,16 @@ def run_served_mix(args) -> dict:
                    "parallelism": "single-gpu", "l2": "mixed sizes; makespan-level timing"},
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "max": float(lat.max())},
+        "latency_below_capacity": below,
+        "capacity_requests_per_s": capacity,
         "makespan_s": makespan,
-        "sequential_fp64": seq,
-        "served_over_sequential": (value / seq["value"]) if seq else None,
+        "sequential": seq or None,
+        "served_over_sequential_fp64": (value / seq["fp64"]["value"]) if seq else None,
+        "served_over_sequential_fp32c": (value / seq["fp32c"]["value"]) if seq else None,
         "server_phases_s": {"load": st.t_admit, "autotune": st.t_autotune, "run_wait": st.t_run,
                             "retire": st.t_retire, "idle_wait": st.t_wait, "launch": st.t_launch,
                             "gpu_chunks": st.t_gpu, "chunks": st.chunks},
+        "request_log": log_path,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"], "traffic": None,
                      "note": "algorithmic bytes of all requests / makespan (host phases included)"},
@@ -497,9 +574,15 @@ def main():
     ap.add_argument("--max-active", type=int, default=128, help="c3: server slots")
     ap.add_argument("--no-sequential", action="store_true", help="c3: skip the one-after-another FP64 run")
     ap.add_argument("--seq-sample", type=int, default=0, help="c3: run only the first R requests sequentially")
+    ap.add_argument("--load", type=float, default=0.75,
+                    help="c3: second served run at this fraction of the measured capacity (0: skip)")
+    ap.add_argument("--request-log", default="", help="c3: write one JSON line per served request to this file")
     ap.add_argument("--snap-every", type=int, default=100, help="snap: steps between SFA frames")
     ap.add_argument("--ref-gpu", action="store_true",
-                    help="also time the reference's own CUDA stepper on the same FP64 workload")
+                    help="also time the reference's own CUDA stepper on the same FP64 workload (always on for c1)")
+    ap.add_argument("--no-targets", action="store_true",
+                    help="c1: skip the short 256^3 FP64 / FP32C runs of the north-star targets")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="c1: skip the reference CUDA stepper")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
@@ -636,11 +719,19 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(params, cols, 10 if params.N <= 128 else 3)
-    if rank == 0 and world == 1 and args.ref_gpu and prec == 0:
+    default_c1 = args.workload == "c1" and not args.n
+    if rank == 0 and world == 1 and prec == 0 and (args.ref_gpu or (default_c1 and not args.no_ref_gpu)):
         rg = reference_gpu(params, cols)
         if rg.get("value"):
             rg["ours_over_reference_gpu"] = value / rg["value"]
         line["reference_gpu"] = rg
+    if rank == 0 and world == 1 and default_c1 and not args.no_targets:
+        # the north-star targets: FP64 >= 70% of HBM at 256^3, FP32C >= 1.8x FP64
+        t64 = short_rate("c2")
+        t32 = short_rate("c2f")
+        line["targets"] = {"fp64_256": t64, "fp32c_256": t32,
+                           "fp32c_over_fp64": t32["value"] / t64["value"],
+                           "goals": {"fp64_roofline_frac": 0.70, "fp32c_over_fp64": 1.8}}
     if rank == 0:
         print(json.dumps(line))
     if dist:

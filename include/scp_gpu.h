@@ -99,7 +99,7 @@ typedef struct {
      * zero = the default terms): mass mode 1 (m_eff^2 = inv_alpha/(1+inv_beta|phi|^2))
      * or 3 (kappa_eff = kappa/(1+kappa_gamma|phi|^2)), Cosserat strain alpha_cs,
      * curl-squared hardening beta_h, chiral helicity kappa_h.  With any of them set the
-     * real mode runs on separate FP64 per-site kernels (FP32C refused). */
+     * real mode runs on its own FP64 plane-ring kernels (FP32C refused). */
     int32_t mode;
     double  inv_alpha, inv_beta, kappa_gamma, alpha_cs, beta_h, kappa_h;
     /* Extensions of the gauged stepper (complex_gauge=1 and g_gauge != 0; ignored
@@ -108,8 +108,8 @@ typedef struct {
      * + (higgs_kap/2) s H^2, H starting at v, or with a tanh cavity of radius
      * higgs_rvoid (scp_sim.c:2802-2817).  Second compact U(1) gauge (g_gauge2 != 0)
      * with per-component charges gauge2_q[3] (scp_config.h:97-103); its links and
-     * field start at zero and are Gauss-projected at init.  Either runs on separate
-     * FP64 per-site kernels in the reference's three-pass form. */
+     * field start at zero and are Gauss-projected at init.  Either runs on one fused
+     * FP64 plane-ring kernel per step. */
     double  higgs_v, higgs_lam, higgs_kap, higgs_rvoid;
     double  g_gauge2;
     double  gauge2_q[3];
@@ -118,7 +118,8 @@ typedef struct {
      * FP64).  Each fabric has its own bag and couples to the links with charge
      * q_fab[f] (q_C, q_Q, q_L); the Gauss law uses sum_f q_f rho_f.  mf_lock_CQ = 1
      * keeps Q equal to C at every step (the Q columns passed to init are then
-     * ignored); 0 evolves Q on its own (scp_config.h:135-149). */
+     * ignored); 0 evolves Q on its own (scp_config.h:135-149).  A step is one FP64
+     * plane-ring kernel per fabric and one for the links. */
     int32_t n_fabrics;
     int32_t mf_lock_CQ;
     double  q_fab[3];
@@ -146,7 +147,10 @@ typedef struct {
     int64_t steps_done;       /* leapfrog steps taken since init */
     double  time;             /* steps_done * dt */
     double  G_offset;         /* frozen Gauss offset measured after projection */
-    int32_t cg_iterations;    /* Gauss projection CG iterations */
+    int32_t cg_iterations;    /* Gauss projection CG iterations after the spectral start
+                                 (the direct FFT solve of the same periodic 7-point problem,
+                                 for power-of-two N up to 512 and other N up to 192): 0 when
+                                 the start already meets the reference's stopping rule */
     int32_t precision_mode;
     int64_t device_bytes;     /* device memory held by the handle */
     double  state_bytes_per_site;   /* persistent bytes per site of the layout */

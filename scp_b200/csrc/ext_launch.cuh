@@ -12,6 +12,7 @@ namespace scp {
 struct HuConsts;
 struct FabConsts;
 struct R6Consts;
+struct DiagConsts;
 
 // Launch geometry of one ring kernel: tile shape, work items, CTAs.
 struct ExtPlan {
@@ -99,5 +100,17 @@ struct R6IO {
 int r6_plan(bool aux, int N, int nsm, ExtPlan *aux_plan, ExtPlan *step_plan);
 cudaError_t r6_step(const ExtPlan &aux_plan, const ExtPlan &step_plan, const R6Consts &c, const R6IO &io,
                     cudaStream_t st);
+
+// First diagnostics reduction of an FP64 state on the plane ring
+// (diag_ring.cuh): 12 matter position arrays, the links and E (when the
+// state carries them), the 12 matter momenta; one partial row per CTA.
+struct DiagRingIO {
+    const double *x[12];
+    const double *th, *E;   // 3 arrays each, or null without links
+    const double *mom;      // 12 arrays
+};
+int diag_ring_plan(bool gauged, bool links, int N, int nsm, ExtPlan *plan);
+cudaError_t diag_ring_pass1(bool gauged, bool links, const ExtPlan &plan, const DiagConsts &c, const DiagRingIO &io,
+                            double *part, cudaStream_t st);
 
 }  // namespace scp

@@ -53,9 +53,11 @@ struct RingView {
     __device__ __forceinline__ double operator()(int f) const { return c[f * S::FIELD]; }
 };
 
-// One work item of model M.
-template <class M, int TX, int TY>
-__device__ __forceinline__ void ring_item(const typename M::Args &a, const TileGrid &tg, int item, double *ring) {
+// One work item of model M; extra arguments (a reduction's per-thread sums)
+// are passed on to M::site.
+template <class M, int TX, int TY, class... Extra>
+__device__ __forceinline__ void ring_item(const typename M::Args &a, const TileGrid &tg, int item, double *ring,
+                                          Extra &...extra) {
     using S = RingShape<M::NR, TX, TY>;
     constexpr int NR = M::NR;
     const int N = a.N;
@@ -118,7 +120,7 @@ __device__ __forceinline__ void ring_item(const typename M::Args &a, const TileG
             v.m = ring + (q & 3) * S::SLOT + own_s;
             v.c = ring + ((q + 1) & 3) * S::SLOT + own_s;
             v.p = ring + ((q + 2) & 3) * S::SLOT + own_s;
-            M::site(a, v, i, j, k, (long long)i * NN + own_g, carry, q == 0);
+            M::site(a, v, i, j, k, (long long)i * NN + own_g, carry, q == 0, extra...);
         }
     }
 }

@@ -28,17 +28,26 @@
 #include "ext_startup.cuh"
 
 #include <cuda.h>   // driver API types only (entry points come through the runtime)
+#include <nvtx3/nvToolsExt.h>   // header-only; ranges are free when no tool is attached
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <mutex>
 
 using namespace scp;
 
 static thread_local char g_cuda_err[256] = "";
+
+// NVTX range over one ABI call (init, step, diag, snapshot), so a timeline
+// from a profiler shows the library's phases by name
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 #define CK(call)                                                                       \
     do {                                                                               \
@@ -117,6 +126,8 @@ struct scp_gpu {
     FabConsts fc{};
     double *kacc = nullptr;      // accumulated currents (3 arrays)
     ExtPlan xplan{}, xplan2{}, lplan{};
+    ExtPlan dplan{};             // first diagnostics reduction on the plane ring (FP64 states)
+    int dplan_ok = 0;
     int nx = 0;                  // position arrays per buffer of the extension layouts
     int device;
     cudaStream_t stream = nullptr;
@@ -855,6 +866,8 @@ static int gext_higgs_energy(scp_gpu *h, double *e) {
 static DiagConsts diag_consts(const scp_gpu *h);
 template <class View>
 static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out);
+static int diag_pass1_ring(scp_gpu *h, const DiagConsts &c, const double *Xm, const double *Pm, const double *th,
+                           const double *E, int *rows);
 
 // slots of the three-fabric layout
 constexpr int kFabL = 15, kFabQ = 27;
@@ -1010,9 +1023,9 @@ static int mf_diag(scp_gpu *h, scp_gpu_diag_out *out) {
     if (rc && rc != SCP_ENONFINITE) return rc;
     const int nb = red_blocks(h->N3);
     const DiagConsts c = diag_consts(h);
-    ViewFabric VL{X + kFabL * n3, P + kFabL * n3, X, P, h->N3};
-    diag_pass1_kernel<ViewFabric><<<nb, kRedThreads, 0, h->stream>>>(VL, c, h->part);
-    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    int nb1 = 0;
+    if ((rc = diag_pass1_ring(h, c, X + kFabL * n3, P + kFabL * n3, X + FTH * n3, P + FTH * n3, &nb1))) return rc;
+    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb1, h->fold);
     CK(cudaGetLastError());
     if ((rc = fold_to_host(h, DS_EC + 1))) return rc;
     double *o = out->v;
@@ -1111,14 +1124,17 @@ static int init_common(const scp_gpu_params *p, const double *const *cols, bool 
 extern "C" {
 
 int scp_gpu_init(const scp_gpu_params *p, const double *const *host_cols, scp_gpu **out) {
+    NvtxRange range_("scp_gpu_init");
     return init_common(p, host_cols, false, out);
 }
 
 int scp_gpu_init_device(const scp_gpu_params *p, const double *const *dev_cols, scp_gpu **out) {
+    NvtxRange range_("scp_gpu_init_device");
     return init_common(p, dev_cols, true, out);
 }
 
 int scp_gpu_step(scp_gpu *h, int nsteps) {
+    NvtxRange range_("scp_gpu_step");
     if (!h || nsteps < 0) return SCP_EINVAL;
     if (nsteps == 0) return SCP_OK;
     CK(cudaSetDevice(h->device));
@@ -1233,13 +1249,41 @@ static DiagConsts diag_consts(const scp_gpu *h) {
     return diag_consts_for(h->p, h->gauged, h->links, h->real, h->G_offset);
 }
 
+// First diagnostics reduction of an FP64 state on the plane ring: matter
+// positions Xm and momenta Pm (12 arrays each), links and E (3 each, or null);
+// the partial rows land in h->part, their count in *rows.
+static int diag_pass1_ring(scp_gpu *h, const DiagConsts &c, const double *Xm, const double *Pm, const double *th,
+                           const double *E, int *rows) {
+    if (!h->dplan_ok) {
+        int nsm = 0;
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+        if (diag_ring_plan(c.gauged, c.links, h->N, nsm, &h->dplan)) return SCP_EUNSUPPORTED;
+        h->dplan_ok = 1;
+    }
+    DiagRingIO io;
+    for (int f = 0; f < 12; f++) io.x[f] = Xm + (size_t)f * h->N3;
+    io.th = th;
+    io.E = E;
+    io.mom = Pm;
+    CK(diag_ring_pass1(c.gauged, c.links, h->dplan, c, io, h->part, h->stream));
+    *rows = h->dplan.grid;
+    return SCP_OK;
+}
+
 template <class View>
 static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
     const scp_gpu_params &p = h->p;
     const DiagConsts c = diag_consts(h);
     const int nb = red_blocks(h->N3);
-    diag_pass1_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->part);
-    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold);
+    int nb1 = nb;
+    if constexpr (std::is_same<View, ViewF64>::value) {
+        const size_t th = (size_t)FTH * h->N3;
+        int rc = diag_pass1_ring(h, c, V.X, V.S, c.links ? V.X + th : nullptr, c.links ? V.S + th : nullptr, &nb1);
+        if (rc) return rc;
+    } else {
+        diag_pass1_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->part);
+    }
+    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb1, h->fold);
     diag_pass2_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->fold, h->part);
     fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold + 40);
     diag_point_kernel<View><<<1, 32, 0, h->stream>>>(V, c, h->fold + 40, p.qdiag_probe1, p.qdiag_probe2,
@@ -1256,6 +1300,7 @@ static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
 extern "C" {
 
 int scp_gpu_diag(scp_gpu *h, scp_gpu_diag_out *out) {
+    NvtxRange range_("scp_gpu_diag");
     if (!h || !out) return SCP_EINVAL;
     CK(cudaSetDevice(h->device));
     if (h->rp) return real_diag(h, out);
@@ -1324,6 +1369,7 @@ static int snapshot_with(scp_gpu *h, const View &V, int dtype, void *const *host
 extern "C" {
 
 int scp_gpu_snapshot(scp_gpu *h, int dtype, void *const *host_cols) {
+    NvtxRange range_("scp_gpu_snapshot");
     if (!h || !host_cols) return SCP_EINVAL;
     if (dtype != SCP_DTYPE_F16 && dtype != SCP_DTYPE_F32 && dtype != SCP_DTYPE_F64) return SCP_EINVAL;
     CK(cudaSetDevice(h->device));
@@ -1402,6 +1448,7 @@ int scp_gpu_snapshot_wait(scp_gpu *h) {
 }
 
 int scp_gpu_snapshot_async(scp_gpu *h, int dtype, void *const *host_cols) {
+    NvtxRange range_("scp_gpu_snapshot_async");
     if (!h || !host_cols) return SCP_EINVAL;
     if (dtype != SCP_DTYPE_F16 && dtype != SCP_DTYPE_F32 && dtype != SCP_DTYPE_F64) return SCP_EINVAL;
     int rc;

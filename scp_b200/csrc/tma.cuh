@@ -187,8 +187,8 @@ struct TmaStage {
 template <int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
 __global__ void __launch_bounds__(TX * TY, (MinBlocks<F64, TX, TY, GAUGED>::value))
 step_tma_kernel(StepIO<F64> io, StepConsts c, TileGrid tg, const __grid_constant__ TmaMaps maps) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    TmaStage<TX, TY, GAUGED> stg(smem_raw, &maps, io.flag);
+    extern __shared__ __align__(16) unsigned char tma_smem[];   // aligned to 128 bytes by TmaStage
+    TmaStage<TX, TY, GAUGED> stg(tma_smem, &maps, io.flag);
     for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) {
         step_item<F64, TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, stg);
         if (__syncthreads_or(stg.timed_out)) return;   // every thread leaves together
