@@ -17,9 +17,13 @@ struct DiagSums {
     double S[DS_NSUM], M[DM_NMAX];
 };
 
-template <bool GAUGED, bool LINKS>
+// One instantiation per GAUGED: states with and without links run the same
+// machine code (the links are a runtime flag, c.links), so a g = 0 run that
+// carries links sums exactly as the run without them.  Without links the
+// th / E slots of the ring are staged from matter arrays and never read.
+template <bool GAUGED>
 struct DiagRing {
-    static constexpr int NR = LINKS ? 18 : 12;   // matter positions, [th, E]
+    static constexpr int NR = 18;                // matter positions, th, E
     static constexpr int TH = 12, EF = 15;
     static constexpr int MIN_CTAS = 1;
     struct Args {
@@ -125,7 +129,7 @@ struct DiagRing {
         S[DS_CX] += x * rho2;
         S[DS_CY] += y * rho2;
         S[DS_CZ] += z * rho2;
-        if (LINKS) {   // Gauss law and E_em (also with g = 0: then only E^2/2)
+        if (c.links) {   // Gauss law and E_em (also with g = 0: then only E^2/2)
             const double E0 = v(EF), E1 = v(EF + 1), E2 = v(EF + 2);
             const double divE = (E0 - v.at(EF, -1, 0, 0) + E1 - v.at(EF + 1, 0, -1, 0) + E2 - v.at(EF + 2, 0, 0, -1)) / c.dx;
             double rho = 0.0;
@@ -159,8 +163,8 @@ struct DiagRing {
     }
 };
 
-template <bool GAUGED, bool LINKS, int TX, int TY>
-__global__ void __launch_bounds__(TX *TY, 1) diag_ring_kernel(typename DiagRing<GAUGED, LINKS>::Args a, TileGrid tg,
+template <bool GAUGED, int TX, int TY>
+__global__ void __launch_bounds__(TX *TY, 1) diag_ring_kernel(typename DiagRing<GAUGED>::Args a, TileGrid tg,
                                                               double *part) {
     extern __shared__ __align__(16) double ring[];
     __shared__ double scratch[kDiag1Q * 32];
@@ -170,7 +174,7 @@ __global__ void __launch_bounds__(TX *TY, 1) diag_ring_kernel(typename DiagRing<
 #pragma unroll
     for (int q = 0; q < DM_NMAX; q++) acc.M[q] = 0.0;
     for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x)
-        ring_item<DiagRing<GAUGED, LINKS>, TX, TY>(a, tg, item, ring, acc);
+        ring_item<DiagRing<GAUGED>, TX, TY>(a, tg, item, ring, acc);
     block_fold<DS_NSUM, DM_NMAX>(acc.S, acc.M, scratch, part);
 }
 

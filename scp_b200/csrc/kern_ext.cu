@@ -120,11 +120,11 @@ cudaError_t link_step(const ExtPlan &p, const FabConsts &c, const LinkIO &io, cu
 }
 
 namespace {
-template <bool G, bool L>
+template <bool G>
 int diag_plan_t(int N, int nsm, ExtPlan *p) {
-    using M = DiagRing<G, L>;
+    using M = DiagRing<G>;
     using S = RingShape<M::NR, kExtTX, kExtTY>;
-    auto fn = diag_ring_kernel<G, L, kExtTX, kExtTY>;
+    auto fn = diag_ring_kernel<G, kExtTX, kExtTY>;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_bytes) != cudaSuccess)
         return -1;
     int occ = 0;
@@ -135,33 +135,30 @@ int diag_plan_t(int N, int nsm, ExtPlan *p) {
     p->smem = S::smem_bytes;
     return 0;
 }
-template <bool G, bool L>
+template <bool G>
 cudaError_t diag_launch_t(const ExtPlan &p, const DiagConsts &c, const DiagRingIO &io, double *part,
                           cudaStream_t st) {
-    typename DiagRing<G, L>::Args a;
+    typename DiagRing<G>::Args a;
     for (int f = 0; f < 12; f++) a.src.f[f] = io.x[f];
-    if (L)
-        for (int d = 0; d < 3; d++) {
-            a.src.f[DiagRing<G, L>::TH + d] = io.th + d * c.N3;
-            a.src.f[DiagRing<G, L>::EF + d] = io.E + d * c.N3;
-        }
+    for (int d = 0; d < 3; d++) {   // without links: any valid arrays, never read
+        a.src.f[DiagRing<G>::TH + d] = io.th ? io.th + d * c.N3 : io.x[d];
+        a.src.f[DiagRing<G>::EF + d] = io.E ? io.E + d * c.N3 : io.x[3 + d];
+    }
     a.N = c.N;
     a.c = c;
     a.mom = io.mom;
-    diag_ring_kernel<G, L, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg, part);
+    diag_ring_kernel<G, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg, part);
     return cudaGetLastError();
 }
 }  // namespace
 
-int diag_ring_plan(bool gauged, bool links, int N, int nsm, ExtPlan *plan) {
-    if (gauged) return diag_plan_t<true, true>(N, nsm, plan);
-    return links ? diag_plan_t<false, true>(N, nsm, plan) : diag_plan_t<false, false>(N, nsm, plan);
+int diag_ring_plan(bool gauged, bool, int N, int nsm, ExtPlan *plan) {
+    return gauged ? diag_plan_t<true>(N, nsm, plan) : diag_plan_t<false>(N, nsm, plan);
 }
 
-cudaError_t diag_ring_pass1(bool gauged, bool links, const ExtPlan &plan, const DiagConsts &c, const DiagRingIO &io,
+cudaError_t diag_ring_pass1(bool gauged, bool, const ExtPlan &plan, const DiagConsts &c, const DiagRingIO &io,
                             double *part, cudaStream_t st) {
-    if (gauged) return diag_launch_t<true, true>(plan, c, io, part, st);
-    return links ? diag_launch_t<false, true>(plan, c, io, part, st) : diag_launch_t<false, false>(plan, c, io, part, st);
+    return gauged ? diag_launch_t<true>(plan, c, io, part, st) : diag_launch_t<false>(plan, c, io, part, st);
 }
 
 int r6_plan(bool aux, int N, int nsm, ExtPlan *aux_plan, ExtPlan *step_plan) {

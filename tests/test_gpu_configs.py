@@ -23,7 +23,9 @@ from scp_b200.api import Simulation
 pytestmark = pytest.mark.gpu
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-# sums that cancel to roundoff are compared with an absolute floor
+# sums that cancel to roundoff (a net-neutral pair of balls) are compared with
+# an absolute floor: summed over 2.6e5 - 2.1e6 sites in another order, the
+# reference's own values of these sit at 1e-11
 ROUNDOFF = ("gauss_max", "gauss_l2", "Q_flux", "Q_phi", "Q_theta", "Q_total", "Q_core", "Q_p0", "Q_p1", "Q_p2",
             "E_coupling")
 
@@ -44,7 +46,7 @@ def check_tsv(have_rows, want_rows, header):
             continue
         ref, got = want[:, ci], have[:, DIAG_NAMES.index(h)]
         scale = np.maximum(np.abs(ref), 1e-9)
-        tol = np.maximum(1e-5 * scale, 1e-11) if h in ROUNDOFF else 2e-6 * scale
+        tol = np.maximum(1e-5 * scale, 1e-9) if h in ROUNDOFF else 2e-6 * scale
         bad = np.abs(got - ref) > tol
         assert not bad.any(), (h, int(np.argmax(bad)), got[bad][:3], ref[bad][:3])
 
