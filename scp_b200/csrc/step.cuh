@@ -121,6 +121,7 @@ template <class P, int TX, int TY, bool GAUGED>
 struct CpStage {
     using T = typename P::T;
     using LY = StepLayout<P, TX, TY, GAUGED>;
+    static constexpr int NSLOT = 3;   // ring slots: planes i, i+1 resident, i+2 in flight
     static constexpr int NF = LY::NF, NR = LY::NR, PX = LY::PX, PY = LY::PY, NT = LY::NT;
     T *xs;
     int N;
@@ -187,8 +188,9 @@ struct CpStage {
         }
     }
     __device__ __forceinline__ void commit() { cp_async_commit(); }
-    // everything issued so far has landed (for this thread; a barrier follows)
-    __device__ __forceinline__ void wait(int) { cp_async_wait<0>(); }
+    // this thread's copies have landed, all but the PENDING latest groups (a barrier follows)
+    template <int PENDING>
+    __device__ __forceinline__ void wait(int) { cp_async_wait<PENDING>(); }
     __device__ __forceinline__ bool failed() const { return false; }
     __device__ __forceinline__ T at(int slot, int f, int r, int col) const {
         return xs[((slot * NR + f) * PY + r) * PX + col];
@@ -251,8 +253,8 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
         issue_plane(i0 - 1, 0);
         issue_plane(i0, 1);
         stg.commit();
-        stg.wait(0);
-        stg.wait(1);
+        stg.template wait<0>(0);
+        stg.template wait<0>(1);
         __syncthreads();
         T xm[12];          // x(i-1) at this thread's site, matter fields
 #pragma unroll
@@ -264,14 +266,19 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             P0m = plaq_sin(0, 0, 1, ty + 1, tx + 1);
             P2m = plaq_sin(2, 0, 1, ty + 1, tx + 1);
         }
-        issue_plane(i0 + 1, 2);
+        // planes i0+1 .. i0+NS-2 (NS ring slots: NS-2 planes ahead in flight)
+        constexpr int NS = Stage::NSLOT;
+#pragma unroll
+        for (int q = 1; q <= NS - 2; q++)
+            if (i0 + q <= i1) issue_plane(i0 + q, q + 1);
         stg.commit();
 
         for (int i = i0; i < i1; i++) {
-            const int sc = (i - i0 + 1) % 3, sp = (i - i0 + 2) % 3, sn = (i - i0) % 3;
-            stg.wait(sp);
+            // plane p sits in slot (p - i0 + 1) mod NS; plane i + NS - 1 reuses the slot of i - 1
+            const int sc = (i - i0 + 1) % NS, sp = (i - i0 + 2) % NS, sn = (i - i0) % NS;
+            stg.template wait<NS - 3>(sp);   // the copies of planes beyond i+1 may stay in flight
             __syncthreads();
-            if (i + 2 <= i1) issue_plane(i + 2, sn);
+            if (i + NS - 1 <= i1) issue_plane(i + NS - 1, sn);
             stg.commit();
             const long long site = (long long)i * N * N + oc;
             T w[NF];

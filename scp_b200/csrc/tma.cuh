@@ -60,6 +60,10 @@ __device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap *map
 constexpr unsigned kTmaWaitLimit = 1u << 24;   // try_wait rounds before a wait gives up
 constexpr int kFlagTimeout = 2;                 // bit of the handle's flag word: a bounded wait gave up
 
+// Ring depth of the TMA staging: planes i, i+1 resident and i+2, i+3 in flight
+// (a deeper ring costs shared memory only, no registers).
+constexpr int kTmaSlots = 4;
+
 template <int TX, int TY, bool GAUGED>
 struct TmaLayout {
     static constexpr int NF = GAUGED ? 15 : 12;
@@ -72,8 +76,8 @@ struct TmaLayout {
     static constexpr int NHALO = 2 * TY * NF + (GAUGED ? 6 : 0); // halo-column doubles per plane
     static constexpr int HPT = (NHALO + NT - 1) / NT;
     static constexpr unsigned PLANE_BYTES = (unsigned)(NF * MAIN * sizeof(double));
-    // 3 slots, 3 mbarriers, 128 bytes of alignment slack
-    static constexpr size_t smem_bytes = sizeof(double) * 3 * SLOT + 3 * 8 + 128;
+    // kTmaSlots slots, one mbarrier each, 128 bytes of alignment slack
+    static constexpr size_t smem_bytes = sizeof(double) * kTmaSlots * SLOT + kTmaSlots * 8 + 128;
     static_assert(TX * sizeof(double) % 16 == 0, "TMA box rows are whole 16-byte units");
     static_assert(TX <= 256 && ROWS <= 256, "TMA box dimensions");
 };
@@ -83,6 +87,7 @@ struct TmaStage {
     using T = double;
     using LY = TmaLayout<TX, TY, GAUGED>;
     static constexpr int NF = LY::NF;
+    static constexpr int NSLOT = kTmaSlots;
     double *xs;
     unsigned bar0;           // shared address of the slot-0 mbarrier (slot s at bar0 + 8 s)
     unsigned phase = 0;      // bit s: parity of the next completion of slot s
@@ -98,9 +103,9 @@ struct TmaStage {
     __device__ __forceinline__ TmaStage(unsigned char *smem, const TmaMaps *m, int *fl) : maps(m), flag(fl) {
         const uintptr_t a = (reinterpret_cast<uintptr_t>(smem) + 127) & ~(uintptr_t)127;
         xs = reinterpret_cast<double *>(a);
-        bar0 = smem_u32(xs + 3 * LY::SLOT);
+        bar0 = smem_u32(xs + kTmaSlots * LY::SLOT);
         if (threadIdx.x == 0) {
-            for (int s = 0; s < 3; s++) mbar_init(bar0 + 8 * s, 1);
+            for (int s = 0; s < kTmaSlots; s++) mbar_init(bar0 + 8 * s, 1);
             asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         }
         __syncthreads();
@@ -163,10 +168,12 @@ struct TmaStage {
             if (h_g[q] >= 0) cp_async8(sb + h_s[q], gb + h_g[q]);
     }
     __device__ __forceinline__ void commit() { cp_async_commit(); }
-    // the block loads of slot s and this thread's halo copies have landed;
-    // a wait that gives up sets the timeout bit and lets the launch finish
+    // the block loads of slot s and this thread's halo copies (all but the
+    // PENDING latest groups) have landed; a wait that gives up sets the
+    // timeout bit and lets the launch finish
+    template <int PENDING>
     __device__ __forceinline__ void wait(int s) {
-        cp_async_wait<0>();
+        cp_async_wait<PENDING>();
         const unsigned par = (phase >> s) & 1u;
         unsigned n = 0;
         while (!mbar_try_wait(bar0 + 8 * s, par)) {
