@@ -10,19 +10,28 @@ namespace scp {
 
 namespace {
 
-constexpr int kExtTX = 32, kExtTY = 8;
+// Tile of a ring model: 128 threads, so that two CTAs share an SM and one
+// CTA's plane barrier overlaps the other's work; 32 x 4 while the 4-slot ring
+// of NR fields fits twice in shared memory, 16 x 8 (narrower halo rows) for
+// the widest rings.
+template <class M>
+struct TileOf {
+    static constexpr int TX = (M::NR <= 17) ? 32 : 16;
+    static constexpr int TY = (M::NR <= 17) ? 4 : 8;
+    static constexpr int NT = TX * TY;
+};
 
 template <class M>
 int ring_plan(int N, int nsm, ExtPlan *p) {
-    using S = RingShape<M::NR, kExtTX, kExtTY>;
-    auto fn = ring_kernel<M, kExtTX, kExtTY>;
+    constexpr int TX = TileOf<M>::TX, TY = TileOf<M>::TY;
+    using S = RingShape<M::NR, TX, TY>;
+    auto fn = ring_kernel<M, TX, TY>;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_bytes) != cudaSuccess)
         return -1;
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kExtTX * kExtTY, S::smem_bytes) != cudaSuccess ||
-        occ < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, TX * TY, S::smem_bytes) != cudaSuccess || occ < 1)
         return -1;
-    plan_ring_tiles(N, kExtTX, kExtTY, nsm * occ, p);
+    plan_ring_tiles(N, TX, TY, nsm * occ, p);
     p->smem = S::smem_bytes;
     return 0;
 }
@@ -43,7 +52,7 @@ cudaError_t hu_launch(const ExtPlan &p, const HuConsts &c, const HuIO &io, cudaS
     a.first = io.first;
     a.sync = io.sync;
     a.damp = io.damp;
-    ring_kernel<M, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg);
+    ring_kernel<M, TileOf<M>::TX, TileOf<M>::TY><<<p.grid, TileOf<M>::NT, p.smem, st>>>(a, p.tg);
     return cudaGetLastError();
 }
 
@@ -91,7 +100,7 @@ cudaError_t fabric_launch(const ExtPlan &p, const FabConsts &c, const FabIO &io,
     a.sync = io.sync;
     a.damp = io.damp;
     a.accumulate = io.accumulate;
-    ring_kernel<M, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg);
+    ring_kernel<M, TileOf<M>::TX, TileOf<M>::TY><<<p.grid, TileOf<M>::NT, p.smem, st>>>(a, p.tg);
     return cudaGetLastError();
 }
 }  // namespace
@@ -115,7 +124,8 @@ cudaError_t link_step(const ExtPlan &p, const FabConsts &c, const LinkIO &io, cu
     a.first = io.first;
     a.sync = io.sync;
     a.damp = io.damp;
-    ring_kernel<LinkPass, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg);
+    using T = TileOf<LinkPass>;
+    ring_kernel<LinkPass, T::TX, T::TY><<<p.grid, T::NT, p.smem, st>>>(a, p.tg);
     return cudaGetLastError();
 }
 
@@ -123,15 +133,15 @@ namespace {
 template <bool G>
 int diag_plan_t(int N, int nsm, ExtPlan *p) {
     using M = DiagRing<G>;
-    using S = RingShape<M::NR, kExtTX, kExtTY>;
-    auto fn = diag_ring_kernel<G, kExtTX, kExtTY>;
+    constexpr int TX = TileOf<M>::TX, TY = TileOf<M>::TY;
+    using S = RingShape<M::NR, TX, TY>;
+    auto fn = diag_ring_kernel<G, TX, TY>;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem_bytes) != cudaSuccess)
         return -1;
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kExtTX * kExtTY, S::smem_bytes) != cudaSuccess ||
-        occ < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, TX * TY, S::smem_bytes) != cudaSuccess || occ < 1)
         return -1;
-    plan_ring_tiles(N, kExtTX, kExtTY, nsm * occ, p);
+    plan_ring_tiles(N, TX, TY, nsm * occ, p);
     p->smem = S::smem_bytes;
     return 0;
 }
@@ -147,7 +157,8 @@ cudaError_t diag_launch_t(const ExtPlan &p, const DiagConsts &c, const DiagRingI
     a.N = c.N;
     a.c = c;
     a.mom = io.mom;
-    diag_ring_kernel<G, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg, part);
+    using T = TileOf<DiagRing<G>>;
+    diag_ring_kernel<G, T::TX, T::TY><<<p.grid, T::NT, p.smem, st>>>(a, p.tg, part);
     return cudaGetLastError();
 }
 }  // namespace
@@ -188,7 +199,7 @@ cudaError_t r6_launch(const ExtPlan &p, const R6Consts &c, const R6IO &io, cudaS
     a.first = io.first;
     a.sync = io.sync;
     a.damp = io.damp;
-    ring_kernel<M, kExtTX, kExtTY><<<p.grid, kExtTX * kExtTY, p.smem, st>>>(a, p.tg);
+    ring_kernel<M, TileOf<M>::TX, TileOf<M>::TY><<<p.grid, TileOf<M>::NT, p.smem, st>>>(a, p.tg);
     return cudaGetLastError();
 }
 }  // namespace
@@ -201,7 +212,8 @@ cudaError_t r6_step(const ExtPlan &aux_plan, const ExtPlan &step_plan, const R6C
     a.N = c.N;
     a.c = c;
     a.aux = io.aux;
-    ring_kernel<R6Aux, kExtTX, kExtTY><<<aux_plan.grid, kExtTX * kExtTY, aux_plan.smem, st>>>(a, aux_plan.tg);
+    using T = TileOf<R6Aux>;
+    ring_kernel<R6Aux, T::TX, T::TY><<<aux_plan.grid, T::NT, aux_plan.smem, st>>>(a, aux_plan.tg);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return r6_launch<true>(step_plan, c, io, st);
