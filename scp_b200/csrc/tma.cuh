@@ -101,8 +101,11 @@ struct TmaStage {
     bool timed_out = false;
 
     __device__ __forceinline__ TmaStage(unsigned char *smem, const TmaMaps *m, int *fl) : maps(m), flag(fl) {
-        const uintptr_t a = (reinterpret_cast<uintptr_t>(smem) + 127) & ~(uintptr_t)127;
-        xs = reinterpret_cast<double *>(a);
+        // round up to 128 bytes by offsetting the shared array itself (an
+        // integer round trip would hide the address space and turn every ring
+        // read into a generic load)
+        const unsigned off = (128u - (smem_u32(smem) & 127u)) & 127u;
+        xs = reinterpret_cast<double *>(smem + off);
         bar0 = smem_u32(xs + kTmaSlots * LY::SLOT);
         if (threadIdx.x == 0) {
             for (int s = 0; s < kTmaSlots; s++) mbar_init(bar0 + 8 * s, 1);
