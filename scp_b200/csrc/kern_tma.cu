@@ -10,6 +10,11 @@ TmaStepFn pick_tma(bool g, bool f, bool s, bool d) {
     SCP_PICK16(step_tma_kernel, TX, TY);
 }
 
+template <int TX, int TY>
+CpmStepFn pick_cpm(bool g, bool f, bool s, bool d) {
+    SCP_PICK16(step_cpm_kernel, TX, TY);
+}
+
 }  // namespace
 
 TmaStepFn step_tma_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
@@ -19,6 +24,15 @@ TmaStepFn step_tma_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
     }
     *smem = g ? TmaLayout<32, 4, true>::smem_bytes : TmaLayout<32, 4, false>::smem_bytes;
     return pick_tma<32, 4>(g, f, s, d);
+}
+
+CpmStepFn step_cpm_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
+    if (shape == 2) {
+        *smem = g ? CpMomStage<32, 8, true>::smem_bytes : CpMomStage<32, 8, false>::smem_bytes;
+        return pick_cpm<32, 8>(g, f, s, d);
+    }
+    *smem = g ? CpMomStage<32, 4, true>::smem_bytes : CpMomStage<32, 4, false>::smem_bytes;
+    return pick_cpm<32, 4>(g, f, s, d);
 }
 
 }  // namespace scp

@@ -5,6 +5,7 @@
 // header declares the selectors that return a kernel's host stub and its
 // dynamic shared-memory size for a tile shape and variant.
 #pragma once
+#include <cuda.h>
 #include <stddef.h>
 
 #include "step.cuh"
@@ -36,6 +37,9 @@ MultiFn<F32C> multi2_fn(int shape, bool g, bool d, size_t *smem);
 struct TmaMaps;
 using TmaStepFn = void (*)(StepIO<F64>, StepConsts, TileGrid, const TmaMaps);
 TmaStepFn step_tma_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
+// FP64 kernels with the cp.async position ring and TMA-staged momenta (tma.cuh)
+using CpmStepFn = void (*)(StepIO<F64>, StepConsts, TileGrid, const CUtensorMap);
+CpmStepFn step_cpm_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
 
 template <class P>
 StepFnT<P> step_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);

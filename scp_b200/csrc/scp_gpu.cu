@@ -155,10 +155,12 @@ struct scp_gpu {
     size_t snap_dev_bytes = 0;
     cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
     int snap_pending = 0;
-    // TMA plane staging of the FP64 fused step (tma.cuh): the tensor maps of
-    // X[0] and X[1]
+    // plane staging of the FP64 fused step: 0 the cp.async ring, 1 TMA tile
+    // loads of the positions (tensor maps of X[0], X[1]), 2 the cp.async ring
+    // with TMA-staged momenta (tensor maps of W and S)
     int tma = 0;
     TmaMaps tmaps[2];
+    CUtensorMap mmaps[2];
     // launch geometry
     int shape;
     int pairs = 0;               // 1: two-site packed FP32C kernel
@@ -322,29 +324,56 @@ static bool encode_maps(const double *X, int N, int nf, int tx, int ty, TmaMaps 
     return true;
 }
 
-// TMA staging applies to FP64 grids cut into full tiles, with a 16-byte row
-// pitch and at least two tile rows along j; SCP_STAGING=cp in the environment
-// keeps the cp.async ring (for side-by-side measurements).
-static bool tma_eligible(const scp_gpu *h, int shape) {
-    if (h->prec != SCP_PREC_FP64 || (shape != 1 && shape != 2)) return false;
-    const char *e = getenv("SCP_STAGING");
-    if (e && strcmp(e, "cp") == 0) return false;
+// The tensor map of one FP64 momentum buffer: (k, j, i, field), box TX x TY.
+static bool encode_mom_map(const double *W, int N, int nf, int tx, int ty, CUtensorMap *m) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t n = (cuuint64_t)N;
+    const cuuint64_t dims[4] = {n, n, n, (cuuint64_t)nf};
+    const cuuint64_t strides[3] = {n * 8, n * n * 8, n * n * n * 8};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const cuuint32_t box[4] = {(cuuint32_t)tx, (cuuint32_t)ty, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, (void *)W, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Staging of the FP64 step.  The TMA forms apply to grids cut into full
+// tiles, with a 16-byte row pitch and at least two tile rows along j; the
+// default there is the cp.async position ring with TMA-staged momenta (2).
+// SCP_STAGING in the environment selects another form for side-by-side
+// measurements: cp (0), tma (1: TMA tile loads of the positions), cpm (2).
+static int staging_mode(const scp_gpu *h, int shape) {
+    if (h->prec != SCP_PREC_FP64 || (shape != 1 && shape != 2)) return 0;
     const TileShape ts = kShapes[shape];
     const int N = h->N;
-    return N % 2 == 0 && N % ts.tx == 0 && N % ts.ty == 0 && N >= 2 * ts.ty && N >= ts.tx;
+    if (!(N % 2 == 0 && N % ts.tx == 0 && N % ts.ty == 0 && N >= 2 * ts.ty && N >= ts.tx)) return 0;
+    const char *e = getenv("SCP_STAGING");
+    if (e && strcmp(e, "cp") == 0) return 0;
+    if (e && strcmp(e, "tma") == 0) return 1;
+    return 2;
 }
 
 static int setup_tma(scp_gpu *h, int *occ) {
     const TileShape ts = kShapes[h->shape];
     size_t smem = 0;
+    const void *probe = nullptr;
     for (int v = 0; v < 8; v++) {
-        TmaStepFn fn = step_tma_fn(h->shape, h->gauged, v & 1, (v >> 1) & 1, (v >> 2) & 1, &smem);
-        CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const bool f = v & 1, sy = (v >> 1) & 1, d = (v >> 2) & 1;
+        const void *fn = (h->tma == 1) ? (const void *)step_tma_fn(h->shape, h->gauged, f, sy, d, &smem)
+                                       : (const void *)step_cpm_fn(h->shape, h->gauged, f, sy, d, &smem);
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (v == 0) probe = fn;
     }
-    TmaStepFn fn = step_tma_fn(h->shape, h->gauged, false, false, false, &smem);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, (const void *)fn, ts.tx * ts.ty, smem));
-    for (int b = 0; b < 2; b++)
-        if (!encode_maps(h->X[b], h->N, h->nf, ts.tx, ts.ty, &h->tmaps[b])) return SCP_EUNSUPPORTED;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, probe, ts.tx * ts.ty, smem));
+    if (h->tma == 1) {
+        for (int b = 0; b < 2; b++)
+            if (!encode_maps(h->X[b], h->N, h->nf, ts.tx, ts.ty, &h->tmaps[b])) return SCP_EUNSUPPORTED;
+    } else {
+        if (!encode_mom_map(h->W, h->N, h->nf, ts.tx, ts.ty, &h->mmaps[0]) ||
+            !encode_mom_map(h->S, h->N, h->nf, ts.tx, ts.ty, &h->mmaps[1]))
+            return SCP_EUNSUPPORTED;
+    }
     return SCP_OK;
 }
 
@@ -359,7 +388,7 @@ static int setup_launch(scp_gpu *h) {
     const TileShape ts = kShapes[shape];
     h->threads = ts.tx * ts.ty / (pairs ? 2 : 1);
     int occ = 0, rc;
-    h->tma = tma_eligible(h, shape) ? 1 : 0;
+    h->tma = staging_mode(h, shape);
     if (h->tma) rc = setup_tma(h, &occ);
     else if (pairs) rc = occupancy2_of(h, shape, &occ);
     else if (h->prec == SCP_PREC_FP64) rc = occupancy_of<F64>(h, shape, &occ);
@@ -385,9 +414,12 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         io.wout = h->W;
         io.sout = h->S;
         io.flag = h->flag;
-        if (h->tma) {
+        if (h->tma == 1) {
             TmaStepFn fn = step_tma_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
             fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg, h->tmaps[h->cur]);
+        } else if (h->tma == 2) {
+            CpmStepFn fn = step_cpm_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
+            fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg, h->mmaps[first ? 1 : 0]);
         } else {
             StepFnT<F64> fn = step_fn<F64>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
             fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);

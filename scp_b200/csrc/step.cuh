@@ -122,6 +122,10 @@ struct CpStage {
     using T = typename P::T;
     using LY = StepLayout<P, TX, TY, GAUGED>;
     static constexpr int NSLOT = 3;   // ring slots: planes i, i+1 resident, i+2 in flight
+    static constexpr bool MOM = false;   // momenta read from global memory at the site
+    __device__ __forceinline__ void issue_mom(int, int) {}
+    __device__ __forceinline__ void wait_mom(int) {}
+    __device__ __forceinline__ T mom(int, int) const { return T(0); }
     static constexpr int NF = LY::NF, NR = LY::NR, PX = LY::PX, PY = LY::PY, NT = LY::NT;
     T *xs;
     int N;
@@ -271,21 +275,31 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
 #pragma unroll
         for (int q = 1; q <= NS - 2; q++)
             if (i0 + q <= i1) issue_plane(i0 + q, q + 1);
+        if constexpr (Stage::MOM) stg.issue_mom(i0, 0);   // momenta of the first plane
         stg.commit();
 
         for (int i = i0; i < i1; i++) {
             // plane p sits in slot (p - i0 + 1) mod NS; plane i + NS - 1 reuses the slot of i - 1
             const int sc = (i - i0 + 1) % NS, sp = (i - i0 + 2) % NS, sn = (i - i0) % NS;
             stg.template wait<NS - 3>(sp);   // the copies of planes beyond i+1 may stay in flight
+            if constexpr (Stage::MOM) stg.wait_mom((i - i0) & 1);
             __syncthreads();
             if (i + NS - 1 <= i1) issue_plane(i + NS - 1, sn);
+            if constexpr (Stage::MOM) {   // momenta of the next plane, into the slot plane i-1 used
+                if (i + 1 < i1) stg.issue_mom(i + 1, (i + 1 - i0) & 1);
+            }
             stg.commit();
             const long long site = (long long)i * N * N + oc;
             T w[NF];
             uint16_t lo[P::COMP ? 12 : 1];
             if (act) {
+                if constexpr (Stage::MOM) {
 #pragma unroll
-                for (int f = 0; f < NF; f++) w[f] = ldg_t(io.win + f * N3 + site);
+                    for (int f = 0; f < NF; f++) w[f] = stg.mom((i - i0) & 1, f);
+                } else {
+#pragma unroll
+                    for (int f = 0; f < NF; f++) w[f] = ldg_t(io.win + f * N3 + site);
+                }
                 if constexpr (P::COMP) {
 #pragma unroll
                     for (int f = 0; f < 12; f++) lo[f] = __ldg(io.loin + f * N3 + site);

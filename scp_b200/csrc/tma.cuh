@@ -88,6 +88,10 @@ struct TmaStage {
     using LY = TmaLayout<TX, TY, GAUGED>;
     static constexpr int NF = LY::NF;
     static constexpr int NSLOT = kTmaSlots;
+    static constexpr bool MOM = false;   // momenta read from global memory at the site
+    __device__ __forceinline__ void issue_mom(int, int) {}
+    __device__ __forceinline__ void wait_mom(int) {}
+    __device__ __forceinline__ double mom(int, int) const { return 0.0; }
     double *xs;
     unsigned bar0;           // shared address of the slot-0 mbarrier (slot s at bar0 + 8 s)
     unsigned phase = 0;      // bit s: parity of the next completion of slot s
@@ -193,6 +197,84 @@ struct TmaStage {
         return xs[slot * LY::SLOT + f * LY::FS + off];
     }
 };
+
+// The cp.async position ring with the momenta staged through TMA: one dense
+// TX x TY box per field and plane (no halo, so no wrap and no split boxes),
+// loaded one plane ahead into two slots with an mbarrier each, and read by
+// each thread at its own site from shared memory instead of from global
+// memory.  The tensor map covers the handle's momentum buffer that the launch
+// reads (W, or S on the first launch).
+template <int TX, int TY, bool GAUGED>
+struct CpMomStage : CpStage<F64, TX, TY, GAUGED> {
+    using Base = CpStage<F64, TX, TY, GAUGED>;
+    static constexpr bool MOM = true;
+    static constexpr int NF = Base::NF;
+    static constexpr int MSLOT = NF * TX * TY;                    // doubles per momentum slot
+    static constexpr unsigned MOM_BYTES = (unsigned)(MSLOT * sizeof(double));
+    static constexpr size_t ring_bytes = Base::LY::smem_bytes;
+    // position ring, 128 bytes of slack, 2 momentum slots, 2 mbarriers
+    static constexpr size_t smem_bytes = ring_bytes + 128 + 2 * MOM_BYTES + 16;
+    double *ms;
+    unsigned mbar0;
+    unsigned mphase = 0;
+    const CUtensorMap *mmap;
+    int *flag;
+    int k0, j0;
+    bool timed_out = false;
+
+    __device__ __forceinline__ CpMomStage(unsigned char *smem, const CUtensorMap *m, int *fl)
+        : Base(smem), mmap(m), flag(fl) {
+        const unsigned base = smem_u32(smem);
+        const unsigned off = ((base + (unsigned)ring_bytes + 127u) & ~127u) - base;
+        ms = reinterpret_cast<double *>(smem + off);
+        mbar0 = smem_u32(ms + 2 * MSLOT);
+        if (threadIdx.x == 0) {
+            mbar_init(mbar0, 1);
+            mbar_init(mbar0 + 8, 1);
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+        __syncthreads();
+    }
+    __device__ __forceinline__ void begin(const StepConsts &c, int k0_, int j0_, int nk, int nj) {
+        Base::begin(c, k0_, j0_, nk, nj);
+        k0 = k0_;
+        j0 = j0_;
+    }
+    __device__ __forceinline__ void issue_mom(int p, int slot) {
+        if (threadIdx.x < 32) {   // warp 0: one lane per field
+            const unsigned bar = mbar0 + 8 * slot;
+            if (threadIdx.x == 0) mbar_expect_tx(bar, MOM_BYTES);
+            __syncwarp();
+            for (int f = threadIdx.x; f < NF; f += 32)
+                tma_load_4d(smem_u32(ms + slot * MSLOT + f * TX * TY), mmap, k0, j0, p, f, bar);
+        }
+    }
+    __device__ __forceinline__ void wait_mom(int slot) {
+        const unsigned par = (mphase >> slot) & 1u;
+        unsigned n = 0;
+        while (!mbar_try_wait(mbar0 + 8 * slot, par)) {
+            if (++n >= kTmaWaitLimit) {
+                if (!timed_out) atomicOr(flag, kFlagTimeout);
+                timed_out = true;
+                break;
+            }
+        }
+        mphase ^= 1u << slot;
+    }
+    // this thread's momentum f (site (ty, tx) of the tile)
+    __device__ __forceinline__ double mom(int slot, int f) const { return ms[slot * MSLOT + f * TX * TY + threadIdx.x]; }
+};
+
+template <int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
+__global__ void __launch_bounds__(TX * TY, (MinBlocks<F64, TX, TY, GAUGED>::value))
+step_cpm_kernel(StepIO<F64> io, StepConsts c, TileGrid tg, const __grid_constant__ CUtensorMap mmap) {
+    extern __shared__ __align__(16) unsigned char cpm_smem[];
+    CpMomStage<TX, TY, GAUGED> stg(cpm_smem, &mmap, io.flag);
+    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) {
+        step_item<F64, TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, stg);
+        if (__syncthreads_or(stg.timed_out)) return;
+    }
+}
 
 template <int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
 __global__ void __launch_bounds__(TX * TY, (MinBlocks<F64, TX, TY, GAUGED>::value))

@@ -1,6 +1,7 @@
-"""The FP64 fused step with TMA plane staging (tile loads of every field's
-plane through tensor maps, halo columns by cp.async) against the same step
-with the cp.async ring: the same arithmetic on the same values, so the two
+"""The FP64 fused step with its TMA staging forms -- tile loads of every
+field's plane through tensor maps (halo columns by cp.async), and the
+cp.async position ring with TMA-staged momenta -- against the same step with
+the plain cp.async ring: the same arithmetic on the same values, so all
 agree bit for bit, on interior and j-edge tiles, gauged and ungauged, with
 and without the sponge, across several calls."""
 import os
@@ -8,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from scp_b200 import Params, seeds
+from scp_b200 import seeds
 from scp_b200.api import Simulation
 
 pytestmark = pytest.mark.gpu
@@ -42,19 +43,23 @@ def test_tma_staging_matches_cp_ring(gpu, N, gauged, tile, over):
     st = seeds.small_state(N, gauged, seed=N + tile, tile_variant=tile, **over)
     calls = (1, 5, 6)
     t_tma, a, da = _run(st.params, st.cols(), "tma", calls)
+    t_cpm, m, dm = _run(st.params, st.cols(), "cpm", calls)
     t_cp, b, db = _run(st.params, st.cols(), "cp", calls)
     assert t_cp == 0
-    # full tiles only: 40 is not a multiple of the 32-wide tile
+    # full tiles only: 40 and 48 are not multiples of the 32-wide tile
     assert t_tma == (1 if N % 32 == 0 else 0)
-    for x, y in zip(a, b):
-        assert np.array_equal(x, y)
+    assert t_cpm == (2 if N % 32 == 0 else 0)
+    for x, y, z in zip(a, m, b):
+        assert np.array_equal(x, z)
+        assert np.array_equal(y, z)
     assert np.array_equal(da, db)
+    assert np.array_equal(dm, db)
 
 
 def test_tma_staging_is_default_on_the_bench_grid(gpu):
-    """The gauged 128^3 bench grid runs the TMA path by default."""
+    """The gauged 128^3 bench grid runs with TMA-staged momenta by default."""
     p = seeds.params_for("c1", N=128)
     st = seeds.small_state(128, True, seed=3, L=p.L)
     os.environ.pop("SCP_STAGING", None)
     with Simulation(st.params, st.cols()) as sim:
-        assert sim.info().tma_staging == 1
+        assert sim.info().tma_staging == 2
