@@ -157,11 +157,11 @@ typedef struct {
     double  step_bytes_per_site;    /* algorithmic bytes moved per site-update */
     int32_t tile_x, tile_y, seg_len; /* tile shape in use */
     int32_t sites_per_thread; /* 2: two-site packed FP32C kernel (even N), else 1 */
-    int32_t tma_staging;      /* plane staging of the FP64 step on full tiles of the default
-                                 shapes: 2 cp.async position ring + TMA-staged momenta (the
-                                 default), 1 TMA tile loads of the positions, 0 cp.async ring
-                                 only (every other grid and precision); SCP_STAGING=cpm|tma|cp
-                                 in the environment selects one */
+    int32_t tma_staging;      /* plane staging of the FP64 step: 0 the cp.async ring (the
+                                 default); on full tiles of the default shapes SCP_STAGING=tma
+                                 in the environment selects TMA tile loads of the positions (1)
+                                 and SCP_STAGING=cpm the cp.async ring with TMA-staged momenta
+                                 (2), both bit-identical to 0 */
 } scp_gpu_info;
 
 typedef struct scp_gpu scp_gpu;

@@ -338,20 +338,23 @@ static bool encode_mom_map(const double *W, int N, int nf, int tx, int ty, CUten
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Staging of the FP64 step.  The TMA forms apply to grids cut into full
-// tiles, with a 16-byte row pitch and at least two tile rows along j; the
-// default there is the cp.async position ring with TMA-staged momenta (2).
-// SCP_STAGING in the environment selects another form for side-by-side
-// measurements: cp (0), tma (1: TMA tile loads of the positions), cpm (2).
+// Staging of the FP64 step: the cp.async ring (0) by default.  The TMA forms
+// apply to grids cut into full tiles, with a 16-byte row pitch and at least
+// two tile rows along j, and are selected by SCP_STAGING in the environment:
+// tma (1: TMA tile loads of the positions) or cpm (2: the cp.async position
+// ring with TMA-staged momenta).  Both give the same bits as the default and
+// ran slower on B200 (0.282 and 0.296 against 0.227 ms per 128^3 gauged
+// step): the step is bound by shared-memory traffic and FP64 dependency
+// chains, which the TMA forms do not shorten.
 static int staging_mode(const scp_gpu *h, int shape) {
     if (h->prec != SCP_PREC_FP64 || (shape != 1 && shape != 2)) return 0;
     const TileShape ts = kShapes[shape];
     const int N = h->N;
     if (!(N % 2 == 0 && N % ts.tx == 0 && N % ts.ty == 0 && N >= 2 * ts.ty && N >= ts.tx)) return 0;
     const char *e = getenv("SCP_STAGING");
-    if (e && strcmp(e, "cp") == 0) return 0;
     if (e && strcmp(e, "tma") == 0) return 1;
-    return 2;
+    if (e && strcmp(e, "cpm") == 0) return 2;
+    return 0;
 }
 
 static int setup_tma(scp_gpu *h, int *occ) {

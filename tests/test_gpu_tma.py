@@ -56,10 +56,11 @@ def test_tma_staging_matches_cp_ring(gpu, N, gauged, tile, over):
     assert np.array_equal(dm, db)
 
 
-def test_tma_staging_is_default_on_the_bench_grid(gpu):
-    """The gauged 128^3 bench grid runs with TMA-staged momenta by default."""
+def test_staging_default_is_the_cp_ring(gpu):
+    """Without SCP_STAGING the bench grid runs the cp.async ring (the fastest
+    form measured); the TMA forms are selected only on request."""
     p = seeds.params_for("c1", N=128)
     st = seeds.small_state(128, True, seed=3, L=p.L)
     os.environ.pop("SCP_STAGING", None)
     with Simulation(st.params, st.cols()) as sim:
-        assert sim.info().tma_staging == 2
+        assert sim.info().tma_staging == 0
