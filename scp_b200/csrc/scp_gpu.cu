@@ -165,8 +165,10 @@ struct scp_gpu {
     int shape;
     int pairs = 0;               // 1: two-site packed FP32C kernel
     int threads = 0;
-    TileGrid tg;
+    TileGrid tg;                 // item plan (the server's tables)
     int grid;
+    TileGrid tg_run;             // plan of the single-grid launches (balanced when large enough)
+    int grid_run = 0;
     int64_t steps = 0;
     double G_offset = 0.0;
     int cg_iters = 0;
@@ -256,6 +258,20 @@ static void plan_tiles(scp_gpu *h, int tx, int ty, int slots) {
     tg.nitems = ntiles * tg.nseg;
     h->tg = tg;
     h->grid = tg.nitems < slots ? tg.nitems : slots;
+    // The single-grid launches split the (column, plane) pairs evenly over all
+    // resident CTAs instead (TileGrid seg = 0) once every CTA gets at least 8
+    // planes: whole-item waves leave slots idle (256 items on 296 slots at
+    // 128^3), equal shares do not, for two halo planes per extra piece.  The
+    // server's multi-request kernels keep the item plan above.
+    const long long pairs = (long long)ntiles * N;
+    h->tg_run = tg;
+    h->grid_run = h->grid;
+    if (pairs >= 8LL * slots) {
+        h->tg_run.seg = 0;
+        h->tg_run.nseg = 0;
+        h->tg_run.nitems = 0;
+        h->grid_run = slots;
+    }
 }
 
 template <class P>
@@ -419,13 +435,13 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         io.flag = h->flag;
         if (h->tma == 1) {
             TmaStepFn fn = step_tma_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
-            fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg, h->tmaps[h->cur]);
+            fn<<<h->grid_run, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg_run, h->tmaps[h->cur]);
         } else if (h->tma == 2) {
             CpmStepFn fn = step_cpm_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
-            fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg, h->mmaps[first ? 1 : 0]);
+            fn<<<h->grid_run, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg_run, h->mmaps[first ? 1 : 0]);
         } else {
             StepFnT<F64> fn = step_fn<F64>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
-            fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+            fn<<<h->grid_run, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg_run);
         }
     } else {
         StepIO<F32C> io;
@@ -441,10 +457,10 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         io.flag = h->flag;
         if (h->pairs) {
             StepFnT<F32C> fn = step2_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
-            fn<<<h->grid, h->threads, smem, h->stream>>>(io, h->c, h->tg);
+            fn<<<h->grid_run, h->threads, smem, h->stream>>>(io, h->c, h->tg_run);
         } else {
             StepFnT<F32C> fn = step_fn<F32C>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
-            fn<<<h->grid, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg);
+            fn<<<h->grid_run, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg_run);
         }
     }
     CK(cudaGetLastError());
@@ -1531,7 +1547,7 @@ int scp_gpu_get_info(const scp_gpu *h, scp_gpu_info *info) {
     info->step_bytes_per_site = 2.0 * info->state_bytes_per_site;
     info->tile_x = kShapes[h->shape].tx;
     info->tile_y = kShapes[h->shape].ty;
-    info->seg_len = h->tg.seg;
+    info->seg_len = h->tg_run.seg;   // 0: balanced shares of (column, plane) pairs
     info->sites_per_thread = h->pairs ? 2 : 1;
     info->tma_staging = h->tma;
     return SCP_OK;

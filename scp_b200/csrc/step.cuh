@@ -205,7 +205,7 @@ struct CpStage {
 // sync and damp are uniform per call; the single-grid kernel passes them as
 // constants, the multi-request kernel per request.  Stage stages the planes.
 template <class P, int TX, int TY, bool GAUGED, bool FIRST, class Stage>
-__device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts &c, const TileGrid &tg, int item,
+__device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts &c, const Piece &pc,
                                           const bool SYNC, const bool DAMP, Stage &stg) {
     using T = typename P::T;
     using LY = StepLayout<P, TX, TY, GAUGED>;
@@ -221,11 +221,8 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
     const float hdt_lo = (float)(c.hdt - (double)(float)c.hdt);
 
     {
-        const int kt = item % tg.ntx;
-        const int jt = (item / tg.ntx) % tg.nty;
-        const int sg = item / (tg.ntx * tg.nty);
-        const int k0 = kt * TX, j0 = jt * TY;
-        const int i0 = sg * tg.seg, i1 = min(i0 + tg.seg, N);
+        const int k0 = pc.kt * TX, j0 = pc.jt * TY;
+        const int i0 = pc.i0, i1 = pc.i1;
         const int k = k0 + tx, j = j0 + ty;
         const int nk = min(k0 + TX, N) - k0, nj = min(j0 + TY, N) - j0;   // valid extent of the tile
         const bool act = (tx < nk) && (ty < nj);
@@ -576,8 +573,7 @@ __global__ void __launch_bounds__(TX * TY, (MinBlocks<P, TX, TY, GAUGED>::value)
 step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CpStage<P, TX, TY, GAUGED> stg(smem_raw);
-    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x)
-        step_item<P, TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, stg);
+    for_each_piece(tg, c.N, [&](const Piece &pc) { step_item<P, TX, TY, GAUGED, FIRST>(io, c, pc, SYNC, DAMP, stg); });
 }
 
 // ---------------------------------------------------------------- many grids per launch
@@ -638,7 +634,7 @@ step_multi_kernel(const ReqTable<P> *tab, int k) {
         const StepConsts c = q.c;
         const TileGrid tg = q.tg;
         CpStage<P, TX, TY, GAUGED> stg(smem_raw);
-        step_item<P, TX, TY, GAUGED, false>(io, c, tg, item - q.item0, false, DAMP, stg);
+        step_item<P, TX, TY, GAUGED, false>(io, c, piece_of_item(tg, item - q.item0, c.N), false, DAMP, stg);
     }
 }
 

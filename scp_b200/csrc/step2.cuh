@@ -64,7 +64,7 @@ __device__ __forceinline__ void link_wrap_c(float *th, float *lo) {
 }
 
 template <int TX, int TY, bool GAUGED, bool FIRST>
-__device__ __forceinline__ void step_item2(const StepIO<F32C> &io, const StepConsts &c, const TileGrid &tg, int item,
+__device__ __forceinline__ void step_item2(const StepIO<F32C> &io, const StepConsts &c, const Piece &pc,
                                            const bool SYNC, const bool DAMP, unsigned char *smem_raw) {
     using LY = Step2Layout<TX, TY, GAUGED>;
     constexpr int NF = LY::NF, NR = LY::NR, PX = LY::PX, PY = LY::PY, NT = LY::NT, HX = TX / 2;
@@ -82,11 +82,8 @@ __device__ __forceinline__ void step_item2(const StepIO<F32C> &io, const StepCon
     const V2 dt((float)c.dt), hdt((float)c.hdt), idx1((float)c.idx1), idx2((float)c.idx2);
     const V2 dt_lo((float)(c.dt - (double)(float)c.dt)), hdt_lo((float)(c.hdt - (double)(float)c.hdt));
 
-    const int kt = item % tg.ntx;
-    const int jt = (item / tg.ntx) % tg.nty;
-    const int sg = item / (tg.ntx * tg.nty);
-    const int k0 = kt * TX, j0 = jt * TY;
-    const int i0 = sg * tg.seg, i1 = min(i0 + tg.seg, N);
+    const int k0 = pc.kt * TX, j0 = pc.jt * TY;
+    const int i0 = pc.i0, i1 = pc.i1;
     const int k = k0 + 2 * tx2, j = j0 + ty;
     const int nk = min(k0 + TX, N) - k0, nj = min(j0 + TY, N) - j0;   // nk is even
     const bool act = (2 * tx2 < nk) && (ty < nj);
@@ -430,8 +427,7 @@ template <int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
 __global__ void __launch_bounds__(Step2Layout<TX, TY, GAUGED>::NT, Step2Layout<TX, TY, GAUGED>::MIN_BLOCKS)
 step2_kernel(StepIO<F32C> io, StepConsts c, TileGrid tg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x)
-        step_item2<TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, smem_raw);
+    for_each_piece(tg, c.N, [&](const Piece &pc) { step_item2<TX, TY, GAUGED, FIRST>(io, c, pc, SYNC, DAMP, smem_raw); });
 }
 
 // many FP32C requests of even N per launch (table semantics as step_multi_kernel)
@@ -447,7 +443,7 @@ step2_multi_kernel(const ReqTable<F32C> *tab, int k) {
         const StepIO<F32C> io = q.io[(int)((s - q.s0) & 1)];
         const StepConsts c = q.c;
         const TileGrid tg = q.tg;
-        step_item2<TX, TY, GAUGED, false>(io, c, tg, item - q.item0, false, DAMP, smem_raw);
+        step_item2<TX, TY, GAUGED, false>(io, c, piece_of_item(tg, item - q.item0, c.N), false, DAMP, smem_raw);
     }
 }
 

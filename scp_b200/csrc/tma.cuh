@@ -270,10 +270,12 @@ __global__ void __launch_bounds__(TX * TY, (MinBlocks<F64, TX, TY, GAUGED>::valu
 step_cpm_kernel(StepIO<F64> io, StepConsts c, TileGrid tg, const __grid_constant__ CUtensorMap mmap) {
     extern __shared__ __align__(16) unsigned char cpm_smem[];
     CpMomStage<TX, TY, GAUGED> stg(cpm_smem, &mmap, io.flag);
-    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) {
-        step_item<F64, TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, stg);
-        if (__syncthreads_or(stg.timed_out)) return;
-    }
+    bool stop = false;
+    for_each_piece(tg, c.N, [&](const Piece &pc) {
+        if (stop) return;
+        step_item<F64, TX, TY, GAUGED, FIRST>(io, c, pc, SYNC, DAMP, stg);
+        stop = __syncthreads_or(stg.timed_out);   // every thread leaves together
+    });
 }
 
 template <int TX, int TY, bool GAUGED, bool FIRST, bool SYNC, bool DAMP>
@@ -281,10 +283,12 @@ __global__ void __launch_bounds__(TX * TY, (MinBlocks<F64, TX, TY, GAUGED>::valu
 step_tma_kernel(StepIO<F64> io, StepConsts c, TileGrid tg, const __grid_constant__ TmaMaps maps) {
     extern __shared__ __align__(16) unsigned char tma_smem[];   // aligned to 128 bytes by TmaStage
     TmaStage<TX, TY, GAUGED> stg(tma_smem, &maps, io.flag);
-    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) {
-        step_item<F64, TX, TY, GAUGED, FIRST>(io, c, tg, item, SYNC, DAMP, stg);
-        if (__syncthreads_or(stg.timed_out)) return;   // every thread leaves together
-    }
+    bool stop = false;
+    for_each_piece(tg, c.N, [&](const Piece &pc) {
+        if (stop) return;
+        step_item<F64, TX, TY, GAUGED, FIRST>(io, c, pc, SYNC, DAMP, stg);
+        stop = __syncthreads_or(stg.timed_out);   // every thread leaves together
+    });
 }
 
 }  // namespace scp
