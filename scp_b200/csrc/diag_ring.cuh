@@ -173,8 +173,7 @@ __global__ void __launch_bounds__(TX *TY, 1) diag_ring_kernel(typename DiagRing<
     for (int q = 0; q < DS_NSUM; q++) acc.S[q] = 0.0;
 #pragma unroll
     for (int q = 0; q < DM_NMAX; q++) acc.M[q] = 0.0;
-    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x)
-        ring_item<DiagRing<GAUGED>, TX, TY>(a, tg, item, ring, acc);
+    for_each_piece(tg, a.N, [&](const Piece &pc) { ring_item<DiagRing<GAUGED>, TX, TY>(a, pc, ring, acc); });
     block_fold<DS_NSUM, DM_NMAX>(acc.S, acc.M, scratch, part);
 }
 

@@ -43,8 +43,14 @@ inline void plan_ring_tiles(int N, int tx, int ty, int slots, ExtPlan *p) {
     tg.nitems = ntiles * tg.nseg;
     p->tx = tx;
     p->ty = ty;
-    p->tg = tg;
     p->grid = tg.nitems < slots ? tg.nitems : slots;
+    if ((long long)ntiles * N >= 8LL * slots) {   // equal shares of (column, plane) pairs
+        tg.seg = 0;
+        tg.nseg = 0;
+        tg.nitems = 0;
+        p->grid = slots;
+    }
+    p->tg = tg;
 }
 
 // Higgs condensate and / or second gauge: positions and momenta are NR

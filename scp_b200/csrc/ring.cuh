@@ -1,8 +1,9 @@
 // ring.cuh -- plane-ring tile walker of the extension steppers (Higgs and
 // second gauge, three fabrics, the real mode's optional terms).
 //
-// Work items are the same as the fused step's: a (TX x TY) column of sites in
-// (k, j) times a segment of planes along i (TileGrid).  A CTA streams its
+// Work is split as the fused step's: (TX x TY) columns of sites in (k, j),
+// run over planes along i in pieces (TileGrid: item segments, or equal
+// balanced shares of all (column, plane) pairs).  A CTA streams its
 // column plane by plane through a four-slot shared-memory ring that holds
 // planes i-1, i, i+1 of every staged field, each with a one-site halo in j
 // and k (corners included), while plane i+2 is in flight through cp.async.
@@ -56,17 +57,14 @@ struct RingView {
 // One work item of model M; extra arguments (a reduction's per-thread sums)
 // are passed on to M::site.
 template <class M, int TX, int TY, class... Extra>
-__device__ __forceinline__ void ring_item(const typename M::Args &a, const TileGrid &tg, int item, double *ring,
+__device__ __forceinline__ void ring_item(const typename M::Args &a, const Piece &pc, double *ring,
                                           Extra &...extra) {
     using S = RingShape<M::NR, TX, TY>;
     constexpr int NR = M::NR;
     const int N = a.N;
     const long long NN = (long long)N * N;
-    const int kt = item % tg.ntx;
-    const int jt = (item / tg.ntx) % tg.nty;
-    const int sg = item / (tg.ntx * tg.nty);
-    const int k0 = kt * TX, j0 = jt * TY;
-    const int i0 = sg * tg.seg, i1 = min(i0 + tg.seg, N);
+    const int k0 = pc.kt * TX, j0 = pc.jt * TY;
+    const int i0 = pc.i0, i1 = pc.i1;
     const int nk = min(TX, N - k0), nj = min(TY, N - j0);
     const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
     const bool own = (tx < nk) && (ty < nj);
@@ -128,7 +126,7 @@ __device__ __forceinline__ void ring_item(const typename M::Args &a, const TileG
 template <class M, int TX, int TY>
 __global__ void __launch_bounds__(TX *TY, M::MIN_CTAS) ring_kernel(typename M::Args a, TileGrid tg) {
     extern __shared__ __align__(16) double ring[];
-    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) ring_item<M, TX, TY>(a, tg, item, ring);
+    for_each_piece(tg, a.N, [&](const Piece &pc) { ring_item<M, TX, TY>(a, pc, ring); });
 }
 
 // sponge factor 1 - rate * s^2 of the absorbing boundary at site (i, j, k),
