@@ -21,11 +21,7 @@ struct StepConsts {
 };
 
 // Work decomposition of the persistent step kernels: the grid is cut into
-// (TX x TY) columns in (k, j) and segments of seg planes along i.  seg = 0
-// selects the balanced split: CTA b of G takes the b-th of G equal, contiguous
-// ranges of all (column, plane) pairs in column-major order, so every CTA
-// runs the same number of planes (up to one) and a range may cover the end
-// of one column and the start of the next.
+// (TX x TY) columns in (k, j) and segments of seg planes along i.
 struct TileGrid {
     int ntx, nty, nseg, seg;
     int nitems;
@@ -36,6 +32,8 @@ struct Piece {
     int kt, jt, i0, i1;
 };
 
+// Work item -> piece.  Items enumerate the columns fastest and the segments
+// last, so the CTAs of one wave start on the same plane and walk i in step.
 __device__ __forceinline__ Piece piece_of_item(const TileGrid &tg, int item, int N) {
     Piece p;
     p.kt = item % tg.ntx;
@@ -46,40 +44,10 @@ __device__ __forceinline__ Piece piece_of_item(const TileGrid &tg, int item, int
     return p;
 }
 
-// Every piece of this CTA's share, in order.
+// Every piece of this CTA, in order (items blockIdx.x, + gridDim.x, ...).
 template <class F>
 __device__ __forceinline__ void for_each_piece(const TileGrid &tg, int N, F &&f) {
-    if (tg.seg > 0) {
-        for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) f(piece_of_item(tg, item, N));
-        return;
-    }
-    const long long T = (long long)tg.ntx * tg.nty * N;
-    long long q = T * blockIdx.x / gridDim.x;
-    const long long e = T * (blockIdx.x + 1) / gridDim.x;
-    while (q < e) {
-        const long long col = q / N;
-        Piece p;
-        p.kt = (int)(col % tg.ntx);
-        p.jt = (int)(col / tg.ntx);
-        p.i0 = (int)(q - col * N);
-        p.i1 = (int)min((long long)N, (long long)p.i0 + (e - q));
-        f(p);
-        q += p.i1 - p.i0;
-    }
-}
-
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
-    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int NPEND>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+    for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) f(piece_of_item(tg, item, N));
 }
 
 // Streaming store (evict-first): outputs are not re-read by this launch.

@@ -44,12 +44,6 @@ inline void plan_ring_tiles(int N, int tx, int ty, int slots, ExtPlan *p) {
     p->tx = tx;
     p->ty = ty;
     p->grid = tg.nitems < slots ? tg.nitems : slots;
-    if ((long long)ntiles * N >= 8LL * slots) {   // equal shares of (column, plane) pairs
-        tg.seg = 0;
-        tg.nseg = 0;
-        tg.nitems = 0;
-        p->grid = slots;
-    }
     p->tg = tg;
 }
 

@@ -1,9 +1,8 @@
 // ring.cuh -- plane-ring tile walker of the extension steppers (Higgs and
 // second gauge, three fabrics, the real mode's optional terms).
 //
-// Work is split as the fused step's: (TX x TY) columns of sites in (k, j),
-// run over planes along i in pieces (TileGrid: item segments, or equal
-// balanced shares of all (column, plane) pairs).  A CTA streams its
+// Work is split as the fused step's: (TX x TY) columns of sites in (k, j)
+// times segments of planes along i (TileGrid items).  A CTA streams its
 // column plane by plane through a four-slot shared-memory ring that holds
 // planes i-1, i, i+1 of every staged field, each with a one-site halo in j
 // and k (corners included), while plane i+2 is in flight through cp.async.
