@@ -50,6 +50,20 @@ __device__ __forceinline__ void for_each_piece(const TileGrid &tg, int N, F &&f)
     for (int item = blockIdx.x; item < tg.nitems; item += gridDim.x) f(piece_of_item(tg, item, N));
 }
 
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+}
+
 // Streaming store (evict-first): outputs are not re-read by this launch.
 __device__ __forceinline__ void st_cs(double *p, double v) { __stcs(p, v); }
 __device__ __forceinline__ void st_cs(float *p, float v) { __stcs(p, v); }
