@@ -307,10 +307,12 @@ def served_once(reqs, args, rate_label: float, log_path: str | None):
         ids, makespan, lat = serve.run_served(reqs, srv, realtime=True)
         clocks = clk.stop()
         st = srv.stats()
-        bad = [i for i in ids if srv.status(i).state != serve.DONE]
+        bad = [(i, r) for i, r in zip(ids, reqs) if srv.status(i).state != serve.DONE]
+        bad_info = [f"id {i}: state {srv.status(i).state} rc {srv.status(i).rc} N {r.params.N} "
+                    f"e {r.params.g_gauge if r.params.complex_gauge else 0.0} steps {r.nsteps}" for i, r in bad]
         recs = request_lines(reqs, ids, srv)
     if bad:
-        raise RuntimeError(f"{len(bad)} served requests failed")
+        raise RuntimeError(f"{len(bad)} served requests failed: " + "; ".join(bad_info[:8]))
     if log_path:
         with open(log_path, "a") as f:
             for rec in recs:
