@@ -33,6 +33,10 @@ struct DiagRing {
         const double *mom;   // the 12 matter momenta (N^3 arrays)
     };
     struct Carry {};
+    __device__ static void prefetch(const Args &A, long long idx) {
+#pragma unroll
+        for (int f = 0; f < 12; f++) prefetch_l2(A.mom + f * A.c.N3 + idx);
+    }
 
     template <class V>
     __device__ static void site(const Args &A, const V &v, int i, int j, int k, long long idx, Carry &, bool,

@@ -62,6 +62,14 @@ struct FabricPass {
         double cmx, smx;      // the same for qx
     };
 
+    __device__ static void prefetch(const Args &A, long long idx) {
+#pragma unroll
+        for (int f = 0; f < 12; f++) prefetch_l2(A.win + f * A.c.N3 + idx);
+        if (A.accumulate)
+#pragma unroll
+            for (int d = 0; d < 3; d++) prefetch_l2(A.kacc + d * A.c.N3 + idx);
+    }
+
     template <class V>
     __device__ static void site(const Args &A, const V &v, int i, int j, int k, long long idx, Carry &cy,
                                 bool first_plane) {
@@ -163,6 +171,14 @@ struct LinkPass {
     struct Carry {
         double pm[2];         // plaquette sines (0,1), (2,0) at x - i
     };
+
+    __device__ static void prefetch(const Args &A, long long idx) {
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            prefetch_l2(A.win + d * A.c.N3 + idx);
+            prefetch_l2(A.kacc + d * A.c.N3 + idx);
+        }
+    }
 
     template <class V>
     __device__ static void site(const Args &A, const V &v, int i, int j, int k, long long idx, Carry &cy,

@@ -63,6 +63,11 @@ struct HiggsU1 {
         double pm[2], pm2[2];                    // plaquette sines (0,1), (2,0) at x - i, both gauges
     };
 
+    __device__ static void prefetch(const Args &A, long long idx) {
+#pragma unroll
+        for (int f = 0; f < NR; f++) prefetch_l2(A.win + f * A.c.N3 + idx);
+    }
+
     template <class V>
     __device__ static void site(const Args &A, const V &v, int i, int j, int k, long long idx, Carry &cy,
                                 bool first_plane) {

@@ -61,6 +61,7 @@ struct R6Aux {
         double *aux;          // 6 arrays
     };
     struct Carry {};
+    __device__ static void prefetch(const Args &, long long) {}
     template <class V>
     __device__ static void site(const Args &A, const V &v, int, int, int, long long idx, Carry &, bool) {
         const R6Consts &c = A.c;
@@ -96,6 +97,10 @@ struct R6Step {
         int first, sync, damp;
     };
     struct Carry {};
+    __device__ static void prefetch(const Args &A, long long idx) {
+#pragma unroll
+        for (int f = 0; f < 6; f++) prefetch_l2(A.win + f * A.c.N3 + idx);
+    }
 
     template <class V>
     __device__ static void site(const Args &A, const V &v, int i, int j, int k, long long idx, Carry &, bool) {

@@ -17,6 +17,9 @@
 //   Args               kernel arguments, with `RingSrc<NR> src` and `int N`
 //   Carry              per-thread state kept along the i walk
 //   site(args, view, i, j, k, idx, carry, first)   the work at one site
+//   prefetch(args, idx)  L2 prefetch of what site() will read from global
+//                        memory at idx on the next plane (its momenta), so the
+//                        loads at the end of the next site update hit L2
 // and runs as ring_kernel<Model, TX, TY>.
 #pragma once
 #include "common.cuh"
@@ -117,6 +120,7 @@ __device__ __forceinline__ void ring_item(const typename M::Args &a, const Piece
             v.m = ring + (q & 3) * S::SLOT + own_s;
             v.c = ring + ((q + 1) & 3) * S::SLOT + own_s;
             v.p = ring + ((q + 2) & 3) * S::SLOT + own_s;
+            if (i + 1 < i1) M::prefetch(a, (long long)(i + 1) * NN + own_g);
             M::site(a, v, i, j, k, (long long)i * NN + own_g, carry, q == 0, extra...);
         }
     }
@@ -126,6 +130,11 @@ template <class M, int TX, int TY>
 __global__ void __launch_bounds__(TX *TY, M::MIN_CTAS) ring_kernel(typename M::Args a, TileGrid tg) {
     extern __shared__ __align__(16) double ring[];
     for_each_piece(tg, a.N, [&](const Piece &pc) { ring_item<M, TX, TY>(a, pc, ring); });
+}
+
+// Bring the line holding p into L2 ahead of its use (no register, no wait).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
 }
 
 // sponge factor 1 - rate * s^2 of the absorbing boundary at site (i, j, k),
