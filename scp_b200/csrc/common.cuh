@@ -18,6 +18,7 @@ struct StepConsts {
     double dt, hdt, gad;          // gad = -g*dx*dt (link drift prefactor)
     double g, stp;                // stp = 1/(g dx^3) (staple prefactor)
     double L, dx, damp_width, damp_rate;
+    int prefetch;                 // 1: prefetch the next plane's momenta into L2 at the top of a plane
 };
 
 // Work decomposition of the persistent step kernels: the grid is cut into
@@ -62,6 +63,11 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int NPEND>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
+}
+
+// Bring the line holding p into L2 ahead of its use (a hint: no register, no wait).
+__device__ __forceinline__ void prefetch_line_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
 }
 
 // Streaming store (evict-first): outputs are not re-read by this launch.

@@ -132,10 +132,7 @@ __global__ void __launch_bounds__(TX *TY, M::MIN_CTAS) ring_kernel(typename M::A
     for_each_piece(tg, a.N, [&](const Piece &pc) { ring_item<M, TX, TY>(a, pc, ring); });
 }
 
-// Bring the line holding p into L2 ahead of its use (no register, no wait).
-__device__ __forceinline__ void prefetch_l2(const void *p) {
-    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
-}
+__device__ __forceinline__ void prefetch_l2(const void *p) { prefetch_line_l2(p); }
 
 // sponge factor 1 - rate * s^2 of the absorbing boundary at site (i, j, k),
 // 1 inside radius L - width (apply_damping, sfa/sim/scp_sim.c:1440-1473)

@@ -223,6 +223,10 @@ static void fill_consts(scp_gpu *h) {
     c.L = p.L; c.dx = p.dx;
     c.damp_width = p.damp_width;
     c.damp_rate = p.damp_rate;
+    // next-plane momentum prefetch of the fused step (SCP_PREFETCH=0|1 in the
+    // environment; off by default)
+    const char *e = getenv("SCP_PREFETCH");
+    c.prefetch = (e && e[0] == '1') ? 1 : 0;
 }
 
 static bool damping_on(const scp_gpu *h) {

@@ -287,6 +287,10 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             }
             stg.commit();
             const long long site = (long long)i * N * N + oc;
+            if (c.prefetch && act && i + 1 < i1) {
+#pragma unroll
+                for (int f = 0; f < NF; f++) prefetch_line_l2(io.win + f * N3 + site + (long long)N * N);
+            }
             T w[NF];
             uint16_t lo[P::COMP ? 12 : 1];
             if (act) {

@@ -200,6 +200,12 @@ __device__ __forceinline__ void step_item2(const StepIO<F32C> &io, const StepCon
         cp_async_commit();
         if (!act) continue;
         const long long site = (long long)i * N * N + oc;
+        if (c.prefetch && i + 1 < i1) {
+#pragma unroll
+            for (int f = 0; f < NF; f++) prefetch_line_l2(io.win + f * N3 + site + (long long)N * N);
+#pragma unroll
+            for (int f = 0; f < 12; f++) prefetch_line_l2(io.loin + f * N3 + site + (long long)N * N);
+        }
         V2 w[NF];
         uint32_t lo[12];
 #pragma unroll
