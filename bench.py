@@ -630,10 +630,10 @@ def main():
     over = dict(N=args.n, L=(args.n - 1) / 4.0) if args.n else {}
     params = seeds.params_for(seed, precision=prec, device=local, tile_variant=args.tile, **over,
                               **WORKLOAD_OVER.get(args.workload, {}))
-    # kernels per step: one fused launch, or the three per-site sweeps of the
-    # extensions (and their closing kick after the last step)
-    ext = params.complex_gauge and (params.higgs_v > 0 or params.g_gauge2 != 0 or params.n_fabrics == 3)
-    launches_per_step = 3 if ext else 1
+    # kernels per step: one fused launch (the Higgs / second-gauge stepper
+    # too); with three fabrics one per moving fabric plus the link update
+    fab = params.complex_gauge and params.n_fabrics == 3
+    launches_per_step = ((3 if params.mf_lock_CQ else 4) if fab else 1)
     st = workload_state(args.workload, params)
     cols = st.cols()
     n3 = params.N ** 3
@@ -657,6 +657,14 @@ def main():
     info = sim.info()
     ms_max = max_over_ranks(ms, dist, f"cuda:{local}")
     ms_step = ms_max / args.steps
+    # one diagnostics call (reductions, point values and their copy to the
+    # host), warm, as the host sees it
+    for _ in range(3):
+        sim.diag_vector()
+    t0 = time.perf_counter()
+    for _ in range(10):
+        sim.diag_vector()
+    diag_ms = (time.perf_counter() - t0) / 10 * 1e3
     value = replica_throughput(n3 * args.steps, world, ms_max * 1e-3)
     bytes_site = info.step_bytes_per_site
     achieved = bytes_site * n3 / (ms / args.steps * 1e-3) / 1e9
@@ -715,7 +723,9 @@ def main():
                      "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "bytes_per_site": bytes_site,
                      "traffic": (lambda t: t * n3 if t else None)(profiled_traffic(args.workload))},
-        "gpu_launches": args.steps * launches_per_step + (1 if ext else 0),
+        "gpu_launches": args.steps * launches_per_step,
+        "diag": {"ms_per_call": diag_ms, "step_equivalents": diag_ms / ms_step,
+                 "includes": "energies, charges, Gauss residual, point values, copy to the host"},
         "clocks": clocks,
         "e2e": e2e,
     }

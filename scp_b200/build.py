@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v"]
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("scp_gpu.cu", "kern_f64.cu", "kern_f32c.cu", "kern_pair.cu", "kern_ext.cu", "kern_tma.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("scp_gpu.cu", "kern_f64.cu", "kern_f32c.cu", "kern_pair.cu", "kern_ext.cu", "kern_tma.cu", "kern_duo.cu")]
 OUT = os.path.join(HERE, "libscpgpu.so")
 OBJDIR = os.path.join(HERE, "_build")
 

@@ -98,14 +98,25 @@ struct HiggsU1 {
             if (G2) {
                 const double t2 = v(TH2 + d);
                 const double t1m = nb(v, TH + d, d, -1), t2m = nb(v, TH2 + d, d, -1);
+                // components of equal charge share their phase (the default
+                // charges 1, 1, -2): the same angle, so the same cos / sin
+                const bool same10 = c.q[1] == c.q[0], same20 = c.q[2] == c.q[0], same21 = c.q[2] == c.q[1];
 #pragma unroll
                 for (int a = 0; a < 3; a++) {
-                    sincos_any(t1 + c.q[a] * t2, &sP[a], &cP[a]);
+                    const int src = (a == 1 && same10) ? 0 : (a == 2 && same20) ? 0 : (a == 2 && same21) ? 1 : a;
+                    if (src == a) {
+                        sincos_any(t1 + c.q[a] * t2, &sP[a], &cP[a]);
+                        if (d != 0) sincos_any(t1m + c.q[a] * t2m, &sM[a], &cM[a]);
+                    } else if (src == 0) {
+                        sP[a] = sP[0]; cP[a] = cP[0];
+                        if (d != 0) { sM[a] = sM[0]; cM[a] = cM[0]; }
+                    } else {
+                        sP[a] = sP[1]; cP[a] = cP[1];
+                        if (d != 0) { sM[a] = sM[1]; cM[a] = cM[1]; }
+                    }
                     if (d == 0) {
                         cM[a] = cy.cm[a]; sM[a] = cy.sm[a];
                         cy.cm[a] = cP[a]; cy.sm[a] = sP[a];
-                    } else {
-                        sincos_any(t1m + c.q[a] * t2m, &sM[a], &cM[a]);
                     }
                 }
             } else {

@@ -41,6 +41,9 @@ TmaStepFn step_tma_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
 using CpmStepFn = void (*)(StepIO<F64>, StepConsts, TileGrid, const CUtensorMap);
 CpmStepFn step_cpm_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
 
+// gauged FP64 kernels with two threads per site (step_duo.cuh; tile 32 x 4)
+StepFnT<F64> step_duo_fn(bool f, bool s, bool d, size_t *smem);
+
 template <class P>
 StepFnT<P> step_fn(int shape, bool g, bool f, bool s, bool d, size_t *smem);
 template <>

@@ -155,9 +155,10 @@ struct scp_gpu {
     size_t snap_dev_bytes = 0;
     cudaEvent_t snap_ready = nullptr, snap_done = nullptr;
     int snap_pending = 0;
-    // plane staging of the FP64 fused step: 0 the cp.async ring, 1 TMA tile
-    // loads of the positions (tensor maps of X[0], X[1]), 2 the cp.async ring
-    // with TMA-staged momenta (tensor maps of W and S)
+    // form of the FP64 fused step: 0 the cp.async ring, 1 TMA tile loads of
+    // the positions (tensor maps of X[0], X[1]), 2 the cp.async ring with
+    // TMA-staged momenta (tensor maps of W and S), 3 the gauged step with two
+    // threads per site (step_duo.cuh)
     int tma = 0;
     TmaMaps tmaps[2];
     CUtensorMap mmaps[2];
@@ -361,13 +362,27 @@ static bool encode_mom_map(const double *W, int N, int nf, int tx, int ty, CUten
 // chains, which the TMA forms do not shorten.
 static int staging_mode(const scp_gpu *h, int shape) {
     if (h->prec != SCP_PREC_FP64 || (shape != 1 && shape != 2)) return 0;
+    const char *e = getenv("SCP_STAGING");
+    if (h->gauged && shape == 1 && e && strcmp(e, "duo") == 0) return 3;
     const TileShape ts = kShapes[shape];
     const int N = h->N;
     if (!(N % 2 == 0 && N % ts.tx == 0 && N % ts.ty == 0 && N >= 2 * ts.ty && N >= ts.tx)) return 0;
-    const char *e = getenv("SCP_STAGING");
     if (e && strcmp(e, "tma") == 0) return 1;
     if (e && strcmp(e, "cpm") == 0) return 2;
     return 0;
+}
+
+// the two-threads-per-site kernels: shared-memory cap of every variant, and
+// the CTAs of 2 x 32 x 4 threads one SM holds
+static int setup_duo(scp_gpu *h, int *occ) {
+    size_t smem = 0;
+    for (int v = 0; v < 8; v++) {
+        StepFnT<F64> fn = step_duo_fn(v & 1, (v >> 1) & 1, (v >> 2) & 1, &smem);
+        CK(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    StepFnT<F64> fn = step_duo_fn(false, false, false, &smem);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, (const void *)fn, h->threads, smem));
+    return SCP_OK;
 }
 
 static int setup_tma(scp_gpu *h, int *occ) {
@@ -405,7 +420,10 @@ static int setup_launch(scp_gpu *h) {
     h->threads = ts.tx * ts.ty / (pairs ? 2 : 1);
     int occ = 0, rc;
     h->tma = staging_mode(h, shape);
-    if (h->tma) rc = setup_tma(h, &occ);
+    if (h->tma == 3) {
+        h->threads = 2 * ts.tx * ts.ty;
+        rc = setup_duo(h, &occ);
+    } else if (h->tma) rc = setup_tma(h, &occ);
     else if (pairs) rc = occupancy2_of(h, shape, &occ);
     else if (h->prec == SCP_PREC_FP64) rc = occupancy_of<F64>(h, shape, &occ);
     else rc = occupancy_of<F32C>(h, shape, &occ);
@@ -436,6 +454,9 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         } else if (h->tma == 2) {
             CpmStepFn fn = step_cpm_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
             fn<<<h->grid_run, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg_run, h->mmaps[first ? 1 : 0]);
+        } else if (h->tma == 3) {
+            StepFnT<F64> fn = step_duo_fn(first, sync, damping_on(h), &smem);
+            fn<<<h->grid_run, h->threads, smem, h->stream>>>(io, h->c, h->tg_run);
         } else {
             StepFnT<F64> fn = step_fn<F64>(h->shape, h->gauged, first, sync, damping_on(h), &smem);
             fn<<<h->grid_run, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg_run);
