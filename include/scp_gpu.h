@@ -157,11 +157,13 @@ typedef struct {
     double  step_bytes_per_site;    /* algorithmic bytes moved per site-update */
     int32_t tile_x, tile_y, seg_len; /* tile shape in use */
     int32_t sites_per_thread; /* 2: two-site packed FP32C kernel (even N), else 1 */
-    int32_t tma_staging;      /* plane staging of the FP64 step: 0 the cp.async ring (the
-                                 default); on full tiles of the default shapes SCP_STAGING=tma
-                                 in the environment selects TMA tile loads of the positions (1)
-                                 and SCP_STAGING=cpm the cp.async ring with TMA-staged momenta
-                                 (2), both bit-identical to 0 */
+    int32_t tma_staging;      /* form of the FP64 step: 0 the cp.async ring (the default); on
+                                 full tiles of the default shapes SCP_STAGING=tma in the
+                                 environment selects TMA tile loads of the positions (1) and
+                                 SCP_STAGING=cpm the cp.async ring with TMA-staged momenta (2),
+                                 both bit-identical to 0; on gauged grids with the default tile
+                                 SCP_STAGING=duo selects two threads per site (3, equal to 0 up
+                                 to roundoff) */
 } scp_gpu_info;
 
 typedef struct scp_gpu scp_gpu;
