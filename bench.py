@@ -207,24 +207,33 @@ def l2_label(state_bytes: float) -> str:
     return f"state {mb:.0f} MB is within ~2x L2 (126 MB): steps are L2-aided, not an HBM roofline figure"
 
 
-def reference_gpu(params, cols, n_short: int = 50, n_long: int = 250) -> dict:
+def reference_gpu(params, cols, lengths=(50, 1050, 2050, 3050)) -> dict:
     """The reference's own CUDA stepper (sfa/sim/scp_sim.cu, recompiled
     unmodified for sm_100a into oracle/_ref/scp_sim_cuda) on the same
     workload.  Its Wall line starts its clock before the t=0 diagnostics and
-    snapshot (scp_sim.cu:5405-5457), so the per-step time is taken from two
-    runs of different length: (total_long - total_short) / (n_long - n_short)."""
+    snapshot (scp_sim.cu:5405-5457), about 10 s of host work at 128^3 that
+    varies by tens of ms from run to run, so the per-step time is the
+    least-squares slope of the total over runs of several lengths (3000
+    steps apart at the ends, well above that jitter).  The first run of a
+    process is slower by most of a second (device and module set-up), so one
+    untimed run comes first."""
     import oracle
     if not os.path.exists(oracle.REF_GPU_BIN):
         return {"value": None, "unit": METRIC, "note": "reference CUDA binary not built"}
+    oracle.run_reference(params, cols, lengths[0], diag_every=lengths[0], read_final=False,
+                         binary=oracle.REF_GPU_BIN)
     tot = {}
-    for n in (n_short, n_long):
+    for n in lengths:
         r = oracle.run_reference(params, cols, n, diag_every=n, read_final=False, binary=oracle.REF_GPU_BIN)
         tot[n] = r["wall_ms_per_step"] * n
-    ms = (tot[n_long] - tot[n_short]) / (n_long - n_short)
-    return {"value": params.N ** 3 / (ms * 1e-3), "unit": METRIC, "ms_per_step": ms,
-            "runs_ms_total": {str(k): v for k, v in tot.items()},
+    xs = np.array(list(tot), dtype=float)
+    ys = np.array([tot[n] for n in tot])
+    ms, b = np.polyfit(xs, ys, 1)
+    resid = float(np.max(np.abs(ys - (ms * xs + b))))
+    return {"value": params.N ** 3 / (ms * 1e-3), "unit": METRIC, "ms_per_step": float(ms),
+            "runs_ms_total": {str(k): v for k, v in tot.items()}, "fit_max_residual_ms": resid,
             "kind": "reference sfa/sim/scp_sim.cu recompiled for sm_100a, FP64, its own loop clock, "
-                    "difference of a 250-step and a 50-step run"}
+                    "slope of the loop time over runs of " + ", ".join(str(n) for n in lengths) + " steps"}
 
 
 def short_rate(workload: str, steps: int = 20, warmup: int = 5) -> dict:
@@ -657,10 +666,19 @@ def main():
     info = sim.info()
     ms_max = max_over_ranks(ms, dist, f"cuda:{local}")
     ms_step = ms_max / args.steps
-    # one diagnostics call (reductions, point values and their copy to the
-    # host), warm, as the host sees it
+    # diagnostics as the reference's loop uses them: 10 steps, then one
+    # diagnostics call (reductions, point values, copy to the host), timed on
+    # the host; what the cycle takes beyond 10 device-timed steps is the cost
+    # of a diagnostic (the synchronous launch's own sums included).  A repeat
+    # call on an unchanged state times the call alone.
     for _ in range(3):
+        sim.step(10)
         sim.diag_vector()
+    t0 = time.perf_counter()
+    for _ in range(10):
+        sim.step(10)
+        sim.diag_vector()
+    cycle_ms = (time.perf_counter() - t0) / 10 * 1e3
     t0 = time.perf_counter()
     for _ in range(10):
         sim.diag_vector()
@@ -724,7 +742,8 @@ def main():
                      "bytes_per_site": bytes_site,
                      "traffic": (lambda t: t * n3 if t else None)(profiled_traffic(args.workload))},
         "gpu_launches": args.steps * launches_per_step,
-        "diag": {"ms_per_call": diag_ms, "step_equivalents": diag_ms / ms_step,
+        "diag": {"ms_per_call": diag_ms, "cycle_10_steps_ms": cycle_ms,
+                 "step_equivalents": (cycle_ms - 10 * ms_step) / ms_step,
                  "includes": "energies, charges, Gauss residual, point values, copy to the host"},
         "clocks": clocks,
         "e2e": e2e,

@@ -19,6 +19,9 @@ struct StepConsts {
     double g, stp;                // stp = 1/(g dx^3) (staple prefactor)
     double L, dx, damp_width, damp_rate;
     int prefetch;                 // 1: prefetch the next plane's momenta into L2 at the top of a plane
+    // diagnostics summed by synchronous FP64 launches: cell volume, core
+    // radius^2 of Q_core, plaquette-energy prefactor 1/(g^2 dx^4)
+    double dV, R2, bpre;
 };
 
 // Work decomposition of the persistent step kernels: the grid is cut into

@@ -44,6 +44,17 @@ enum : int {
 };
 constexpr int kDiag1Q = DS_NSUM + DM_NMAX;
 
+// per-thread sums and maxima of the pass-1 slots
+struct DiagSums {
+    double S[DS_NSUM], M[DM_NMAX];
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (int q = 0; q < DS_NSUM; q++) S[q] = 0.0;
+#pragma unroll
+        for (int q = 0; q < DM_NMAX; q++) M[q] = 0.0;
+    }
+};
+
 template <class View>
 __global__ void __launch_bounds__(kRedThreads) diag_pass1_kernel(View V, DiagConsts c, double *part) {
     __shared__ double scratch[kDiag1Q * 32];
@@ -221,16 +232,69 @@ __global__ void __launch_bounds__(kRedThreads) diag_pass2_kernel(View V, DiagCon
     block_fold<1, 1>(S, M, scratch, part);
 }
 
+// Pass 2 after a synchronous step launch that summed pass 1 itself (step.cuh,
+// StepIO::dpart): r_core and the argmax site as diag_pass2_kernel, and the
+// Gauss-law slots of pass 1 (compute_gauss, scp_sim.c:2186-2243), which need
+// E_{n+1} of the neighbouring sites, from the charge density the launch
+// stored (rho, N^3; links only).
+// part per CTA: sums [rsum, GL2, NOM, FSUM, NC], maxima [-min_idx, GMAX].
+template <class View>
+__global__ void __launch_bounds__(kRedThreads) diag_pass2g_kernel(View V, DiagConsts c, const double *fin1,
+                                                                  const double *rho, double *part) {
+    __shared__ double scratch[7 * 32];
+    const double M0 = fin1[DS_M0] * c.dV;
+    const double cx = M0 < 1e-30 ? 0.0 : fin1[DS_CX] * c.dV / M0;
+    const double cy = M0 < 1e-30 ? 0.0 : fin1[DS_CY] * c.dV / M0;
+    const double cz = M0 < 1e-30 ? 0.0 : fin1[DS_CZ] * c.dV / M0;
+    const double sthr = fin1[DS_NSUM + DM_SMAX] * (1.0 - 1e-12);
+    const int N = c.N;
+    const long long NN = (long long)N * N;
+    double S[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, M[2] = {-INFINITY, 0.0};
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < c.N3;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        site_ijk(idx, N, &i, &j, &k);
+        const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
+        double rho2 = 0.0, sp = 1.0;
+        for (int a = 0; a < 3; a++) {
+            const double u = V.q(FU + a, idx), v = V.q(FV + a, idx);
+            rho2 += u * u + v * v;
+            sp *= u * u + v * v;
+        }
+        S[0] += ((x - cx) * (x - cx) + (y - cy) * (y - cy) + (z - cz) * (z - cz)) * rho2;
+        if (sp >= sthr) M[0] = fmax(M[0], -(double)idx);
+        if (c.links) {
+            const long long im = (long long)wrapi(i - 1, N) * NN + (long long)j * N + k;
+            const long long jm = (long long)i * NN + (long long)wrapi(j - 1, N) * N + k;
+            const long long km = (long long)i * NN + (long long)j * N + wrapi(k - 1, N);
+            const double E0 = V.p(FTH, idx), E1 = V.p(FTH + 1, idx), E2 = V.p(FTH + 2, idx);
+            const double divE = (E0 - V.p(FTH, im) + E1 - V.p(FTH + 1, jm) + E2 - V.p(FTH + 2, km)) / c.dx;
+            const double G = divE - c.g * rho[idx];
+            if (x * x + y * y + z * z < c.Rint2) {
+                M[1] = fmax(M[1], fabs(G - c.G_offset));
+                S[1] += (G - c.G_offset) * (G - c.G_offset);
+                S[2] += 1.0;
+            }
+            if (fabs(x) <= c.Rcube && fabs(y) <= c.Rcube && fabs(z) <= c.Rcube) {
+                S[3] += divE * c.dV;
+                S[4] += 1.0;
+            }
+        }
+    }
+    block_fold<5, 2>(S, M, scratch, part);
+}
+
 // Final scalar reads: omega_core at the argmax-s site and the two theta probes.
 // out[0]=omega_core out[1..4]=thp1u thp1v thp2u thp2v
+// negidx_p: the folded -(lowest qualifying site index).
 template <class View>
-__global__ void diag_point_kernel(View V, DiagConsts c, const double *fin2, double probe1, double probe2,
+__global__ void diag_point_kernel(View V, DiagConsts c, const double *negidx_p, double probe1, double probe2,
                                   double *out) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const int N = c.N;
     const long long NN = (long long)N * N;
     out[0] = 0.0;
-    const double negidx = fin2[1];
+    const double negidx = *negidx_p;
     if (isfinite(negidx)) {
         const long long idx = (long long)(-negidx);
         const double u0 = V.q(FU, idx), v0 = V.q(FV, idx), ud0 = V.p(FU, idx), vd0 = V.p(FV, idx);

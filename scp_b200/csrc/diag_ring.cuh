@@ -13,10 +13,6 @@
 
 namespace scp {
 
-struct DiagSums {
-    double S[DS_NSUM], M[DM_NMAX];
-};
-
 // One instantiation per GAUGED: states with and without links run the same
 // machine code (the links are a runtime flag, c.links), so a g = 0 run that
 // carries links sums exactly as the run without them.  Without links the

@@ -160,6 +160,11 @@ struct scp_gpu {
     // TMA-staged momenta (tensor maps of W and S), 3 the gauged step with two
     // threads per site (step_duo.cuh)
     int tma = 0;
+    // diagnostics summed by the synchronous FP64 step launch (classic form,
+    // gauged or without links): per-CTA partials, the Gauss charge density,
+    // and whether the partials describe the current state
+    double *dpart = nullptr, *drho = nullptr;
+    int dfuse = 0, dvalid = 0;
     TmaMaps tmaps[2];
     CUtensorMap mmaps[2];
     // launch geometry
@@ -228,6 +233,9 @@ static void fill_consts(scp_gpu *h) {
     // environment; off by default)
     const char *e = getenv("SCP_PREFETCH");
     c.prefetch = (e && e[0] == '1') ? 1 : 0;
+    c.dV = p.dx * p.dx * p.dx;
+    c.R2 = p.qdiag_radius * p.qdiag_radius;
+    c.bpre = gauged ? 1.0 / (p.g_gauge * p.g_gauge * p.dx * p.dx * p.dx * p.dx) : 0.0;
 }
 
 static bool damping_on(const scp_gpu *h) {
@@ -448,6 +456,10 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         io.wout = h->W;
         io.sout = h->S;
         io.flag = h->flag;
+        const bool dg = sync && !first && h->dfuse;
+        io.dpart = dg ? h->dpart : nullptr;
+        io.drho = dg ? h->drho : nullptr;
+        h->dvalid = dg ? 1 : 0;
         if (h->tma == 1) {
             TmaStepFn fn = step_tma_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
             fn<<<h->grid_run, ts.tx * ts.ty, smem, h->stream>>>(io, h->c, h->tg_run, h->tmaps[h->cur]);
@@ -473,6 +485,7 @@ static int launch_step(scp_gpu *h, bool first, bool sync) {
         io.wout = h->W32;
         io.sout = h->S32;
         io.flag = h->flag;
+        h->dvalid = 0;
         if (h->pairs) {
             StepFnT<F32C> fn = step2_fn(h->shape, h->gauged, first, sync, damping_on(h), &smem);
             fn<<<h->grid_run, h->threads, smem, h->stream>>>(io, h->c, h->tg_run);
@@ -710,6 +723,19 @@ static int init_body(scp_gpu *h, const double *const *cols, bool on_device) {
     if ((rc = setup_launch(h))) return rc;
     CK(cudaMallocAsync(&h->stage, sizeof(double) * n3, h->stream));
     h->dev_bytes += sizeof(double) * n3;
+    // the classic FP64 step sums the first diagnostics pass in its synchronous
+    // launches (not with links at g = 0, whose step carries no th / E);
+    // SCP_FUSED_DIAG=0 in the environment keeps the separate pass
+    const char *fd = getenv("SCP_FUSED_DIAG");
+    if (h->prec == SCP_PREC_FP64 && h->tma == 0 && (h->gauged || !h->links) && !(fd && fd[0] == '0')) {
+        CK(cudaMallocAsync(&h->dpart, sizeof(double) * kDiag1Q * (size_t)h->grid_run, h->stream));
+        h->dev_bytes += sizeof(double) * kDiag1Q * (size_t)h->grid_run;
+        if (h->gauged) {
+            CK(cudaMallocAsync(&h->drho, sizeof(double) * n3, h->stream));
+            h->dev_bytes += sizeof(double) * n3;
+        }
+        h->dfuse = 1;
+    }
     h->cur = 0;
     if (h->prec == SCP_PREC_FP64) return launch_step(h, true, false);
     // FP32-compensated buffers: X32[0..1], W32, S32 (fp32, NF arrays), LO[0..1]
@@ -1345,23 +1371,53 @@ static int diag_with(scp_gpu *h, const View &V, scp_gpu_diag_out *out) {
     const DiagConsts c = diag_consts(h);
     const int nb = red_blocks(h->N3);
     int nb1 = nb;
+    const double *part1 = h->part;
+    // pass 1 already summed by the synchronous step launch that produced this state
+    const bool fused = std::is_same<View, ViewF64>::value && h->dvalid;
     if constexpr (std::is_same<View, ViewF64>::value) {
-        const size_t th = (size_t)FTH * h->N3;
-        int rc = diag_pass1_ring(h, c, V.X, V.S, c.links ? V.X + th : nullptr, c.links ? V.S + th : nullptr, &nb1);
-        if (rc) return rc;
+        if (fused) {
+            nb1 = h->grid_run;
+            part1 = h->dpart;
+        } else {
+            const size_t th = (size_t)FTH * h->N3;
+            int rc = diag_pass1_ring(h, c, V.X, V.S, c.links ? V.X + th : nullptr, c.links ? V.S + th : nullptr,
+                                     &nb1);
+            if (rc) return rc;
+        }
     } else {
         diag_pass1_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->part);
     }
-    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(h->part, nb1, h->fold);
-    diag_pass2_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->fold, h->part);
-    fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold + 40);
-    diag_point_kernel<View><<<1, 32, 0, h->stream>>>(V, c, h->fold + 40, p.qdiag_probe1, p.qdiag_probe2,
-                                                        h->point);
+    fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, h->stream>>>(part1, nb1, h->fold);
+    // pass 2 (r_core, argmax site), with the Gauss-law slots when pass 1 was fused
+    const bool gauss2 = fused && c.links;
+    const double *negidx;
+    if (gauss2) {
+        diag_pass2g_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->fold, h->drho, h->part);
+        fold_partials_kernel<5, 2><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold + 44);
+        negidx = h->fold + 49;
+    } else {
+        diag_pass2_kernel<View><<<nb, kRedThreads, 0, h->stream>>>(V, c, h->fold, h->part);
+        fold_partials_kernel<1, 1><<<1, 1024, 0, h->stream>>>(h->part, nb, h->fold + 40);
+        negidx = h->fold + 41;
+    }
+    diag_point_kernel<View><<<1, 32, 0, h->stream>>>(V, c, negidx, p.qdiag_probe1, p.qdiag_probe2, h->point);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * 42, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(h->h_small + 48, h->point, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_small, h->fold, sizeof(double) * 51, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->h_small + 56, h->point, sizeof(double) * 5, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    diag_assemble(h->h_small, h->h_small + 40, h->h_small + 48, c, h->N3, p.g_gauge, out);
+    double f1[kDiag1Q], f2[2] = {h->h_small[40], h->h_small[41]};
+    memcpy(f1, h->h_small, sizeof f1);
+    if (gauss2) {   // [rsum, GL2, NOM, FSUM, NC | -min_idx, GMAX]
+        const double *g = h->h_small + 44;
+        f2[0] = g[0];
+        f2[1] = g[5];
+        f1[DS_GL2] = g[1];
+        f1[DS_NOM] = g[2];
+        f1[DS_FSUM] = g[3];
+        f1[DS_NC] = g[4];
+        f1[DS_NSUM + DM_GMAX] = g[6];
+    }
+    diag_assemble(f1, f2, h->h_small + 56, c, h->N3, p.g_gauge, out);
     if (!isfinite(out->v[SCP_DIAG_E_TOTAL])) return SCP_ENONFINITE;
     return SCP_OK;
 }
@@ -1594,7 +1650,7 @@ void scp_gpu_free(scp_gpu *h) {
     if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
     if (h->stream) {
         void *bufs[] = {h->slab32, h->slab, h->part, h->fold, h->cg, h->point, h->flag, h->count, h->stage,
-                        h->snap_dev, h->raux, h->kacc};
+                        h->snap_dev, h->raux, h->kacc, h->dpart, h->drho};
         for (void *b : bufs)
             if (b) cudaFreeAsync(b, h->stream);
         cudaStreamSynchronize(h->stream);
@@ -1805,7 +1861,7 @@ extern "C" int scp_gpu_diag_noalloc(const scp_gpu_params *pp, const double *cons
     fold_partials_kernel<DS_NSUM, DM_NMAX><<<1, 1024, 0, st>>>(part, nb, fold);
     diag_pass2_kernel<ViewCols><<<nb, kRedThreads, 0, st>>>(V, c, fold, part);
     fold_partials_kernel<1, 1><<<1, 1024, 0, st>>>(part, nb, fold + 40);
-    diag_point_kernel<ViewCols><<<1, 32, 0, st>>>(V, c, fold + 40, p.qdiag_probe1, p.qdiag_probe2, point);
+    diag_point_kernel<ViewCols><<<1, 32, 0, st>>>(V, c, fold + 41, p.qdiag_probe1, p.qdiag_probe2, point);
     CK(cudaGetLastError());
     double h[53];
     CK(cudaMemcpyAsync(h, fold, sizeof(double) * 42, cudaMemcpyDeviceToHost, st));

@@ -41,6 +41,7 @@
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "diag.cuh"
 #include "trig.cuh"
 
 namespace scp {
@@ -67,6 +68,12 @@ struct StepIO {
     T *wout;                // NF arrays: w_{n+1} (may alias win)
     T *sout;                // NF arrays: v_{n+1}, E_{n+1} (SYNC only)
     int *flag;              // nonfinite flag (SYNC only)
+    // FP64 SYNC launches of the single-grid kernel: when set, the launch also
+    // sums the first diagnostics pass at (x_{n+1}, v_{n+1}) -- one partial of
+    // DS_NSUM + DM_NMAX slots per CTA into dpart -- and stores the Gauss-law
+    // charge density of every site into drho (gauged)
+    double *dpart = nullptr;
+    double *drho = nullptr;
 };
 
 // gauge-quantity slots of the per-plane shared array
@@ -204,9 +211,15 @@ struct CpStage {
 // One work item (a TX x TY column over one segment of planes) of one grid.
 // sync and damp are uniform per call; the single-grid kernel passes them as
 // constants, the multi-request kernel per request.  Stage stages the planes.
+// dsum (FP64 SYNC launches only): per-thread sums of the first diagnostics
+// pass over this item's sites, the per-site terms of diag_ring.cuh / diag.cuh
+// (compute_energy_complex[_gauge], compute_charges, sfa/sim/scp_sim.c:1823-2169)
+// evaluated from the values the step holds; the Gauss-law slots are left to
+// a pass that reads E of the neighbouring sites.
 template <class P, int TX, int TY, bool GAUGED, bool FIRST, class Stage>
 __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts &c, const Piece &pc,
-                                          const bool SYNC, const bool DAMP, Stage &stg) {
+                                          const bool SYNC, const bool DAMP, Stage &stg, DiagSums *dsum = nullptr) {
+    const bool DG = !P::COMP && dsum != nullptr;
     using T = typename P::T;
     using LY = StepLayout<P, TX, TY, GAUGED>;
     constexpr int NF = LY::NF;
@@ -233,6 +246,13 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
         // sine of the plaquette angle th_a(y) + th_b(y+a) - th_a(y+b) - th_b(y) of plane
         // (a,b) = (0,1) (1,2) (2,0) [q = 0, 1, 2] at ring position (r, col) of slot sc,
         // the next plane in slot sp (compute_forces_complex_gauge pass B, scp_sim.c:1090-1109)
+        // the F64 plaquette angle itself (diagnostics: its cosine)
+        auto plaq_angle = [&](int q, int sc, int sp, int r, int col) -> double {
+            const int a = q, b = (q + 1) % 3;
+            const int sa = (a == 0) ? sp : sc, ra = r + (a == 1 ? 1 : 0), ca = col + (a == 2 ? 1 : 0);
+            const int sb = (b == 0) ? sp : sc, rb = r + (b == 1 ? 1 : 0), cb = col + (b == 2 ? 1 : 0);
+            return XS(sc, FTH + a, r, col) + XS(sa, FTH + b, ra, ca) - XS(sb, FTH + a, rb, cb) - XS(sc, FTH + b, r, col);
+        };
         auto plaq_sin = [&](int q, int sc, int sp, int r, int col) -> T {
             const int a = q, b = (q + 1) % 3;
             // th_b(y+a): the next plane for a = 0, else the neighbour row (a = 1) or column (a = 2)
@@ -322,6 +342,7 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             const T Vp = T(0.5) * (T)c.mu / (den * den);
             const T rest[3] = {s1 * s2, s0 * s2, s0 * s1};
             const T m2 = (T)c.m2, mt2 = (T)c.mtheta2, eta = (T)c.eta;
+            double bbE = 0.0;   // diagnostics: sum of 1 - cos of this site's three plaquettes
 
             if (!GAUGED) {
                 // compute_forces_complex, scp_sim.c:931-994
@@ -360,6 +381,27 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                     x = ctr[FTV + a];
                     acc[FTV + a] = lap(FTV + a) - mt2 * x + eta * curl(FV, a);
                 }
+                if constexpr (!P::COMP) {
+                    if (DG) {   // gradient energies and the Cosserat coupling energy
+                        double eg = 0.0, etg = 0.0;
+#pragma unroll
+                        for (int d = 0; d < 3; d++) {
+#pragma unroll
+                            for (int q = 0; q < 6; q++) {
+                                const int fre = q < 3 ? FU + q : FTU + q - 3, fim = q < 3 ? FV + q : FTV + q - 3;
+                                const double DR = (nb(fre, 2 * d) - nb(fre, 2 * d + 1)) * idx1;
+                                const double DI = (nb(fim, 2 * d) - nb(fim, 2 * d + 1)) * idx1;
+                                if (q < 3) eg += DR * DR + DI * DI;
+                                else etg += DR * DR + DI * DI;
+                            }
+                        }
+                        dsum->S[DS_EG] += 0.5 * eg * c.dV;
+                        dsum->S[DS_ETG] += 0.5 * etg * c.dV;
+#pragma unroll
+                        for (int a = 0; a < 3; a++)
+                            dsum->S[DS_EC] -= c.eta * (ctr[FU + a] * curl(FTU, a) + ctr[FV + a] * curl(FTV, a)) * c.dV;
+                    }
+                }
             } else {
                 // compute_forces_complex_gauge pass C, scp_sim.c:1112-1262
                 // complex fields q=0..2 Phi_a, q=3..5 Theta_a
@@ -371,6 +413,7 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 // central differences D = (transported(x+d) - transported(x-d))/(2dx);
                 // one subtraction either way round, as the reference forms it
                 T crT[3], ciT[3], crP[3], ciP[3];
+                double egP = 0.0, egT = 0.0;   // diagnostics: squared covariant differences
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
                     // link d at x (pass A, scp_sim.c:1072-1079) and at x - d
@@ -398,6 +441,13 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                         }
                         const T TRp = cP * up - sP * vp, TIp = cP * vp + sP * up;
                         const T TRm = cM * um + sM * vm, TIm = cM * vm - sM * um;
+                        if constexpr (!P::COMP) {
+                            if (DG) {
+                                const double DRe = (TRp - TRm) * idx1, DIe = (TIp - TIm) * idx1;
+                                if (q < 3) egP += DRe * DRe + DIe * DIe;
+                                else egT += DRe * DRe + DIe * DIe;
+                            }
+                        }
                         if constexpr (P::COMP) {   // accumulate (transported - centre) differences
                             const T cu = fu[q], cv = fv[q];
                             if (d == 0) { lapU[q] = (TRp - cu) + (TRm - cu); lapV[q] = (TIp - cv) + (TIm - cv); }
@@ -458,6 +508,20 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 const T st1 = -(P0 - P0m) + (P1 - P1km);
                 const T st2 = (P2 - P2m) - (P1 - P1jm);
                 P0m = P0; P2m = P2;   // x - i of the next plane
+                if constexpr (!P::COMP) {
+                    if (DG) {
+                        dsum->S[DS_EG] += 0.5 * egP * c.dV;
+                        dsum->S[DS_ETG] += 0.5 * egT * c.dV;
+#pragma unroll
+                        for (int a = 0; a < 3; a++) dsum->S[DS_EC] -= c.eta * (fu[a] * crT[a] + fv[a] * ciT[a]) * c.dV;
+                        double sn, cs;
+#pragma unroll
+                        for (int q = 0; q < 3; q++) {
+                            sincos_any(plaq_angle(q, sc, sp, ty + 1, tx + 1), &sn, &cs);
+                            bbE += 1.0 - cs;
+                        }
+                    }
+                }
                 const T stp = (T)c.stp, gg = (T)c.g;
                 K[0] = stp * st0 + gg * K[0];
                 K[1] = stp * st1 + gg * K[1];
@@ -489,6 +553,7 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 }
             }
             bool bad = false;
+            double vv[NF];   // diagnostics: v_{n+1}, E_{n+1}
 #pragma unroll
             for (int f = 0; f < 12; f++) {
                 T v, wn, xn;
@@ -512,6 +577,7 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                     if (DAMP && !FIRST) v *= dmp;
                     wn = v + hdt * acc[f];
                     xn = ctr[f] + dt * wn;
+                    vv[f] = v;
                 }
                 st_cs(io.xout + f * N3 + site, xn);
                 io.wout[f * N3 + site] = wn;
@@ -548,6 +614,7 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                         if (DAMP && !FIRST) E *= dmp;
                         Eh = E + hdt * K[d];
                         th = link_wrap(ctr[FTH + d] + gad * Eh);
+                        vv[FTH + d] = E;
                     }
                     st_cs(io.xout + (FTH + d) * N3 + site, th);
                     io.wout[(FTH + d) * N3 + site] = Eh;
@@ -558,6 +625,62 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 }
             }
             if (SYNC && bad) atomicOr(io.flag, 1);
+            if constexpr (!P::COMP) {
+                if (DG) {   // energies, charges, core and centroid moments at (x_{n+1}, v_{n+1})
+                    double *S = dsum->S, *M = dsum->M;
+                    const double dV = c.dV;
+                    double s2[3];
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        const double u = ctr[FU + a], w0 = ctr[FV + a], tu = ctr[FTU + a], tv = ctr[FTV + a];
+                        s2[a] = u * u + w0 * w0;
+                        const double pu = vv[FU + a], pv = vv[FV + a], ptu = vv[FTU + a], ptv = vv[FTV + a];
+                        S[DS_EPK] += 0.5 * (pu * pu + pv * pv) * dV;
+                        S[DS_ETK] += 0.5 * (ptu * ptu + ptv * ptv) * dV;
+                        S[DS_EM] += 0.5 * c.m2 * s2[a] * dV;
+                        S[DS_ETM] += 0.5 * c.mtheta2 * (tu * tu + tv * tv) * dV;
+                        M[DM_PM] = fmax(M[DM_PM], sqrt(s2[a]));
+                    }
+                    const double s3 = s2[0] * s2[1] * s2[2];
+                    S[DS_EP] += (c.mu / 2.0) * s3 / (1.0 + c.kappa * s3) * dV;
+                    M[DM_PMAX] = fmax(M[DM_PMAX], sqrt(s3));
+                    S[DS_PINT] += sqrt(s3) * dV;
+#pragma unroll
+                    for (int a = 0; a < 3; a++) S[DS_TRS] += ctr[FTU + a] * ctr[FTU + a] + ctr[FTV + a] * ctr[FTV + a];
+                    const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
+                    double rho2 = 0.0, qp = 0.0, qt = 0.0, sprod = 1.0;
+#pragma unroll
+                    for (int a = 0; a < 3; a++) {
+                        const double qa = ctr[FU + a] * vv[FV + a] - ctr[FV + a] * vv[FU + a];
+                        qp += qa;
+                        S[DS_QP0 + a] += qa;
+                        qt += ctr[FTU + a] * vv[FTV + a] - ctr[FTV + a] * vv[FTU + a];
+                        const double s2a = ctr[FU + a] * ctr[FU + a] + ctr[FV + a] * ctr[FV + a];
+                        rho2 += s2a;
+                        sprod *= s2a;
+                    }
+                    S[DS_QP] += qp;
+                    S[DS_QT] += qt;
+                    if (x * x + y * y + z * z <= c.R2) S[DS_QC] += qp + qt;
+                    M[DM_SMAX] = fmax(M[DM_SMAX], sprod);
+                    S[DS_M0] += rho2;
+                    S[DS_CX] += x * rho2;
+                    S[DS_CY] += y * rho2;
+                    S[DS_CZ] += z * rho2;
+                    if (GAUGED) {   // charge density of the Gauss law; E_em
+                        double rho = 0.0;
+#pragma unroll
+                        for (int a = 0; a < 3; a++)
+                            rho += ctr[FU + a] * vv[FV + a] - ctr[FV + a] * vv[FU + a] +
+                                   ctr[FTU + a] * vv[FTV + a] - ctr[FTV + a] * vv[FTU + a];
+                        io.drho[site] = rho;
+                        const double E0 = vv[FTH], E1 = vv[FTH + 1], E2 = vv[FTH + 2];
+                        double ee = 0.5 * (E0 * E0 + E1 * E1 + E2 * E2);
+                        ee += c.bpre * bbE;
+                        S[DS_EEM] += ee * dV;
+                    }
+                }
+            }
 #pragma unroll
             for (int f = 0; f < 12; f++) xm[f] = ctr[f];
         }
@@ -577,6 +700,18 @@ __global__ void __launch_bounds__(TX * TY, (MinBlocks<P, TX, TY, GAUGED>::value)
 step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CpStage<P, TX, TY, GAUGED> stg(smem_raw);
+    if constexpr (SYNC && !FIRST && !P::COMP) {
+        if (io.dpart) {   // uniform: this launch also sums the first diagnostics pass
+            DiagSums acc;
+            acc.clear();
+            for_each_piece(tg, c.N, [&](const Piece &pc) {
+                step_item<P, TX, TY, GAUGED, FIRST>(io, c, pc, SYNC, DAMP, stg, &acc);
+            });
+            __syncthreads();   // the ring is free: its first 7.4 KB serve as the fold's scratch
+            block_fold<DS_NSUM, DM_NMAX>(acc.S, acc.M, reinterpret_cast<double *>(smem_raw), io.dpart);
+            return;
+        }
+    }
     for_each_piece(tg, c.N, [&](const Piece &pc) { step_item<P, TX, TY, GAUGED, FIRST>(io, c, pc, SYNC, DAMP, stg); });
 }
 

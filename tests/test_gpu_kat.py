@@ -72,8 +72,12 @@ def test_zero_coupling_runs_the_ungauged_stepper(gpu, prec):
             assert np.array_equal(A[c], want), c
         else:
             assert np.max(np.abs(A[c] - want)) <= 1e-7 * max(np.max(np.abs(want)), 1e-30), c
+    # the same per-site terms; the ungauged FP64 handle sums them inside its
+    # synchronous step launch, the g = 0 one in the separate pass, so the
+    # totals agree to roundoff (the energy is the ungauged one: E_em, which the
+    # gauged energy would add, is of order 1e-3 here)
     for key in ("E_total", "E_grad", "Q_total", "s_max", "r_core"):
-        assert da[key] == db[key], key
+        assert abs(da[key] - db[key]) <= 1e-12 * max(abs(db[key]), 1.0), key
     N, dx = p.N, p.dx
     E = [A[27 + d].reshape(N, N, N) for d in range(3)]
     div = sum(E[d] - np.roll(E[d], 1, axis=d) for d in range(3)) / dx
