@@ -42,6 +42,9 @@ struct DiagRing {
         const double dV = c.dV, idx1 = c.idx1;
         double* S = acc.S;
         double* M = acc.M;
+        double mu_[12];   // matter momenta at this site, loaded first (latency under the stencil)
+#pragma unroll
+        for (int f = 0; f < 12; f++) mu_[f] = A.mom[f * N3 + idx];
         double fu[6], fv[6];
 #pragma unroll
         for (int a = 0; a < 3; a++) {
@@ -71,9 +74,6 @@ struct DiagRing {
                 }
             }
         }
-        double mu_[12];   // matter momenta at this site
-#pragma unroll
-        for (int f = 0; f < 12; f++) mu_[f] = A.mom[f * N3 + idx];
         double s2[3];
 #pragma unroll
         for (int a = 0; a < 3; a++) {

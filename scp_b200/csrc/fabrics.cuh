@@ -75,6 +75,15 @@ struct FabricPass {
                                 bool first_plane) {
         const FabConsts &c = A.c;
         const long long N3 = c.N3;
+        // the momenta and the accumulated currents are loaded first, so their
+        // latency passes under the stencil instead of stalling the kicks
+        double wv[12], kin[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int f = 0; f < 12; f++) wv[f] = A.win[f * N3 + idx];
+        if (A.accumulate) {
+#pragma unroll
+            for (int d = 0; d < 3; d++) kin[d] = A.kacc[d * N3 + idx];
+        }
         double own[12];
 #pragma unroll
         for (int f = 0; f < 12; f++) own[f] = v(f);
@@ -128,17 +137,14 @@ struct FabricPass {
             acc[MTV + a] = (o.lsum[MTV + a] - 6.0 * tw) * c.idx2 - c.mtheta2 * tw + c.eta * o.curlP[3 + a];
         }
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            double *kp = A.kacc + d * N3 + idx;
-            *kp = A.accumulate ? *kp + kc[d] : kc[d];
-        }
+        for (int d = 0; d < 3; d++) A.kacc[d * N3 + idx] = A.accumulate ? kin[d] + kc[d] : kc[d];
         const Leap leap{c.hdt, c.dt, A.first != 0};
         const double dmp = (A.damp && !A.first) ? sponge_at(i, j, k, c.L, c.dx, c.damp_width, c.damp_rate) : 1.0;
         bool bad = false;
 #pragma unroll
         for (int f = 0; f < 12; f++) {
             double vv, wn;
-            leap(A.win[f * N3 + idx], acc[f], dmp, &vv, &wn);
+            leap(wv[f], acc[f], dmp, &vv, &wn);
             const double x = own[f] + c.dt * wn;
             st_cs(A.xout + f * N3 + idx, x);
             A.wout[f * N3 + idx] = wn;
@@ -185,6 +191,13 @@ struct LinkPass {
                                 bool first_plane) {
         const FabConsts &c = A.c;
         const long long N3 = c.N3;
+        // E and the accumulated currents first: their latency passes under the staples
+        double wv[3], kin[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            wv[d] = A.win[d * N3 + idx];
+            kin[d] = A.kacc[d * N3 + idx];
+        }
         if (first_plane) {
             cy.pm[0] = plaquette_sin(v, 0, 0, -1, 0, 0);
             cy.pm[1] = plaquette_sin(v, 0, 2, -1, 0, 0);
@@ -198,9 +211,9 @@ struct LinkPass {
         bool bad = false;
 #pragma unroll
         for (int d = 0; d < 3; d++) {
-            const double K = c.stp * st[d] + A.kacc[d * N3 + idx];
+            const double K = c.stp * st[d] + kin[d];
             double E, Eh;
-            leap(A.win[d * N3 + idx], K, dmp, &E, &Eh);
+            leap(wv[d], K, dmp, &E, &Eh);
             const double th = wrap_angle(v(d) + c.gad * Eh);
             st_cs(A.xout + d * N3 + idx, th);
             A.wout[d * N3 + idx] = Eh;

@@ -73,6 +73,11 @@ struct HiggsU1 {
                                 bool first_plane) {
         const HuConsts &c = A.c;
         const long long N3 = c.N3;
+        // the matter momenta are loaded first, so their latency passes under
+        // the stencil instead of stalling the kicks
+        double wv[15];
+#pragma unroll
+        for (int f = 0; f < 15; f++) wv[f] = A.win[f * N3 + idx];
         double own[12];
 #pragma unroll
         for (int f = 0; f < 12; f++) own[f] = v(f);
@@ -191,13 +196,13 @@ struct HiggsU1 {
 #pragma unroll
         for (int f = 0; f < 12; f++) {
             double vv, wn;
-            leap(A.win[f * N3 + idx], acc[f], dmp, &vv, &wn);
+            leap(wv[f], acc[f], dmp, &vv, &wn);
             put(f, own[f] + c.dt * wn, vv, wn);
         }
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             double E, Eh;
-            leap(A.win[(TH + d) * N3 + idx], K[d], dmp, &E, &Eh);
+            leap(wv[TH + d], K[d], dmp, &E, &Eh);
             put(TH + d, wrap_angle(v(TH + d) + c.gad * Eh), E, Eh);
         }
         if (G2) {

@@ -106,6 +106,10 @@ struct R6Step {
     __device__ static void site(const Args &A, const V &v, int i, int j, int k, long long idx, Carry &, bool) {
         const R6Consts &c = A.c;
         const long long N3 = c.N3;
+        // momenta first: their latency passes under the stencil
+        double wv[6];
+#pragma unroll
+        for (int f = 0; f < 6; f++) wv[f] = A.win[f * N3 + idx];
         const double p[3] = {v(0), v(1), v(2)}, t[3] = {v(3), v(4), v(5)};
         const double sig = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
         const double m2e = (c.mode == 1) ? c.ia / (1.0 + c.ib * sig) : c.m2;
@@ -166,7 +170,7 @@ struct R6Step {
 #pragma unroll
         for (int f = 0; f < 6; f++) {
             double vv, wn;
-            leap(A.win[f * N3 + idx], acc[f], dmp, &vv, &wn);
+            leap(wv[f], acc[f], dmp, &vv, &wn);
             const double x = (f < 3 ? p[f] : t[f - 3]) + c.dt * wn;
             st_cs(A.xout + f * N3 + idx, x);
             A.wout[f * N3 + idx] = wn;
