@@ -75,9 +75,9 @@ struct HiggsU1 {
         const long long N3 = c.N3;
         // the matter momenta are loaded first, so their latency passes under
         // the stencil instead of stalling the kicks
-        double wv[15];
+        double wv[NR];
 #pragma unroll
-        for (int f = 0; f < 15; f++) wv[f] = A.win[f * N3 + idx];
+        for (int f = 0; f < NR; f++) wv[f] = A.win[f * N3 + idx];
         double own[12];
 #pragma unroll
         for (int f = 0; f < 12; f++) own[f] = v(f);
@@ -209,13 +209,13 @@ struct HiggsU1 {
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 double E2, E2h;
-                leap(A.win[(TH2 + d) * N3 + idx], K2[d], 1.0, &E2, &E2h);
+                leap(wv[TH2 + d], K2[d], 1.0, &E2, &E2h);
                 put(TH2 + d, wrap_angle(v(TH2 + d) + c.gad2 * E2h), E2, E2h);
             }
         }
         if (HIGGS) {
             double hd, hdh;
-            leap(A.win[HF * N3 + idx], accH, 1.0, &hd, &hdh);
+            leap(wv[HF], accH, 1.0, &hd, &hdh);
             put(HF, h + c.dt * hdh, hd, hdh);
         }
         if (A.sync && bad) atomicOr(A.flag, 1);

@@ -1,5 +1,7 @@
 // kern_ext.cu -- instantiations and launchers of the extension steppers'
 // ring kernels (Higgs condensate / second gauge, three fabrics).
+#include <stdlib.h>
+
 #include "diag_ring.cuh"
 #include "ext_launch.cuh"
 #include "fabrics.cuh"
@@ -9,6 +11,16 @@
 namespace scp {
 
 namespace {
+
+// L2 prefetch of the next plane's momenta in the ring kernels: on unless
+// SCP_RING_PREFETCH=0 in the environment (read once)
+int ring_prefetch() {
+    static const int on = [] {
+        const char *e = getenv("SCP_RING_PREFETCH");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on;
+}
 
 // Tile of a ring model: 128 threads, so that two CTAs share an SM and one
 // CTA's plane barrier overlaps the other's work; 32 x 4 while the 4-slot ring
@@ -42,6 +54,7 @@ cudaError_t hu_launch(const ExtPlan &p, const HuConsts &c, const HuIO &io, cudaS
     typename M::Args a;
     const long long n3 = c.N3;
     for (int f = 0; f < M::NR; f++) a.src.f[f] = io.x + f * n3;
+    a.src.prefetch = ring_prefetch();
     a.N = c.N;
     a.c = c;
     a.win = io.win;
@@ -84,6 +97,7 @@ cudaError_t fabric_launch(const ExtPlan &p, const FabConsts &c, const FabIO &io,
     const long long n3 = c.N3;
     for (int f = 0; f < 12; f++) a.src.f[f] = io.x + f * n3;
     for (int d = 0; d < 3; d++) a.src.f[M::TH + d] = io.th + d * n3;
+    a.src.prefetch = ring_prefetch();
     a.N = c.N;
     a.c = c;
     a.qf = io.qf;
@@ -113,6 +127,7 @@ cudaError_t link_step(const ExtPlan &p, const FabConsts &c, const LinkIO &io, cu
     LinkPass::Args a;
     const long long n3 = c.N3;
     for (int d = 0; d < 3; d++) a.src.f[d] = io.th + d * n3;
+    a.src.prefetch = ring_prefetch();
     a.N = c.N;
     a.c = c;
     a.kacc = io.kacc;

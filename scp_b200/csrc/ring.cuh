@@ -29,6 +29,7 @@ namespace scp {
 template <int NR>
 struct RingSrc {
     const double *f[NR];
+    int prefetch = 1;   // 0: no L2 prefetch of the next plane's momenta
 };
 
 template <int NR, int TX, int TY>
@@ -120,7 +121,7 @@ __device__ __forceinline__ void ring_item(const typename M::Args &a, const Piece
             v.m = ring + (q & 3) * S::SLOT + own_s;
             v.c = ring + ((q + 1) & 3) * S::SLOT + own_s;
             v.p = ring + ((q + 2) & 3) * S::SLOT + own_s;
-            if (i + 1 < i1) M::prefetch(a, (long long)(i + 1) * NN + own_g);
+            if (a.src.prefetch && i + 1 < i1) M::prefetch(a, (long long)(i + 1) * NN + own_g);
             M::site(a, v, i, j, k, (long long)i * NN + own_g, carry, q == 0, extra...);
         }
     }
