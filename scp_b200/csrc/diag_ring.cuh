@@ -28,15 +28,17 @@ struct DiagRing {
         DiagConsts c;
         const double *mom;   // the 12 matter momenta (N^3 arrays)
     };
-    struct Carry {};
+    struct Carry {
+        double cm0, sm0;   // cos / sin of link 0 at x - i (gauged)
+    };
     __device__ static void prefetch(const Args &A, long long idx) {
 #pragma unroll
         for (int f = 0; f < 12; f++) prefetch_l2(A.mom + f * A.c.N3 + idx);
     }
 
     template <class V>
-    __device__ static void site(const Args &A, const V &v, int i, int j, int k, long long idx, Carry &, bool,
-                                DiagSums &acc) {
+    __device__ static void site(const Args &A, const V &v, int i, int j, int k, long long idx, Carry &cy,
+                                bool first_plane, DiagSums &acc) {
         const DiagConsts &c = A.c;
         const long long N3 = c.N3;
         const double dV = c.dV, idx1 = c.idx1;
@@ -51,29 +53,54 @@ struct DiagRing {
             fu[a] = v(FU + a); fv[a] = v(FV + a);
             fu[3 + a] = v(FTU + a); fv[3 + a] = v(FTV + a);
         }
-        // central differences, transported by the links when gauged
-        double DR[3][6], DI[3][6];
+        // central differences, transported by the links when gauged, summed
+        // into the gradient energies as the directions come in; the curl of
+        // Theta (D_{a+1} Theta_{a+2} - D_{a+2} Theta_{a+1}) is built the same way
+        double eg = 0.0, etg = 0.0, cr[3], ci[3];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
             double cP = 1.0, sP = 0.0, cM = 1.0, sM = 0.0;
             if (GAUGED) {
                 sincos_any(v(TH + d), &sP, &cP);
-                sincos_any(nb(v, TH + d, d, -1), &sM, &cM);
+                if (d == 0) {   // link 0 at x - i: this thread's value from the previous plane
+                    if (first_plane) sincos_any(nb(v, TH, 0, -1), &cy.sm0, &cy.cm0);
+                    sM = cy.sm0; cM = cy.cm0;
+                    cy.sm0 = sP; cy.cm0 = cP;
+                } else {
+                    sincos_any(nb(v, TH + d, d, -1), &sM, &cM);
+                }
             }
 #pragma unroll
             for (int q = 0; q < 6; q++) {
                 const int fre = q < 3 ? FU + q : FTU + q - 3, fim = q < 3 ? FV + q : FTV + q - 3;
                 const double up = nb(v, fre, d, 1), vp = nb(v, fim, d, 1);
                 const double um = nb(v, fre, d, -1), vm = nb(v, fim, d, -1);
+                double DR, DI;
                 if (GAUGED) {
-                    DR[d][q] = ((cP * up - sP * vp) - (cM * um + sM * vm)) * idx1;
-                    DI[d][q] = ((cP * vp + sP * up) - (cM * vm - sM * um)) * idx1;
+                    DR = ((cP * up - sP * vp) - (cM * um + sM * vm)) * idx1;
+                    DI = ((cP * vp + sP * up) - (cM * vm - sM * um)) * idx1;
                 } else {
-                    DR[d][q] = (up - um) * idx1;
-                    DI[d][q] = (vp - vm) * idx1;
+                    DR = (up - um) * idx1;
+                    DI = (vp - vm) * idx1;
+                }
+                if (q < 3) eg += DR * DR + DI * DI;
+                else etg += DR * DR + DI * DI;
+                const int qa = q - 3;
+                if (GAUGED && q >= 3 && qa != d) {
+                    if (qa == (d + 1) % 3) {            // plus term of component a = d + 2
+                        const int a = (d + 2) % 3;
+                        if (d < (a + 2) % 3) { cr[a] = DR; ci[a] = DI; }
+                        else { cr[a] = DR - cr[a]; ci[a] = DI - ci[a]; }
+                    } else {                            // minus term of component a = d + 1
+                        const int a = (d + 1) % 3;
+                        if (d < (a + 1) % 3) { cr[a] = DR; ci[a] = DI; }
+                        else { cr[a] = cr[a] - DR; ci[a] = ci[a] - DI; }
+                    }
                 }
             }
         }
+        S[DS_EG] += 0.5 * eg * dV;
+        S[DS_ETG] += 0.5 * etg * dV;
         double s2[3];
 #pragma unroll
         for (int a = 0; a < 3; a++) {
@@ -81,26 +108,16 @@ struct DiagRing {
             const double pu = mu_[FU + a], pv = mu_[FV + a], ptu = mu_[FTU + a], ptv = mu_[FTV + a];
             S[DS_EPK] += 0.5 * (pu * pu + pv * pv) * dV;
             S[DS_ETK] += 0.5 * (ptu * ptu + ptv * ptv) * dV;
-            S[DS_EG] += 0.5 * (DR[0][a] * DR[0][a] + DR[1][a] * DR[1][a] + DR[2][a] * DR[2][a] +
-                               DI[0][a] * DI[0][a] + DI[1][a] * DI[1][a] + DI[2][a] * DI[2][a]) * dV;
             S[DS_EM] += 0.5 * c.m2 * s2[a] * dV;
-            S[DS_ETG] += 0.5 * (DR[0][3 + a] * DR[0][3 + a] + DR[1][3 + a] * DR[1][3 + a] +
-                                DR[2][3 + a] * DR[2][3 + a] + DI[0][3 + a] * DI[0][3 + a] +
-                                DI[1][3 + a] * DI[1][3 + a] + DI[2][3 + a] * DI[2][3 + a]) * dV;
             S[DS_ETM] += 0.5 * c.mtheta2 * (fu[3 + a] * fu[3 + a] + fv[3 + a] * fv[3 + a]) * dV;
             M[DM_PM] = fmax(M[DM_PM], sqrt(s2[a]));
-            // curl of Theta: D_{a+1} Theta_{a+2} - D_{a+2} Theta_{a+1}
-            const int d1 = (a + 1) % 3, d2 = (a + 2) % 3;
-            double cr, ci;
-            if (GAUGED) {
-                cr = DR[d1][3 + d2] - DR[d2][3 + d1];
-                ci = DI[d1][3 + d2] - DI[d2][3 + d1];
-            } else {
+            if (!GAUGED) {   // curl_component of theta (scp_sim.c:409-415, :1868-1870)
+                const int d1 = (a + 1) % 3, d2 = (a + 2) % 3;
                 const int fa = FTU + d2, fb = FTU + d1, ga = FTV + d2, gb = FTV + d1;
-                cr = (nb(v, fa, d1, 1) - nb(v, fa, d1, -1) - nb(v, fb, d2, 1) + nb(v, fb, d2, -1)) * idx1;
-                ci = (nb(v, ga, d1, 1) - nb(v, ga, d1, -1) - nb(v, gb, d2, 1) + nb(v, gb, d2, -1)) * idx1;
+                cr[a] = (nb(v, fa, d1, 1) - nb(v, fa, d1, -1) - nb(v, fb, d2, 1) + nb(v, fb, d2, -1)) * idx1;
+                ci[a] = (nb(v, ga, d1, 1) - nb(v, ga, d1, -1) - nb(v, gb, d2, 1) + nb(v, gb, d2, -1)) * idx1;
             }
-            S[DS_EC] -= c.eta * (fu[a] * cr + fv[a] * ci) * dV;
+            S[DS_EC] -= c.eta * (fu[a] * cr[a] + fv[a] * ci[a]) * dV;
         }
         const double s = s2[0] * s2[1] * s2[2];
         S[DS_EP] += (c.mu / 2.0) * s / (1.0 + c.kappa * s) * dV;

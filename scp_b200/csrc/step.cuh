@@ -40,6 +40,8 @@
 #pragma once
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "diag.cuh"
 #include "trig.cuh"
@@ -211,6 +213,95 @@ struct CpStage {
 // One work item (a TX x TY column over one segment of planes) of one grid.
 // sync and damp are uniform per call; the single-grid kernel passes them as
 // constants, the multi-request kernel per request.  Stage stages the planes.
+// Per-site gradient, coupling and plaquette terms of the gauged diagnostics
+// (the energy's covariant gradients, eta (Phi . curl Theta), 1 - cos of the
+// three plaquettes; compute_energy_complex_gauge, sfa/sim/scp_sim.c:1930-2036)
+// for a synchronous FP64 launch that sums the first diagnostics pass: the
+// covariant differences are formed again from the ring (planes i, i+1) and
+// the thread's x(i-1).  Every input passes through an opaque copy first, so
+// that none of this arithmetic can merge with the force's (which would change
+// how the force's multiply-adds are fused): the launch advances the state bit
+// for bit as one that sums nothing.
+struct DiagGrad {
+    double eg, etg, ec, bb;
+};
+struct Plane12 {
+    double v[12];
+};
+
+__device__ __forceinline__ double opaque(double x) {
+    asm volatile("" : "+d"(x));
+    return x;
+}
+
+template <int TX, int TY>
+__device__ __forceinline__ DiagGrad diag_grad_gauged(const double *xs, int sc, int sp, int r, int col,
+                                                     const Plane12 &xm_in, double c0m_in, double s0m_in,
+                                                     double idx1_in) {
+    constexpr int NR = 15, PX = TX + 2, PY = TY + 2;
+    auto X = [&](int slot, int f, int rr, int cc) -> double {
+        return opaque(xs[((slot * NR + f) * PY + rr) * PX + cc]);
+    };
+    Plane12 xm;
+#pragma unroll
+    for (int f = 0; f < 12; f++) xm.v[f] = opaque(xm_in.v[f]);
+    const double c0m = opaque(c0m_in), s0m = opaque(s0m_in), idx1 = opaque(idx1_in);
+    DiagGrad o{0.0, 0.0, 0.0, 0.0};
+    double cr[3], ci[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        double cP, sP, cM, sM;
+        sincos_bounded(X(sc, FTH + d, r, col), &sP, &cP);
+        if (d == 0) { cM = c0m; sM = s0m; }
+        else if (d == 1) sincos_bounded(X(sc, FTH + 1, r - 1, col), &sM, &cM);
+        else sincos_bounded(X(sc, FTH + 2, r, col - 1), &sM, &cM);
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            const int fre = q < 3 ? FU + q : FTU + q - 3, fim = q < 3 ? FV + q : FTV + q - 3;
+            double up, vp, um, vm;
+            if (d == 0) {
+                up = X(sp, fre, r, col); vp = X(sp, fim, r, col);
+                um = xm.v[fre]; vm = xm.v[fim];
+            } else if (d == 1) {
+                up = X(sc, fre, r + 1, col); vp = X(sc, fim, r + 1, col);
+                um = X(sc, fre, r - 1, col); vm = X(sc, fim, r - 1, col);
+            } else {
+                up = X(sc, fre, r, col + 1); vp = X(sc, fim, r, col + 1);
+                um = X(sc, fre, r, col - 1); vm = X(sc, fim, r, col - 1);
+            }
+            const double DR = ((cP * up - sP * vp) - (cM * um + sM * vm)) * idx1;
+            const double DI = ((cP * vp + sP * up) - (cM * vm - sM * um)) * idx1;
+            if (q < 3) o.eg += DR * DR + DI * DI;
+            else o.etg += DR * DR + DI * DI;
+            const int qa = q - 3;
+            if (q >= 3 && qa != d) {   // curl of Theta: D_{a+1} Theta_{a+2} - D_{a+2} Theta_{a+1}
+                if (qa == (d + 1) % 3) {
+                    const int a = (d + 2) % 3;
+                    if (d < (a + 2) % 3) { cr[a] = DR; ci[a] = DI; }
+                    else { cr[a] = DR - cr[a]; ci[a] = DI - ci[a]; }
+                } else {
+                    const int a = (d + 1) % 3;
+                    if (d < (a + 1) % 3) { cr[a] = DR; ci[a] = DI; }
+                    else { cr[a] = cr[a] - DR; ci[a] = ci[a] - DI; }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++) o.ec += X(sc, FU + a, r, col) * cr[a] + X(sc, FV + a, r, col) * ci[a];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {   // plaquette (q, q+1) at x, the next plane in slot sp
+        const int a = q, b = (q + 1) % 3;
+        const int sa = (a == 0) ? sp : sc, ra = r + (a == 1 ? 1 : 0), ca = col + (a == 2 ? 1 : 0);
+        const int sb = (b == 0) ? sp : sc, rb = r + (b == 1 ? 1 : 0), cb = col + (b == 2 ? 1 : 0);
+        double sn, cs;
+        sincos_any(X(sc, FTH + a, r, col) + X(sa, FTH + b, ra, ca) - X(sb, FTH + a, rb, cb) - X(sc, FTH + b, r, col),
+                   &sn, &cs);
+        o.bb += 1.0 - cs;
+    }
+    return o;
+}
+
 // dsum (FP64 SYNC launches only): per-thread sums of the first diagnostics
 // pass over this item's sites, the per-site terms of diag_ring.cuh / diag.cuh
 // (compute_energy_complex[_gauge], compute_charges, sfa/sim/scp_sim.c:1823-2169)
@@ -246,13 +337,6 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
         // sine of the plaquette angle th_a(y) + th_b(y+a) - th_a(y+b) - th_b(y) of plane
         // (a,b) = (0,1) (1,2) (2,0) [q = 0, 1, 2] at ring position (r, col) of slot sc,
         // the next plane in slot sp (compute_forces_complex_gauge pass B, scp_sim.c:1090-1109)
-        // the F64 plaquette angle itself (diagnostics: its cosine)
-        auto plaq_angle = [&](int q, int sc, int sp, int r, int col) -> double {
-            const int a = q, b = (q + 1) % 3;
-            const int sa = (a == 0) ? sp : sc, ra = r + (a == 1 ? 1 : 0), ca = col + (a == 2 ? 1 : 0);
-            const int sb = (b == 0) ? sp : sc, rb = r + (b == 1 ? 1 : 0), cb = col + (b == 2 ? 1 : 0);
-            return XS(sc, FTH + a, r, col) + XS(sa, FTH + b, ra, ca) - XS(sb, FTH + a, rb, cb) - XS(sc, FTH + b, r, col);
-        };
         auto plaq_sin = [&](int q, int sc, int sp, int r, int col) -> T {
             const int a = q, b = (q + 1) % 3;
             // th_b(y+a): the next plane for a = 0, else the neighbour row (a = 1) or column (a = 2)
@@ -342,7 +426,7 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             const T Vp = T(0.5) * (T)c.mu / (den * den);
             const T rest[3] = {s1 * s2, s0 * s2, s0 * s1};
             const T m2 = (T)c.m2, mt2 = (T)c.mtheta2, eta = (T)c.eta;
-            double bbE = 0.0;   // diagnostics: sum of 1 - cos of this site's three plaquettes
+            const double c0d = (double)c0m, s0d = (double)s0m;   // link 0 at x - i (diagnostics)
 
             if (!GAUGED) {
                 // compute_forces_complex, scp_sim.c:931-994
@@ -389,10 +473,12 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
 #pragma unroll
                             for (int q = 0; q < 6; q++) {
                                 const int fre = q < 3 ? FU + q : FTU + q - 3, fim = q < 3 ? FV + q : FTV + q - 3;
-                                const double DR = (nb(fre, 2 * d) - nb(fre, 2 * d + 1)) * idx1;
-                                const double DI = (nb(fim, 2 * d) - nb(fim, 2 * d + 1)) * idx1;
-                                if (q < 3) eg += DR * DR + DI * DI;
-                                else etg += DR * DR + DI * DI;
+                                // rounded products of their own (the step's fused ones stay as they are)
+                                const double DR = __dmul_rn(nb(fre, 2 * d) - nb(fre, 2 * d + 1), idx1);
+                                const double DI = __dmul_rn(nb(fim, 2 * d) - nb(fim, 2 * d + 1), idx1);
+                                const double e2 = __fma_rn(DR, DR, __dmul_rn(DI, DI));
+                                if (q < 3) eg += e2;
+                                else etg += e2;
                             }
                         }
                         dsum->S[DS_EG] += 0.5 * eg * c.dV;
@@ -413,7 +499,6 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 // central differences D = (transported(x+d) - transported(x-d))/(2dx);
                 // one subtraction either way round, as the reference forms it
                 T crT[3], ciT[3], crP[3], ciP[3];
-                double egP = 0.0, egT = 0.0;   // diagnostics: squared covariant differences
 #pragma unroll
                 for (int d = 0; d < 3; d++) {
                     // link d at x (pass A, scp_sim.c:1072-1079) and at x - d
@@ -441,13 +526,6 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                         }
                         const T TRp = cP * up - sP * vp, TIp = cP * vp + sP * up;
                         const T TRm = cM * um + sM * vm, TIm = cM * vm - sM * um;
-                        if constexpr (!P::COMP) {
-                            if (DG) {
-                                const double DRe = (TRp - TRm) * idx1, DIe = (TIp - TIm) * idx1;
-                                if (q < 3) egP += DRe * DRe + DIe * DIe;
-                                else egT += DRe * DRe + DIe * DIe;
-                            }
-                        }
                         if constexpr (P::COMP) {   // accumulate (transported - centre) differences
                             const T cu = fu[q], cv = fv[q];
                             if (d == 0) { lapU[q] = (TRp - cu) + (TRm - cu); lapV[q] = (TIp - cv) + (TIm - cv); }
@@ -508,20 +586,6 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 const T st1 = -(P0 - P0m) + (P1 - P1km);
                 const T st2 = (P2 - P2m) - (P1 - P1jm);
                 P0m = P0; P2m = P2;   // x - i of the next plane
-                if constexpr (!P::COMP) {
-                    if (DG) {
-                        dsum->S[DS_EG] += 0.5 * egP * c.dV;
-                        dsum->S[DS_ETG] += 0.5 * egT * c.dV;
-#pragma unroll
-                        for (int a = 0; a < 3; a++) dsum->S[DS_EC] -= c.eta * (fu[a] * crT[a] + fv[a] * ciT[a]) * c.dV;
-                        double sn, cs;
-#pragma unroll
-                        for (int q = 0; q < 3; q++) {
-                            sincos_any(plaq_angle(q, sc, sp, ty + 1, tx + 1), &sn, &cs);
-                            bbE += 1.0 - cs;
-                        }
-                    }
-                }
                 const T stp = (T)c.stp, gg = (T)c.g;
                 K[0] = stp * st0 + gg * K[0];
                 K[1] = stp * st1 + gg * K[1];
@@ -627,18 +691,22 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             if (SYNC && bad) atomicOr(io.flag, 1);
             if constexpr (!P::COMP) {
                 if (DG) {   // energies, charges, core and centroid moments at (x_{n+1}, v_{n+1})
+                    // squares of the positions by rounded products of their own, so
+                    // that they do not merge with the force's (whose fused
+                    // multiply-adds would then change): the step's arithmetic is the
+                    // same with and without these sums
                     double *S = dsum->S, *M = dsum->M;
                     const double dV = c.dV;
                     double s2[3];
 #pragma unroll
                     for (int a = 0; a < 3; a++) {
                         const double u = ctr[FU + a], w0 = ctr[FV + a], tu = ctr[FTU + a], tv = ctr[FTV + a];
-                        s2[a] = u * u + w0 * w0;
+                        s2[a] = __fma_rn(u, u, __dmul_rn(w0, w0));
                         const double pu = vv[FU + a], pv = vv[FV + a], ptu = vv[FTU + a], ptv = vv[FTV + a];
                         S[DS_EPK] += 0.5 * (pu * pu + pv * pv) * dV;
                         S[DS_ETK] += 0.5 * (ptu * ptu + ptv * ptv) * dV;
                         S[DS_EM] += 0.5 * c.m2 * s2[a] * dV;
-                        S[DS_ETM] += 0.5 * c.mtheta2 * (tu * tu + tv * tv) * dV;
+                        S[DS_ETM] += 0.5 * c.mtheta2 * __fma_rn(tu, tu, __dmul_rn(tv, tv)) * dV;
                         M[DM_PM] = fmax(M[DM_PM], sqrt(s2[a]));
                     }
                     const double s3 = s2[0] * s2[1] * s2[2];
@@ -646,7 +714,8 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                     M[DM_PMAX] = fmax(M[DM_PMAX], sqrt(s3));
                     S[DS_PINT] += sqrt(s3) * dV;
 #pragma unroll
-                    for (int a = 0; a < 3; a++) S[DS_TRS] += ctr[FTU + a] * ctr[FTU + a] + ctr[FTV + a] * ctr[FTV + a];
+                    for (int a = 0; a < 3; a++)
+                        S[DS_TRS] += __fma_rn(ctr[FTU + a], ctr[FTU + a], __dmul_rn(ctr[FTV + a], ctr[FTV + a]));
                     const double x = -c.L + i * c.dx, y = -c.L + j * c.dx, z = -c.L + k * c.dx;
                     double rho2 = 0.0, qp = 0.0, qt = 0.0, sprod = 1.0;
 #pragma unroll
@@ -655,7 +724,7 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                         qp += qa;
                         S[DS_QP0 + a] += qa;
                         qt += ctr[FTU + a] * vv[FTV + a] - ctr[FTV + a] * vv[FTU + a];
-                        const double s2a = ctr[FU + a] * ctr[FU + a] + ctr[FV + a] * ctr[FV + a];
+                        const double s2a = s2[a];
                         rho2 += s2a;
                         sprod *= s2a;
                     }
@@ -667,7 +736,17 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                     S[DS_CX] += x * rho2;
                     S[DS_CY] += y * rho2;
                     S[DS_CZ] += z * rho2;
-                    if (GAUGED) {   // charge density of the Gauss law; E_em
+                    if constexpr (GAUGED && std::is_same<Stage, CpStage<P, TX, TY, GAUGED>>::value) {
+                        // gradient, coupling and plaquette energies; Gauss charge density; E_em
+                        Plane12 xp;
+#pragma unroll
+                        for (int f = 0; f < 12; f++) xp.v[f] = (double)xm[f];
+                        const DiagGrad gr = diag_grad_gauged<TX, TY>(stg.xs, sc, sp, ty + 1, tx + 1, xp, c0d, s0d,
+                                                                     c.idx1);
+                        S[DS_EG] += 0.5 * gr.eg * dV;
+                        S[DS_ETG] += 0.5 * gr.etg * dV;
+                        S[DS_EC] -= c.eta * gr.ec * dV;
+                        const double bbE = gr.bb;
                         double rho = 0.0;
 #pragma unroll
                         for (int a = 0; a < 3; a++)

@@ -74,3 +74,28 @@ def test_fused_diag_matches_oracle(gpu):
             for q in range(31):
                 tol = 1e-9 * max(abs(r[q]), 1.0) if q in _CANCELLING else 1e-11 * max(abs(r[q]), 1e-300)
                 assert abs(g[q] - r[q]) <= tol, (n, q, g[q], r[q])
+
+
+@pytest.mark.parametrize("gauged", [True, False])
+def test_fused_diag_leaves_the_state_unchanged(gpu, gauged):
+    """The synchronous launch that sums the diagnostics advances the state
+    bit for bit as the one that does not, so a run does not depend on its
+    diagnostics cadence."""
+    st = seeds.small_state(32, gauged, seed=9)
+    out = {}
+    for fused in (True, False):
+        old = os.environ.get("SCP_FUSED_DIAG")
+        os.environ["SCP_FUSED_DIAG"] = "1" if fused else "0"
+        try:
+            with Simulation(st.params, st.cols()) as sim:
+                for n in (1, 4, 6):
+                    sim.step(n)
+                    sim.diag_vector()
+                out[fused] = sim.snapshot()
+        finally:
+            if old is None:
+                del os.environ["SCP_FUSED_DIAG"]
+            else:
+                os.environ["SCP_FUSED_DIAG"] = old
+    for a, b in zip(out[True], out[False]):
+        assert np.array_equal(a, b)

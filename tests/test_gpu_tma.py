@@ -52,8 +52,10 @@ def test_tma_staging_matches_cp_ring(gpu, N, gauged, tile, over):
     for x, y, z in zip(a, m, b):
         assert np.array_equal(x, z)
         assert np.array_equal(y, z)
-    assert np.array_equal(da, db)
-    assert np.array_equal(dm, db)
+    # the TMA forms take the separate diagnostics pass; the cp.async ring's
+    # synchronous launch sums the same terms itself, in another order
+    assert np.allclose(da, db, rtol=1e-11, atol=1e-9)
+    assert np.array_equal(dm, da)
 
 
 def test_staging_default_is_the_cp_ring(gpu):
