@@ -16,13 +16,19 @@ size_t smem_one(bool g) {
     return g ? StepLayout<P, TX, TY, true>::smem_bytes : StepLayout<P, TX, TY, false>::smem_bytes;
 }
 
+// the synchronous FP64 launches also hold the diagnostics sums (DiagSmem)
+template <class P, int TX, int TY>
+size_t smem_variant(bool g, bool f, bool s) {
+    return smem_one<P, TX, TY>(g) + ((s && !f && !P::COMP) ? DiagSmem::bytes(TX * TY) : 0);
+}
+
 template <class P>
 StepFnT<P> select_one(int shape, bool g, bool f, bool s, bool d, size_t *smem) {
     switch (shape) {
-        case 2: *smem = smem_one<P, 32, 8>(g); return pick_one<P, 32, 8>(g, f, s, d);
-        case 3: *smem = smem_one<P, 16, 8>(g); return pick_one<P, 16, 8>(g, f, s, d);
-        case 4: *smem = smem_one<P, 64, 2>(g); return pick_one<P, 64, 2>(g, f, s, d);
-        default: *smem = smem_one<P, 32, 4>(g); return pick_one<P, 32, 4>(g, f, s, d);
+        case 2: *smem = smem_variant<P, 32, 8>(g, f, s); return pick_one<P, 32, 8>(g, f, s, d);
+        case 3: *smem = smem_variant<P, 16, 8>(g, f, s); return pick_one<P, 16, 8>(g, f, s, d);
+        case 4: *smem = smem_variant<P, 64, 2>(g, f, s); return pick_one<P, 64, 2>(g, f, s, d);
+        default: *smem = smem_variant<P, 32, 4>(g, f, s); return pick_one<P, 32, 4>(g, f, s, d);
     }
 }
 

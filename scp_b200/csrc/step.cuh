@@ -230,7 +230,7 @@ struct Plane12 {
 };
 
 __device__ __forceinline__ double opaque(double x) {
-    asm volatile("" : "+d"(x));
+    asm("" : "+d"(x));
     return x;
 }
 
@@ -302,6 +302,22 @@ __device__ __forceinline__ DiagGrad diag_grad_gauged(const double *xs, int sc, i
     return o;
 }
 
+// Per-thread sums and maxima of the first diagnostics pass kept in shared
+// memory (slot q of thread t at q * NT + t), so that the synchronous launch
+// that sums them keeps its registers for the force.
+struct DiagSmem {
+    double *base;
+    int nt;
+    struct Ref {
+        double *p;
+        int nt;
+        __device__ __forceinline__ double &operator[](int q) const { return p[q * nt]; }
+    };
+    __device__ __forceinline__ Ref S() const { return Ref{base + threadIdx.x, nt}; }
+    __device__ __forceinline__ Ref M() const { return Ref{base + DS_NSUM * nt + threadIdx.x, nt}; }
+    static constexpr size_t bytes(int nt) { return sizeof(double) * kDiag1Q * (size_t)nt; }
+};
+
 // dsum (FP64 SYNC launches only): per-thread sums of the first diagnostics
 // pass over this item's sites, the per-site terms of diag_ring.cuh / diag.cuh
 // (compute_energy_complex[_gauge], compute_charges, sfa/sim/scp_sim.c:1823-2169)
@@ -309,7 +325,7 @@ __device__ __forceinline__ DiagGrad diag_grad_gauged(const double *xs, int sc, i
 // a pass that reads E of the neighbouring sites.
 template <class P, int TX, int TY, bool GAUGED, bool FIRST, class Stage>
 __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts &c, const Piece &pc,
-                                          const bool SYNC, const bool DAMP, Stage &stg, DiagSums *dsum = nullptr) {
+                                          const bool SYNC, const bool DAMP, Stage &stg, const DiagSmem *dsum = nullptr) {
     const bool DG = !P::COMP && dsum != nullptr;
     using T = typename P::T;
     using LY = StepLayout<P, TX, TY, GAUGED>;
@@ -411,6 +427,18 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                 }
             }
             if (!act) continue;
+            // diagnostics: gradient, coupling and plaquette terms, formed before the
+            // force while few of its values are live (link 0 at x - i is still the carry)
+            DiagGrad gr{0.0, 0.0, 0.0, 0.0};
+            if constexpr (!P::COMP && GAUGED && std::is_same<Stage, CpStage<P, TX, TY, GAUGED>>::value) {
+                if (DG) {
+                    Plane12 xp;
+#pragma unroll
+                    for (int f = 0; f < 12; f++) xp.v[f] = (double)xm[f];
+                    gr = diag_grad_gauged<TX, TY>(stg.xs, sc, sp, ty + 1, tx + 1, xp, (double)c0m, (double)s0m,
+                                                  c.idx1);
+                }
+            }
 
             T acc[12];
             T K[3] = {T(0), T(0), T(0)};
@@ -426,7 +454,6 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
             const T Vp = T(0.5) * (T)c.mu / (den * den);
             const T rest[3] = {s1 * s2, s0 * s2, s0 * s1};
             const T m2 = (T)c.m2, mt2 = (T)c.mtheta2, eta = (T)c.eta;
-            const double c0d = (double)c0m, s0d = (double)s0m;   // link 0 at x - i (diagnostics)
 
             if (!GAUGED) {
                 // compute_forces_complex, scp_sim.c:931-994
@@ -481,11 +508,12 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                                 else etg += e2;
                             }
                         }
-                        dsum->S[DS_EG] += 0.5 * eg * c.dV;
-                        dsum->S[DS_ETG] += 0.5 * etg * c.dV;
+                        const auto S = dsum->S();
+                        S[DS_EG] += 0.5 * eg * c.dV;
+                        S[DS_ETG] += 0.5 * etg * c.dV;
 #pragma unroll
                         for (int a = 0; a < 3; a++)
-                            dsum->S[DS_EC] -= c.eta * (ctr[FU + a] * curl(FTU, a) + ctr[FV + a] * curl(FTV, a)) * c.dV;
+                            S[DS_EC] -= c.eta * (ctr[FU + a] * curl(FTU, a) + ctr[FV + a] * curl(FTV, a)) * c.dV;
                     }
                 }
             } else {
@@ -695,7 +723,8 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                     // that they do not merge with the force's (whose fused
                     // multiply-adds would then change): the step's arithmetic is the
                     // same with and without these sums
-                    double *S = dsum->S, *M = dsum->M;
+                    const auto S = dsum->S();
+                    const auto M = dsum->M();
                     const double dV = c.dV;
                     double s2[3];
 #pragma unroll
@@ -738,11 +767,6 @@ __device__ __forceinline__ void step_item(const StepIO<P> &io, const StepConsts 
                     S[DS_CZ] += z * rho2;
                     if constexpr (GAUGED && std::is_same<Stage, CpStage<P, TX, TY, GAUGED>>::value) {
                         // gradient, coupling and plaquette energies; Gauss charge density; E_em
-                        Plane12 xp;
-#pragma unroll
-                        for (int f = 0; f < 12; f++) xp.v[f] = (double)xm[f];
-                        const DiagGrad gr = diag_grad_gauged<TX, TY>(stg.xs, sc, sp, ty + 1, tx + 1, xp, c0d, s0d,
-                                                                     c.idx1);
                         S[DS_EG] += 0.5 * gr.eg * dV;
                         S[DS_ETG] += 0.5 * gr.etg * dV;
                         S[DS_EC] -= c.eta * gr.ec * dV;
@@ -781,12 +805,19 @@ step_kernel(StepIO<P> io, StepConsts c, TileGrid tg) {
     CpStage<P, TX, TY, GAUGED> stg(smem_raw);
     if constexpr (SYNC && !FIRST && !P::COMP) {
         if (io.dpart) {   // uniform: this launch also sums the first diagnostics pass
-            DiagSums acc;
-            acc.clear();
+            using LY = StepLayout<P, TX, TY, GAUGED>;
+            const DiagSmem dsm{reinterpret_cast<double *>(smem_raw + LY::smem_bytes), TX * TY};
+#pragma unroll
+            for (int q = 0; q < kDiag1Q; q++) dsm.base[q * TX * TY + threadIdx.x] = 0.0;
             for_each_piece(tg, c.N, [&](const Piece &pc) {
-                step_item<P, TX, TY, GAUGED, FIRST>(io, c, pc, SYNC, DAMP, stg, &acc);
+                step_item<P, TX, TY, GAUGED, FIRST>(io, c, pc, SYNC, DAMP, stg, &dsm);
             });
             __syncthreads();   // the ring is free: its first 7.4 KB serve as the fold's scratch
+            DiagSums acc;
+#pragma unroll
+            for (int q = 0; q < DS_NSUM; q++) acc.S[q] = dsm.S()[q];
+#pragma unroll
+            for (int q = 0; q < DM_NMAX; q++) acc.M[q] = dsm.M()[q];
             block_fold<DS_NSUM, DM_NMAX>(acc.S, acc.M, reinterpret_cast<double *>(smem_raw), io.dpart);
             return;
         }
