@@ -78,9 +78,6 @@ struct StepIO {
     double *drho = nullptr;
 };
 
-// gauge-quantity slots of the per-plane shared array
-enum : int { GQ_C0 = 0, GQ_S0 = 3, GQ_P0 = 6, GQ_N = 9 };
-
 template <class P, int TX, int TY, bool GAUGED>
 struct StepLayout {
     using T = typename P::T;
@@ -88,8 +85,6 @@ struct StepLayout {
     static constexpr int NR = NF + ((P::COMP && GAUGED) ? 3 : 0);   // ring fields (+ link lo parts)
     static constexpr int PX = TX + 2, PY = TY + 2;
     static constexpr int PLANE = NR * PY * PX;            // elements per ring slot
-    static constexpr int GX = TX + 1, GY = TY + 1;
-    static constexpr int GPLANE = GQ_N * GY * GX;
     static constexpr int NT = TX * TY;
     static constexpr int NHALO = 2 * TX + 2 * TY + (GAUGED ? 2 : 0);
     static constexpr int HPT = (NHALO + NT - 1) / NT;      // halo sites per thread (max)
