@@ -597,15 +597,9 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank, world, local = env_rank()
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as dist_mod
-        torch.cuda.set_device(local)
-        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-        dist = dist_mod
-
     if args.impl == "reference":
+        # the reference's stepper runs on the host cores: rank 0 alone times it,
+        # the other ranks leave at once (no process group, no GPU needed)
         if args.workload in ("c3", "c2acc", "c4acc", "snap"):
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "this workload exercises the library's "
@@ -615,9 +609,15 @@ def main():
         line = run_reference_arm(args, rank, world)
         if rank == 0 and line:
             print(json.dumps(line))
-        if dist:
-            dist.destroy_process_group()
         return
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = dist_mod
 
     if args.workload == "c3":
         if world > 1:
