@@ -592,7 +592,7 @@ def main():
     ap.add_argument("--ref-gpu", action="store_true",
                     help="also time the reference's own CUDA stepper on the same FP64 workload (always on for c1)")
     ap.add_argument("--no-targets", action="store_true",
-                    help="c1: skip the short 256^3 FP64 / FP32C runs of the north-star targets")
+                    help="c1: skip the short 256^3 FP64 / FP32C runs of the performance targets")
     ap.add_argument("--no-ref-gpu", action="store_true", help="c1: skip the reference CUDA stepper")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -757,7 +757,7 @@ def main():
             rg["ours_over_reference_gpu"] = value / rg["value"]
         line["reference_gpu"] = rg
     if rank == 0 and world == 1 and default_c1 and not args.no_targets:
-        # the north-star targets: FP64 >= 70% of HBM at 256^3, FP32C >= 1.8x FP64
+        # the performance targets: FP64 >= 70% of HBM at 256^3, FP32C >= 1.8x FP64
         t64 = short_rate("c2")
         t32 = short_rate("c2f")
         line["targets"] = {"fp64_256": t64, "fp32c_256": t32,
